@@ -1,0 +1,286 @@
+// extern "C" boundary (include/fastmc_b200.h) over fmc::Chain.
+#include <cstring>
+#include <string>
+
+#include "../../include/fastmc_b200.h"
+#include "fmc_chain.h"
+
+struct fmc_chain {
+  fmc::Chain impl;
+  // displace pass 1 of the drop-in ewald1_guest call stores the molecule's old sites here
+  int pending_g = -1, pending_n = 0;
+  double pending_old[3 * fmc::kMaxGuestSites];
+};
+
+namespace {
+thread_local std::string g_err;
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+#define CHECK_CHAIN(c) \
+  if (!(c)) return fail(-1, "null chain handle")
+}  // namespace
+
+extern "C" {
+
+int fmc_version(void) { return 10400; }
+
+const char* fmc_last_error(void) { return g_err.c_str(); }
+
+int fmc_chain_open(const char* dir, const int* seed, int device, fmc_chain** out) {
+  if (!dir || !seed || !out) return fail(-1, "null argument");
+  fmc_chain* c = new fmc_chain();
+  std::string err;
+  int rc = c->impl.open(dir, seed, device, err);
+  if (rc) {
+    delete c;
+    *out = nullptr;
+    return fail(rc, err);
+  }
+  *out = c;
+  return 0;
+}
+
+void fmc_chain_close(fmc_chain* c) { delete c; }
+
+int fmc_chain_info(fmc_chain* c, int* ints, double* dbls) {
+  CHECK_CHAIN(c);
+  const fmc::Chain& C = c->impl;
+  const fmc::HostSystem& S = C.sys;
+  int nv = S.nvox[0] * S.nvox[1] * S.nvox[2];
+  int iv[16] = {S.cell.imcon, S.deck.kmax[0], S.deck.kmax[1], S.deck.kmax[2], S.K, C.totatm, (int)C.sp.size(),
+                S.ntypes, S.mxgrid, S.nf, C.gcmccount, nv, C.gcap, 0, 0, 0};
+  double dv[16] = {S.alpha, S.rcut, S.deck.delr, S.cell.volm, S.engunit, S.deck.temp, S.beta, S.drewd, S.dlrpot,
+                   C.spenergy, C.dlpeng, C.ewald1sum, C.elrc, C.energy.empty() ? 0.0 : C.energy[0], S.statvolm, 0.0};
+  if (ints) std::memcpy(ints, iv, sizeof(iv));
+  if (dbls) std::memcpy(dbls, dv, sizeof(dv));
+  return 0;
+}
+
+int fmc_ewald1(fmc_chain* c, double* engcpe, int* newld) {
+  CHECK_CHAIN(c);
+  double e = 0.0;
+  int rc = c->impl.full_recip(&e);
+  if (rc) return fail(rc, "ewald1 failed on the device");
+  if (engcpe) *engcpe = e;
+  if (newld) *newld = c->impl.sys.K;
+  return 0;
+}
+
+int fmc_ewald1_guest(fmc_chain* c, int iguest, int natms, const double* xyz, int move, int pass, double* engcpe) {
+  CHECK_CHAIN(c);
+  fmc::Chain& C = c->impl;
+  if (iguest < 0 || iguest >= (int)C.sp.size()) return fail(-1, "species index out of range");
+  if (natms != C.sp[iguest].nsite) return fail(-1, "natms differs from the species' site count");
+  double out[3];
+  if (move == FMC_DISPLACE && pass == 1) {
+    c->pending_g = iguest;
+    c->pending_n = natms;
+    std::memcpy(c->pending_old, xyz, sizeof(double) * 3 * natms);
+    if (engcpe) *engcpe = 0.0;
+    return 0;
+  }
+  fmc::PassArgs A;
+  std::memset(&A, 0, sizeof(A));
+  const fmc::GuestSpecies& G = C.sys.deck.guests[iguest];
+  A.move = move == FMC_DISPLACE ? fmc::kDisplace : (move == FMC_DELETE ? fmc::kDelete : fmc::kInsert);
+  if (A.move == fmc::kDisplace && c->pending_g != iguest) return fail(-1, "displace pass 2 without pass 1");
+  A.nbk = fmc::pass_recip_blocks(C.dsys.view);
+  A.do_real = 0;
+  A.nold = A.move == fmc::kInsert ? 0 : natms;
+  A.nnew = A.move == fmc::kDelete ? 0 : natms;
+  A.ex_lo = A.ex_hi = -1;
+  A.engsic = C.sys.engsic[iguest];
+  const double* olds = A.move == fmc::kDisplace ? c->pending_old : xyz;
+  int w = 0;
+  for (int i = 0; i < A.nold; i++, w++) {
+    A.x[w] = olds[3 * i];
+    A.y[w] = olds[3 * i + 1];
+    A.z[w] = olds[3 * i + 2];
+    A.q[w] = G.charge[i];
+    A.type[w] = (unsigned char)G.type[i];
+  }
+  for (int i = 0; i < A.nnew; i++, w++) {
+    A.x[w] = xyz[3 * i];
+    A.y[w] = xyz[3 * i + 1];
+    A.z[w] = xyz[3 * i + 2];
+    A.q[w] = G.charge[i];
+    A.type[w] = (unsigned char)G.type[i];
+  }
+  cudaError_t e = fmc::launch_pass(C.dsys.view, C.guest_view(), A, C.sk, C.sk_new, C.W, C.st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(C.h_result, C.W.result, sizeof(double) * 3, cudaMemcpyDeviceToHost, C.st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(C.st);
+  if (e != cudaSuccess) return fail(-100 - (int)e, cudaGetErrorString(e));
+  out[0] = C.h_result[0];
+  if (A.move == fmc::kDisplace) c->pending_g = -1;
+  if (engcpe) *engcpe = out[0];
+  return 0;
+}
+
+int fmc_guest_realspace(fmc_chain* c, int iguest, int natms, const double* xyz, int mol, double* ewld2, double* vdw) {
+  CHECK_CHAIN(c);
+  fmc::Chain& C = c->impl;
+  if (iguest < 0 || iguest >= (int)C.sp.size()) return fail(-1, "species index out of range");
+  if (natms != C.sp[iguest].nsite) return fail(-1, "natms differs from the species' site count");
+  if (mol >= C.sp[iguest].nmol) return fail(-1, "molecule index out of range");
+  fmc::PassArgs A;
+  std::memset(&A, 0, sizeof(A));
+  const fmc::GuestSpecies& G = C.sys.deck.guests[iguest];
+  A.move = fmc::kInsert;
+  A.nbk = 0;
+  A.do_real = 1;
+  A.nold = 0;
+  A.nnew = natms;
+  A.ex_lo = A.ex_hi = -1;
+  if (mol >= 0) {
+    A.ex_lo = C.sp[iguest].seg_off + mol * natms;
+    A.ex_hi = A.ex_lo + natms;
+  }
+  for (int i = 0; i < natms; i++) {
+    A.x[i] = xyz[3 * i];
+    A.y[i] = xyz[3 * i + 1];
+    A.z[i] = xyz[3 * i + 2];
+    A.q[i] = G.charge[i];
+    A.type[i] = (unsigned char)G.type[i];
+  }
+  cudaError_t e = fmc::launch_pass(C.dsys.view, C.guest_view(), A, C.sk, C.sk_new, C.W, C.st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(C.h_result, C.W.result, sizeof(double) * 3, cudaMemcpyDeviceToHost, C.st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(C.st);
+  if (e != cudaSuccess) return fail(-100 - (int)e, cudaGetErrorString(e));
+  if (ewld2) *ewld2 = C.h_result[1];
+  if (vdw) *vdw = C.h_result[2];
+  return 0;
+}
+
+int fmc_commit(fmc_chain* c, int move, int iguest, int mol, const double* xyz) {
+  CHECK_CHAIN(c);
+  fmc::Chain& C = c->impl;
+  if (iguest < 0 || iguest >= (int)C.sp.size()) return fail(-1, "species index out of range");
+  int m = move == FMC_DELETE ? fmc::kDelete : (move == FMC_INSERT ? fmc::kInsert : fmc::kDisplace);
+  if (m != fmc::kInsert && (mol < 0 || mol >= C.sp[iguest].nmol)) return fail(-1, "molecule index out of range");
+  int rc = C.commit(m, iguest, mol, xyz);
+  if (rc == -75) return fail(75, "too many atoms in specified system");
+  if (rc) return fail(rc, "commit failed on the device");
+  cudaError_t e = cudaStreamSynchronize(C.st);
+  if (e != cudaSuccess) return fail(-100 - (int)e, cudaGetErrorString(e));
+  return 0;
+}
+
+int fmc_set_guests(fmc_chain* c, int iguest, int nmol, const double* xyz) {
+  CHECK_CHAIN(c);
+  fmc::Chain& C = c->impl;
+  if (iguest < 0 || iguest >= (int)C.sp.size()) return fail(-1, "species index out of range");
+  int rc = C.set_guests(iguest, nmol, xyz);
+  if (rc == -75) return fail(75, "too many atoms in specified system");
+  if (rc) return fail(rc, "guest upload failed");
+  rc = C.full_recip(nullptr);
+  if (rc) return fail(rc, "ewald1 failed on the device");
+  return 0;
+}
+
+int fmc_single_point(fmc_chain* c, double* spenergy, double* dlpeng) {
+  CHECK_CHAIN(c);
+  int rc = c->impl.single_point();
+  if (rc) return fail(rc, "single point failed on the device");
+  if (spenergy) *spenergy = c->impl.spenergy;
+  if (dlpeng) *dlpeng = c->impl.dlpeng;
+  return 0;
+}
+
+int fmc_get_sk(fmc_chain* c, int pending, double* re, double* im) {
+  CHECK_CHAIN(c);
+  fmc::Chain& C = c->impl;
+  std::vector<double2> h(C.sys.K);
+  cudaError_t e = cudaMemcpyAsync(h.data(), pending ? C.sk_new : C.sk, sizeof(double2) * C.sys.K,
+                                  cudaMemcpyDeviceToHost, C.st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(C.st);
+  if (e != cudaSuccess) return fail(-100 - (int)e, cudaGetErrorString(e));
+  for (int k = 0; k < C.sys.K; k++) {
+    if (re) re[k] = h[k].x;
+    if (im) im[k] = h[k].y;
+  }
+  return 0;
+}
+
+int fmc_kvectors(fmc_chain* c, int* lmn, double* akk) {
+  CHECK_CHAIN(c);
+  const fmc::HostSystem& S = c->impl.sys;
+  for (int k = 0; k < S.K; k++) {
+    if (lmn) {
+      lmn[3 * k] = S.kl[k];
+      lmn[3 * k + 1] = S.km[k];
+      lmn[3 * k + 2] = S.kn[k];
+    }
+    if (akk) akk[k] = S.akk[k];
+  }
+  return 0;
+}
+
+int fmc_run(fmc_chain* c, int nmoves, fmc_move_record* trace) {
+  CHECK_CHAIN(c);
+  static_assert(sizeof(fmc_move_record) == sizeof(fmc::MoveRecord), "record layout");
+  for (int i = 0; i < nmoves; i++) {
+    int rc = c->impl.step(trace ? reinterpret_cast<fmc::MoveRecord*>(trace + i) : nullptr);
+    if (rc == -75) return fail(75, "too many atoms in specified system");
+    if (rc) return fail(rc, "move loop failed");
+  }
+  return 0;
+}
+
+int fmc_guest_coords(fmc_chain* c, int iguest, double* xyz, int* nmol, int* nsite) {
+  CHECK_CHAIN(c);
+  fmc::Chain& C = c->impl;
+  if (iguest < 0 || iguest >= (int)C.sp.size()) return fail(-1, "species index out of range");
+  if (nmol) *nmol = C.sp[iguest].nmol;
+  if (nsite) *nsite = C.sp[iguest].nsite;
+  if (xyz) std::memcpy(xyz, C.sp[iguest].xyz.data(), sizeof(double) * C.sp[iguest].xyz.size());
+  return 0;
+}
+
+int fmc_stats(fmc_chain* c, int iguest, double* out) {
+  CHECK_CHAIN(c);
+  fmc::Chain& C = c->impl;
+  if (iguest < 0 || iguest >= (int)C.sp.size()) return fail(-1, "species index out of range");
+  for (int i = 0; i < 5; i++) out[i] = C.chainstats[14 * iguest + 1 + i];
+  out[5] = (double)C.prodcount;
+  return 0;
+}
+
+int fmc_deck_inspect(const char* dir, int* ints, double* dbls, int* lmn, double* akk, double* erc, double* charges,
+                     int* K, int* nerc) {
+  if (!dir) return fail(-1, "null argument");
+  fmc::InputDeck deck;
+  std::string err;
+  int rc = fmc::read_input_deck(dir, deck, err);
+  if (rc) return fail(rc, err);
+  fmc::HostSystem S;
+  rc = fmc::build_host_system(deck, S, err);
+  if (rc) return fail(rc, err);
+  int nv = S.nvox[0] * S.nvox[1] * S.nvox[2];
+  int natoms = S.nf;
+  for (auto& g : deck.guests) natoms += g.nmols * g.nsite;
+  int iv[16] = {S.cell.imcon, deck.kmax[0], deck.kmax[1], deck.kmax[2], S.K, natoms, (int)deck.guests.size(),
+                S.ntypes, S.mxgrid, S.nf, 0, nv, 0, (int)S.vox_atoms.size(), 0, 0};
+  double dv[16] = {S.alpha, S.rcut, deck.delr, S.cell.volm, S.engunit, deck.temp, S.beta, S.drewd, S.dlrpot,
+                   0, 0, 0, 0, 0, S.statvolm, 0};
+  if (ints) std::memcpy(ints, iv, sizeof(iv));
+  if (dbls) std::memcpy(dbls, dv, sizeof(dv));
+  for (int k = 0; k < S.K; k++) {
+    if (lmn) {
+      lmn[3 * k] = S.kl[k];
+      lmn[3 * k + 1] = S.km[k];
+      lmn[3 * k + 2] = S.kn[k];
+    }
+    if (akk) akk[k] = S.akk[k];
+  }
+  if (erc)
+    for (int i = 0; i <= S.mxgrid; i++) erc[i] = S.erc[i];
+  if (charges)
+    for (int i = 0; i < S.nf; i++) charges[i] = S.fq[i];
+  if (K) *K = S.K;
+  if (nerc) *nerc = S.mxgrid + 1;
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,637 @@
+// Chain: device upload, single-point set-up and the plain-path host move loop.
+#include "fmc_chain.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+namespace fmc {
+
+#define FMC_CUDA(expr)                         \
+  do {                                         \
+    cudaError_t e_ = (expr);                   \
+    if (e_ != cudaSuccess) return sync_error(e_, &err); \
+  } while (0)
+
+namespace {
+
+template <class T>
+cudaError_t dalloc(std::vector<void*>& keep, T** p, size_t n) {
+  cudaError_t e = cudaMalloc((void**)p, std::max<size_t>(n, 1) * sizeof(T));
+  if (e == cudaSuccess) keep.push_back(*p);
+  return e;
+}
+
+template <class T>
+cudaError_t upload(std::vector<void*>& keep, const T** out, const std::vector<T>& v) {
+  T* p = nullptr;
+  cudaError_t e = dalloc(keep, &p, v.size());
+  if (e != cudaSuccess) return e;
+  if (!v.empty()) e = cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+  *out = p;
+  return e;
+}
+
+}  // namespace
+
+DeviceSystem::~DeviceSystem() {
+  int cur = 0;
+  cudaGetDevice(&cur);
+  cudaSetDevice(device);
+  for (void* p : allocations) cudaFree(p);
+  cudaSetDevice(cur);
+}
+
+int upload_system(const HostSystem& h, DeviceSystem& d, std::string& err) {
+  DevSystem& v = d.view;
+  v.cell = h.cell;
+  v.nf = h.nf;
+  std::vector<double4> fw(h.nf);
+  for (int i = 0; i < h.nf; i++) fw[i] = make_double4(h.fx[i], h.fy[i], h.fz[i], h.fq[i]);
+  cudaError_t e;
+  if ((e = upload(d.allocations, &v.fw, fw)) != cudaSuccess) goto fail;
+  if ((e = upload(d.allocations, &v.fw_type, h.ftype)) != cudaSuccess) goto fail;
+  for (int a = 0; a < 3; a++) v.nvox[a] = h.nvox[a];
+  if ((e = upload(d.allocations, &v.vox_off, h.vox_off)) != cudaSuccess) goto fail;
+  if ((e = upload(d.allocations, &v.vox_atoms, h.vox_atoms)) != cudaSuccess) goto fail;
+  v.rcut2 = h.rcut * h.rcut;
+  v.rdr_e = 1.0 / h.drewd;
+  v.rdr_v = 1.0 / h.dlrpot;
+  if ((e = upload(d.allocations, &v.erc, h.erc)) != cudaSuccess) goto fail;
+  if ((e = upload(d.allocations, &v.vvv, h.vvv)) != cudaSuccess) goto fail;
+  v.tab_stride = h.mxgrid + 1;
+  v.ntypes = h.ntypes;
+  if ((e = upload(d.allocations, &v.pair_row, h.pair_row)) != cudaSuccess) goto fail;
+  v.K = h.K;
+  for (int a = 0; a < 3; a++) v.kmax[a] = h.deck.kmax[a];
+  {
+    std::vector<int> kp(h.K);
+    for (int k = 0; k < h.K; k++) kp[k] = kpack(h.kl[k], h.km[k], h.kn[k]);
+    if ((e = upload(d.allocations, &v.kpack, kp)) != cudaSuccess) goto fail;
+  }
+  if ((e = upload(d.allocations, &v.akk, h.akk)) != cudaSuccess) goto fail;
+  v.recip_pref = h.recip_pref;
+  return 0;
+fail:
+  err = std::string("device upload failed: ") + cudaGetErrorString(e);
+  return -1;
+}
+
+Chain::~Chain() {
+  if (st) {
+    cudaSetDevice(device);
+    cudaStreamSynchronize(st);
+    for (void* p : {(void*)sk, (void*)sk_new, (void*)gsite, (void*)gtype, (void*)W.recip_part, (void*)W.site_e,
+                    (void*)W.counter, (void*)W.result, (void*)recip_scratch, (void*)recip_parts, (void*)all_atoms})
+      if (p) cudaFree(p);
+    if (h_result) cudaFreeHost(h_result);
+    cudaStreamDestroy(st);
+  }
+}
+
+int Chain::sync_error(cudaError_t e, std::string* err) {
+  if (err) *err = std::string("CUDA error: ") + cudaGetErrorString(e);
+  return -100 - (int)e;
+}
+
+GuestView Chain::guest_view() const {
+  GuestView G{};
+  G.site = gsite;
+  G.type = gtype;
+  G.nseg = (int)sp.size();
+  for (int g = 0; g < G.nseg; g++) {
+    G.seg_off[g] = sp[g].seg_off;
+    G.seg_len[g] = sp[g].nmol * sp[g].nsite;
+  }
+  return G;
+}
+
+int Chain::open(const std::string& dir, const int seed[4], int dev, std::string& err) {
+  InputDeck deck;
+  int rc = read_input_deck(dir, deck, err);
+  if (rc) return rc;
+  if ((int)deck.guests.size() > kMaxGuestTypes) {
+    err = "more guest species than supported";
+    return -5;
+  }
+  for (int f : deck.ffrz)
+    if (f == 0) {
+      err = "framework atoms must be frozen (rigid framework)";
+      return -6;
+    }
+  rc = build_host_system(deck, sys, err);
+  if (rc) return rc;
+  device = dev;
+  dsys.device = dev;
+  FMC_CUDA(cudaSetDevice(dev));
+  FMC_CUDA(configure_kernels());
+  FMC_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  rc = upload_system(sys, dsys, err);
+  if (rc) return rc;
+  const int K = sys.K, ng = (int)deck.guests.size();
+  // guest segments: preloaded molecules + the reference's guest-atom budget (error 75)
+  sp.assign(ng, Species());
+  int off = 0;
+  for (int g = 0; g < ng; g++) {
+    const GuestSpecies& G = deck.guests[g];
+    sp[g].nsite = G.nsite;
+    sp[g].seg_off = off;
+    sp[g].cap_sites = G.nmols * G.nsite + deck.maxguest;
+    sp[g].nmol = G.nmols;
+    sp[g].xyz = G.xyz;
+    off += sp[g].cap_sites;
+  }
+  gcap = off;
+  FMC_CUDA(cudaMalloc(&sk, sizeof(double2) * std::max(K, 1)));
+  FMC_CUDA(cudaMalloc(&sk_new, sizeof(double2) * std::max(K, 1)));
+  FMC_CUDA(cudaMalloc(&gsite, sizeof(double4) * std::max(gcap, 1)));
+  FMC_CUDA(cudaMalloc(&gtype, sizeof(int) * std::max(gcap, 1)));
+  FMC_CUDA(cudaMalloc(&W.recip_part, sizeof(double) * (pass_recip_blocks(dsys.view) + 1)));
+  FMC_CUDA(cudaMalloc(&W.site_e, sizeof(double) * 2 * kMaxPassSites));
+  FMC_CUDA(cudaMalloc(&W.counter, sizeof(unsigned)));
+  FMC_CUDA(cudaMemset(W.counter, 0, sizeof(unsigned)));
+  FMC_CUDA(cudaMalloc(&W.result, sizeof(double) * 4));
+  FMC_CUDA(cudaMallocHost(&h_result, sizeof(double) * 64));
+  all_cap = sys.nf + gcap;
+  FMC_CUDA(cudaMalloc(&all_atoms, sizeof(double4) * std::max(all_cap, 1)));
+  recip_scratch_n = recip_scratch_doubles(dsys.view, all_cap);
+  FMC_CUDA(cudaMalloc(&recip_scratch, sizeof(double) * recip_scratch_n));
+  FMC_CUDA(cudaMalloc(&recip_parts, sizeof(double) * (recip_nparts(dsys.view) + 1)));
+  // upload preloaded guests
+  for (int g = 0; g < ng; g++) {
+    rc = set_guests(g, sp[g].nmol, sp[g].xyz.data());
+    if (rc) {
+      err = "guest upload failed";
+      return rc;
+    }
+  }
+  totatm = sys.nf;
+  for (auto& s : sp) totatm += s.nmol * s.nsite;
+  framatm = totatm;
+  rc = single_point();
+  if (rc) {
+    err = "single-point set-up failed on the device";
+    return rc;
+  }
+  // move-loop state (gcmc.f:320-588)
+  duni_seed(rng, seed[0], seed[1], seed[2], seed[3]);
+  duni_next(rng);  // gcmc.f:335-336: the second duni() call consumes one draw
+  energy.assign(ng, spenergy);
+  delE.assign(ng, 0.0);
+  elrc = 0.0;  // the move loop's elrc starts at zero (gcmc.f:131-132)
+  delrdisp.assign(ng, deck.delr);
+  tran_delr.assign(ng, deck.delr);
+  accept_disp.assign(ng, 0);
+  disp_count.assign(ng, 0);
+  accept_tran.assign(ng, 0);
+  tran_count.assign(ng, 0);
+  rotangle = kPi / 3.0;
+  rota_rotangle = rotangle;
+  chainstats.assign(1 + 14 * ng, 0.0);
+  production = (deck.eqsteps == 0);
+  return 0;
+}
+
+int Chain::set_guests(int g, int nmol, const double* xyz) {
+  Species& s = sp[g];
+  if (nmol * s.nsite > s.cap_sites) return -75;
+  s.nmol = nmol;
+  s.xyz.assign(xyz, xyz + 3 * nmol * s.nsite);
+  const GuestSpecies& G = sys.deck.guests[g];
+  std::vector<double4> a(std::max(nmol * s.nsite, 1));
+  std::vector<int> t(std::max(nmol * s.nsite, 1));
+  for (int m = 0; m < nmol; m++)
+    for (int i = 0; i < s.nsite; i++) {
+      int j = m * s.nsite + i;
+      a[j] = make_double4(xyz[3 * j], xyz[3 * j + 1], xyz[3 * j + 2], G.charge[i]);
+      t[j] = G.type[i];
+    }
+  cudaError_t e = cudaMemcpyAsync(gsite + s.seg_off, a.data(), sizeof(double4) * nmol * s.nsite,
+                                  cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(gtype + s.seg_off, t.data(), sizeof(int) * nmol * s.nsite, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return sync_error(e);
+  totatm = sys.nf;
+  for (auto& x : sp) totatm += x.nmol * x.nsite;
+  return 0;
+}
+
+// S(k) over all current atoms: guests in species order, then the framework (condense order).
+int Chain::full_recip(double* e_out) {
+  int n = 0;
+  cudaError_t e = cudaSuccess;
+  for (auto& s : sp) {
+    int len = s.nmol * s.nsite;
+    if (len) e = cudaMemcpyAsync(all_atoms + n, gsite + s.seg_off, sizeof(double4) * len, cudaMemcpyDeviceToDevice, st);
+    n += len;
+  }
+  if (e == cudaSuccess && sys.nf)
+    e = cudaMemcpyAsync(all_atoms + n, dsys.view.fw, sizeof(double4) * sys.nf, cudaMemcpyDeviceToDevice, st);
+  n += sys.nf;
+  if (e == cudaSuccess) e = launch_recip_full(dsys.view, all_atoms, n, sk, recip_scratch, recip_parts, st);
+  std::vector<double> parts(recip_nparts(dsys.view));
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(parts.data(), recip_parts, sizeof(double) * parts.size(), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return sync_error(e);
+  double q2 = 0.0;
+  for (int g = 0; g < (int)sp.size(); g++)
+    for (int m = 0; m < sp[g].nmol; m++)
+      for (int i = 0; i < sp[g].nsite; i++) q2 = q2 + sys.deck.guests[g].charge[i] * sys.deck.guests[g].charge[i];
+  for (int i = 0; i < sys.nf; i++) q2 = q2 + sys.fq[i] * sys.fq[i];
+  double engsic = -kR4pie0 * sys.alpha * q2 / kSqrPi;
+  if (e_out) *e_out = recip_energy_from_parts(dsys.view, parts.data()) + engsic;
+  return 0;
+}
+
+// single_point (gcmc.f:2518-2710): framework-only and full reciprocal energies, guest
+// real-space energies (guest-framework once, guest-guest halved), the intramolecular
+// correction and the tail correction.
+int Chain::single_point() {
+  // framework only
+  cudaError_t e = launch_recip_full(dsys.view, dsys.view.fw, sys.nf, sk, recip_scratch, recip_parts, st);
+  std::vector<double> parts(recip_nparts(dsys.view));
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(parts.data(), recip_parts, sizeof(double) * parts.size(), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return sync_error(e);
+  double q2f = 0.0;
+  for (int i = 0; i < sys.nf; i++) q2f = q2f + sys.fq[i] * sys.fq[i];
+  ewald1sum = recip_energy_from_parts(dsys.view, parts.data()) + (-kR4pie0 * sys.alpha * q2f / kSqrPi);
+  double eall = 0.0;
+  int rc = full_recip(&eall);
+  if (rc) return rc;
+  // numtyp / numfrz over all atoms (lrcorrect, vdw_terms.f:542-553)
+  numtyp.assign(sys.ntypes + 1, 0);
+  numfrz.assign(sys.ntypes + 1, 0);
+  for (int i = 0; i < sys.nf; i++) {
+    numtyp[sys.ftype[i]]++;
+    if (sys.ffrz[i]) numfrz[sys.ftype[i]]++;
+  }
+  int nguest_sites = 0;
+  for (int g = 0; g < (int)sp.size(); g++)
+    for (int m = 0; m < sp[g].nmol; m++)
+      for (int i = 0; i < sp[g].nsite; i++) {
+        numtyp[sys.deck.guests[g].type[i]]++;
+        nguest_sites++;
+      }
+  double elrc0 = lrc_energy(sys, numtyp, numfrz);
+  double ewald1eng = 0, e2 = 0, ev = 0, e3 = 0;
+  if (nguest_sites > 0) {
+    ewald1eng = eall - ewald1sum;
+    // one entry per guest site: its index and its own molecule's site range
+    std::vector<int> idx, lo, hi;
+    for (int g = 0; g < (int)sp.size(); g++)
+      for (int m = 0; m < sp[g].nmol; m++)
+        for (int i = 0; i < sp[g].nsite; i++) {
+          idx.push_back(sp[g].seg_off + m * sp[g].nsite + i);
+          lo.push_back(sp[g].seg_off + m * sp[g].nsite);
+          hi.push_back(sp[g].seg_off + (m + 1) * sp[g].nsite);
+        }
+    const int n = (int)idx.size();
+    int* dbuf = nullptr;
+    double* dout = nullptr;
+    e = cudaMalloc(&dbuf, sizeof(int) * 3 * n);
+    if (e == cudaSuccess) e = cudaMalloc(&dout, sizeof(double) * 4 * n);
+    std::vector<int> packed;
+    packed.insert(packed.end(), idx.begin(), idx.end());
+    packed.insert(packed.end(), lo.begin(), lo.end());
+    packed.insert(packed.end(), hi.begin(), hi.end());
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dbuf, packed.data(), sizeof(int) * 3 * n, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = launch_single_point_rs(dsys.view, guest_view(), n, dbuf, dbuf + n, dbuf + 2 * n, dout, st);
+    std::vector<double> out(4 * n);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out.data(), dout, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(dbuf);
+    cudaFree(dout);
+    if (e != cudaSuccess) return sync_error(e);
+    double cf = 0, vf = 0, cg = 0, vg = 0;
+    for (int i = 0; i < n; i++) {
+      cf += out[4 * i];
+      vf += out[4 * i + 1];
+      cg += out[4 * i + 2];
+      vg += out[4 * i + 3];
+    }
+    e2 = cf + 0.5 * cg;
+    ev = vf + 0.5 * vg;
+    // intramolecular exclusion correction from the actual coordinates (ewald3 over the
+    // exclusion lists, gcmc.f:2676-2697)
+    for (int g = 0; g < (int)sp.size(); g++) {
+      const GuestSpecies& G = sys.deck.guests[g];
+      for (int m = 0; m < sp[g].nmol; m++) {
+        const double* X = sp[g].xyz.data() + 3 * m * sp[g].nsite;
+        for (int i = 0; i < sp[g].nsite; i++) {
+          double part = 0.0;
+          for (int j = i + 1; j < sp[g].nsite; j++) {
+            double dx = X[3 * i] - X[3 * j], dy = X[3 * i + 1] - X[3 * j + 1], dz = X[3 * i + 2] - X[3 * j + 2];
+            min_image(sys.cell, dx, dy, dz);
+            double r = std::sqrt(dx * dx + dy * dy + dz * dz);
+            part = part - ewald3_pair(sys.alpha, G.charge[i] * kR4pie0 * G.charge[j], r);
+          }
+          e3 = e3 + part;
+        }
+      }
+    }
+    double ecoulg = ewald1eng + e2 + e3, evdwg = ev + elrc0;
+    spenergy = (ecoulg + evdwg) / sys.engunit;
+  } else {
+    spenergy = 0.0;
+  }
+  dlpeng = (ewald1eng + ewald1sum + e2 + ev + elrc0 + e3) / sys.engunit;
+  return 0;
+}
+
+int Chain::pass(int move, int g, int mol, const double* old_xyz, const double* new_xyz, double out[3]) {
+  PassArgs A;
+  std::memset(&A, 0, sizeof(A));
+  const GuestSpecies& G = sys.deck.guests[g];
+  const Species& s = sp[g];
+  A.move = move;
+  A.nbk = pass_recip_blocks(dsys.view);
+  A.do_real = 1;
+  A.nold = (move == kInsert) ? 0 : s.nsite;
+  A.nnew = (move == kDelete) ? 0 : s.nsite;
+  A.ex_lo = A.ex_hi = -1;
+  if (mol >= 0) {
+    A.ex_lo = s.seg_off + mol * s.nsite;
+    A.ex_hi = A.ex_lo + s.nsite;
+  }
+  A.engsic = sys.engsic[g];
+  int w = 0;
+  for (int i = 0; i < A.nold; i++, w++) {
+    A.x[w] = old_xyz[3 * i];
+    A.y[w] = old_xyz[3 * i + 1];
+    A.z[w] = old_xyz[3 * i + 2];
+    A.q[w] = G.charge[i];
+    A.type[w] = (unsigned char)G.type[i];
+  }
+  for (int i = 0; i < A.nnew; i++, w++) {
+    A.x[w] = new_xyz[3 * i];
+    A.y[w] = new_xyz[3 * i + 1];
+    A.z[w] = new_xyz[3 * i + 2];
+    A.q[w] = G.charge[i];
+    A.type[w] = (unsigned char)G.type[i];
+  }
+  cudaError_t e = launch_pass(dsys.view, guest_view(), A, sk, sk_new, W, st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h_result, W.result, sizeof(double) * 3, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return sync_error(e);
+  out[0] = h_result[0];
+  out[1] = h_result[1];
+  out[2] = h_result[2];
+  passes++;
+  return 0;
+}
+
+int Chain::commit(int move, int g, int mol, const double* new_xyz) {
+  Species& s = sp[g];
+  const GuestSpecies& G = sys.deck.guests[g];
+  CommitArgs C;
+  std::memset(&C, 0, sizeof(C));
+  C.op = move;
+  C.ns = s.nsite;
+  if (move == kInsert) {
+    if ((s.nmol + 1) * s.nsite > s.cap_sites) return -75;
+    C.lo = s.seg_off + s.nmol * s.nsite;
+  } else {
+    C.lo = s.seg_off + mol * s.nsite;
+  }
+  C.seg_end = s.seg_off + s.nmol * s.nsite;
+  if (move != kDelete)
+    for (int i = 0; i < s.nsite; i++) {
+      C.x[i] = new_xyz[3 * i];
+      C.y[i] = new_xyz[3 * i + 1];
+      C.z[i] = new_xyz[3 * i + 2];
+      C.q[i] = G.charge[i];
+      C.type[i] = G.type[i];
+    }
+  cudaError_t e = launch_commit(sys.K, sk, sk_new, C, gsite, gtype, st);
+  if (e != cudaSuccess) return sync_error(e);
+  // host mirror (framwkxxx updates of gcmc.f:966-970, 1134-1138, 1352-1357)
+  int n3 = 3 * s.nsite;
+  if (move == kInsert) {
+    s.xyz.insert(s.xyz.end(), new_xyz, new_xyz + n3);
+    s.nmol++;
+    totatm += s.nsite;
+  } else if (move == kDelete) {
+    s.xyz.erase(s.xyz.begin() + (size_t)mol * n3, s.xyz.begin() + (size_t)(mol + 1) * n3);
+    s.nmol--;
+    totatm -= s.nsite;
+  } else {
+    std::copy(new_xyz, new_xyz + n3, s.xyz.begin() + (size_t)mol * n3);
+  }
+  return 0;
+}
+
+// One iteration of the move loop (gcmc.f:589-1380 + rolling statistics 1814-1860).
+int Chain::step(MoveRecord* rec) {
+  const InputDeck& d = sys.deck;
+  const int ng = (int)sp.size();
+  gcmccount++;
+  if (gcmccount % 400 == 0) {
+    int totalguests = 0;
+    for (auto& s : sp) totalguests += s.nmol;
+    if (production) {
+      if (d.mcsteps < 0) {
+        for (int t = 4; t > 0; t--) tick_tock[t] = tick_tock[t - 1];
+        tick_tock[0] = !(prodcount < (long long)(-d.mcsteps) * (totalguests + 1));
+        bool all = true;
+        for (bool b : tick_tock) all = all && b;
+        if (all) lgchk = false;
+      } else if (prodcount >= d.mcsteps) {
+        lgchk = false;
+      }
+    } else if (d.eqsteps > 0) {
+      if (gcmccount >= d.eqsteps) production = true;
+    } else if (d.eqsteps < 0) {
+      for (int t = 4; t > 0; t--) tick_tock[t] = tick_tock[t - 1];
+      tick_tock[0] = !((long long)gcmccount < (long long)(-d.eqsteps) * (totalguests + 1));
+      bool all = true;
+      for (bool b : tick_tock) all = all && b;
+      if (all) {
+        production = true;
+        for (bool& b : tick_tock) b = false;
+      }
+    }
+  }
+  int g = 0;
+  if (ng > 1) g = (int)std::floor(duni_next(rng) * ng);
+  double randmov = duni_next(rng);
+  const std::array<double, 9>& c = sys.mvcum[g];
+  int mtype;
+  if (randmov < c[0]) mtype = kInsert;
+  else if (randmov < c[1]) mtype = kDelete;
+  else if (randmov < c[2]) mtype = kDisplace;
+  else if (randmov < c[5]) return -3;  // jump/flex/swap (rejected at set-up)
+  else if (randmov < c[6]) mtype = kTranslate;
+  else if (randmov < c[7]) mtype = kRotate;
+  else if (randmov < c[8]) return -3;
+  else mtype = kDisplace;
+  Species& s = sp[g];
+  const GuestSpecies& G = d.guests[g];
+  const int natms = s.nsite, nmols = s.nmol;
+  // step-size adaptation (gcmc.f:794-834), applied on every iteration whose counter sits on
+  // a multiple of 50/100
+  if (nmols >= 1 && disp_count[g] >= 1) {
+    if (disp_count[g] % 100 == 0) {
+      if ((accept_disp[g] / (double)disp_count[g]) > d.disp_ratio[g]) delrdisp[g] = delrdisp[g] * 1.05;
+      else if (delrdisp[g] > kDelrMin) delrdisp[g] = delrdisp[g] * 0.95;
+    } else if (disp_count[g] % 50 == 0) {
+      if ((accept_disp[g] / (double)disp_count[g]) > d.disp_ratio[g]) rotangle = rotangle * 1.05;
+      else if (rotangle > kMinAngle) rotangle = rotangle * 0.95;
+    }
+  }
+  if (nmols >= 1 && tran_count[g] >= 1 && tran_count[g] % 100 == 0) {
+    if ((accept_tran[g] / (double)tran_count[g]) > d.tran_ratio[g]) tran_delr[g] = tran_delr[g] * 1.05;
+    else if (tran_delr[g] > kDelrMin) tran_delr[g] = tran_delr[g] * 0.95;
+  }
+  if (nmols >= 1 && rota_count >= 1 && rota_count % 100 == 0) {
+    if ((accept_rota / (double)rota_count) > d.rota_ratio) rota_rotangle = rota_rotangle * 1.05;
+    else if (rota_rotangle > kMinAngle) rota_rotangle = rota_rotangle * 0.95;
+  }
+  if (nmols == 0) mtype = kInsert;
+  MoveRecord R;
+  std::memset(&R, 0, sizeof(R));
+  R.step = gcmccount;
+  R.iguest = g;
+  R.mtype = mtype;
+  bool accepted = false;
+  double e[3] = {0, 0, 0}, ewld3 = 0, delrc = 0, estep = 0, rande = -1;
+  double oldx[3 * kMaxGuestSites], newx[3 * kMaxGuestSites];
+  delE[g] = 0.0;
+  int rc = 0;
+  if (mtype == kInsert) {
+    ins_count++;
+    if ((totatm - framatm) + natms >= d.maxguest) return -75;
+    double r[7];
+    for (int i = 0; i < 7; i++) r[i] = duni_next(rng);
+    double x[kMaxGuestSites], y[kMaxGuestSites], z[kMaxGuestSites];
+    trial_insert(sys.cell, G.tx.data(), G.ty.data(), G.tz.data(), natms, r, x, y, z);
+    for (int i = 0; i < natms; i++) {
+      newx[3 * i] = x[i];
+      newx[3 * i + 1] = y[i];
+      newx[3 * i + 2] = z[i];
+    }
+    if ((rc = pass(kInsert, g, -1, nullptr, newx, e))) return rc;
+    for (int i = 0; i < natms; i++) numtyp[G.type[i]]++;
+    delrc = lrc_energy(sys, numtyp, numfrz) - elrc;
+    ewld3 = sys.ewald3en[g];
+    estep = (e[0] + e[1] + ewld3 + e[2] + delrc) / sys.engunit;
+    rande = duni_next(rng);
+    accepted = accept_move(estep, rande, sys.statvolm, d.press[g], nmols, d.temp, sys.beta, kInsert);
+    if (accepted) {
+      delE[g] = estep;
+      accept_ins++;
+      if ((rc = commit(kInsert, g, -1, newx))) return rc;
+      elrc = elrc + delrc;
+      energy[g] += delE[g];
+    } else {
+      for (int i = 0; i < natms; i++) numtyp[G.type[i]]--;
+    }
+  } else if (mtype == kDelete) {
+    del_count++;
+    int randchoice = (int)std::floor(duni_next(rng) * nmols) + 1;
+    R.randchoice = randchoice;
+    int mol = randchoice - 1;
+    std::copy(s.xyz.begin() + (size_t)mol * 3 * natms, s.xyz.begin() + (size_t)(mol + 1) * 3 * natms, oldx);
+    for (int i = 0; i < natms; i++) numtyp[G.type[i]]--;
+    delrc = lrc_energy(sys, numtyp, numfrz) - elrc;
+    if ((rc = pass(kDelete, g, mol, oldx, nullptr, e))) return rc;
+    ewld3 = sys.ewald3en[g];
+    estep = (e[0] - e[1] - ewld3 - e[2] + delrc) / sys.engunit;
+    rande = duni_next(rng);
+    accepted = accept_move(estep, rande, sys.statvolm, d.press[g], nmols, d.temp, sys.beta, kDelete);
+    if (accepted) {
+      delE[g] = estep;
+      accept_del++;
+      if ((rc = commit(kDelete, g, mol, nullptr))) return rc;
+      elrc = elrc + delrc;
+      energy[g] += delE[g];
+    } else {
+      for (int i = 0; i < natms; i++) numtyp[G.type[i]]++;
+    }
+  } else {
+    double r[7], dis_delr, dis_rot;
+    if (mtype == kTranslate) {
+      tran_count[g]++;
+      r[0] = duni_next(rng);
+      r[1] = duni_next(rng);
+      r[2] = duni_next(rng);
+      r[3] = r[4] = r[5] = r[6] = 0.0;
+      dis_delr = tran_delr[g];
+      dis_rot = 0.0;
+    } else if (mtype == kRotate) {
+      rota_count++;
+      r[0] = r[1] = r[2] = 0.5;
+      for (int i = 3; i < 7; i++) r[i] = duni_next(rng);
+      dis_delr = 0.0;
+      dis_rot = rota_rotangle;
+    } else {
+      disp_count[g]++;
+      for (int i = 0; i < 7; i++) r[i] = duni_next(rng);
+      dis_delr = delrdisp[g];
+      dis_rot = rotangle;
+    }
+    int randchoice = (int)std::floor(duni_next(rng) * nmols) + 1;
+    R.randchoice = randchoice;
+    int mol = randchoice - 1;
+    std::copy(s.xyz.begin() + (size_t)mol * 3 * natms, s.xyz.begin() + (size_t)(mol + 1) * 3 * natms, oldx);
+    double x[kMaxGuestSites], y[kMaxGuestSites], z[kMaxGuestSites];
+    for (int i = 0; i < natms; i++) {
+      x[i] = oldx[3 * i];
+      y[i] = oldx[3 * i + 1];
+      z[i] = oldx[3 * i + 2];
+    }
+    trial_displace(sys.cell, G.mass.data(), natms, dis_delr, dis_rot, r, x, y, z);
+    for (int i = 0; i < natms; i++) {
+      newx[3 * i] = x[i];
+      newx[3 * i + 1] = y[i];
+      newx[3 * i + 2] = z[i];
+    }
+    if ((rc = pass(kDisplace, g, mol, oldx, newx, e))) return rc;
+    estep = (e[0] + e[1] + e[2]) / sys.engunit;
+    if (estep < 0.0) {
+      accepted = true;
+    } else {
+      rande = duni_next(rng);
+      accepted = accept_move(estep, rande, sys.statvolm, d.press[g], nmols, d.temp, sys.beta, kDisplace);
+    }
+    if (accepted) {
+      delE[g] = estep;
+      if (mtype == kTranslate) accept_tran[g]++;
+      else if (mtype == kRotate) accept_rota++;
+      else accept_disp[g]++;
+      if ((rc = commit(kDisplace, g, mol, newx))) return rc;
+      energy[g] += delE[g];
+    }
+  }
+  if (production && ((d.laccsample && accepted) || !d.laccsample)) {
+    prodcount++;
+    chainstats[0] = (double)prodcount;
+    double pc = (double)prodcount;
+    for (int i = 0; i < ng; i++) {
+      double dm = (double)sp[i].nmol, m2 = dm * dm, en = energy[i], e2 = en * en;
+      double* cs = chainstats.data() + 14 * i;
+      cs[1] = cs[1] + (dm - cs[1]) / pc;
+      cs[2] = cs[2] + (en - cs[2]) / pc;
+      cs[3] = cs[3] + (en * dm - cs[3]) / pc;
+      cs[4] = cs[4] + (m2 - cs[4]) / pc;
+      cs[5] = cs[5] + (e2 - cs[5]) / pc;
+    }
+  }
+  R.accepted = accepted;
+  R.nmols_after = s.nmol;
+  R.ewld1 = e[0];
+  R.ewld2 = (mtype == kInsert || mtype == kDelete) ? e[1] : e[1];
+  R.ewld3 = ewld3;
+  R.vdw = e[2];
+  R.delrc = delrc;
+  R.estep = estep;
+  R.rande = rande;
+  R.energy_after = energy[g];
+  if (rec) *rec = R;
+  return 0;
+}
+
+}  // namespace fmc

@@ -1,0 +1,89 @@
+// One GCMC chain on one GPU: device-resident system + S(k) + guest sites, and the host move
+// loop of the plain path (gcmc.f:589-1380 restated, energies from fmc_kernels.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "fmc_kernels.h"
+#include "fmc_system.h"
+
+namespace fmc {
+
+// Per-move record, identical in layout to fmc_move_record of the C ABI.
+struct MoveRecord {
+  int32_t step, iguest, mtype, randchoice, accepted, nmols_after, pad0, pad1;
+  double ewld1, ewld2, ewld3, vdw, delrc, estep, rande, energy_after;
+};
+
+// Device copy of one system (immutable arrays) -- shared by chains of the same framework.
+struct DeviceSystem {
+  DevSystem view{};
+  std::vector<void*> allocations;
+  int device = 0;
+  ~DeviceSystem();
+};
+
+int upload_system(const HostSystem& h, DeviceSystem& d, std::string& err);
+
+struct Species {
+  int nsite = 0, seg_off = 0, cap_sites = 0, nmol = 0;
+  std::vector<double> xyz;  // 3*nmol*nsite, molecule-major (framwkxxx of the reference)
+};
+
+class Chain {
+ public:
+  HostSystem sys;
+  DeviceSystem dsys;
+  int device = 0;
+  cudaStream_t st = nullptr;
+  // device chain state
+  double2* sk = nullptr;
+  double2* sk_new = nullptr;
+  double4* gsite = nullptr;
+  int* gtype = nullptr;
+  int gcap = 0;
+  PassScratch W{};
+  double* h_result = nullptr;  // pinned
+  double* recip_scratch = nullptr;
+  double* recip_parts = nullptr;
+  size_t recip_scratch_n = 0;
+  double4* all_atoms = nullptr;
+  int all_cap = 0;
+  // host mirror
+  std::vector<Species> sp;
+  int totatm = 0, framatm = 0;
+  std::vector<int> numtyp, numfrz;
+  double elrc = 0;
+  std::vector<double> energy, delE;
+  // set-up energies
+  double spenergy = 0, dlpeng = 0, ewald1sum = 0;
+  // move-loop control (gcmc.f:320-588)
+  Duni rng{};
+  int gcmccount = 0;
+  std::vector<double> delrdisp, tran_delr;
+  std::vector<int> accept_disp, disp_count, accept_tran, tran_count;
+  int accept_rota = 0, rota_count = 0, accept_ins = 0, accept_del = 0, ins_count = 0, del_count = 0;
+  double rotangle = kPi / 3.0, rota_rotangle = kPi / 3.0;
+  bool production = false, lgchk = true;
+  long long prodcount = 0;
+  bool tick_tock[5] = {false, false, false, false, false};
+  std::vector<double> chainstats;  // 1 + 14*ntpguest, <N>,<E>,<EN>,<N^2>,<E^2> rolling
+  // timing of the device passes
+  long long passes = 0;
+
+  ~Chain();
+  int open(const std::string& dir, const int seed[4], int device, std::string& err);
+  GuestView guest_view() const;
+  // Energies of one trial pass.  old_xyz/new_xyz are interleaved xyz of the molecule's sites.
+  int pass(int move, int g, int mol, const double* old_xyz, const double* new_xyz, double out[3]);
+  int commit(int move, int g, int mol, const double* new_xyz);
+  int full_recip(double* e_recip_plus_self);  // S(k) over all current atoms (ewald1)
+  int single_point();
+  int step(MoveRecord* rec);
+  int set_guests(int g, int nmol, const double* xyz);  // replace species g (condense equivalent)
+  int sync_error(cudaError_t e, std::string* err = nullptr);
+};
+
+}  // namespace fmc

@@ -1,0 +1,235 @@
+// Host/device shared pieces of the GCMC trial-move path: constants, the duni generator,
+// minimum-image conventions, trial-move generators and the acceptance test.  Everything here
+// is plain arithmetic usable from the host move loop (plain path) and from the persistent
+// batched kernel, so both make the same decisions from the same random numbers.
+#pragma once
+#include <cmath>
+#include <cstdint>
+
+#if defined(__CUDACC__)
+#define FMC_HD __host__ __device__ __forceinline__
+#else
+#define FMC_HD inline
+#endif
+
+namespace fmc {
+
+// Physical constants and limits, utility_pack.f:71-113
+constexpr double kPi = 3.141592653589793;
+constexpr double kSqrPi = 1.7724538509055159;
+constexpr double kR4pie0 = 138935.4835;      // e^2/(4 pi eps0 A) in 10 J/mol
+constexpr double kKboltz = 1.9872041e-3;     // kcal/mol/K
+constexpr double kBoltz = 1.3806503e-23;     // J/K
+constexpr double kMinAngle = kPi / 18.0;     // utility_pack.f:86
+constexpr double kDelrMin = 0.1;             // utility_pack.f:90
+constexpr int kMaxGuestSites = 50;           // mxguestsite, utility_pack.f:76
+constexpr int kMaxGuestTypes = 4;
+
+enum MoveType : int { kInsert = 1, kDelete = 2, kDisplace = 3, kTranslate = 4, kRotate = 5 };
+
+// ------------------------------------------------------------------ duni
+// Marsaglia-Zaman-Tsang universal generator in IEEE single precision, as duni in
+// gcmc.f:2712-2805, with the clock-derived seed replaced by an explicit (i,j,k,l).
+struct Duni {
+  float u[97];
+  float c;
+  int ir, jr;
+};
+
+FMC_HD void duni_seed(Duni& d, int i, int j, int k, int l) {
+  d.ir = 97;
+  d.jr = 33;
+  for (int ii = 0; ii < 97; ii++) {
+    float s = 0.0f, t = 0.5f;
+    for (int jj = 0; jj < 24; jj++) {
+      int m = (((i * j) % 179) * k) % 179;
+      i = j;
+      j = k;
+      k = m;
+      l = (53 * l + 1) % 169;
+      if ((l * m) % 64 >= 32) s = s + t;
+      t = 0.5f * t;
+    }
+    d.u[ii] = s;
+  }
+  d.c = 362436.0f / 16777216.0f;
+}
+
+FMC_HD double duni_next(Duni& d) {
+  const float cd = 7654321.0f / 16777216.0f, cm = 16777213.0f / 16777216.0f;
+  float uni = d.u[d.ir - 1] - d.u[d.jr - 1];
+  if (uni < 0.0f) uni = uni + 1.0f;
+  d.u[d.ir - 1] = uni;
+  d.ir = d.ir - 1;
+  if (d.ir == 0) d.ir = 97;
+  d.jr = d.jr - 1;
+  if (d.jr == 0) d.jr = 97;
+  d.c = d.c - cd;
+  if (d.c < 0.0f) d.c = d.c + cm;
+  uni = uni - d.c;
+  if (uni < 0.0f) uni = uni + 1.0f;
+  return (double)uni;
+}
+
+// ------------------------------------------------------------------ cell geometry
+struct CellGeom {
+  double h[9];    // cell vectors a,b,c (cell(1..9) of the reference, a = h[0..2])
+  double rh[9];   // inverse (invert, utility_pack.f:1417)
+  double volm;    // volume used by Ewald and acceptance
+  int imcon;
+};
+
+// Fortran nint: nearest integer, halves away from zero.
+FMC_HD double fnint(double x) { return round(x); }
+
+// Minimum image of one separation vector for imcon 1, 2, 3 (images, utility_pack.f:1138-1202).
+FMC_HD void min_image(const CellGeom& c, double& x, double& y, double& z) {
+  if (c.imcon == 1) {
+    const double a = c.h[0], ra = 1.0 / a;
+    x = x - a * fnint(ra * x);
+    y = y - a * fnint(ra * y);
+    z = z - a * fnint(ra * z);
+  } else if (c.imcon == 2) {
+    x = x - c.h[0] * fnint((1.0 / c.h[0]) * x);
+    y = y - c.h[4] * fnint((1.0 / c.h[4]) * y);
+    z = z - c.h[8] * fnint((1.0 / c.h[8]) * z);
+  } else if (c.imcon == 3) {
+    const double* r = c.rh;
+    double sx = r[0] * x + r[3] * y + r[6] * z;
+    double sy = r[1] * x + r[4] * y + r[7] * z;
+    double sz = r[2] * x + r[5] * y + r[8] * z;
+    sx = sx - fnint(sx);
+    sy = sy - fnint(sy);
+    sz = sz - fnint(sz);
+    x = c.h[0] * sx + c.h[3] * sy + c.h[6] * sz;
+    y = c.h[1] * sx + c.h[4] * sy + c.h[7] * sz;
+    z = c.h[2] * sx + c.h[5] * sy + c.h[8] * sz;
+  }
+}
+
+// ------------------------------------------------------------------ trial generators
+// rotation (utility_pack.f:2887-2926) of n sites by the quaternion q.
+FMC_HD void rotate_sites(double* x, double* y, double* z, int n, const double q[4]) {
+  const double q1 = q[0], q2 = q[1], q3 = q[2], q4 = q[3];
+  const double Q0 = 2.0 * q2 * q2 + 2.0 * q1 * q1 - 1.0, Q1 = 2.0 * q2 * q3 - 2.0 * q1 * q4;
+  const double Q2 = 2.0 * q2 * q4 + 2.0 * q1 * q3, Q3 = 2.0 * q2 * q3 + 2.0 * q1 * q4;
+  const double Q4 = 2.0 * q1 * q1 + 2.0 * q3 * q3 - 1.0, Q5 = 2.0 * q3 * q4 - 2.0 * q1 * q2;
+  const double Q6 = 2.0 * q2 * q4 - 2.0 * q1 * q3, Q7 = 2.0 * q3 * q4 + 2.0 * q1 * q2;
+  const double Q8 = 2.0 * q4 * q4 + 2.0 * q1 * q1 - 1.0;
+  for (int i = 0; i < n; i++) {
+    double tx = Q0 * x[i] + Q1 * y[i] + Q2 * z[i];
+    double ty = Q3 * x[i] + Q4 * y[i] + Q5 * z[i];
+    double tz = Q6 * x[i] + Q7 * y[i] + Q8 * z[i];
+    x[i] = tx;
+    y[i] = ty;
+    z[i] = tz;
+  }
+}
+
+// Quaternion of angle theta about the axis (2r2-1, 2r3-1, 2r4-1)/norm (random_ins, random_rot).
+FMC_HD void axis_angle_quat(double theta, double r2, double r3, double r4, double q[4]) {
+  double b1 = 2.0 * r2 - 1.0, b2 = 2.0 * r3 - 1.0, b3 = 2.0 * r4 - 1.0;
+  double st = sin(theta / 2.0);
+  double norm = sqrt(b1 * b1 + b2 * b2 + b3 * b3);
+  q[0] = cos(theta / 2.0);
+  q[1] = st * (b1 / norm);
+  q[2] = st * (b2 / norm);
+  q[3] = st * (b3 / norm);
+}
+
+// random_ins (utility_pack.f:2545-2650): template sites rotated by a random quaternion and
+// placed with their COM at fractional (ra, rb, rc).
+FMC_HD void trial_insert(const CellGeom& c, const double* tx, const double* ty, const double* tz, int n,
+                         const double r[7], double* x, double* y, double* z) {
+  const double* h = c.h;
+  double xc = r[0] * h[0] + r[1] * h[3] + r[2] * h[6];
+  double yc = r[0] * h[1] + r[1] * h[4] + r[2] * h[7];
+  double zc = r[0] * h[2] + r[1] * h[5] + r[2] * h[8];
+  for (int i = 0; i < n; i++) {
+    x[i] = tx[i];
+    y[i] = ty[i];
+    z[i] = tz[i];
+  }
+  double q[4];
+  axis_angle_quat(r[3] * 2.0 * kPi, r[4], r[5], r[6], q);
+  rotate_sites(x, y, z, n, q);
+  for (int i = 0; i < n; i++) {
+    x[i] = x[i] + xc;
+    y[i] = y[i] + yc;
+    z[i] = z[i] + zc;
+  }
+}
+
+// random_disp + random_rot (utility_pack.f:2679-2763, 2929-3000): translate by
+// (2r-1)*delr/2 per Cartesian axis, wrap the mass COM into the cell, rotate about it.
+FMC_HD void trial_displace(const CellGeom& c, const double* mass, int n, double delr, double rotangle,
+                           const double r[7], double* x, double* y, double* z) {
+  const double half = delr * 0.5;
+  const double dx = (2.0 * r[0] - 1.0) * half, dy = (2.0 * r[1] - 1.0) * half, dz = (2.0 * r[2] - 1.0) * half;
+  double w = 0.0, sx = 0.0, sy = 0.0, sz = 0.0;
+  for (int i = 0; i < n; i++) {
+    x[i] = dx + x[i];
+    y[i] = dy + y[i];
+    z[i] = dz + z[i];
+  }
+  for (int i = 0; i < n; i++) {
+    w = w + mass[i];
+    sx = sx + x[i] * mass[i];
+    sy = sy + y[i] * mass[i];
+    sz = sz + z[i] * mass[i];
+  }
+  double cx = sx / w, cy = sy / w, cz = sz / w;
+  const double* rh = c.rh;
+  const double* h = c.h;
+  double fx = rh[0] * cx + rh[3] * cy + rh[6] * cz;
+  double fy = rh[1] * cx + rh[4] * cy + rh[7] * cz;
+  double fz = rh[2] * cx + rh[5] * cy + rh[8] * cz;
+  fx = fx - floor(fx);
+  fy = fy - floor(fy);
+  fz = fz - floor(fz);
+  double wx = h[0] * fx + h[3] * fy + h[6] * fz;
+  double wy = h[1] * fx + h[4] * fy + h[7] * fz;
+  double wz = h[2] * fx + h[5] * fy + h[8] * fz;
+  double shx = wx - cx, shy = wy - cy, shz = wz - cz;
+  for (int i = 0; i < n; i++) {
+    x[i] = x[i] + shx - wx;
+    y[i] = y[i] + shy - wy;
+    z[i] = z[i] + shz - wz;
+  }
+  double q[4];
+  axis_angle_quat(r[3] * rotangle, r[4], r[5], r[6], q);
+  rotate_sites(x, y, z, n, q);
+  for (int i = 0; i < n; i++) {
+    x[i] = x[i] + wx;
+    y[i] = y[i] + wy;
+    z[i] = z[i] + wz;
+  }
+}
+
+// energy_eval (utility_pack.f:3049-3095).  volm in m^3, press in Pa, eng in kcal/mol.
+FMC_HD bool accept_move(double eng, double rande, double volm_m3, double press, int ngsts, double temp,
+                        double beta, int move) {
+  double test = 0.0;
+  if (-1 * beta * eng > 700.0)
+    test = exp(700.0);
+  else if (move == kDisplace)
+    test = exp(-1.0 * beta * eng);
+  else if (move == kInsert)
+    test = volm_m3 * press / ((ngsts + 1) * kBoltz * temp) * exp(-1.0 * beta * eng);
+  else if (move == kDelete)
+    test = fabs(press) < 1e-7 ? 1.0 : ngsts * kBoltz * temp / (volm_m3 * press) * exp(-1.0 * beta * eng);
+  return rande < test;
+}
+
+// 3-point interpolation of a tabulated function on r_l = l*dr (ewald.f:670-684,
+// vdw_terms.f:476-489).  tab[0] is defined as tab[1].
+FMC_HD double interp3(const double* tab, double rrr, double rdr) {
+  int l = (int)(rrr * rdr);
+  double ppp = rrr * rdr - (double)l;
+  double v0 = tab[l], v1 = tab[l + 1], v2 = tab[l + 2];
+  double t1 = v0 + (v1 - v0) * ppp;
+  double t2 = v1 + (v2 - v1) * (ppp - 1.0);
+  return t1 + (t2 - t1) * ppp * 0.5;
+}
+
+}  // namespace fmc

@@ -1,0 +1,53 @@
+// FastMC input deck: CONTROL / FIELD / CONFIG read with the reference's record rules
+// (parse_module.f) and directive order (utility_pack.f:176-457 initscan, readinputs.f
+// readfield/readconfig/readcontrol).  Errors carry the reference's error codes (error.f).
+#pragma once
+#include <array>
+#include <string>
+#include <vector>
+
+namespace fmc {
+
+struct GuestSpecies {
+  std::string name;
+  int nsite = 0;
+  std::vector<std::string> site_name;
+  std::vector<double> mass, charge;
+  std::vector<double> tx, ty, tz;  // template, centred on the mass COM (readinputs.f:246-268)
+  std::vector<int> type;           // 1-based unique atom type (readinputs.f:218-236)
+  int nmols = 0;                   // molecules present in CONFIG
+  std::vector<double> xyz;         // 3*nmols*nsite, interleaved, molecule-major
+};
+
+struct InputDeck {
+  // initscan
+  int imcon = 0, keyfce = 0, kmax[3] = {0, 0, 0};
+  double cell[9] = {0};
+  double volm = 0, rcut = 0, rvdw = 0, alpha = 0, delr = 0;
+  int maxguest = 3000;
+  // readfield
+  double engunit = 1.0;
+  std::vector<std::string> types;  // unique atom types in FIELD order
+  std::vector<GuestSpecies> guests;
+  // framework atoms in condensed order (all non-guest molecules, FIELD order)
+  std::vector<double> fx, fy, fz, fq;
+  std::vector<int> ftype, ffrz;
+  int ntpvdw = 0, maxvdw = 0, mxgrid = 0;
+  std::vector<int> ltpvdw, lstvdw;           // [1..maxvdw+1]
+  std::vector<std::array<double, 5>> prmvdw;  // [1..maxvdw+1], energies in internal units
+  // readcontrol
+  double temp = 0;
+  int mcsteps = 1, eqsteps = 0, nwind = 100000;
+  bool laccsample = false, lspe = false;
+  std::vector<double> press;  // Pa, per guest
+  std::vector<std::array<double, 9>> movefreq;  // ins,del,dis,jmp,flx,swp,tra,rot,mjp (raw)
+  std::vector<double> disp_ratio, tran_ratio;
+  double rota_ratio = 0.5;
+};
+
+// Reads dir/{CONTROL,FIELD,CONFIG}.  Returns 0, or the reference's error code (>0); `err`
+// receives a message.  Directives outside this path (restart, pressure equilibration) are
+// rejected with a negative code.
+int read_input_deck(const std::string& dir, InputDeck& deck, std::string& err);
+
+}  // namespace fmc

@@ -1,0 +1,304 @@
+// FP64 kernels of the plain (one trial per launch) GPU path.
+//
+// fmc_pass_kernel   : one launch per trial move.  Blocks [0, nbk) compute the reciprocal
+//                     change over all K k-vectors (ewald1_guest, ewald.f:32-365): per-site
+//                     axis phase tables in shared memory, one k-vector per thread, S_new to
+//                     scratch, akk*(|S_new|^2-|S_old|^2) reduced per block.  Blocks [nbk, ...)
+//                     compute the real-space erfc Coulomb + tabulated vdW energy of one
+//                     trial site each (ewald2 + srfrce over the neighbour set that
+//                     guestlistgen would build).  The last block to finish combines the
+//                     block partials in a fixed order (deterministic) into {ewld1, ewld2, vdw}.
+// fmc_commit_kernel : S(k) <- S_new and the guest-site array update of an accepted move.
+// fmc_recip_*       : full S(k) of a set of atoms (ewald1, ewald.f:368-630).
+// fmc_sp_kernel     : per-guest-site real-space energies for the single-point energy.
+#include "fmc_device.cuh"
+#include "fmc_kernels.h"
+
+namespace fmc {
+
+constexpr int kPassThreads = 256;
+
+// ------------------------------------------------------------------------------ pass
+__global__ void __launch_bounds__(kPassThreads) fmc_pass_kernel(DevSystem S, GuestView G, PassArgs A,
+                                                                const double2* __restrict__ sk, double2* sk_new,
+                                                                PassScratch W) {
+  extern __shared__ double2 sm_tab[];
+  __shared__ double red[32 * 2];
+  __shared__ bool am_last;
+  const int nsite = A.nold + A.nnew;
+  const int nbk = A.nbk;
+  const int tid = threadIdx.x;
+  if ((int)blockIdx.x < nbk) {
+    // ---- reciprocal space
+    const int k1 = S.kmax[0], k2 = S.kmax[1], k3 = S.kmax[2];
+    const int stride = (k1 + 1) + (k2 + 1) + (k3 + 1);
+    for (int w = tid; w < nsite * 3; w += blockDim.x) {
+      int s = w / 3, ax = w % 3;
+      double f[3];
+      frac_coords(S.cell, A.x[s], A.y[s], A.z[s], f);
+      double2* t = sm_tab + s * stride + (ax == 0 ? 0 : (ax == 1 ? k1 + 1 : k1 + k2 + 2));
+      axis_phases(f[ax], S.kmax[ax], t);
+    }
+    __syncthreads();
+    double v[1] = {0.0};
+    int k = blockIdx.x * blockDim.x + tid;
+    if (k < S.K) {
+      int l, m, n;
+      kunpack(S.kpack[k], l, m, n);
+      int am = m < 0 ? -m : m, an = n < 0 ? -n : n;
+      double2 aold = make_double2(0.0, 0.0), anew = make_double2(0.0, 0.0);
+      for (int s = 0; s < nsite; s++) {
+        const double2* t = sm_tab + s * stride;
+        double2 e1 = t[l], e2 = t[k1 + 1 + am], e3 = t[k1 + k2 + 2 + an];
+        double2 c = m >= 0 ? cmul(e1, e2) : cmulc(e1, e2);
+        c = n >= 0 ? cmul(c, e3) : cmulc(c, e3);
+        double q = A.q[s];
+        if (s < A.nold) {
+          aold.x += q * c.x;
+          aold.y += q * c.y;
+        } else {
+          anew.x += q * c.x;
+          anew.y += q * c.y;
+        }
+      }
+      double2 so = sk[k], sn;
+      if (A.move == kInsert)
+        sn = make_double2(anew.x + so.x, anew.y + so.y);
+      else if (A.move == kDelete)
+        sn = make_double2(so.x - aold.x, so.y - aold.y);
+      else
+        sn = make_double2((so.x - aold.x) + anew.x, (so.y - aold.y) + anew.y);
+      sk_new[k] = sn;
+      v[0] = S.akk[k] * (sn.x * sn.x + sn.y * sn.y - so.x * so.x - so.y * so.y);
+    }
+    block_sum<1>(v, red);
+    if (tid == 0) W.recip_part[blockIdx.x] = v[0];
+  } else {
+    // ---- real space of one trial site
+    const int s = blockIdx.x - nbk;
+    double v[2] = {0.0, 0.0};
+    double ec_fw = 0.0, ev_fw = 0.0, ec_g = 0.0, ev_g = 0.0;
+    site_partial(S, G, A.x[s], A.y[s], A.z[s], A.q[s], A.type[s], A.ex_lo, A.ex_hi, tid, blockDim.x, ec_fw, ev_fw,
+                 ec_g, ev_g);
+    v[0] = ec_g + ec_fw;
+    v[1] = ev_g + ev_fw;
+    block_sum<2>(v, red);
+    if (tid == 0) {
+      W.site_e[2 * s] = v[0];
+      W.site_e[2 * s + 1] = v[1];
+    }
+  }
+  // ---- last block combines in a fixed order
+  if (tid == 0) {
+    __threadfence();
+    unsigned done = atomicAdd(W.counter, 1u);
+    am_last = (done == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (am_last && tid == 0) {
+    __threadfence();
+    double r = 0.0;
+    for (int b = 0; b < nbk; b++) r += ((volatile double*)W.recip_part)[b];
+    double ewld1 = S.recip_pref * r;
+    if (A.move == kInsert) ewld1 = ewld1 + A.engsic;
+    if (A.move == kDelete) ewld1 = ewld1 - A.engsic;
+    double e2 = 0.0, ev = 0.0;
+    const volatile double* se = W.site_e;
+    for (int s = 0; s < (A.do_real ? nsite : 0); s++) {
+      if (s < A.nold && A.move == kDisplace) {
+        e2 = e2 - se[2 * s];
+        ev = ev - se[2 * s + 1];
+      } else {
+        e2 = e2 + se[2 * s];
+        ev = ev + se[2 * s + 1];
+      }
+    }
+    W.result[0] = ewld1;
+    W.result[1] = e2;
+    W.result[2] = ev;
+    *W.counter = 0u;
+  }
+}
+
+int pass_smem_bytes(const DevSystem& S, int nsite) {
+  return nsite * ((S.kmax[0] + 1) + (S.kmax[1] + 1) + (S.kmax[2] + 1)) * (int)sizeof(double2);
+}
+
+int pass_recip_blocks(const DevSystem& S) { return (S.K + kPassThreads - 1) / kPassThreads; }
+
+cudaError_t launch_pass(const DevSystem& S, const GuestView& G, const PassArgs& A, const double2* sk, double2* sk_new,
+                        const PassScratch& W, cudaStream_t st) {
+  int nsite = A.nold + A.nnew;
+  int smem = A.nbk > 0 ? pass_smem_bytes(S, nsite) : 0;
+  int grid = A.nbk + (A.do_real ? nsite : 0);
+  if (grid == 0) return cudaSuccess;
+  fmc_pass_kernel<<<grid, kPassThreads, smem, st>>>(S, G, A, sk, sk_new, W);
+  return cudaGetLastError();
+}
+
+cudaError_t configure_kernels() {
+  return cudaFuncSetAttribute(fmc_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+}
+
+// ------------------------------------------------------------------------------ commit
+__global__ void fmc_commit_kernel(int K, double2* sk, const double2* __restrict__ sk_new, CommitArgs C,
+                                  double4* site, int* type) {
+  if ((int)blockIdx.x < (int)gridDim.x - 1) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < K; k += (gridDim.x - 1) * blockDim.x) sk[k] = sk_new[k];
+    return;
+  }
+  // last block: guest-site segment update
+  const int tid = threadIdx.x;
+  if (C.op == kDelete) {
+    // remove [lo, lo+ns) and shift the rest of the segment down, preserving order
+    const int ns = C.ns;
+    for (int base = C.lo; base < C.seg_end - ns; base += blockDim.x) {
+      int i = base + tid;
+      double4 a;
+      int t = 0;
+      bool act = i < C.seg_end - ns;
+      if (act) {
+        a = site[i + ns];
+        t = type[i + ns];
+      }
+      __syncthreads();
+      if (act) {
+        site[i] = a;
+        type[i] = t;
+      }
+      __syncthreads();
+    }
+  } else if (tid < C.ns) {
+    // insert writes at the segment end, displace overwrites the molecule
+    site[C.lo + tid] = make_double4(C.x[tid], C.y[tid], C.z[tid], C.q[tid]);
+    type[C.lo + tid] = C.type[tid];
+  }
+}
+
+cudaError_t launch_commit(int K, double2* sk, const double2* sk_new, const CommitArgs& C, double4* site, int* type,
+                          cudaStream_t st) {
+  int nb = (K + 255) / 256;
+  if (nb > 64) nb = 64;
+  fmc_commit_kernel<<<nb + 1, 256, 0, st>>>(K, sk, sk_new, C, site, type);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------ full S(k)
+// partial[c*K + k] = sum over the atoms of chunk c (in order) of q e^{i k.r}
+constexpr int kRecipThreads = 128;
+
+__global__ void __launch_bounds__(kRecipThreads) fmc_recip_partial_kernel(DevSystem S, const double4* __restrict__ atoms,
+                                                                          int natoms, int chunk, double2* partial) {
+  extern __shared__ double2 sm_tab[];
+  __shared__ double sq[256];
+  const int k1 = S.kmax[0], k2 = S.kmax[1], k3 = S.kmax[2];
+  const int stride = (k1 + 1) + (k2 + 1) + (k3 + 1);
+  const int c = blockIdx.y, a0 = c * chunk;
+  const int na = min(chunk, natoms - a0);
+  for (int w = threadIdx.x; w < na * 3; w += blockDim.x) {
+    int s = w / 3, ax = w % 3;
+    double4 a = atoms[a0 + s];
+    double f[3];
+    frac_coords(S.cell, a.x, a.y, a.z, f);
+    double2* t = sm_tab + s * stride + (ax == 0 ? 0 : (ax == 1 ? k1 + 1 : k1 + k2 + 2));
+    axis_phases(f[ax], S.kmax[ax], t);
+    if (ax == 0) sq[s] = a.w;
+  }
+  __syncthreads();
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= S.K) return;
+  int l, m, n;
+  kunpack(S.kpack[k], l, m, n);
+  int am = m < 0 ? -m : m, an = n < 0 ? -n : n;
+  double2 acc = make_double2(0.0, 0.0);
+  for (int s = 0; s < na; s++) {
+    const double2* t = sm_tab + s * stride;
+    double2 e1 = t[l], e2 = t[k1 + 1 + am], e3 = t[k1 + k2 + 2 + an];
+    double2 cc = m >= 0 ? cmul(e1, e2) : cmulc(e1, e2);
+    cc = n >= 0 ? cmul(cc, e3) : cmulc(cc, e3);
+    acc.x += sq[s] * cc.x;
+    acc.y += sq[s] * cc.y;
+  }
+  partial[(size_t)c * S.K + k] = acc;
+}
+
+// S[k] = sum_c partial[c][k]; energy sum akk |S|^2 per block into part[]
+__global__ void fmc_recip_reduce_kernel(DevSystem S, const double2* __restrict__ partial, int nchunk, double2* sk,
+                                        double* part) {
+  __shared__ double red[32];
+  int k = blockIdx.x * blockDim.x + threadIdx.x;
+  double v[1] = {0.0};
+  if (k < S.K) {
+    double2 s = make_double2(0.0, 0.0);
+    for (int c = 0; c < nchunk; c++) {
+      double2 p = partial[(size_t)c * S.K + k];
+      s.x += p.x;
+      s.y += p.y;
+    }
+    sk[k] = s;
+    v[0] = S.akk[k] * (s.x * s.x + s.y * s.y);
+  }
+  block_sum<1>(v, red);
+  if (threadIdx.x == 0) part[blockIdx.x] = v[0];
+}
+
+int recip_chunk(const DevSystem& S) {
+  int stride = (S.kmax[0] + 1) + (S.kmax[1] + 1) + (S.kmax[2] + 1);
+  int c = (48 * 1024) / (stride * (int)sizeof(double2));
+  if (c > 256) c = 256;
+  return c < 1 ? 1 : c;
+}
+
+size_t recip_scratch_doubles(const DevSystem& S, int natoms) {
+  int chunk = recip_chunk(S);
+  int nchunk = (natoms + chunk - 1) / chunk;
+  return (size_t)nchunk * S.K * 2 + 8;
+}
+
+int recip_nparts(const DevSystem& S) { return (S.K + 255) / 256; }
+
+cudaError_t launch_recip_full(const DevSystem& S, const double4* atoms, int natoms, double2* sk, double* scratch,
+                              double* parts, cudaStream_t st) {
+  int chunk = recip_chunk(S);
+  int nchunk = (natoms + chunk - 1) / chunk;
+  if (nchunk == 0) {
+    cudaMemsetAsync(sk, 0, sizeof(double2) * S.K, st);
+    return cudaMemsetAsync(parts, 0, sizeof(double) * recip_nparts(S), st);
+  }
+  int stride = (S.kmax[0] + 1) + (S.kmax[1] + 1) + (S.kmax[2] + 1);
+  double2* partial = reinterpret_cast<double2*>(scratch);
+  dim3 g((S.K + kRecipThreads - 1) / kRecipThreads, nchunk);
+  fmc_recip_partial_kernel<<<g, kRecipThreads, chunk * stride * sizeof(double2), st>>>(S, atoms, natoms, chunk,
+                                                                                      partial);
+  fmc_recip_reduce_kernel<<<recip_nparts(S), 256, 0, st>>>(S, partial, nchunk, sk, parts);
+  return cudaGetLastError();
+}
+
+double recip_energy_from_parts(const DevSystem& S, const double* host_parts) {
+  double r = 0.0;
+  for (int b = 0; b < recip_nparts(S); b++) r += host_parts[b];
+  return S.recip_pref * r;
+}
+
+// ------------------------------------------------------------------------------ single point
+// For entry b: site i = sites[b]; out[4*b + {0,1,2,3}] = {coulomb vs framework, vdw vs
+// framework, coulomb vs other guests, vdw vs other guests}; own molecule = [lo[b], hi[b]).
+__global__ void fmc_sp_kernel(DevSystem S, GuestView G, const int* __restrict__ sites, const int* __restrict__ lo,
+                              const int* __restrict__ hi, double* out) {
+  __shared__ double red[32 * 4];
+  const int b = blockIdx.x, i = sites[b];
+  double4 a = G.site[i];
+  double v[4] = {0.0, 0.0, 0.0, 0.0};
+  site_partial(S, G, a.x, a.y, a.z, a.w, G.type[i], lo[b], hi[b], threadIdx.x, blockDim.x, v[0], v[1], v[2], v[3]);
+  block_sum<4>(v, red);
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 4; k++) out[4 * b + k] = v[k];
+}
+
+cudaError_t launch_single_point_rs(const DevSystem& S, const GuestView& G, int nsites, const int* sites, const int* lo,
+                                   const int* hi, double* out, cudaStream_t st) {
+  if (nsites > 0) fmc_sp_kernel<<<nsites, 256, 0, st>>>(S, G, sites, lo, hi, out);
+  return cudaGetLastError();
+}
+
+}  // namespace fmc

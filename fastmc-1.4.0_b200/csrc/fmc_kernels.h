@@ -1,0 +1,56 @@
+// Launch interfaces of the plain-path FP64 kernels (fmc_kernels.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "fmc_device.cuh"
+
+namespace fmc {
+
+// One trial pass: the sites whose reciprocal and real-space contributions change.
+// Sites [0, nold) are the molecule's current positions (removed), sites [nold, nold+nnew)
+// the trial positions (added).  insert: nold=0; delete: nnew=0; displace: both, fused.
+struct PassArgs {
+  int move;           // kInsert / kDelete / kDisplace
+  int nbk;            // reciprocal blocks (0: skip the reciprocal part)
+  int do_real;        // 1: one real-space block per site
+  int nold, nnew;
+  int ex_lo, ex_hi;   // guest-site range of the moving molecule (excluded from real space)
+  double engsic;      // self-interaction term of the species (ewald.f:87-93)
+  double x[kMaxPassSites], y[kMaxPassSites], z[kMaxPassSites], q[kMaxPassSites];
+  unsigned char type[kMaxPassSites];
+};
+
+// Scratch of one pass launch (global memory beyond inputs and outputs).
+struct PassScratch {
+  double* recip_part;  // [ceil(K/256)]
+  double* site_e;      // [2*kMaxPassSites]
+  unsigned* counter;   // last-block ticket, left at zero by the kernel
+  double* result;      // {ewld1, ewld2, vdw}
+};
+
+struct CommitArgs {
+  int op;       // kInsert / kDelete / kDisplace
+  int lo;       // first site index of the molecule (insert: segment end)
+  int ns;       // sites per molecule
+  int seg_end;  // delete: current end of the species segment
+  double x[kMaxGuestSites], y[kMaxGuestSites], z[kMaxGuestSites], q[kMaxGuestSites];
+  int type[kMaxGuestSites];
+};
+
+int pass_smem_bytes(const DevSystem& S, int nsite);
+int pass_recip_blocks(const DevSystem& S);
+cudaError_t configure_kernels();  // once per device, before the first launch
+cudaError_t launch_pass(const DevSystem& S, const GuestView& G, const PassArgs& A, const double2* sk, double2* sk_new,
+                        const PassScratch& W, cudaStream_t st);
+cudaError_t launch_commit(int K, double2* sk, const double2* sk_new, const CommitArgs& C, double4* site, int* type,
+                          cudaStream_t st);
+size_t recip_scratch_doubles(const DevSystem& S, int natoms);
+int recip_nparts(const DevSystem& S);
+// Full S(k) of `natoms` atoms {x,y,z,q} into sk; per-block sums of akk|S|^2 into parts.
+cudaError_t launch_recip_full(const DevSystem& S, const double4* atoms, int natoms, double2* sk, double* scratch,
+                              double* parts, cudaStream_t st);
+double recip_energy_from_parts(const DevSystem& S, const double* host_parts);
+cudaError_t launch_single_point_rs(const DevSystem& S, const GuestView& G, int nsites, const int* sites, const int* lo,
+                                   const int* hi, double* out, cudaStream_t st);
+
+}  // namespace fmc

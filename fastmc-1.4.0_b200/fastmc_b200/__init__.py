@@ -1,0 +1,137 @@
+"""B200-native GCMC trial-move energy path of FastMC 1.4.0.
+
+Host-side mirror of the reference's operator interface: a `Chain` opened from a FastMC input
+directory (CONTROL / FIELD / CONFIG) exposes the reference's energy routines (ewald1,
+ewald1_guest, guest real space = guestlistgen + ewald2 + srfrce, single_point) and its move
+loop, all evaluated on the GPU through libfastmc_b200.so.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import DELETE, DISPLACE, INSERT, MOVE_DTYPE, ROTATE, TRANSLATE, FastMCError, check, dp, ip, lib
+
+__all__ = ["Chain", "deck_inspect", "FastMCError", "INSERT", "DELETE", "DISPLACE", "TRANSLATE", "ROTATE",
+           "MOVE_DTYPE"]
+
+_INFO_INTS = ["imcon", "kmax1", "kmax2", "kmax3", "K", "natoms", "nspecies", "ntypes", "mxgrid", "nframework",
+              "moves", "nvoxels", "guest_capacity", "voxel_entries", "r14", "r15"]
+_INFO_DBLS = ["alpha", "rcut", "delr", "volm", "engunit", "temp", "beta", "drewd", "dlrpot", "spenergy", "dlpeng",
+              "ewald1sum", "elrc", "energy", "statvolm", "r15"]
+
+
+def deck_inspect(directory):
+    """Parse a deck and build its tables on the host (no GPU).  Returns a dict."""
+    ints = np.zeros(16, dtype=np.int32)
+    dbls = np.zeros(16)
+    K, nerc = ctypes.c_int(0), ctypes.c_int(0)
+    d = str(directory).encode()
+    check(lib().fmc_deck_inspect(d, ip(ints), dp(dbls), None, None, None, None, ctypes.byref(K), ctypes.byref(nerc)))
+    info = dict(zip(_INFO_INTS, ints.tolist()))
+    info.update(zip(_INFO_DBLS, dbls.tolist()))
+    lmn = np.zeros((K.value, 3), dtype=np.int32)
+    akk = np.zeros(K.value)
+    erc = np.zeros(nerc.value)
+    q = np.zeros(max(info["nframework"], 1))
+    check(lib().fmc_deck_inspect(d, None, None, ip(lmn), dp(akk), dp(erc), dp(q), ctypes.byref(K),
+                                 ctypes.byref(nerc)))
+    info.update(lmn=lmn, akk=akk, erc=erc, charges=q[: info["nframework"]])
+    return info
+
+
+class Chain:
+    """One GCMC chain on one GPU (the plain FP64 path)."""
+
+    def __init__(self, directory, seed=(12, 34, 56, 78), device=0):
+        self.h = ctypes.c_void_p()
+        s = np.asarray(seed, dtype=np.int32)
+        check(lib().fmc_chain_open(str(directory).encode(), ip(s), int(device), ctypes.byref(self.h)))
+
+    def close(self):
+        if self.h:
+            lib().fmc_chain_close(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self):
+        ints = np.zeros(16, dtype=np.int32)
+        dbls = np.zeros(16)
+        check(lib().fmc_chain_info(self.h, ip(ints), dp(dbls)))
+        out = dict(zip(_INFO_INTS, ints.tolist()))
+        out.update(zip(_INFO_DBLS, dbls.tolist()))
+        return out
+
+    # ---- reference energy routines
+    def ewald1(self):
+        e, k = ctypes.c_double(0), ctypes.c_int(0)
+        check(lib().fmc_ewald1(self.h, ctypes.byref(e), ctypes.byref(k)))
+        return e.value
+
+    def ewald1_guest(self, iguest, xyz, move, pass_=1):
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+        e = ctypes.c_double(0)
+        check(lib().fmc_ewald1_guest(self.h, int(iguest), xyz.shape[0], dp(xyz), int(move), int(pass_),
+                                     ctypes.byref(e)))
+        return e.value
+
+    def guest_realspace(self, iguest, xyz, mol=-1):
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+        e2, ev = ctypes.c_double(0), ctypes.c_double(0)
+        check(lib().fmc_guest_realspace(self.h, int(iguest), xyz.shape[0], dp(xyz), int(mol), ctypes.byref(e2),
+                                        ctypes.byref(ev)))
+        return e2.value, ev.value
+
+    def commit(self, move, iguest, mol, xyz=None):
+        x = None if xyz is None else np.ascontiguousarray(xyz, dtype=np.float64)
+        check(lib().fmc_commit(self.h, int(move), int(iguest), int(mol), None if x is None else dp(x)))
+
+    def set_guests(self, iguest, xyz):
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64)
+        nsite = xyz.shape[1] if xyz.ndim == 3 else None
+        nmol = xyz.shape[0] if xyz.ndim == 3 else 0
+        if nsite is None:
+            raise ValueError("xyz must be (nmol, nsite, 3)")
+        check(lib().fmc_set_guests(self.h, int(iguest), nmol, dp(xyz)))
+
+    def single_point(self):
+        a, b = ctypes.c_double(0), ctypes.c_double(0)
+        check(lib().fmc_single_point(self.h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def sk(self, pending=False):
+        K = self.info()["K"]
+        re, im = np.zeros(K), np.zeros(K)
+        check(lib().fmc_get_sk(self.h, int(bool(pending)), dp(re), dp(im)))
+        return re + 1j * im
+
+    def kvectors(self):
+        K = self.info()["K"]
+        lmn = np.zeros((K, 3), dtype=np.int32)
+        akk = np.zeros(K)
+        check(lib().fmc_kvectors(self.h, ip(lmn), dp(akk)))
+        return lmn, akk
+
+    # ---- move loop
+    def run(self, nmoves, trace=True):
+        rec = np.zeros(nmoves, dtype=MOVE_DTYPE) if trace else None
+        check(lib().fmc_run(self.h, int(nmoves), rec.ctypes.data if trace else None))
+        return rec
+
+    def guest_coords(self, iguest=0):
+        """Coordinates of species `iguest` as (nmol, nsite, 3), molecule order of the reference."""
+        n, ns = ctypes.c_int(0), ctypes.c_int(0)
+        check(lib().fmc_guest_coords(self.h, int(iguest), None, ctypes.byref(n), ctypes.byref(ns)))
+        buf = np.zeros((max(n.value, 1), ns.value, 3))
+        check(lib().fmc_guest_coords(self.h, int(iguest), dp(buf), ctypes.byref(n), ctypes.byref(ns)))
+        return buf[: n.value]
+
+    def stats(self, iguest=0):
+        out = np.zeros(6)
+        check(lib().fmc_stats(self.h, int(iguest), dp(out)))
+        return dict(zip(["N", "E", "EN", "N2", "E2", "prodcount"], out.tolist()))

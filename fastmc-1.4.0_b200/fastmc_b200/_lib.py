@@ -1,0 +1,82 @@
+"""ctypes binding of libfastmc_b200.so (the C ABI declared in include/fastmc_b200.h).
+
+The library is built in-tree by fastmc-1.4.0_b200/build.py.  There is no fallback: if the
+shared library is missing or fails to load, every call raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(_PKG, "lib", "libfastmc_b200.so")
+
+MOVE_DTYPE = np.dtype([
+    ("step", np.int32), ("iguest", np.int32), ("mtype", np.int32), ("randchoice", np.int32),
+    ("accepted", np.int32), ("nmols_after", np.int32), ("pad0", np.int32), ("pad1", np.int32),
+    ("ewld1", np.float64), ("ewld2", np.float64), ("ewld3", np.float64), ("vdw", np.float64),
+    ("delrc", np.float64), ("estep", np.float64), ("rande", np.float64), ("energy_after", np.float64),
+])
+
+INSERT, DELETE, DISPLACE, TRANSLATE, ROTATE = 1, 2, 3, 4, 5
+
+# Every function the C ABI exports: name -> (restype, argtypes)
+_vp, _ip, _dp, _ci, _cd = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double), \
+    ctypes.c_int, ctypes.c_double
+SIGNATURES = {
+    "fmc_version": (_ci, []),
+    "fmc_last_error": (ctypes.c_char_p, []),
+    "fmc_chain_open": (_ci, [ctypes.c_char_p, _ip, _ci, ctypes.POINTER(_vp)]),
+    "fmc_chain_close": (None, [_vp]),
+    "fmc_chain_info": (_ci, [_vp, _ip, _dp]),
+    "fmc_ewald1": (_ci, [_vp, _dp, _ip]),
+    "fmc_ewald1_guest": (_ci, [_vp, _ci, _ci, _dp, _ci, _ci, _dp]),
+    "fmc_guest_realspace": (_ci, [_vp, _ci, _ci, _dp, _ci, _dp, _dp]),
+    "fmc_commit": (_ci, [_vp, _ci, _ci, _ci, _dp]),
+    "fmc_set_guests": (_ci, [_vp, _ci, _ci, _dp]),
+    "fmc_single_point": (_ci, [_vp, _dp, _dp]),
+    "fmc_get_sk": (_ci, [_vp, _ci, _dp, _dp]),
+    "fmc_kvectors": (_ci, [_vp, _ip, _dp]),
+    "fmc_run": (_ci, [_vp, _ci, _vp]),
+    "fmc_guest_coords": (_ci, [_vp, _ci, _dp, _ip, _ip]),
+    "fmc_stats": (_ci, [_vp, _ci, _dp]),
+    "fmc_deck_inspect": (_ci, [ctypes.c_char_p, _ip, _dp, _ip, _dp, _dp, _dp, _ip, _ip]),
+}
+
+_lib = None
+
+
+class FastMCError(RuntimeError):
+    """Error returned by the library; `code` is the reference's error code when > 0."""
+
+    def __init__(self, code, msg):
+        super().__init__(f"FastMC error {code}: {msg}")
+        self.code = code
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FastMCError(-1, f"{LIB_PATH} is missing; build it with fastmc-1.4.0_b200/build.py")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc):
+    if rc != 0:
+        raise FastMCError(rc, lib().fmc_last_error().decode())
+    return rc
+
+
+def dp(a):
+    return a.ctypes.data_as(_dp)
+
+
+def ip(a):
+    return a.ctypes.data_as(_ip)

@@ -1,0 +1,114 @@
+/* fastmc_b200.h -- C ABI of the B200 GCMC trial-move energy path.
+ *
+ * Drop-in boundary for FastMC 1.4.0's energy routines.  Plain C types only: pointers, sizes,
+ * int status codes.  Status: 0 = ok; > 0 = the reference's own error code (error.f: 3, 4, 25,
+ * 52-55, 75, 95, 380, 410, 2311, 2312); < 0 = this library (-2 directive outside the path,
+ * -3 move type outside the path, -4 cell convention outside imcon 1-3, -5 too many species,
+ * -6 non-rigid framework, -100-e = CUDA error e).  fmc_last_error() gives the message of the
+ * calling thread's last failure.
+ *
+ * Coordinates are Angstrom, interleaved x,y,z per site; energies follow the reference's
+ * internal units (10 J/mol) unless stated as kcal/mol.  Host pointers are caller-owned and
+ * only read or written during the call.  One chain handle must not be used by two host threads
+ * at once; distinct handles may.
+ */
+#ifndef FASTMC_B200_H
+#define FASTMC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct fmc_chain fmc_chain;
+
+/* Move-type codes (gcmc.f:753-778): insert, delete, displace (translate+rotate),
+ * translate-only, rotate-only. */
+#define FMC_INSERT 1
+#define FMC_DELETE 2
+#define FMC_DISPLACE 3
+#define FMC_TRANSLATE 4
+#define FMC_ROTATE 5
+
+/* One attempted move of the move loop; energies as in gcmc.f:946,1112,1328 (internal units
+ * except estep and energy_after, kcal/mol). */
+typedef struct fmc_move_record {
+  int32_t step, iguest, mtype, randchoice, accepted, nmols_after, pad0, pad1;
+  double ewld1, ewld2, ewld3, vdw, delrc, estep, rande, energy_after;
+} fmc_move_record;
+
+int fmc_version(void);
+const char* fmc_last_error(void);
+
+/* Reads dir/CONTROL, dir/FIELD and dir/CONFIG (readinputs.f:11-914, utility_pack.f:176-457),
+ * builds the tables (erfcgen ewald.f:1; forgen vdw_terms.f:189), uploads the rigid framework,
+ * computes the single-point energy (gcmc.f:2518-2710) and S(k) of all atoms (gcmc.f:522), and
+ * seeds duni (gcmc.f:2712) with seed[0..3] = the (i,j,k,l) the reference prints. */
+int fmc_chain_open(const char* dir, const int* seed, int device, fmc_chain** out);
+void fmc_chain_close(fmc_chain* c);
+
+/* ints[0..15]: imcon, kmax1, kmax2, kmax3, K (newld), total atoms, guest species, atom types,
+ * mxgrid, framework atoms, moves done, voxel count, guest-site capacity, 0, 0, 0.
+ * dbls[0..15]: alpha, rcut, delr, volume, engunit, temperature, beta, drewd, dlrpot,
+ * spenergy (kcal/mol), dlpeng (kcal/mol), framework recip+self (internal), elrc, energy of
+ * species 0 (kcal/mol), volume in m^3, 0. */
+int fmc_chain_info(fmc_chain* c, int* ints, double* dbls);
+
+/* ewald1 (ewald.f:368-630): recomputes S(k) over every atom now present and returns the
+ * reciprocal + self energy (internal units) and K. */
+int fmc_ewald1(fmc_chain* c, double* engcpe, int* newld);
+
+/* ewald1_guest (ewald.f:32-365) for one pass of species `iguest` (0-based) with `natms`
+ * sites at xyz.  move: FMC_INSERT, FMC_DELETE, FMC_DISPLACE; pass 1 or 2 for FMC_DISPLACE as
+ * in the reference (pass 1 stores the old sites and returns 0; pass 2 returns the energy of
+ * the displacement).  S_new stays on the device until fmc_commit. */
+int fmc_ewald1_guest(fmc_chain* c, int iguest, int natms, const double* xyz, int move, int pass, double* engcpe);
+
+/* guestlistgen + images + ewald2 + srfrce (utility_pack.f:3113-3177, ewald.f:632-694,
+ * vdw_terms.f:398-498): real-space Coulomb and vdW of the sites at xyz against every atom
+ * except molecule `mol` (0-based index within the species, -1 for none). */
+int fmc_guest_realspace(fmc_chain* c, int iguest, int natms, const double* xyz, int mol, double* ewld2, double* vdw);
+
+/* Accept the last evaluated move: S(k) <- S_new (gcmc.f:971-974) and the species' site
+ * arrays updated (insert appends at the end, delete removes molecule `mol` keeping order,
+ * displace overwrites molecule `mol`; gcmc.f:966-970, 1134-1138, 1352-1357). */
+int fmc_commit(fmc_chain* c, int move, int iguest, int mol, const double* xyz);
+
+/* Replaces all molecules of species `iguest` (the condense of utility_pack.f:3325), then
+ * recomputes S(k).  xyz holds nmol*nsite sites, molecule-major. */
+int fmc_set_guests(fmc_chain* c, int iguest, int nmol, const double* xyz);
+
+/* single_point (gcmc.f:2518-2710) of the current state: guest energy and the DL_POLY total,
+ * both kcal/mol. */
+int fmc_single_point(fmc_chain* c, double* spenergy, double* dlpeng);
+
+/* S(k) (current, or the pending S_new) as separate real/imaginary arrays of K values. */
+int fmc_get_sk(fmc_chain* c, int pending, double* re, double* im);
+/* k-vector table in the reference's order: lmn[3K] and akk[K]. */
+int fmc_kvectors(fmc_chain* c, int* lmn, double* akk);
+
+/* The plain GPU move loop: `nmoves` iterations of gcmc.f:589-1380 on the host with every
+ * energy evaluated on the device; trace (nullable) receives one record per move. */
+int fmc_run(fmc_chain* c, int nmoves, fmc_move_record* trace);
+
+/* Guest coordinates of species `iguest` (nmol*nsite sites, molecule-major); *nmol and *nsite
+ * are set; xyz may be NULL to query the counts. */
+int fmc_guest_coords(fmc_chain* c, int iguest, double* xyz, int* nmol, int* nsite);
+
+/* Rolling production statistics of species `iguest` (gcmc.f:1814-1860):
+ * out[0..5] = <N>, <E>, <EN>, <N^2>, <E^2>, production moves counted. */
+int fmc_stats(fmc_chain* c, int iguest, double* out);
+
+/* Host-only (no GPU needed): parse a deck and build its tables.  ints/dbls as in
+ * fmc_chain_info (entries that need the device are zero).  Any of lmn[3K], akk[K], erc[mxgrid+1],
+ * charges[framework atoms] may be NULL; *K and *nerc return the sizes. */
+int fmc_deck_inspect(const char* dir, int* ints, double* dbls, int* lmn, double* akk, double* erc, double* charges,
+                     int* K, int* nerc);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FASTMC_B200_H */

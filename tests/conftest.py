@@ -1,0 +1,57 @@
+import os
+import subprocess
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PKG = os.path.join(ROOT, "fastmc-1.4.0_b200")
+for p in (PKG, os.path.join(ROOT, "oracle")):
+    if p not in sys.path:
+        sys.path.insert(0, p)
+
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a B200 (runs through the CUDA library)")
+
+
+@pytest.fixture(scope="session")
+def oracle_mod():
+    import oracle
+
+    oracle.build()
+    return oracle
+
+
+@pytest.fixture(scope="session")
+def fmc():
+    lib = os.path.join(PKG, "lib", "libfastmc_b200.so")
+    if not os.path.exists(lib):
+        subprocess.run([sys.executable, os.path.join(PKG, "build.py")], check=True)
+    import fastmc_b200
+
+    return fastmc_b200
+
+
+@pytest.fixture(scope="session")
+def decks(tmp_path_factory):
+    """Synthetic input decks shared by the tests."""
+    from fastmc_b200 import synth
+
+    root = tmp_path_factory.mktemp("decks")
+    out = {
+        "small": synth.write_plain_small(str(root / "small")),
+        "large": synth.write_plain_large(str(root / "large")),
+        "calf20": os.path.join(GOLDEN, "calf20"),
+    }
+    fws = synth.batched_frameworks(3, seed=11)
+    for i, fw in enumerate(fws):
+        L = [fw.cell[j, j] for j in range(3)]
+        out[f"ortho{i}"] = synth.write_inputs(str(root / f"ortho{i}"), fw, ["CO2"], [1.0], 298.0,
+                                              tuple(synth.kmax_for(x) for x in L))
+    fw = fws[0]
+    out["mixture"] = synth.write_inputs(str(root / "mixture"), fw, ["CO2", "N2"], [0.15, 0.85], 298.0,
+                                        tuple(synth.kmax_for(fw.cell[j, j]) for j in range(3)))
+    return out

@@ -1,0 +1,70 @@
+"""Regenerate the golden fixtures under tests/golden/ from the reference's shipped example.
+
+Run in a container where the reference checkout is mounted (default /root/reference):
+
+    python tests/golden/make_golden.py [/path/to/reference]
+
+It copies the CALF-20 example inputs (CONTROL, FIELD, CONFIG) of
+examples/restart/1_restart_example_with_completed_long_simulation_data/ and converts the
+final chain state in branch01/REVIVE (Fortran unformatted sequential records, layout of
+revive, utility_pack.f:1800-1815) into revive_guests.npy.  The known answers recorded in
+expected.json come from that example's OUTPUT and REVIVE:
+
+* OUTPUT:108  duni seed "103 112 53 153"
+* OUTPUT:113  "Energy reported by DL_POLY: -11190.606165" (empty framework, recip + self)
+* REVIVE      energy(1) = -731.5072668178669 kcal/mol for the 90-CO2 state it stores
+"""
+import json
+import os
+import shutil
+import struct
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+EXAMPLE = "examples/restart/1_restart_example_with_completed_long_simulation_data"
+
+
+def read_fortran_records(path):
+    data = open(path, "rb").read()
+    recs, o = [], 0
+    while o < len(data):
+        n = struct.unpack("<i", data[o:o + 4])[0]
+        recs.append(data[o + 4:o + 4 + n])
+        tail = struct.unpack("<i", data[o + 4 + n:o + 8 + n])[0]
+        assert tail == n, "corrupt record marker"
+        o += 8 + n
+    return recs
+
+
+def main(ref):
+    src = os.path.join(ref, EXAMPLE)
+    out = os.path.join(HERE, "calf20")
+    os.makedirs(out, exist_ok=True)
+    for f in ("CONTROL", "FIELD", "CONFIG"):
+        shutil.copyfile(os.path.join(src, f), os.path.join(out, f))
+    recs = read_fortran_records(os.path.join(src, "branch01", "REVIVE"))
+    nummols = np.frombuffer(recs[1], "<i4")
+    nco2 = int(nummols[0])
+    gx, gy, gz = (np.frombuffer(recs[4 + i], "<f8") for i in range(3))
+    guests = np.stack([gx, gy, gz], axis=1).reshape(nco2, 3, 3)
+    energy = float(np.frombuffer(recs[-1], "<f8")[0])
+    np.save(os.path.join(out, "revive_guests.npy"), guests)
+    expected = {
+        "seed": [103, 112, 53, 153],
+        "dlpeng_empty_kcal": -11190.606165,
+        "dlpeng_empty_digits": 6,
+        "kmax": [9, 8, 8],
+        "K": 870,
+        "revive_nummols": [int(v) for v in nummols],
+        "revive_energy_kcal": energy,
+        "source": EXAMPLE + " (OUTPUT lines 108, 113; branch01/REVIVE)",
+    }
+    with open(os.path.join(out, "expected.json"), "w") as f:
+        json.dump(expected, f, indent=1)
+    print("wrote", out)
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

@@ -1,0 +1,107 @@
+"""Host logic of the product (no GPU): C-ABI exports, deck reading and tables against the oracle,
+the reference's error codes."""
+import os
+import re
+import shutil
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+
+def header_symbols():
+    text = open(os.path.join(ROOT, "include", "fastmc_b200.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(fmc_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol(fmc):
+    import ctypes
+
+    from fastmc_b200 import _lib
+
+    L = ctypes.CDLL(_lib.LIB_PATH)
+    syms = header_symbols()
+    assert len(syms) >= 15
+    for s in syms:
+        assert hasattr(L, s), s
+    assert set(syms) == set(_lib.SIGNATURES), "python binding and header disagree"
+    assert L.fmc_version() == 10400
+
+
+@pytest.mark.parametrize("name", ["calf20", "small", "large", "ortho0", "ortho1", "mixture"])
+def test_deck_tables_match_oracle_bit_exact(fmc, oracle_mod, decks, name):
+    info = fmc.deck_inspect(decks[name])
+    orc = oracle_mod.Chain(decks[name])
+    lmn, akk = orc.kvectors()
+    assert info["K"] == len(akk)
+    assert np.array_equal(info["lmn"], lmn)
+    assert np.array_equal(info["akk"], akk)
+    assert np.array_equal(info["erc"], orc.erc())
+    s = orc.scalars()
+    for k in ("alpha", "rcut", "volm", "engunit", "beta", "drewd", "dlrpot", "statvolm"):
+        assert info[k] == s[k], k
+    _, q, _, _ = orc.atoms()
+    assert np.array_equal(info["charges"], q[len(q) - info["nframework"]:])
+
+
+def _copy_deck(src, dst):
+    shutil.copytree(src, dst)
+    return dst
+
+
+def _edit(path, old, new):
+    t = open(path).read()
+    assert old in t
+    open(path, "w").write(t.replace(old, new, 1))
+
+
+CASES = [
+    ("CONTROL", "temperature", "# temperature", 380),   # temperature missing
+    ("CONTROL", "move insert", "wibble insert", 3),     # unknown directive
+    ("CONTROL", "ewald sum", "# ewald sum", 2311),      # no Ewald sum
+    ("CONTROL", "&guest 1", "&guest 2", 2312),          # guest index not in FIELD
+    ("CONTROL", "finish", "", 53),                      # CONTROL ends early
+    ("CONFIG", "Zn   ", "Qq   ", 25),                   # wrong atom label
+    ("FIELD", "close", "", 52),                         # FIELD ends early
+    ("FIELD", "UNITS kcal", "UNITS kcal\nbogus line", 4),  # unknown FIELD directive
+    ("CONTROL", "cutoff 12.500000", "cutoff 14.000000", 95),  # cutoff beyond half width
+]
+
+
+@pytest.mark.parametrize("fname,old,new,code", CASES)
+def test_reference_error_codes(fmc, oracle_mod, decks, tmp_path, fname, old, new, code):
+    d = _copy_deck(decks["small"], str(tmp_path / "deck"))
+    _edit(os.path.join(d, fname), old, new)
+    with pytest.raises(fmc.FastMCError) as e:
+        fmc.deck_inspect(d)
+    assert e.value.code == code
+    with pytest.raises(oracle_mod.OracleError) as eo:
+        oracle_mod.Chain(d)
+    assert eo.value.code == code
+
+
+def test_cubic_cell_consistency_error_410(fmc, oracle_mod, decks, tmp_path):
+    d = _copy_deck(decks["small"], str(tmp_path / "deck"))
+    lines = open(os.path.join(d, "CONFIG")).read().split("\n")
+    lines[3] = "".join(f"{v:20.12f}" for v in (0.0, 25.9, 0.0))
+    open(os.path.join(d, "CONFIG"), "w").write("\n".join(lines))
+    with pytest.raises(fmc.FastMCError) as e:
+        fmc.deck_inspect(d)
+    assert e.value.code == 410
+    with pytest.raises(oracle_mod.OracleError) as eo:
+        oracle_mod.Chain(d)
+    assert eo.value.code == 410
+
+
+def test_dblstr_semantics_through_ewald_line(fmc, oracle_mod, decks, tmp_path):
+    # 'ewald precision 1d-6' goes through the DL_POLY precision rule in both readers
+    d = _copy_deck(decks["small"], str(tmp_path / "deck"))
+    _edit(os.path.join(d, "CONTROL"), "ewald sum 0.260000 8 8 8", "ewald precision 1d-6")
+    info = fmc.deck_inspect(d)
+    orc = oracle_mod.Chain(d)
+    i = orc.ints()
+    assert (info["kmax1"], info["kmax2"], info["kmax3"]) == (i["kmax1"], i["kmax2"], i["kmax3"])
+    assert info["alpha"] == orc.scalars()["alpha"]
+    assert info["K"] == i["newld"]

@@ -1,0 +1,74 @@
+"""The FP64 oracle against every known answer the reference ships (no GPU needed)."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+
+CALF = os.path.join(GOLDEN, "calf20")
+
+
+def expected():
+    with open(os.path.join(CALF, "expected.json")) as f:
+        return json.load(f)
+
+
+def test_duni_matches_published_universal_generator_vector(oracle_mod):
+    # Marsaglia-Zaman universal generator known answer (F. James, Comput. Phys. Commun. 60
+    # (1990) 329, RANMAR test): seeds (12,34,56,78); numbers 20001..20006 times 4096^2.
+    s = oracle_mod.duni_stream((12, 34, 56, 78), 20006)
+    assert (s[20000:] * 4096.0 * 4096.0).tolist() == [6533892.0, 14220222.0, 7275067.0, 6172232.0, 8354498.0,
+                                                       10633180.0]
+
+
+def test_calf20_precision_rule_and_kvectors(oracle_mod):
+    c = oracle_mod.Chain(CALF, seed=expected()["seed"])
+    i = c.ints()
+    assert [i["kmax1"], i["kmax2"], i["kmax3"]] == expected()["kmax"]
+    assert i["newld"] == expected()["K"]
+    assert i["imcon"] == 3
+    assert abs(c.scalars()["alpha"] - 0.25396) < 5e-6
+
+
+def test_calf20_empty_framework_energy_pin(oracle_mod):
+    c = oracle_mod.Chain(CALF, seed=expected()["seed"])
+    # printed with 6 decimals in the reference OUTPUT
+    assert abs(c.scalars()["dlpeng"] - expected()["dlpeng_empty_kcal"]) <= 5e-7
+
+
+def test_revive_state_single_point_pin(oracle_mod):
+    c = oracle_mod.Chain(CALF, seed=expected()["seed"])
+    guests = np.load(os.path.join(CALF, "revive_guests.npy"))
+    c.load_guests(0, guests.reshape(-1, 3))
+    e = c.scalars()["spenergy"]
+    ref = expected()["revive_energy_kcal"]
+    assert abs(e - ref) / abs(ref) < 1e-9
+
+
+def test_move_loop_energy_bookkeeping(oracle_mod, decks):
+    c = oracle_mod.Chain(decks["small"], seed=(12, 34, 56, 78))
+    tr = c.run(3000)
+    acc = tr["accepted"] == 1
+    assert np.isclose(np.sum(tr["estep"][acc]), tr["energy_after"][-1], rtol=0, atol=1e-6)
+    # every insert attempt while empty is forced; molecule count changes only on accepted ins/del
+    dn = np.diff(np.concatenate([[0], tr["nmols_after"]]))
+    assert np.all(dn[(tr["mtype"] == 1) & acc] == 1)
+    assert np.all(dn[(tr["mtype"] == 2) & acc] == -1)
+    assert np.all(dn[~acc] == 0)
+    # the running energy equals a fresh single point of the final state (drift bound)
+    coords = c.guest_coords(0)
+    e_run = c.scalars()["energy"]
+    c2 = oracle_mod.Chain(decks["small"], seed=(12, 34, 56, 78))
+    c2.load_guests(0, coords.reshape(-1, 3))
+    assert abs(c2.scalars()["spenergy"] - e_run) <= 1e-8 * max(1.0, abs(e_run))
+
+
+def test_rng_draw_order_displacement_skips_rande_when_downhill(oracle_mod, decks):
+    c = oracle_mod.Chain(decks["small"], seed=(12, 34, 56, 78))
+    tr = c.run(3000)
+    disp = np.isin(tr["mtype"], [3, 4, 5])
+    down = disp & (tr["estep"] < 0)
+    assert np.all(tr["rande"][down] == -1.0)
+    assert np.all(tr["accepted"][down] == 1)
