@@ -247,6 +247,45 @@ int fmc_stats(fmc_chain* c, int iguest, double* out) {
   return 0;
 }
 
+int fmc_chain_profile(fmc_chain* c, int enable, double* out) {
+  CHECK_CHAIN(c);
+  fmc::Chain& C = c->impl;
+  if (enable < 0) {
+    C.passes = C.commits = C.pass_timed = 0;
+    C.pass_ms = 0.0;
+  }
+  C.profile = enable != 0;
+  if (out) {
+    const fmc::HostSystem& S = C.sys;
+    int nv = S.nvox[0] * S.nvox[1] * S.nvox[2];
+    out[0] = (double)C.passes;
+    out[1] = (double)C.commits;
+    out[2] = (double)C.pass_timed;
+    out[3] = C.pass_ms;
+    out[4] = (double)S.K;
+    out[5] = nv ? (double)S.vox_atoms.size() / nv : 0.0;
+  }
+  return 0;
+}
+
+int fmc_run_timed(fmc_chain* c, int nmoves, fmc_move_record* trace, float* device_ms) {
+  CHECK_CHAIN(c);
+  fmc::Chain& C = c->impl;
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  cudaEventRecord(a, C.st);
+  int rc = fmc_run(c, nmoves, trace);
+  cudaEventRecord(b, C.st);
+  cudaEventSynchronize(b);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (device_ms) *device_ms = ms;
+  return rc;
+}
+
 int fmc_deck_inspect(const char* dir, int* ints, double* dbls, int* lmn, double* akk, double* erc, double* charges,
                      int* K, int* nerc) {
   if (!dir) return fail(-1, "null argument");

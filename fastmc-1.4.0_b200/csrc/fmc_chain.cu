@@ -78,6 +78,8 @@ fail:
 }
 
 Chain::~Chain() {
+  if (ev0) cudaEventDestroy(ev0);
+  if (ev1) cudaEventDestroy(ev1);
   if (st) {
     cudaSetDevice(device);
     cudaStreamSynchronize(st);
@@ -125,6 +127,7 @@ int Chain::open(const std::string& dir, const int seed[4], int dev, std::string&
   dsys.device = dev;
   FMC_CUDA(cudaSetDevice(dev));
   FMC_CUDA(configure_kernels());
+  FMC_CUDA(configure_recip_kernels());
   FMC_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
   rc = upload_system(sys, dsys, err);
   if (rc) return rc;
@@ -373,10 +376,22 @@ int Chain::pass(int move, int g, int mol, const double* old_xyz, const double* n
     A.q[w] = G.charge[i];
     A.type[w] = (unsigned char)G.type[i];
   }
+  if (profile && !ev0) {
+    cudaEventCreate(&ev0);
+    cudaEventCreate(&ev1);
+  }
+  if (profile) cudaEventRecord(ev0, st);
   cudaError_t e = launch_pass(dsys.view, guest_view(), A, sk, sk_new, W, st);
+  if (profile) cudaEventRecord(ev1, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(h_result, W.result, sizeof(double) * 3, cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return sync_error(e);
+  if (profile) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ev0, ev1);
+    pass_ms += ms;
+    pass_timed++;
+  }
   out[0] = h_result[0];
   out[1] = h_result[1];
   out[2] = h_result[2];
@@ -408,6 +423,7 @@ int Chain::commit(int move, int g, int mol, const double* new_xyz) {
     }
   cudaError_t e = launch_commit(sys.K, sk, sk_new, C, gsite, gtype, st);
   if (e != cudaSuccess) return sync_error(e);
+  commits++;
   // host mirror (framwkxxx updates of gcmc.f:966-970, 1134-1138, 1352-1357)
   int n3 = 3 * s.nsite;
   if (move == kInsert) {

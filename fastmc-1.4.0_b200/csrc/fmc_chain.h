@@ -70,8 +70,12 @@ class Chain {
   long long prodcount = 0;
   bool tick_tock[5] = {false, false, false, false, false};
   std::vector<double> chainstats;  // 1 + 14*ntpguest, <N>,<E>,<EN>,<N^2>,<E^2> rolling
-  // timing of the device passes
-  long long passes = 0;
+  // launch accounting and optional CUDA-event timing of the pass kernel
+  long long passes = 0, commits = 0;
+  bool profile = false;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double pass_ms = 0.0;
+  long long pass_timed = 0;
 
   ~Chain();
   int open(const std::string& dir, const int seed[4], int device, std::string& err);

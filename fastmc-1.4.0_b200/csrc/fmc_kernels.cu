@@ -140,6 +140,7 @@ cudaError_t configure_kernels() {
   return cudaFuncSetAttribute(fmc_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
 }
 
+
 // ------------------------------------------------------------------------------ commit
 __global__ void fmc_commit_kernel(int K, double2* sk, const double2* __restrict__ sk_new, CommitArgs C,
                                   double4* site, int* type) {
@@ -244,7 +245,7 @@ __global__ void fmc_recip_reduce_kernel(DevSystem S, const double2* __restrict__
 
 int recip_chunk(const DevSystem& S) {
   int stride = (S.kmax[0] + 1) + (S.kmax[1] + 1) + (S.kmax[2] + 1);
-  int c = (48 * 1024) / (stride * (int)sizeof(double2));
+  int c = (40 * 1024) / (stride * (int)sizeof(double2));  // + 2 KB static charges < 48 KB
   if (c > 256) c = 256;
   return c < 1 ? 1 : c;
 }
@@ -272,6 +273,10 @@ cudaError_t launch_recip_full(const DevSystem& S, const double4* atoms, int nato
                                                                                       partial);
   fmc_recip_reduce_kernel<<<recip_nparts(S), 256, 0, st>>>(S, partial, nchunk, sk, parts);
   return cudaGetLastError();
+}
+
+cudaError_t configure_recip_kernels() {
+  return cudaFuncSetAttribute(fmc_recip_partial_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
 }
 
 double recip_energy_from_parts(const DevSystem& S, const double* host_parts) {

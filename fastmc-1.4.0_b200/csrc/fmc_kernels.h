@@ -40,6 +40,7 @@ struct CommitArgs {
 int pass_smem_bytes(const DevSystem& S, int nsite);
 int pass_recip_blocks(const DevSystem& S);
 cudaError_t configure_kernels();  // once per device, before the first launch
+cudaError_t configure_recip_kernels();
 cudaError_t launch_pass(const DevSystem& S, const GuestView& G, const PassArgs& A, const double2* sk, double2* sk_new,
                         const PassScratch& W, cudaStream_t st);
 cudaError_t launch_commit(int K, double2* sk, const double2* sk_new, const CommitArgs& C, double4* site, int* type,

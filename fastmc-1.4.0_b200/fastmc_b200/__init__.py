@@ -123,6 +123,18 @@ class Chain:
         check(lib().fmc_run(self.h, int(nmoves), rec.ctypes.data if trace else None))
         return rec
 
+    def run_timed(self, nmoves, trace=False):
+        """Runs nmoves; returns (trace or None, device milliseconds from CUDA events)."""
+        rec = np.zeros(nmoves, dtype=MOVE_DTYPE) if trace else None
+        ms = ctypes.c_float(0)
+        check(lib().fmc_run_timed(self.h, int(nmoves), rec.ctypes.data if trace else None, ctypes.byref(ms)))
+        return rec, float(ms.value)
+
+    def profile(self, enable=1):
+        out = np.zeros(6)
+        check(lib().fmc_chain_profile(self.h, int(enable), dp(out)))
+        return dict(zip(["passes", "commits", "timed_passes", "pass_ms", "K", "voxel_mean"], out.tolist()))
+
     def guest_coords(self, iguest=0):
         """Coordinates of species `iguest` as (nmol, nsite, 3), molecule order of the reference."""
         n, ns = ctypes.c_int(0), ctypes.c_int(0)

@@ -40,6 +40,8 @@ SIGNATURES = {
     "fmc_run": (_ci, [_vp, _ci, _vp]),
     "fmc_guest_coords": (_ci, [_vp, _ci, _dp, _ip, _ip]),
     "fmc_stats": (_ci, [_vp, _ci, _dp]),
+    "fmc_chain_profile": (_ci, [_vp, _ci, _dp]),
+    "fmc_run_timed": (_ci, [_vp, _ci, _vp, ctypes.POINTER(ctypes.c_float)]),
     "fmc_deck_inspect": (_ci, [ctypes.c_char_p, _ip, _dp, _ip, _dp, _dp, _dp, _ip, _ip]),
 }
 

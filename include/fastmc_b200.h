@@ -101,6 +101,16 @@ int fmc_guest_coords(fmc_chain* c, int iguest, double* xyz, int* nmol, int* nsit
  * out[0..5] = <N>, <E>, <EN>, <N^2>, <E^2>, production moves counted. */
 int fmc_stats(fmc_chain* c, int iguest, double* out);
 
+/* Launch accounting and timing of the plain path.  enable != 0 turns on CUDA-event timing of
+ * every trial-pass kernel on the chain's stream (enable < 0 also clears the counters).
+ * out[0..5]: trial-pass launches, commit launches, timed pass launches, total timed pass
+ * kernel ms, K, sites scanned per pass (framework voxel-list mean). */
+int fmc_chain_profile(fmc_chain* c, int enable, double* out);
+
+/* fmc_run with the run bracketed by CUDA events on the chain's stream: *device_ms receives
+ * the elapsed device time of the whole run (host move loop included, as it drives the GPU). */
+int fmc_run_timed(fmc_chain* c, int nmoves, fmc_move_record* trace, float* device_ms);
+
 /* Host-only (no GPU needed): parse a deck and build its tables.  ints/dbls as in
  * fmc_chain_info (entries that need the device are zero).  Any of lmn[3K], akk[K], erc[mxgrid+1],
  * charges[framework atoms] may be NULL; *K and *nerc return the sizes. */
