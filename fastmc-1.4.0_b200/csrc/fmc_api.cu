@@ -22,6 +22,10 @@ int fail(int code, const std::string& msg) {
   if (!(c)) return fail(-1, "null chain handle")
 }  // namespace
 
+namespace fmc {
+void set_last_error(const std::string& msg) { g_err = msg; }
+}  // namespace fmc
+
 extern "C" {
 
 int fmc_version(void) { return 10400; }

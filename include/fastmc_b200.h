@@ -111,6 +111,24 @@ int fmc_chain_profile(fmc_chain* c, int enable, double* out);
  * the elapsed device time of the whole run (host move loop included, as it drives the GPU). */
 int fmc_run_timed(fmc_chain* c, int nmoves, fmc_move_record* trace, float* device_ms);
 
+/* Reciprocal-space trial pass that allocates nothing (no counterpart in the reference; its
+ * arithmetic is that of fmc_ewald1_guest).  For callers that may not call cudaMalloc -- a
+ * plug-in whose device memory belongs to the host application's own pool, or a loop where an
+ * allocation must not happen -- and that already hold every buffer on the current device:
+ *   d_lmn[3K] (l,m,n per k-vector, order of fmc_kvectors), d_akk[K], d_sk[2K] (Re,Im pairs),
+ *   outputs d_sk_new[2K] and d_engcpe[1] (the pass energy, internal units, as ewald1_guest);
+ *   host arrays kmax[3], cell[9] (cell vectors a,b,c), sites[4*(nold+nnew)] (x,y,z,q; the nold
+ *   old sites first); recip_pref = 2*(2 pi/V)*r4pie0, engsic the species' self term.
+ * move: FMC_INSERT (nold = 0), FMC_DELETE (nnew = 0) or FMC_DISPLACE (both, one fused pass).
+ * Scratch is a fixed array in the library image sized for K <= 32768 and 1..100 sites; larger
+ * requests are rejected (status -7, message in fmc_last_error()).  The first call on a device
+ * looks up that array's address and should come before any stream capture.  All calls share
+ * the array, so calls that overlap on one GPU race.  Asynchronous on `stream` (a
+ * cudaStream_t, NULL = default stream). */
+int fmc_ewald1_guest_noalloc(int K, const int* kmax, const double* cell, const int* d_lmn, const double* d_akk,
+                             const double* d_sk, int move, int nold, int nnew, const double* sites,
+                             double recip_pref, double engsic, double* d_sk_new, double* d_engcpe, void* stream);
+
 /* Host-only (no GPU needed): parse a deck and build its tables.  ints/dbls as in
  * fmc_chain_info (entries that need the device are zero).  Any of lmn[3K], akk[K], erc[mxgrid+1],
  * charges[framework atoms] may be NULL; *K and *nerc return the sizes. */
