@@ -1,0 +1,101 @@
+// Batched path: many independent GCMC chains advanced by one persistent kernel, one CTA per
+// chain, the whole move loop of gcmc.f:589-1380 on the device.  Chains that share a framework
+// deck (same FIELD / CONFIG / cut-offs / Ewald parameters) share one device system.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "fmc_chain.h"
+
+namespace fmc {
+
+constexpr int kBatchMaxSites = 16;  // sites per guest species on the batched path
+constexpr int kBatchMaxTypes = 16;  // unique atom types
+constexpr int kBatchMaxTab = kBatchMaxTypes * (kBatchMaxTypes + 1) / 2;
+constexpr int kBatchThreads = 256;
+
+struct SpeciesConst {
+  int nsite;
+  double tx[kBatchMaxSites], ty[kBatchMaxSites], tz[kBatchMaxSites];
+  double q[kBatchMaxSites], mass[kBatchMaxSites];
+  int type[kBatchMaxSites];
+  double engsic, ewald3en;
+};
+
+// Per-system constants (device memory, read-only during a launch).
+struct SysConst {
+  DevSystem S;
+  int nspecies, ntypes, lrc_on;
+  SpeciesConst sp[kMaxGuestTypes];
+  double steadd[kBatchMaxTab + 1];
+  int numfrz[kBatchMaxTypes + 1];
+  double engunit, volm, statvolm;
+};
+
+// Per-chain parameters and mutable state (device memory).
+struct ChainDev {
+  int sys;
+  int status;  // 0 ok; 75 guest capacity exhausted; 3 unsupported move drawn
+  // parameters (CONTROL)
+  double temp, beta, press[kMaxGuestTypes], mvcum[kMaxGuestTypes][9];
+  double disp_ratio[kMaxGuestTypes], tran_ratio[kMaxGuestTypes], rota_ratio;
+  int maxguest, mcsteps, eqsteps, laccsample;
+  // move-loop state
+  Duni rng;
+  int gcmccount, totatm, framatm;
+  int nmol[kMaxGuestTypes];
+  int numtyp[kBatchMaxTypes + 1];
+  int disp_count[kMaxGuestTypes], accept_disp[kMaxGuestTypes];
+  int tran_count[kMaxGuestTypes], accept_tran[kMaxGuestTypes];
+  int rota_count, accept_rota, ins_count, del_count, accept_ins, accept_del;
+  double delrdisp[kMaxGuestTypes], tran_delr[kMaxGuestTypes], rotangle, rota_rotangle;
+  double elrc, energy[kMaxGuestTypes];
+  int production, lgchk, tick[5];
+  long long prodcount;
+  double stats[kMaxGuestTypes][5];  // rolling <N>, <E>, <EN>, <N^2>, <E^2>
+  long long moves_done;
+  // buffers
+  double2* sk;
+  double4* gsite;
+  int* gtype;
+  int seg_off[kMaxGuestTypes], seg_cap[kMaxGuestTypes];
+};
+
+struct BatchLaunch {
+  ChainDev* chains;
+  const SysConst* systems;
+  int nchains, moves;
+  MoveRecord* trace;  // [nchains][moves] or null
+  int kmax_smem;      // largest K in the batch rounded up to a multiple of 4 (smem sizing)
+};
+
+cudaError_t launch_batch(const BatchLaunch& L, int smem_bytes, int tab_stride, cudaStream_t st);
+int batch_smem_bytes(int kmax_K, int tab_sites, int tab_stride);
+cudaError_t configure_batch_kernel(int smem_bytes);
+
+class Batch {
+ public:
+  int device = 0;
+  cudaStream_t st = nullptr;
+  std::vector<std::unique_ptr<Chain>> sys_chains;  // one opened chain per unique system
+  std::vector<int> chain_sys;
+  std::vector<SysConst> h_sys;
+  SysConst* d_sys = nullptr;
+  ChainDev* h_chains = nullptr;  // pinned host copy of every chain's control block
+  ChainDev* d_chains = nullptr;
+  std::vector<void*> allocations;
+  MoveRecord* d_trace = nullptr;
+  size_t trace_cap = 0;
+  int kmax_all = 0, tab_sites = 0, tab_stride = 0, smem = 0;
+  int nchains = 0;
+  ~Batch();
+  int open(const std::vector<std::string>& dirs, const std::vector<int>& seeds, int device, std::string& err);
+  // One step: control blocks host->device, `moves` moves of every chain, control blocks (and
+  // the optional per-move trace) device->host.  *ms: CUDA-event time of the kernel alone.
+  int run(int moves, MoveRecord* trace_host, float* ms, std::string& err);
+};
+
+}  // namespace fmc

@@ -1,0 +1,382 @@
+// Host side of the batched path: deduplicated device systems, per-chain state, launches.
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <sstream>
+
+#include "fmc_batch.h"
+
+namespace fmc {
+
+namespace {
+
+std::string slurp(const std::string& path) {
+  std::ifstream f(path);
+  std::stringstream ss;
+  ss << f.rdbuf();
+  return ss.str();
+}
+
+// Chains share a device system when framework, guests, force field, cell and the Ewald /
+// cut-off parameters coincide; temperature, pressures and move mix stay per chain.
+std::string system_key(const std::string& dir, const InputDeck& d) {
+  std::ostringstream k;
+  k.precision(17);
+  k << slurp(dir + "/FIELD") << '\x1f' << slurp(dir + "/CONFIG") << '\x1f' << d.rcut << ' ' << d.rvdw << ' '
+    << d.alpha << ' ' << d.delr << ' ' << d.kmax[0] << ' ' << d.kmax[1] << ' ' << d.kmax[2];
+  return k.str();
+}
+
+}  // namespace
+
+Batch::~Batch() {
+  if (st) {
+    cudaSetDevice(device);
+    cudaStreamSynchronize(st);
+    for (void* p : allocations) cudaFree(p);
+    if (d_trace) cudaFree(d_trace);
+    if (h_chains) cudaFreeHost(h_chains);
+    cudaStreamDestroy(st);
+  }
+}
+
+int Batch::open(const std::vector<std::string>& dirs, const std::vector<int>& seeds, int dev, std::string& err) {
+  device = dev;
+  nchains = (int)dirs.size();
+  if (cudaSetDevice(dev) != cudaSuccess || cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+    err = "cannot select the device";
+    return -100;
+  }
+  std::map<std::string, int> sys_of_key;
+  std::vector<InputDeck> decks(nchains);
+  chain_sys.assign(nchains, 0);
+  for (int c = 0; c < nchains; c++) {
+    int rc = read_input_deck(dirs[c], decks[c], err);
+    if (rc) {
+      err = dirs[c] + ": " + err;
+      return rc;
+    }
+    for (auto& g : decks[c].guests)
+      if (g.nmols) {
+        err = dirs[c] + ": the batched path starts chains from an empty framework (NUMMOLS 0 for guests)";
+        return -8;
+      }
+    std::string key = system_key(dirs[c], decks[c]);
+    auto it = sys_of_key.find(key);
+    if (it == sys_of_key.end()) {
+      auto ch = std::make_unique<Chain>();
+      int s4[4] = {12, 34, 56, 78};
+      rc = ch->open(dirs[c], s4, dev, err);
+      if (rc) {
+        err = dirs[c] + ": " + err;
+        return rc;
+      }
+      int id = (int)sys_chains.size();
+      sys_chains.push_back(std::move(ch));
+      sys_of_key[key] = id;
+      chain_sys[c] = id;
+    } else {
+      chain_sys[c] = it->second;
+    }
+  }
+  // ---- per-system constants
+  h_sys.assign(sys_chains.size(), SysConst());
+  for (size_t i = 0; i < sys_chains.size(); i++) {
+    const Chain& ch = *sys_chains[i];
+    const HostSystem& H = ch.sys;
+    SysConst& Y = h_sys[i];
+    std::memset(&Y, 0, sizeof(Y));
+    Y.S = ch.dsys.view;
+    Y.nspecies = (int)H.deck.guests.size();
+    Y.ntypes = H.ntypes;
+    Y.lrc_on = H.lrc_on;
+    if (Y.ntypes > kBatchMaxTypes) {
+      err = "more atom types than the batched path supports";
+      return -5;
+    }
+    for (int g = 0; g < Y.nspecies; g++) {
+      const GuestSpecies& G = H.deck.guests[g];
+      if (G.nsite > kBatchMaxSites) {
+        err = "guest with more sites than the batched path supports";
+        return -5;
+      }
+      SpeciesConst& P = Y.sp[g];
+      P.nsite = G.nsite;
+      for (int s = 0; s < G.nsite; s++) {
+        P.tx[s] = G.tx[s];
+        P.ty[s] = G.ty[s];
+        P.tz[s] = G.tz[s];
+        P.q[s] = G.charge[s];
+        P.mass[s] = G.mass[s];
+        P.type[s] = G.type[s];
+      }
+      P.engsic = H.engsic[g];
+      P.ewald3en = H.ewald3en[g];
+      tab_sites = std::max(tab_sites, 2 * G.nsite);
+    }
+    for (int t = 1; t < (int)H.steadd.size() && t <= kBatchMaxTab; t++) Y.steadd[t] = H.steadd[t];
+    for (int j = 0; j < H.nf; j++)
+      if (H.ffrz[j]) Y.numfrz[H.ftype[j]]++;
+    Y.engunit = H.engunit;
+    Y.volm = H.cell.volm;
+    Y.statvolm = H.statvolm;
+    kmax_all = std::max(kmax_all, H.K);
+    tab_stride = std::max(tab_stride, H.deck.kmax[0] + H.deck.kmax[1] + H.deck.kmax[2] + 3);
+  }
+  kmax_all = (kmax_all + 3) & ~3;
+  smem = batch_smem_bytes(kmax_all, tab_sites, tab_stride);
+  if (smem > 220 * 1024) {
+    err = "k-vector tables of this batch exceed the shared-memory budget of one CTA";
+    return -9;
+  }
+  if (configure_batch_kernel(smem) != cudaSuccess) {
+    err = "cannot configure the batched kernel";
+    return -100;
+  }
+  // ---- per-chain state
+  if (cudaMallocHost(&h_chains, sizeof(ChainDev) * nchains) != cudaSuccess) {
+    err = "cannot allocate pinned host memory for the chain control blocks";
+    return -100;
+  }
+  for (int c = 0; c < nchains; c++) {
+    const InputDeck& d = decks[c];
+    const Chain& ch = *sys_chains[chain_sys[c]];
+    const HostSystem& H = ch.sys;
+    ChainDev& C = h_chains[c];
+    std::memset(&C, 0, sizeof(C));
+    C.sys = chain_sys[c];
+    C.temp = d.temp;
+    C.beta = 1.0 / (kKboltz * d.temp);
+    const int ng = (int)d.guests.size();
+    for (int g = 0; g < ng; g++) {
+      C.press[g] = d.press[g];
+      std::array<double, 9> f = d.movefreq[g];
+      double nrm = 0;
+      for (double v : f) nrm += v;
+      if (nrm == 0) {
+        nrm = 1;
+        f = {1.0 / 3.0, 1.0 / 3.0, 1.0 / 3.0, 0, 0, 0, 0, 0, 0};
+      }
+      if (f[3] != 0 || f[4] != 0 || f[5] != 0 || f[8] != 0) {
+        err = "jump, flex, swap and multi-jump moves are outside the GCMC trial-move path";
+        return -3;
+      }
+      C.mvcum[g][0] = f[0] / nrm;
+      for (int k = 1; k < 9; k++) C.mvcum[g][k] = C.mvcum[g][k - 1] + (f[k] / nrm);
+      C.disp_ratio[g] = d.disp_ratio[g];
+      C.tran_ratio[g] = d.tran_ratio[g];
+      C.delrdisp[g] = d.delr;
+      C.tran_delr[g] = d.delr;
+      C.energy[g] = ch.spenergy;
+    }
+    C.rota_ratio = d.rota_ratio;
+    C.maxguest = d.maxguest;
+    C.mcsteps = d.mcsteps;
+    C.eqsteps = d.eqsteps;
+    C.laccsample = d.laccsample;
+    duni_seed(C.rng, seeds[4 * c], seeds[4 * c + 1], seeds[4 * c + 2], seeds[4 * c + 3]);
+    duni_next(C.rng);  // gcmc.f:335-336
+    C.totatm = C.framatm = H.nf;
+    for (int j = 0; j < H.nf; j++) C.numtyp[H.ftype[j]]++;
+    C.rotangle = kPi / 3.0;
+    C.rota_rotangle = kPi / 3.0;
+    C.production = d.eqsteps == 0;
+    C.lgchk = 1;
+    // buffers: S(k) starts as the framework's (empty framework), guest segments per species
+    cudaError_t e = cudaMalloc(&C.sk, sizeof(double2) * std::max(H.K, 1));
+    if (e == cudaSuccess) allocations.push_back(C.sk);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(C.sk, ch.sk, sizeof(double2) * H.K, cudaMemcpyDeviceToDevice, st);
+    int off = 0;
+    for (int g = 0; g < ng; g++) {
+      C.seg_off[g] = off;
+      C.seg_cap[g] = d.maxguest;
+      off += d.maxguest;
+    }
+    if (e == cudaSuccess) e = cudaMalloc(&C.gsite, sizeof(double4) * std::max(off, 1));
+    if (e == cudaSuccess) allocations.push_back(C.gsite);
+    if (e == cudaSuccess) e = cudaMalloc(&C.gtype, sizeof(int) * std::max(off, 1));
+    if (e == cudaSuccess) allocations.push_back(C.gtype);
+    if (e != cudaSuccess) {
+      err = std::string("batch allocation failed: ") + cudaGetErrorString(e);
+      return -100 - (int)e;
+    }
+  }
+  cudaError_t e = cudaMalloc(&d_sys, sizeof(SysConst) * h_sys.size());
+  if (e == cudaSuccess) allocations.push_back(d_sys);
+  if (e == cudaSuccess) e = cudaMemcpy(d_sys, h_sys.data(), sizeof(SysConst) * h_sys.size(), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMalloc(&d_chains, sizeof(ChainDev) * nchains);
+  if (e == cudaSuccess) allocations.push_back(d_chains);
+  if (e == cudaSuccess) e = cudaMemcpy(d_chains, h_chains, sizeof(ChainDev) * nchains, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) {
+    err = std::string("batch upload failed: ") + cudaGetErrorString(e);
+    return -100 - (int)e;
+  }
+  return 0;
+}
+
+int Batch::run(int moves, MoveRecord* trace_host, float* ms, std::string& err) {
+  cudaSetDevice(device);
+  BatchLaunch L;
+  L.chains = d_chains;
+  L.systems = d_sys;
+  L.nchains = nchains;
+  L.moves = moves;
+  L.kmax_smem = kmax_all;
+  L.trace = nullptr;
+  cudaError_t e = cudaSuccess;
+  if (trace_host) {
+    size_t need = (size_t)nchains * moves;
+    if (need > trace_cap) {
+      if (d_trace) cudaFree(d_trace);
+      d_trace = nullptr;
+      e = cudaMalloc(&d_trace, sizeof(MoveRecord) * need);
+      trace_cap = e == cudaSuccess ? need : 0;
+    }
+    L.trace = d_trace;
+  }
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  const size_t cb = sizeof(ChainDev) * nchains;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_chains, h_chains, cb, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaEventRecord(a, st);
+  if (e == cudaSuccess) e = launch_batch(L, smem, tab_stride, st);
+  if (e == cudaSuccess) e = cudaEventRecord(b, st);
+  if (e == cudaSuccess && trace_host)
+    e = cudaMemcpyAsync(trace_host, d_trace, sizeof(MoveRecord) * (size_t)nchains * moves, cudaMemcpyDeviceToHost,
+                        st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h_chains, d_chains, cb, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  float t = 0.f;
+  if (e == cudaSuccess) cudaEventElapsedTime(&t, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (e != cudaSuccess) {
+    err = std::string("batched launch failed: ") + cudaGetErrorString(e);
+    return -100 - (int)e;
+  }
+  if (ms) *ms = t;
+  return 0;
+}
+
+}  // namespace fmc
+
+// ============================================================== C ABI of the batched path
+#include "../../include/fastmc_b200.h"
+
+namespace fmc {
+void set_last_error(const std::string& msg);
+}
+
+struct fmc_batch {
+  fmc::Batch impl;
+};
+
+extern "C" {
+
+int fmc_batch_open(int nchains, const char* const* dirs, const int* seeds, int device, fmc_batch** out) {
+  if (!dirs || !seeds || !out || nchains < 1) {
+    fmc::set_last_error("null argument or empty batch");
+    return -1;
+  }
+  fmc_batch* b = new fmc_batch();
+  std::vector<std::string> d(dirs, dirs + nchains);
+  std::vector<int> s(seeds, seeds + 4 * nchains);
+  std::string err;
+  int rc = b->impl.open(d, s, device, err);
+  if (rc) {
+    delete b;
+    *out = nullptr;
+    fmc::set_last_error(err);
+    return rc;
+  }
+  *out = b;
+  return 0;
+}
+
+void fmc_batch_close(fmc_batch* b) { delete b; }
+
+int fmc_batch_run(fmc_batch* b, int moves, fmc_move_record* trace, float* device_ms) {
+  if (!b || moves < 0) {
+    fmc::set_last_error("bad batch handle or move count");
+    return -1;
+  }
+  std::string err;
+  int rc = b->impl.run(moves, reinterpret_cast<fmc::MoveRecord*>(trace), device_ms, err);
+  if (rc) {
+    fmc::set_last_error(err);
+    return rc;
+  }
+  for (int i = 0; i < b->impl.nchains; i++) {
+    const fmc::ChainDev& c = b->impl.h_chains[i];
+    if (c.status) {
+      fmc::set_last_error(c.status == 75 ? "too many atoms in specified system" : "unsupported move drawn");
+      return c.status;
+    }
+  }
+  return 0;
+}
+
+int fmc_batch_chain_state(fmc_batch* b, int chain, double* out) {
+  if (!b || chain < 0 || chain >= b->impl.nchains || !out) {
+    fmc::set_last_error("bad batch handle or chain index");
+    return -1;
+  }
+  const fmc::ChainDev& C = b->impl.h_chains[chain];
+  double v[32] = {0};
+  v[0] = C.status;
+  v[1] = (double)C.moves_done;
+  v[2] = C.gcmccount;
+  for (int g = 0; g < fmc::kMaxGuestTypes; g++) {
+    v[3 + g] = C.nmol[g];
+    v[7 + g] = C.energy[g];
+  }
+  v[11] = C.elrc;
+  v[12] = C.accept_ins;
+  v[13] = C.accept_del;
+  v[14] = C.ins_count;
+  v[15] = C.del_count;
+  v[16] = (double)C.prodcount;
+  for (int k = 0; k < 5; k++) v[17 + k] = C.stats[0][k];
+  v[22] = C.sys;
+  v[23] = b->impl.h_sys[C.sys].S.K;
+  v[24] = b->impl.h_sys[C.sys].S.nf;
+  v[25] = C.temp;
+  v[26] = C.press[0];
+  std::memcpy(out, v, sizeof(v));
+  return 0;
+}
+
+int fmc_batch_guest_coords(fmc_batch* b, int chain, int iguest, double* xyz, int* nmol, int* nsite) {
+  if (!b || chain < 0 || chain >= b->impl.nchains) {
+    fmc::set_last_error("bad batch handle or chain index");
+    return -1;
+  }
+  const fmc::ChainDev& C = b->impl.h_chains[chain];
+  const fmc::SysConst& Y = b->impl.h_sys[C.sys];
+  if (iguest < 0 || iguest >= Y.nspecies) {
+    fmc::set_last_error("species index out of range");
+    return -1;
+  }
+  int ns = Y.sp[iguest].nsite, n = C.nmol[iguest];
+  if (nmol) *nmol = n;
+  if (nsite) *nsite = ns;
+  if (xyz && n) {
+    std::vector<double4> a(n * ns);
+    cudaSetDevice(b->impl.device);
+    cudaError_t e = cudaMemcpy(a.data(), C.gsite + C.seg_off[iguest], sizeof(double4) * n * ns, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) {
+      fmc::set_last_error(cudaGetErrorString(e));
+      return -100 - (int)e;
+    }
+    for (int i = 0; i < n * ns; i++) {
+      xyz[3 * i] = a[i].x;
+      xyz[3 * i + 1] = a[i].y;
+      xyz[3 * i + 2] = a[i].z;
+    }
+  }
+  return 0;
+}
+
+}  // extern "C"

@@ -12,7 +12,7 @@ import numpy as np
 from . import _lib
 from ._lib import DELETE, DISPLACE, INSERT, MOVE_DTYPE, ROTATE, TRANSLATE, FastMCError, check, dp, ip, lib
 
-__all__ = ["Chain", "deck_inspect", "FastMCError", "INSERT", "DELETE", "DISPLACE", "TRANSLATE", "ROTATE",
+__all__ = ["Chain", "Batch", "deck_inspect", "FastMCError", "INSERT", "DELETE", "DISPLACE", "TRANSLATE", "ROTATE",
            "MOVE_DTYPE"]
 
 _INFO_INTS = ["imcon", "kmax1", "kmax2", "kmax3", "K", "natoms", "nspecies", "ntypes", "mxgrid", "nframework",
@@ -147,3 +147,53 @@ class Chain:
         out = np.zeros(6)
         check(lib().fmc_stats(self.h, int(iguest), dp(out)))
         return dict(zip(["N", "E", "EN", "N2", "E2", "prodcount"], out.tolist()))
+
+
+class Batch:
+    """Many independent chains advanced by one persistent kernel (the batched path)."""
+
+    def __init__(self, directories, seeds=None, device=0):
+        dirs = [str(d).encode() for d in directories]
+        n = len(dirs)
+        if seeds is None:
+            seeds = [(12, 34, 56, (78 + i) % 169) for i in range(n)]
+        s = np.ascontiguousarray(np.asarray(seeds, dtype=np.int32).reshape(n, 4))
+        arr = (ctypes.c_char_p * n)(*dirs)
+        self.n = n
+        self.h = ctypes.c_void_p()
+        check(lib().fmc_batch_open(n, arr, ip(s), int(device), ctypes.byref(self.h)))
+
+    def close(self):
+        if self.h:
+            lib().fmc_batch_close(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self, moves, trace=False):
+        """Advance every chain by `moves`; returns (trace[n, moves] or None, device ms)."""
+        rec = np.zeros((self.n, moves), dtype=MOVE_DTYPE) if trace else None
+        ms = ctypes.c_float(0)
+        check(lib().fmc_batch_run(self.h, int(moves), rec.ctypes.data if trace else None, ctypes.byref(ms)))
+        return rec, float(ms.value)
+
+    _STATE = ["status", "moves", "gcmccount", "nmol0", "nmol1", "nmol2", "nmol3", "energy0", "energy1", "energy2",
+              "energy3", "elrc", "accept_ins", "accept_del", "ins_count", "del_count", "prodcount", "N", "E", "EN",
+              "N2", "E2", "system", "K", "nframework", "temp", "press0"]
+
+    def state(self, chain):
+        out = np.zeros(32)
+        check(lib().fmc_batch_chain_state(self.h, int(chain), dp(out)))
+        return dict(zip(self._STATE, out.tolist()))
+
+    def guest_coords(self, chain, iguest=0):
+        n, ns = ctypes.c_int(0), ctypes.c_int(0)
+        check(lib().fmc_batch_guest_coords(self.h, int(chain), int(iguest), None, ctypes.byref(n), ctypes.byref(ns)))
+        buf = np.zeros((max(n.value, 1), ns.value, 3))
+        check(lib().fmc_batch_guest_coords(self.h, int(chain), int(iguest), dp(buf), ctypes.byref(n),
+                                           ctypes.byref(ns)))
+        return buf[: n.value]

@@ -101,6 +101,24 @@ int fmc_guest_coords(fmc_chain* c, int iguest, double* xyz, int* nmol, int* nsit
  * out[0..5] = <N>, <E>, <EN>, <N^2>, <E^2>, production moves counted. */
 int fmc_stats(fmc_chain* c, int iguest, double* out);
 
+/* ---------------------------------------------------------------- batched path
+ * Many independent chains (isotherm points) advanced by one persistent kernel, one CTA per
+ * chain, the whole move loop of gcmc.f:589-1380 on the device (no counterpart in the
+ * reference, which runs one chain per MPI rank, gcmc.f:334-417).  Chains are opened from
+ * their own CONTROL/FIELD/CONFIG directories, must start from an empty framework, and chains
+ * whose FIELD, CONFIG, cut-offs and Ewald parameters coincide share one device system. */
+typedef struct fmc_batch fmc_batch;
+int fmc_batch_open(int nchains, const char* const* dirs, const int* seeds, int device, fmc_batch** out);
+void fmc_batch_close(fmc_batch* b);
+/* Advances every chain by `moves` trial moves in one launch; trace (nullable) receives
+ * nchains*moves records, chain-major; *device_ms is the launch's CUDA-event time. */
+int fmc_batch_run(fmc_batch* b, int moves, fmc_move_record* trace, float* device_ms);
+/* out[0..31]: status, moves done, gcmccount, nmol[4], energy[4] (kcal/mol), elrc, accepted
+ * insertions, accepted deletions, insert attempts, delete attempts, production moves,
+ * species-0 <N>,<E>,<EN>,<N^2>,<E^2>, system index, K, framework atoms, T, P(species 0). */
+int fmc_batch_chain_state(fmc_batch* b, int chain, double* out);
+int fmc_batch_guest_coords(fmc_batch* b, int chain, int iguest, double* xyz, int* nmol, int* nsite);
+
 /* Launch accounting and timing of the plain path.  enable != 0 turns on CUDA-event timing of
  * every trial-pass kernel on the chain's stream (enable < 0 also clears the counters).
  * out[0..5]: trial-pass launches, commit launches, timed pass launches, total timed pass
