@@ -18,10 +18,15 @@ namespace {
 
 struct MoveSmem {
   int mtype, g, mol, nold, nnew, accepted, ex_lo, ex_hi;
-  int commit_lo, seg_end, ns, randchoice;
+  int commit_lo, seg_end, ns, randchoice, need_lrc;
   double delrc, rande;
   double x[2 * kBatchMaxSites], y[2 * kBatchMaxSites], z[2 * kBatchMaxSites], q[2 * kBatchMaxSites];
   int type[2 * kBatchMaxSites];
+  // real-space work list: per trial site its voxel-list start/length and the prefix of
+  // candidates (voxel entries + every guest site) over the sites
+  int vb[2 * kBatchMaxSites], vl[2 * kBatchMaxSites], pre[2 * kBatchMaxSites + 1];
+  int gpre[kMaxGuestTypes + 1];
+  double lrc_term[kBatchMaxTab];
 };
 
 __device__ double lrc_device(const SysConst& Y, const int* numtyp) {
@@ -41,7 +46,8 @@ __device__ double lrc_device(const SysConst& Y, const int* numtyp) {
 
 // Thread 0: bookkeeping of gcmc.f:594-736 (production / termination every 400 moves),
 // random choices and the trial sites.
-__device__ __noinline__ void move_begin(ChainDev& C, const SysConst& Y, MoveSmem& M) {
+__device__ __noinline__ void move_begin(ChainDev& C, const SysConst& Y, const DevSystem& S, MoveSmem& M) {
+  C.prof[7] -= clock64();
   C.gcmccount++;
   if (C.gcmccount % 400 == 0) {
     int totalguests = 0;
@@ -104,6 +110,7 @@ __device__ __noinline__ void move_begin(ChainDev& C, const SysConst& Y, MoveSmem
     else if (C.rota_rotangle > kMinAngle) C.rota_rotangle = C.rota_rotangle * 0.95;
   }
   if (nmols == 0) mtype = kInsert;
+  C.prof[7] += clock64();  // minus the stamp taken at entry: selection + adaptation
   M.mtype = mtype;
   M.g = g;
   M.ns = ns;
@@ -113,6 +120,7 @@ __device__ __noinline__ void move_begin(ChainDev& C, const SysConst& Y, MoveSmem
   M.nold = M.nnew = 0;
   M.delrc = 0.0;
   M.rande = -1.0;
+  M.need_lrc = 0;
   if (mtype < 0) {
     C.status = 3;
     return;
@@ -120,6 +128,7 @@ __device__ __noinline__ void move_begin(ChainDev& C, const SysConst& Y, MoveSmem
   double* x = M.x;
   double* y = M.y;
   double* z = M.z;
+  C.prof[8] -= clock64();  // trial generation and site loads
   if (mtype == kInsert) {
     C.ins_count++;
     if ((C.totatm - C.framatm) + ns >= C.maxguest || (nmols + 1) * ns > C.seg_cap[g]) {
@@ -128,10 +137,10 @@ __device__ __noinline__ void move_begin(ChainDev& C, const SysConst& Y, MoveSmem
     }
     double r[7];
     for (int i = 0; i < 7; i++) r[i] = duni_next(C.rng);
-    trial_insert(Y.S.cell, P.tx, P.ty, P.tz, ns, r, x, y, z);
+    trial_insert(S.cell, P.tx, P.ty, P.tz, ns, r, x, y, z);
     M.nnew = ns;
     for (int i = 0; i < ns; i++) C.numtyp[P.type[i]]++;
-    M.delrc = lrc_device(Y, C.numtyp) - C.elrc;
+    M.need_lrc = 1;
   } else if (mtype == kDelete) {
     C.del_count++;
     int randchoice = (int)floor(duni_next(C.rng) * nmols) + 1;
@@ -147,7 +156,7 @@ __device__ __noinline__ void move_begin(ChainDev& C, const SysConst& Y, MoveSmem
     }
     M.nold = ns;
     for (int i = 0; i < ns; i++) C.numtyp[P.type[i]]--;
-    M.delrc = lrc_device(Y, C.numtyp) - C.elrc;
+    M.need_lrc = 1;
   } else {
     double r[7], dis_delr, dis_rot;
     if (mtype == kTranslate) {
@@ -184,7 +193,7 @@ __device__ __noinline__ void move_begin(ChainDev& C, const SysConst& Y, MoveSmem
       y[ns + i] = a.y;
       z[ns + i] = a.z;
     }
-    trial_displace(Y.S.cell, P.mass, ns, dis_delr, dis_rot, r, x + ns, y + ns, z + ns);
+    trial_displace(S.cell, P.mass, ns, dis_delr, dis_rot, r, x + ns, y + ns, z + ns);
     M.nold = ns;
     M.nnew = ns;
   }
@@ -193,6 +202,7 @@ __device__ __noinline__ void move_begin(ChainDev& C, const SysConst& Y, MoveSmem
     M.q[i] = P.q[s];
     M.type[i] = P.type[s];
   }
+  C.prof[8] += clock64();
 }
 
 // Thread 0: energy assembly, energy_eval, counters, statistics (gcmc.f:941-1380, 1814-1860).
@@ -290,13 +300,70 @@ __device__ __noinline__ void move_end(ChainDev& C, const SysConst& Y, MoveSmem& 
   }
 }
 
+// Tail correction (gstlrcorrect, vdw_terms.f:684-745) by one warp: lane-parallel pair terms,
+// summed by lane 0 in the reference's pair order.
+__device__ __forceinline__ void lrc_warp(const ChainDev& C, const SysConst& Y, MoveSmem& M, int lane) {
+  const int nt = Y.ntypes, ntab = nt * (nt + 1) / 2;
+  const double twopi = 2.0 * kPi, v = Y.volm;
+  for (int p = lane; p < ntab; p += 32) {
+    int i = 1;
+    while (i * (i + 1) / 2 <= p) i++;
+    int j = p - (i - 1) * i / 2 + 1;
+    double den =
+        twopi * ((double)C.numtyp[i] * (double)C.numtyp[j] - (double)Y.numfrz[i] * (double)Y.numfrz[j]) / (v * v);
+    M.lrc_term[p] = v * den * Y.steadd[p + 1];
+  }
+  __syncwarp();
+  if (lane == 0) {
+    double e = 0.0;
+    if (Y.lrc_on)
+      for (int p = 0; p < ntab; p++) e = e + M.lrc_term[p];
+    M.delrc = e - C.elrc;
+  }
+}
+
+// One real-space candidate: a framework atom from a site's voxel list or a guest site.
+struct Cand {
+  double4 a;
+  int type, site;
+  bool live;
+};
+
+__device__ __forceinline__ Cand fetch_candidate(const DevSystem& S, const ChainDev& C, const MoveSmem& M, int nseg,
+                                                int t, int& s) {
+  Cand c;
+  c.live = false;
+  c.site = s;
+  if (t >= M.pre[M.nold + M.nnew]) return c;
+  while (t >= M.pre[s + 1]) s++;
+  c.site = s;
+  int j = t - M.pre[s];
+  if (j < M.vl[s]) {
+    c.a = S.vox_xyzq[M.vb[s] + j];
+    c.type = S.vox_type[M.vb[s] + j];
+    c.live = true;
+  } else {
+    int jg = j - M.vl[s], g = 0;
+    while (g + 1 < nseg && jg >= M.gpre[g + 1]) g++;
+    int site_idx = C.seg_off[g] + (jg - M.gpre[g]);
+    if (site_idx < M.ex_lo || site_idx >= M.ex_hi) {
+      c.a = C.gsite[site_idx];
+      c.type = C.gtype[site_idx];
+      c.live = true;
+    }
+  }
+  return c;
+}
+
 __global__ void __launch_bounds__(kBatchThreads, 2) fmc_batch_kernel(BatchLaunch L, int tab_stride) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ ChainDev C;
   __shared__ MoveSmem M;
-  __shared__ DevSystem S;
+  __shared__ SysConst Ysm;
   __shared__ double red[32 * 3];
-  const int tid = threadIdx.x, cidx = blockIdx.x;
+  __shared__ int prow_s[(kBatchMaxTypes + 1) * (kBatchMaxTypes + 1)];
+  DevSystem& S = Ysm.S;
+  const int tid = threadIdx.x, cidx = blockIdx.x, warp = tid >> 5, lane = tid & 31;
   if (cidx >= L.nchains) return;
   {
     const int* src = reinterpret_cast<const int*>(&L.chains[cidx]);
@@ -304,10 +371,16 @@ __global__ void __launch_bounds__(kBatchThreads, 2) fmc_batch_kernel(BatchLaunch
     for (int i = tid; i < (int)(sizeof(ChainDev) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
   }
   __syncthreads();
-  const SysConst& Y = L.systems[C.sys];
-  if (tid == 0) S = Y.S;
+  {
+    const int* src = reinterpret_cast<const int*>(&L.systems[C.sys]);
+    int* dst = reinterpret_cast<int*>(&Ysm);
+    for (int i = tid; i < (int)(sizeof(SysConst) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
+  }
   __syncthreads();
-  const int K = S.K, Kmax = L.kmax_smem;
+  const SysConst& Y = Ysm;
+  const int K = S.K, Kmax = L.kmax_smem, nseg = Y.nspecies;
+  const int nt1 = S.ntypes + 1;
+  for (int i = tid; i < nt1 * nt1; i += blockDim.x) prow_s[i] = S.pair_row[i];
   double2* Sk = reinterpret_cast<double2*>(smem_raw);
   double2* Sn = Sk + Kmax;
   double* ak = reinterpret_cast<double*>(Sn + Kmax);
@@ -322,31 +395,68 @@ __global__ void __launch_bounds__(kBatchThreads, 2) fmc_batch_kernel(BatchLaunch
   const int stride = k1 + k2 + k3 + 3;
   (void)tab_stride;
   __syncthreads();
+  long long t0 = 0, t1 = 0;
+  const bool prof = L.profile != 0;
   for (int mv = 0; mv < L.moves; mv++) {
-    if (tid == 0) move_begin(C, Y, M);
+    if (prof && tid == 0) t0 = clock64();
+    if (tid == 0) move_begin(C, Y, S, M);
     __syncthreads();
+    if (prof && tid == 0) {
+      t1 = clock64();
+      C.prof[0] += t1 - t0;
+      t0 = t1;
+    }
     if (C.status) break;
     const int nsite = M.nold + M.nnew;
-    for (int w = tid; w < nsite * 3; w += blockDim.x) {
-      int s = w / 3, ax = w % 3;
-      double f[3];
-      frac_coords(S.cell, M.x[s], M.y[s], M.z[s], f);
-      axis_phases(f[ax], S.kmax[ax], tab + s * stride + (ax == 0 ? 0 : (ax == 1 ? k1 + 1 : k1 + k2 + 2)));
+    if (warp == 0) {
+      // phase tables of the trial sites (ewald.f:95-137)
+      for (int w = lane; w < nsite * 3; w += 32) {
+        int st = w / 3, ax = w % 3;
+        double f[3];
+        frac_coords(S.cell, M.x[st], M.y[st], M.z[st], f);
+        axis_phases(f[ax], S.kmax[ax], tab + st * stride + (ax == 0 ? 0 : (ax == 1 ? k1 + 1 : k1 + k2 + 2)));
+      }
+    } else if (warp == 1) {
+      if (M.need_lrc) lrc_warp(C, Y, M, lane);
+    } else if (warp == 2) {
+      // real-space work list: voxel list of every trial site, then every guest site
+      if (lane < nsite) {
+        int v = voxel_of(S, M.x[lane], M.y[lane], M.z[lane]);
+        M.vb[lane] = S.vox_off[v];
+        M.vl[lane] = S.vox_off[v + 1] - S.vox_off[v];
+      }
+      __syncwarp();
+      if (lane == 0) {
+        int gt = 0;
+        M.gpre[0] = 0;
+        for (int g = 0; g < nseg; g++) {
+          gt += C.nmol[g] * Y.sp[g].nsite;
+          M.gpre[g + 1] = gt;
+        }
+        M.pre[0] = 0;
+        for (int st = 0; st < nsite; st++) M.pre[st + 1] = M.pre[st] + M.vl[st] + gt;
+      }
     }
     __syncthreads();
+    if (prof && tid == 0) {
+      t1 = clock64();
+      C.prof[1] += t1 - t0;
+      t0 = t1;
+    }
     double v[3] = {0.0, 0.0, 0.0};
     const int mtype = M.mtype, nold = M.nold;
+    // ---- reciprocal space: this thread's k-vectors
     for (int k = tid; k < K; k += blockDim.x) {
       int l, m, n;
       kunpack(kp[k], l, m, n);
       int am = m < 0 ? -m : m, an = n < 0 ? -n : n;
       double2 aold = make_double2(0.0, 0.0), anew = make_double2(0.0, 0.0);
-      for (int s = 0; s < nsite; s++) {
-        const double2* t = tab + s * stride;
+      for (int st = 0; st < nsite; st++) {
+        const double2* t = tab + st * stride;
         double2 c = m >= 0 ? cmul(t[l], t[k1 + 1 + am]) : cmulc(t[l], t[k1 + 1 + am]);
         c = n >= 0 ? cmul(c, t[k1 + k2 + 2 + an]) : cmulc(c, t[k1 + k2 + 2 + an]);
-        double q = M.q[s];
-        if (s < nold) {
+        double q = M.q[st];
+        if (st < nold) {
           aold.x += q * c.x;
           aold.y += q * c.y;
         } else {
@@ -364,30 +474,49 @@ __global__ void __launch_bounds__(kBatchThreads, 2) fmc_batch_kernel(BatchLaunch
       Sn[k] = sn;
       v[0] += ak[k] * (sn.x * sn.x + sn.y * sn.y - so.x * so.x - so.y * so.y);
     }
-    GuestView G;
-    G.site = C.gsite;
-    G.type = C.gtype;
-    G.nseg = Y.nspecies;
-    for (int g = 0; g < kMaxGuestTypes; g++) {
-      G.seg_off[g] = C.seg_off[g];
-      G.seg_len[g] = g < Y.nspecies ? C.nmol[g] * Y.sp[g].nsite : 0;
-    }
-    const bool sub_old = (mtype != kInsert && mtype != kDelete);
-    for (int s = 0; s < nsite; s++) {
-      double ecf = 0.0, evf = 0.0, ecg = 0.0, evg = 0.0;
-      site_partial(S, G, M.x[s], M.y[s], M.z[s], M.q[s], M.type[s], M.ex_lo, M.ex_hi, tid, blockDim.x, ecf, evf,
-                   ecg, evg);
-      if (sub_old && s < nold) {
-        v[1] -= ecf + ecg;
-        v[2] -= evf + evg;
-      } else {
-        v[1] += ecf + ecg;
-        v[2] += evf + evg;
+    if (prof && tid == 0) C.prof[5] += clock64() - t0;
+    // ---- real space: every (site, candidate) pair, four candidates in flight per thread
+    {
+      const bool sub_old = (mtype != kInsert && mtype != kDelete);
+      const int T = M.pre[nsite];
+      int s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+      for (int base = tid; base < T; base += 4 * kBatchThreads) {
+        Cand c[4];
+        c[0] = fetch_candidate(S, C, M, nseg, base, s0);
+        c[1] = fetch_candidate(S, C, M, nseg, base + kBatchThreads, s1);
+        c[2] = fetch_candidate(S, C, M, nseg, base + 2 * kBatchThreads, s2);
+        c[3] = fetch_candidate(S, C, M, nseg, base + 3 * kBatchThreads, s3);
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+          if (!c[u].live) continue;
+          const int st = c[u].site;
+          double ec = 0.0, ev = 0.0;
+          pair_energy(S, M.x[st] - c[u].a.x, M.y[st] - c[u].a.y, M.z[st] - c[u].a.z, M.q[st] * kR4pie0, c[u].a.w,
+                      prow_s[M.type[st] * nt1 + c[u].type], ec, ev);
+          if (sub_old && st < nold) {
+            v[1] -= ec;
+            v[2] -= ev;
+          } else {
+            v[1] += ec;
+            v[2] += ev;
+          }
+        }
       }
     }
+    if (prof && tid == 0) C.prof[6] += clock64() - t0;
     block_sum<3>(v, red);
+    if (prof && tid == 0) {
+      t1 = clock64();
+      C.prof[2] += t1 - t0;
+      t0 = t1;
+    }
     if (tid == 0) move_end(C, Y, M, v, L.trace ? L.trace + (size_t)cidx * L.moves + mv : nullptr);
     __syncthreads();
+    if (prof && tid == 0) {
+      t1 = clock64();
+      C.prof[3] += t1 - t0;
+      t0 = t1;
+    }
     if (M.accepted) {
       for (int k = tid; k < K; k += blockDim.x) Sk[k] = Sn[k];
       const int ns = M.ns;
@@ -410,12 +539,13 @@ __global__ void __launch_bounds__(kBatchThreads, 2) fmc_batch_kernel(BatchLaunch
           __syncthreads();
         }
       } else if (tid < ns) {
-        int s = (mtype == kInsert) ? tid : ns + tid;
-        C.gsite[M.commit_lo + tid] = make_double4(M.x[s], M.y[s], M.z[s], M.q[s]);
-        C.gtype[M.commit_lo + tid] = M.type[s];
+        int st = (mtype == kInsert) ? tid : ns + tid;
+        C.gsite[M.commit_lo + tid] = make_double4(M.x[st], M.y[st], M.z[st], M.q[st]);
+        C.gtype[M.commit_lo + tid] = M.type[st];
       }
     }
     __syncthreads();
+    if (prof && tid == 0) C.prof[4] += clock64() - t0;
   }
   for (int k = tid; k < K; k += blockDim.x) C.sk[k] = Sk[k];
   __syncthreads();

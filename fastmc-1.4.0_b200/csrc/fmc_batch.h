@@ -57,6 +57,9 @@ struct ChainDev {
   long long prodcount;
   double stats[kMaxGuestTypes][5];  // rolling <N>, <E>, <EN>, <N^2>, <E^2>
   long long moves_done;
+  // SM clock cycles spent per phase when the launch is profiled: begin (thread 0), phase
+  // tables, k-space + real space + reduction, end (thread 0), commit
+  long long prof[12];
   // buffers
   double2* sk;
   double4* gsite;
@@ -70,6 +73,7 @@ struct BatchLaunch {
   int nchains, moves;
   MoveRecord* trace;  // [nchains][moves] or null
   int kmax_smem;      // largest K in the batch rounded up to a multiple of 4 (smem sizing)
+  int profile;        // accumulate per-phase clock counters into ChainDev::prof
 };
 
 cudaError_t launch_batch(const BatchLaunch& L, int smem_bytes, int tab_stride, cudaStream_t st);
@@ -96,6 +100,7 @@ class Batch {
   // One step: control blocks host->device, `moves` moves of every chain, control blocks (and
   // the optional per-move trace) device->host.  *ms: CUDA-event time of the kernel alone.
   int run(int moves, MoveRecord* trace_host, float* ms, std::string& err);
+  int profile = 0;
 };
 
 }  // namespace fmc

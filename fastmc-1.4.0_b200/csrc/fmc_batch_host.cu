@@ -223,6 +223,7 @@ int Batch::run(int moves, MoveRecord* trace_host, float* ms, std::string& err) {
   L.nchains = nchains;
   L.moves = moves;
   L.kmax_smem = kmax_all;
+  L.profile = profile;
   L.trace = nullptr;
   cudaError_t e = cudaSuccess;
   if (trace_host) {
@@ -297,6 +298,15 @@ int fmc_batch_open(int nchains, const char* const* dirs, const int* seeds, int d
 
 void fmc_batch_close(fmc_batch* b) { delete b; }
 
+int fmc_batch_profile(fmc_batch* b, int enable) {
+  if (!b) {
+    fmc::set_last_error("bad batch handle");
+    return -1;
+  }
+  b->impl.profile = enable;
+  return 0;
+}
+
 int fmc_batch_run(fmc_batch* b, int moves, fmc_move_record* trace, float* device_ms) {
   if (!b || moves < 0) {
     fmc::set_last_error("bad batch handle or move count");
@@ -324,7 +334,7 @@ int fmc_batch_chain_state(fmc_batch* b, int chain, double* out) {
     return -1;
   }
   const fmc::ChainDev& C = b->impl.h_chains[chain];
-  double v[32] = {0};
+  double v[40] = {0};
   v[0] = C.status;
   v[1] = (double)C.moves_done;
   v[2] = C.gcmccount;
@@ -344,6 +354,8 @@ int fmc_batch_chain_state(fmc_batch* b, int chain, double* out) {
   v[24] = b->impl.h_sys[C.sys].S.nf;
   v[25] = C.temp;
   v[26] = C.press[0];
+  for (int k = 0; k < 5; k++) v[27 + k] = (double)C.prof[k];
+  for (int k = 5; k < 9; k++) v[k + 27] = (double)C.prof[k];
   std::memcpy(out, v, sizeof(v));
   return 0;
 }

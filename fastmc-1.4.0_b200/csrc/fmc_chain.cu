@@ -54,6 +54,22 @@ int upload_system(const HostSystem& h, DeviceSystem& d, std::string& err) {
   for (int a = 0; a < 3; a++) v.nvox[a] = h.nvox[a];
   if ((e = upload(d.allocations, &v.vox_off, h.vox_off)) != cudaSuccess) goto fail;
   if ((e = upload(d.allocations, &v.vox_atoms, h.vox_atoms)) != cudaSuccess) goto fail;
+  v.vox_atoms16 = nullptr;
+  if (h.nf <= 65535) {
+    std::vector<unsigned short> v16(h.vox_atoms.begin(), h.vox_atoms.end());
+    if ((e = upload(d.allocations, &v.vox_atoms16, v16)) != cudaSuccess) goto fail;
+  }
+  {
+    std::vector<double4> vx(h.vox_atoms.size());
+    std::vector<unsigned char> vt(h.vox_atoms.size());
+    for (size_t i = 0; i < h.vox_atoms.size(); i++) {
+      int j = h.vox_atoms[i];
+      vx[i] = make_double4(h.fx[j], h.fy[j], h.fz[j], h.fq[j]);
+      vt[i] = (unsigned char)h.ftype[j];
+    }
+    if ((e = upload(d.allocations, &v.vox_xyzq, vx)) != cudaSuccess) goto fail;
+    if ((e = upload(d.allocations, &v.vox_type, vt)) != cudaSuccess) goto fail;
+  }
   v.rcut2 = h.rcut * h.rcut;
   v.rdr_e = 1.0 / h.drewd;
   v.rdr_v = 1.0 / h.dlrpot;

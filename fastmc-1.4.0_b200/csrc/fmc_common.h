@@ -75,9 +75,16 @@ FMC_HD double duni_next(Duni& d) {
 struct CellGeom {
   double h[9];    // cell vectors a,b,c (cell(1..9) of the reference, a = h[0..2])
   double rh[9];   // inverse (invert, utility_pack.f:1417)
+  double inv[3];  // 1/h[0], 1/h[4], 1/h[8]: the reciprocals images() forms once per call
   double volm;    // volume used by Ewald and acceptance
   int imcon;
 };
+
+inline void cell_reciprocals(CellGeom& c) {
+  c.inv[0] = 1.0 / c.h[0];
+  c.inv[1] = 1.0 / c.h[4];
+  c.inv[2] = 1.0 / c.h[8];
+}
 
 // Fortran nint: nearest integer, halves away from zero.
 FMC_HD double fnint(double x) { return round(x); }
@@ -85,14 +92,14 @@ FMC_HD double fnint(double x) { return round(x); }
 // Minimum image of one separation vector for imcon 1, 2, 3 (images, utility_pack.f:1138-1202).
 FMC_HD void min_image(const CellGeom& c, double& x, double& y, double& z) {
   if (c.imcon == 1) {
-    const double a = c.h[0], ra = 1.0 / a;
+    const double a = c.h[0], ra = c.inv[0];
     x = x - a * fnint(ra * x);
     y = y - a * fnint(ra * y);
     z = z - a * fnint(ra * z);
   } else if (c.imcon == 2) {
-    x = x - c.h[0] * fnint((1.0 / c.h[0]) * x);
-    y = y - c.h[4] * fnint((1.0 / c.h[4]) * y);
-    z = z - c.h[8] * fnint((1.0 / c.h[8]) * z);
+    x = x - c.h[0] * fnint(c.inv[0] * x);
+    y = y - c.h[4] * fnint(c.inv[1] * y);
+    z = z - c.h[8] * fnint(c.inv[2] * z);
   } else if (c.imcon == 3) {
     const double* r = c.rh;
     double sx = r[0] * x + r[3] * y + r[6] * z;
@@ -129,9 +136,10 @@ FMC_HD void rotate_sites(double* x, double* y, double* z, int n, const double q[
 // Quaternion of angle theta about the axis (2r2-1, 2r3-1, 2r4-1)/norm (random_ins, random_rot).
 FMC_HD void axis_angle_quat(double theta, double r2, double r3, double r4, double q[4]) {
   double b1 = 2.0 * r2 - 1.0, b2 = 2.0 * r3 - 1.0, b3 = 2.0 * r4 - 1.0;
-  double st = sin(theta / 2.0);
+  double st, ct;
+  sincos(theta / 2.0, &st, &ct);
   double norm = sqrt(b1 * b1 + b2 * b2 + b3 * b3);
-  q[0] = cos(theta / 2.0);
+  q[0] = ct;
   q[1] = st * (b1 / norm);
   q[2] = st * (b2 / norm);
   q[3] = st * (b3 / norm);

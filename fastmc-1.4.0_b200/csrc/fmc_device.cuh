@@ -22,6 +22,9 @@ struct DevSystem {
   int nvox[3];
   const int* vox_off;
   const int* vox_atoms;
+  const unsigned short* vox_atoms16;  // the same lists as 16-bit indices (null when nf > 65535)
+  const double4* vox_xyzq;            // the same lists with each entry's atom inlined, and
+  const unsigned char* vox_type;      // its type (coalesced one-hop reads)
   double rcut2, rdr_e, rdr_v;
   const double* erc;
   const double* vvv;
@@ -126,9 +129,8 @@ __device__ __forceinline__ void site_partial(const DevSystem& S, const GuestView
   int v = voxel_of(S, px, py, pz);
   int b = S.vox_off[v], e = S.vox_off[v + 1];
   for (int i = b + tid; i < e; i += nthr) {
-    int j = S.vox_atoms[i];
-    double4 a = S.fw[j];
-    pair_energy(S, px - a.x, py - a.y, pz - a.z, chgea, a.w, prow[S.fw_type[j]], ec_fw, ev_fw);
+    double4 a = S.vox_xyzq[i];
+    pair_energy(S, px - a.x, py - a.y, pz - a.z, chgea, a.w, prow[S.vox_type[i]], ec_fw, ev_fw);
   }
 }
 

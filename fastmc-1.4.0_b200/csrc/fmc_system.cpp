@@ -185,6 +185,7 @@ int build_host_system(const InputDeck& d, HostSystem& s, std::string& err, doubl
   // ---- cell
   for (int i = 0; i < 9; i++) s.cell.h[i] = d.cell[i];
   invert3(d.cell, s.cell.rh);
+  cell_reciprocals(s.cell);
   s.cell.volm = d.volm;
   s.cell.imcon = d.imcon;
   s.rcut = d.rcut;
@@ -210,6 +211,10 @@ int build_host_system(const InputDeck& d, HostSystem& s, std::string& err, doubl
   }
   // ---- vdW tables (forgen) incl. the zero table for undefined pairs
   s.ntypes = (int)d.types.size();
+  if (s.ntypes > 255) {
+    err = "more than 255 unique atom types";
+    return -5;
+  }
   s.ntables = d.ntpvdw + 1;
   s.dlrpot = d.rvdw / (double)(s.mxgrid - 4);
   const int stride = s.mxgrid + 1;

@@ -183,10 +183,14 @@ class Batch:
 
     _STATE = ["status", "moves", "gcmccount", "nmol0", "nmol1", "nmol2", "nmol3", "energy0", "energy1", "energy2",
               "energy3", "elrc", "accept_ins", "accept_del", "ins_count", "del_count", "prodcount", "N", "E", "EN",
-              "N2", "E2", "system", "K", "nframework", "temp", "press0"]
+              "N2", "E2", "system", "K", "nframework", "temp", "press0", "cyc_begin", "cyc_phase", "cyc_sums",
+              "cyc_end", "cyc_commit", "cyc_t0_kspace", "cyc_t0_real", "cyc_select", "cyc_trial"]
+
+    def profile(self, enable=True):
+        check(lib().fmc_batch_profile(self.h, int(bool(enable))))
 
     def state(self, chain):
-        out = np.zeros(32)
+        out = np.zeros(40)
         check(lib().fmc_batch_chain_state(self.h, int(chain), dp(out)))
         return dict(zip(self._STATE, out.tolist()))
 

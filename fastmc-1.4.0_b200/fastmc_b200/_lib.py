@@ -46,6 +46,7 @@ SIGNATURES = {
     "fmc_batch_open": (_ci, [_ci, ctypes.POINTER(ctypes.c_char_p), _ip, _ci, ctypes.POINTER(_vp)]),
     "fmc_batch_close": (None, [_vp]),
     "fmc_batch_run": (_ci, [_vp, _ci, _vp, ctypes.POINTER(ctypes.c_float)]),
+    "fmc_batch_profile": (_ci, [_vp, _ci]),
     "fmc_batch_chain_state": (_ci, [_vp, _ci, _dp]),
     "fmc_batch_guest_coords": (_ci, [_vp, _ci, _ci, _dp, _ip, _ip]),
     "fmc_deck_inspect": (_ci, [ctypes.c_char_p, _ip, _dp, _ip, _dp, _dp, _dp, _ip, _ip]),

@@ -113,9 +113,14 @@ void fmc_batch_close(fmc_batch* b);
 /* Advances every chain by `moves` trial moves in one launch; trace (nullable) receives
  * nchains*moves records, chain-major; *device_ms is the launch's CUDA-event time. */
 int fmc_batch_run(fmc_batch* b, int moves, fmc_move_record* trace, float* device_ms);
-/* out[0..31]: status, moves done, gcmccount, nmol[4], energy[4] (kcal/mol), elrc, accepted
+/* enable != 0: later runs accumulate SM clock cycles per phase of the move (see
+ * fmc_batch_chain_state out[27..31]). */
+int fmc_batch_profile(fmc_batch* b, int enable);
+/* out[0..39]: status, moves done, gcmccount, nmol[4], energy[4] (kcal/mol), elrc, accepted
  * insertions, accepted deletions, insert attempts, delete attempts, production moves,
- * species-0 <N>,<E>,<EN>,<N^2>,<E^2>, system index, K, framework atoms, T, P(species 0). */
+ * species-0 <N>,<E>,<EN>,<N^2>,<E^2>, system index, K, framework atoms, T, P(species 0),
+ * profiled cycles of: trial set-up, phase tables, energy sums, acceptance, commit, then
+ * (thread 0's share) k-space, + real space, move selection, trial generation. */
 int fmc_batch_chain_state(fmc_batch* b, int chain, double* out);
 int fmc_batch_guest_coords(fmc_batch* b, int chain, int iguest, double* xyz, int* nmol, int* nsite);
 
