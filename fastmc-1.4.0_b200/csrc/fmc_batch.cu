@@ -18,8 +18,9 @@ namespace {
 
 struct MoveSmem {
   int mtype, g, mol, nold, nnew, accepted, ex_lo, ex_hi;
-  int commit_lo, seg_end, ns, randchoice, need_lrc;
+  int commit_lo, seg_end, ns, randchoice, need_lrc, rande_drawn, recheck;
   double delrc, rande;
+  double ewld1, ewld2, vdw, ewld3, estep;
   double x[2 * kBatchMaxSites], y[2 * kBatchMaxSites], z[2 * kBatchMaxSites], q[2 * kBatchMaxSites];
   int type[2 * kBatchMaxSites];
   // real-space work list: per trial site its voxel-list start/length and the prefix of
@@ -121,6 +122,8 @@ __device__ __noinline__ void move_begin(ChainDev& C, const SysConst& Y, const De
   M.delrc = 0.0;
   M.rande = -1.0;
   M.need_lrc = 0;
+  M.rande_drawn = 0;
+  M.recheck = 0;
   if (mtype < 0) {
     C.status = 3;
     return;
@@ -205,36 +208,73 @@ __device__ __noinline__ void move_begin(ChainDev& C, const SysConst& Y, const De
   C.prof[8] += clock64();
 }
 
-// Thread 0: energy assembly, energy_eval, counters, statistics (gcmc.f:941-1380, 1814-1860).
-__device__ __noinline__ void move_end(ChainDev& C, const SysConst& Y, MoveSmem& M, const double v[3], MoveRecord* rec) {
+// Thread 0: energy assembly of the move (gcmc.f:946, 1112, 1328).  v = {sum akk*d|S|^2,
+// ewld2, vdw} as reduced by the block.
+__device__ __forceinline__ void assemble(const SysConst& Y, MoveSmem& M, const double* v) {
+  const SpeciesConst& P = Y.sp[M.g];
+  M.ewld1 = Y.S.recip_pref * v[0];
+  M.ewld2 = v[1];
+  M.vdw = v[2];
+  M.ewld3 = 0.0;
+  if (M.mtype == kInsert) {
+    M.ewld1 = M.ewld1 + P.engsic;
+    M.ewld3 = P.ewald3en;
+    M.estep = (M.ewld1 + v[1] + M.ewld3 + v[2] + M.delrc) / Y.engunit;
+  } else if (M.mtype == kDelete) {
+    M.ewld1 = M.ewld1 - P.engsic;
+    M.ewld3 = P.ewald3en;
+    M.estep = (M.ewld1 - v[1] - M.ewld3 - v[2] + M.delrc) / Y.engunit;
+  } else {
+    M.estep = (M.ewld1 + v[1] + v[2]) / Y.engunit;
+  }
+}
+
+// Thread 0: acceptance (energy_eval, utility_pack.f:3049-3095, with the displacement
+// shortcut of gcmc.f:1330-1338).  `band` (kcal/mol) bounds the error of M.estep; when the
+// decision could differ inside that band the move is marked for an FP64 re-evaluation
+// instead (returns 1).  Random numbers are drawn exactly where the reference draws them.
+__device__ __forceinline__ int decide(ChainDev& C, const SysConst& Y, MoveSmem& M, double band) {
+  const int g = M.g, mtype = M.mtype, nmols = C.nmol[g];
+  const double e = M.estep;
+  if (mtype == kInsert || mtype == kDelete) {
+    if (!M.rande_drawn) {
+      M.rande = duni_next(C.rng);
+      M.rande_drawn = 1;
+    }
+    if (band > 0.0) {
+      bool lo = accept_move(e + band, M.rande, Y.statvolm, C.press[g], nmols, C.temp, C.beta, mtype);
+      bool hi = accept_move(e - band, M.rande, Y.statvolm, C.press[g], nmols, C.temp, C.beta, mtype);
+      if (lo != hi) return 1;
+    }
+    M.accepted = accept_move(e, M.rande, Y.statvolm, C.press[g], nmols, C.temp, C.beta, mtype);
+    return 0;
+  }
+  if (band > 0.0 && fabs(e) <= band) return 1;  // the sign decides whether rande is drawn
+  if (e < 0.0) {
+    M.accepted = 1;
+    return 0;
+  }
+  if (!M.rande_drawn) {
+    M.rande = duni_next(C.rng);
+    M.rande_drawn = 1;
+  }
+  if (band > 0.0) {
+    bool lo = accept_move(e + band, M.rande, Y.statvolm, C.press[g], nmols, C.temp, C.beta, kDisplace);
+    bool hi = accept_move(e - band, M.rande, Y.statvolm, C.press[g], nmols, C.temp, C.beta, kDisplace);
+    if (lo != hi) return 1;
+  }
+  M.accepted = accept_move(e, M.rande, Y.statvolm, C.press[g], nmols, C.temp, C.beta, kDisplace);
+  return 0;
+}
+
+// Thread 0: counters, running energy, statistics and the trace record (gcmc.f:954-1380,
+// 1814-1860) once the move is decided.
+__device__ __noinline__ void bookkeep(ChainDev& C, const SysConst& Y, MoveSmem& M, MoveRecord* rec) {
   const int g = M.g, ns = M.ns, mtype = M.mtype;
   const SpeciesConst& P = Y.sp[g];
   const int nmols = C.nmol[g];
-  double ewld1 = Y.S.recip_pref * v[0];
-  double ewld3 = 0.0, estep;
-  bool accepted;
-  if (mtype == kInsert) {
-    ewld1 = ewld1 + P.engsic;
-    ewld3 = P.ewald3en;
-    estep = (ewld1 + v[1] + ewld3 + v[2] + M.delrc) / Y.engunit;
-    M.rande = duni_next(C.rng);
-    accepted = accept_move(estep, M.rande, Y.statvolm, C.press[g], nmols, C.temp, C.beta, kInsert);
-  } else if (mtype == kDelete) {
-    ewld1 = ewld1 - P.engsic;
-    ewld3 = P.ewald3en;
-    estep = (ewld1 - v[1] - ewld3 - v[2] + M.delrc) / Y.engunit;
-    M.rande = duni_next(C.rng);
-    accepted = accept_move(estep, M.rande, Y.statvolm, C.press[g], nmols, C.temp, C.beta, kDelete);
-  } else {
-    estep = (ewld1 + v[1] + v[2]) / Y.engunit;
-    if (estep < 0.0) {
-      accepted = true;
-    } else {
-      M.rande = duni_next(C.rng);
-      accepted = accept_move(estep, M.rande, Y.statvolm, C.press[g], nmols, C.temp, C.beta, kDisplace);
-    }
-  }
-  M.accepted = accepted;
+  const bool accepted = M.accepted;
+  const double estep = M.estep;
   M.seg_end = C.seg_off[g] + nmols * ns;
   if (mtype == kInsert) {
     M.commit_lo = M.seg_end;
@@ -281,6 +321,7 @@ __device__ __noinline__ void move_end(ChainDev& C, const SysConst& Y, MoveSmem& 
     }
   }
   C.moves_done++;
+  C.since_recompute++;
   if (rec) {
     rec->step = C.gcmccount;
     rec->iguest = g;
@@ -288,11 +329,12 @@ __device__ __noinline__ void move_end(ChainDev& C, const SysConst& Y, MoveSmem& 
     rec->randchoice = M.randchoice;
     rec->accepted = accepted;
     rec->nmols_after = C.nmol[g];
-    rec->pad0 = rec->pad1 = 0;
-    rec->ewld1 = ewld1;
-    rec->ewld2 = v[1];
-    rec->ewld3 = ewld3;
-    rec->vdw = v[2];
+    rec->pad0 = M.recheck;
+    rec->pad1 = 0;
+    rec->ewld1 = M.ewld1;
+    rec->ewld2 = M.ewld2;
+    rec->ewld3 = M.ewld3;
+    rec->vdw = M.vdw;
     rec->delrc = M.delrc;
     rec->estep = estep;
     rec->rande = M.rande;
@@ -355,12 +397,202 @@ __device__ __forceinline__ Cand fetch_candidate(const DevSystem& S, const ChainD
   return c;
 }
 
+// ------------------------------------------------------------------ precision-templated stages
+// e^{i 2 pi j s} for j = 0..kmax in FP32: the fractional coordinate is reduced to [0,1) in FP64,
+// the base phase comes from sincospif, higher harmonics from the FP32 recurrence.
+__device__ __forceinline__ void axis_phases_f32(double s, int kmax, float2* tab) {
+  float f = (float)(s - floor(s));
+  float sn, cs;
+  sincospif(2.0f * f, &sn, &cs);
+  tab[0] = make_float2(1.0f, 0.0f);
+  if (kmax >= 1) tab[1] = make_float2(cs, sn);
+  for (int j = 2; j <= kmax; j++) {
+    float2 p = tab[j - 1];
+    tab[j] = make_float2(p.x * cs - p.y * sn, p.y * cs + p.x * sn);
+  }
+}
+
+__device__ __forceinline__ float interp3f(const float* tab, float rrr, float rdr) {
+  float x = rrr * rdr;
+  int l = (int)x;
+  float ppp = x - (float)l;
+  float v0 = tab[l], v1 = tab[l + 1], v2 = tab[l + 2];
+  float t1 = v0 + (v1 - v0) * ppp;
+  float t2 = v1 + (v2 - v1) * (ppp - 1.0f);
+  return t1 + (t2 - t1) * ppp * 0.5f;
+}
+
+// Warp 0: phase tables of the trial sites (ewald.f:95-137) in the working precision.
+template <bool kMixed>
+__device__ __forceinline__ void build_phases(const DevSystem& S, const MoveSmem& M, void* tabv, int stride, int lane) {
+  const int nsite = M.nold + M.nnew, k1 = S.kmax[0], k2 = S.kmax[1];
+  for (int w = lane; w < nsite * 3; w += 32) {
+    int st = w / 3, ax = w % 3;
+    double f[3];
+    frac_coords(S.cell, M.x[st], M.y[st], M.z[st], f);
+    int off = st * stride + (ax == 0 ? 0 : (ax == 1 ? k1 + 1 : k1 + k2 + 2));
+    if (kMixed)
+      axis_phases_f32(f[ax], S.kmax[ax], reinterpret_cast<float2*>(tabv) + off);
+    else
+      axis_phases(f[ax], S.kmax[ax], reinterpret_cast<double2*>(tabv) + off);
+  }
+}
+
+// All threads: this thread's share of the reciprocal sum and of the real-space pairs.
+// v[0] sum akk*d|S|^2, v[1] ewld2, v[2] vdw, v[3] and v[4] the absolute sums that bound the
+// rounding error of v[0] and v[1]+v[2] (mixed precision).  S_new goes to Sn when write_sn.
+template <bool kMixed>
+__device__ __noinline__ void sums(const DevSystem& S, const ChainDev& C, const MoveSmem& M, int nseg,
+                                     const int* prow_s, int nt1, const int* kp, const double* ak,
+                                     const double2* Sk, double2* Sn, const void* tabv, int stride, bool write_sn,
+                                     int fp32_mask, double* v) {
+  const int tid = threadIdx.x, K = S.K, k1 = S.kmax[0], k2 = S.kmax[1];
+  const int nsite = M.nold + M.nnew, nold = M.nold, mtype = M.mtype;
+  for (int k = tid; k < K; k += blockDim.x) {
+    int l, m, n;
+    kunpack(kp[k], l, m, n);
+    int am = m < 0 ? -m : m, an = n < 0 ? -n : n;
+    double2 so = Sk[k], sn;
+    if (kMixed && (fp32_mask & 1)) {
+      const float2* tb = reinterpret_cast<const float2*>(tabv);
+      float2 d = make_float2(0.0f, 0.0f);
+      for (int st = 0; st < nsite; st++) {
+        const float2* t = tb + st * stride;
+        float2 e1 = t[l], e2 = t[k1 + 1 + am], e3 = t[k1 + k2 + 2 + an];
+        float2 c = m >= 0 ? make_float2(e1.x * e2.x - e1.y * e2.y, e1.y * e2.x + e2.y * e1.x)
+                          : make_float2(e1.x * e2.x + e1.y * e2.y, e1.y * e2.x - e2.y * e1.x);
+        c = n >= 0 ? make_float2(c.x * e3.x - c.y * e3.y, c.y * e3.x + e3.y * c.x)
+                   : make_float2(c.x * e3.x + c.y * e3.y, c.y * e3.x - e3.y * c.x);
+        float q = (float)M.q[st];
+        if (st < nold) {
+          d.x -= q * c.x;
+          d.y -= q * c.y;
+        } else {
+          d.x += q * c.x;
+          d.y += q * c.y;
+        }
+      }
+      // dE_k = akk (2 Re(S* dS) + |dS|^2): nothing cancels
+      double dx = (double)d.x, dy = (double)d.y;
+      sn = make_double2(so.x + dx, so.y + dy);
+      double t = 2.0 * (so.x * dx + so.y * dy) + (dx * dx + dy * dy);
+      v[0] += ak[k] * t;
+      v[3] += ak[k] * (2.0 * (fabs(so.x * dx) + fabs(so.y * dy)) + (dx * dx + dy * dy) + fabs(so.x) + fabs(so.y));
+    } else {
+      const double2* tb = reinterpret_cast<const double2*>(tabv);
+      double2 aold = make_double2(0.0, 0.0), anew = make_double2(0.0, 0.0);
+      for (int st = 0; st < nsite; st++) {
+        const double2* t = tb + st * stride;
+        double2 c = m >= 0 ? cmul(t[l], t[k1 + 1 + am]) : cmulc(t[l], t[k1 + 1 + am]);
+        c = n >= 0 ? cmul(c, t[k1 + k2 + 2 + an]) : cmulc(c, t[k1 + k2 + 2 + an]);
+        double q = M.q[st];
+        if (st < nold) {
+          aold.x += q * c.x;
+          aold.y += q * c.y;
+        } else {
+          anew.x += q * c.x;
+          anew.y += q * c.y;
+        }
+      }
+      if (mtype == kInsert)
+        sn = make_double2(anew.x + so.x, anew.y + so.y);
+      else if (mtype == kDelete)
+        sn = make_double2(so.x - aold.x, so.y - aold.y);
+      else
+        sn = make_double2((so.x - aold.x) + anew.x, (so.y - aold.y) + anew.y);
+      v[0] += ak[k] * (sn.x * sn.x + sn.y * sn.y - so.x * so.x - so.y * so.y);
+    }
+    if (write_sn) Sn[k] = sn;
+  }
+  // real space: every (site, candidate) pair, four candidates in flight per thread
+  const bool sub_old = (mtype != kInsert && mtype != kDelete);
+  const int T = M.pre[nsite];
+  const float rdrf_e = (float)S.rdr_e, rdrf_v = (float)S.rdr_v;
+  int s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+  for (int base = tid; base < T; base += 4 * kBatchThreads) {
+    Cand c[4];
+    c[0] = fetch_candidate(S, C, M, nseg, base, s0);
+    c[1] = fetch_candidate(S, C, M, nseg, base + kBatchThreads, s1);
+    c[2] = fetch_candidate(S, C, M, nseg, base + 2 * kBatchThreads, s2);
+    c[3] = fetch_candidate(S, C, M, nseg, base + 3 * kBatchThreads, s3);
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      if (!c[u].live) continue;
+      const int st = c[u].site;
+      const int row = prow_s[M.type[st] * nt1 + c[u].type];
+      double ec = 0.0, ev = 0.0;
+      if (kMixed && (fp32_mask & 6)) {
+        // FP32 for the components selected by fp32_mask (bit 1 Coulomb, bit 2 vdW); the
+        // separation and minimum image stay FP64
+        double dx = M.x[st] - c[u].a.x, dy = M.y[st] - c[u].a.y, dz = M.z[st] - c[u].a.z;
+        min_image(S.cell, dx, dy, dz);
+        double rsq = dx * dx + dy * dy + dz * dz;
+        if (rsq < S.rcut2) {
+          const bool need64 = (fp32_mask & 6) != 6;
+          double r = need64 ? sqrt(rsq) : 0.0;
+          float rf = need64 ? (float)r : sqrtf((float)rsq);
+          double chgprd = M.q[st] * kR4pie0 * c[u].a.w;
+          if (fabs(chgprd) > 1e-10) {
+            if (fp32_mask & 2)
+              ec = (double)(interp3f(S.erc_f, rf, rdrf_e) * (float)chgprd);
+            else
+              ec = interp3(S.erc, r, S.rdr_e) * chgprd;
+          }
+          if (row >= 0) {
+            if (fp32_mask & 4)
+              ev = (double)interp3f(S.vvv_f + (size_t)row * S.tab_stride, rf, rdrf_v);
+            else
+              ev = interp3(S.vvv + (size_t)row * S.tab_stride, r, S.rdr_v);
+          }
+        }
+        v[4] += ((fp32_mask & 2) ? fabs(ec) : 0.0) + ((fp32_mask & 4) ? fabs(ev) : 0.0);
+      } else {
+        pair_energy(S, M.x[st] - c[u].a.x, M.y[st] - c[u].a.y, M.z[st] - c[u].a.z, M.q[st] * kR4pie0, c[u].a.w,
+                    row, ec, ev);
+      }
+      if (sub_old && st < nold) {
+        v[1] -= ec;
+        v[2] -= ev;
+      } else {
+        v[1] += ec;
+        v[2] += ev;
+      }
+    }
+  }
+}
+
+// All threads: FP64 recompute of S(k) = S_framework(k) + sum over guest sites (bounds the drift
+// of the mixed-precision running sums).  Each thread owns its k-vectors.
+__device__ __forceinline__ void recompute_sk(const DevSystem& S, const SysConst& Y, const ChainDev& C, int nseg,
+                                             const int* kp, double2* Sk) {
+  for (int k = threadIdx.x; k < S.K; k += blockDim.x) {
+    int l, m, n;
+    kunpack(kp[k], l, m, n);
+    double2 acc = Y.sk_fw[k];
+    for (int g = 0; g < nseg; g++) {
+      int lo = C.seg_off[g], hi = lo + C.nmol[g] * Y.sp[g].nsite;
+      for (int j = lo; j < hi; j++) {
+        double4 a = C.gsite[j];
+        double f[3];
+        frac_coords(S.cell, a.x, a.y, a.z, f);
+        double th = (double)l * f[0] + (double)m * f[1] + (double)n * f[2];
+        th = th - floor(th);
+        double sn, cs;
+        sincospi(2.0 * th, &sn, &cs);
+        acc.x += a.w * cs;
+        acc.y += a.w * sn;
+      }
+    }
+    Sk[k] = acc;
+  }
+}
+
 __global__ void __launch_bounds__(kBatchThreads, 2) fmc_batch_kernel(BatchLaunch L, int tab_stride) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ ChainDev C;
   __shared__ MoveSmem M;
   __shared__ SysConst Ysm;
-  __shared__ double red[32 * 3];
+  __shared__ double red[32 * 5];
   __shared__ int prow_s[(kBatchMaxTypes + 1) * (kBatchMaxTypes + 1)];
   DevSystem& S = Ysm.S;
   const int tid = threadIdx.x, cidx = blockIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -380,24 +612,32 @@ __global__ void __launch_bounds__(kBatchThreads, 2) fmc_batch_kernel(BatchLaunch
   const SysConst& Y = Ysm;
   const int K = S.K, Kmax = L.kmax_smem, nseg = Y.nspecies;
   const int nt1 = S.ntypes + 1;
+  const bool mixed = L.mixed != 0;
   for (int i = tid; i < nt1 * nt1; i += blockDim.x) prow_s[i] = S.pair_row[i];
   double2* Sk = reinterpret_cast<double2*>(smem_raw);
   double2* Sn = Sk + Kmax;
   double* ak = reinterpret_cast<double*>(Sn + Kmax);
   int* kp = reinterpret_cast<int*>(ak + Kmax);
-  double2* tab = reinterpret_cast<double2*>(kp + ((Kmax + 3) & ~3));
+  void* tab = reinterpret_cast<void*>(kp + ((Kmax + 3) & ~3));
   for (int k = tid; k < K; k += blockDim.x) {
     Sk[k] = C.sk[k];
     ak[k] = S.akk[k];
     kp[k] = S.kpack[k];
   }
-  const int k1 = S.kmax[0], k2 = S.kmax[1], k3 = S.kmax[2];
-  const int stride = k1 + k2 + k3 + 3;
+  const int stride = S.kmax[0] + S.kmax[1] + S.kmax[2] + 3;
   (void)tab_stride;
   __syncthreads();
   long long t0 = 0, t1 = 0;
   const bool prof = L.profile != 0;
   for (int mv = 0; mv < L.moves; mv++) {
+    if (mixed && L.recompute_every > 0 && C.since_recompute >= L.recompute_every) {
+      recompute_sk(S, Y, C, nseg, kp, Sk);
+      __syncthreads();
+      if (tid == 0) {
+        C.since_recompute = 0;
+        C.recomputes++;
+      }
+    }
     if (prof && tid == 0) t0 = clock64();
     if (tid == 0) move_begin(C, Y, S, M);
     __syncthreads();
@@ -409,13 +649,10 @@ __global__ void __launch_bounds__(kBatchThreads, 2) fmc_batch_kernel(BatchLaunch
     if (C.status) break;
     const int nsite = M.nold + M.nnew;
     if (warp == 0) {
-      // phase tables of the trial sites (ewald.f:95-137)
-      for (int w = lane; w < nsite * 3; w += 32) {
-        int st = w / 3, ax = w % 3;
-        double f[3];
-        frac_coords(S.cell, M.x[st], M.y[st], M.z[st], f);
-        axis_phases(f[ax], S.kmax[ax], tab + st * stride + (ax == 0 ? 0 : (ax == 1 ? k1 + 1 : k1 + k2 + 2)));
-      }
+      if (mixed && (L.mixed & 1))
+        build_phases<true>(S, M, tab, stride, lane);
+      else
+        build_phases<false>(S, M, tab, stride, lane);
     } else if (warp == 1) {
       if (M.need_lrc) lrc_warp(C, Y, M, lane);
     } else if (warp == 2) {
@@ -443,74 +680,62 @@ __global__ void __launch_bounds__(kBatchThreads, 2) fmc_batch_kernel(BatchLaunch
       C.prof[1] += t1 - t0;
       t0 = t1;
     }
-    double v[3] = {0.0, 0.0, 0.0};
-    const int mtype = M.mtype, nold = M.nold;
-    // ---- reciprocal space: this thread's k-vectors
-    for (int k = tid; k < K; k += blockDim.x) {
-      int l, m, n;
-      kunpack(kp[k], l, m, n);
-      int am = m < 0 ? -m : m, an = n < 0 ? -n : n;
-      double2 aold = make_double2(0.0, 0.0), anew = make_double2(0.0, 0.0);
-      for (int st = 0; st < nsite; st++) {
-        const double2* t = tab + st * stride;
-        double2 c = m >= 0 ? cmul(t[l], t[k1 + 1 + am]) : cmulc(t[l], t[k1 + 1 + am]);
-        c = n >= 0 ? cmul(c, t[k1 + k2 + 2 + an]) : cmulc(c, t[k1 + k2 + 2 + an]);
-        double q = M.q[st];
-        if (st < nold) {
-          aold.x += q * c.x;
-          aold.y += q * c.y;
-        } else {
-          anew.x += q * c.x;
-          anew.y += q * c.y;
-        }
-      }
-      double2 so = Sk[k], sn;
-      if (mtype == kInsert)
-        sn = make_double2(anew.x + so.x, anew.y + so.y);
-      else if (mtype == kDelete)
-        sn = make_double2(so.x - aold.x, so.y - aold.y);
-      else
-        sn = make_double2((so.x - aold.x) + anew.x, (so.y - aold.y) + anew.y);
-      Sn[k] = sn;
-      v[0] += ak[k] * (sn.x * sn.x + sn.y * sn.y - so.x * so.x - so.y * so.y);
-    }
-    if (prof && tid == 0) C.prof[5] += clock64() - t0;
-    // ---- real space: every (site, candidate) pair, four candidates in flight per thread
-    {
-      const bool sub_old = (mtype != kInsert && mtype != kDelete);
-      const int T = M.pre[nsite];
-      int s0 = 0, s1 = 0, s2 = 0, s3 = 0;
-      for (int base = tid; base < T; base += 4 * kBatchThreads) {
-        Cand c[4];
-        c[0] = fetch_candidate(S, C, M, nseg, base, s0);
-        c[1] = fetch_candidate(S, C, M, nseg, base + kBatchThreads, s1);
-        c[2] = fetch_candidate(S, C, M, nseg, base + 2 * kBatchThreads, s2);
-        c[3] = fetch_candidate(S, C, M, nseg, base + 3 * kBatchThreads, s3);
-#pragma unroll
-        for (int u = 0; u < 4; u++) {
-          if (!c[u].live) continue;
-          const int st = c[u].site;
-          double ec = 0.0, ev = 0.0;
-          pair_energy(S, M.x[st] - c[u].a.x, M.y[st] - c[u].a.y, M.z[st] - c[u].a.z, M.q[st] * kR4pie0, c[u].a.w,
-                      prow_s[M.type[st] * nt1 + c[u].type], ec, ev);
-          if (sub_old && st < nold) {
-            v[1] -= ec;
-            v[2] -= ev;
-          } else {
-            v[1] += ec;
-            v[2] += ev;
-          }
-        }
-      }
-    }
+    double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    if (mixed)
+      sums<true>(S, C, M, nseg, prow_s, nt1, kp, ak, Sk, Sn, tab, stride, true, L.mixed, v);
+    else
+      sums<false>(S, C, M, nseg, prow_s, nt1, kp, ak, Sk, Sn, tab, stride, true, 0, v);
     if (prof && tid == 0) C.prof[6] += clock64() - t0;
-    block_sum<3>(v, red);
+    block_sum<5>(v, red);
     if (prof && tid == 0) {
       t1 = clock64();
       C.prof[2] += t1 - t0;
       t0 = t1;
     }
-    if (tid == 0) move_end(C, Y, M, v, L.trace ? L.trace + (size_t)cidx * L.moves + mv : nullptr);
+    if (tid == 0) {
+      assemble(Y, M, v);
+      double band = 0.0;
+      if (mixed) {
+        // error band: relative FP32 bound on every term (a few ulp of float)
+        const double eps = 4.0e-6;
+        band = eps * (Y.S.recip_pref * v[3] + v[4]) / Y.engunit + 1e-9;
+      }
+      M.recheck = decide(C, Y, M, band);
+    }
+    __syncthreads();
+    if (mixed && (M.recheck || L.shadow)) {
+      // FP64 evaluation of the same move: decisive when the margin fell inside the band,
+      // recorded (shadow) otherwise
+      const bool decisive = M.recheck != 0;
+      if (warp == 0) build_phases<false>(S, M, tab, stride, lane);
+      __syncthreads();
+      double w[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+      sums<false>(S, C, M, nseg, prow_s, nt1, kp, ak, Sk, Sn, tab, stride, decisive, 0, w);
+      block_sum<5>(w, red);
+      if (tid == 0) {
+        double e32 = M.estep;
+        double r1 = M.ewld1, r2 = M.ewld2, r3 = M.vdw;
+        assemble(Y, M, w);
+        if (L.shadow) {
+          double* sh = L.shadow + 4 * ((size_t)cidx * L.moves + mv);
+          sh[0] = M.ewld1;
+          sh[1] = M.ewld2;
+          sh[2] = M.vdw;
+          sh[3] = M.estep;
+        }
+        if (decisive) {
+          C.rechecks++;
+          decide(C, Y, M, 0.0);
+        } else {
+          M.estep = e32;
+          M.ewld1 = r1;
+          M.ewld2 = r2;
+          M.vdw = r3;
+        }
+      }
+      __syncthreads();
+    }
+    if (tid == 0) bookkeep(C, Y, M, L.trace ? L.trace + (size_t)cidx * L.moves + mv : nullptr);
     __syncthreads();
     if (prof && tid == 0) {
       t1 = clock64();
@@ -519,7 +744,7 @@ __global__ void __launch_bounds__(kBatchThreads, 2) fmc_batch_kernel(BatchLaunch
     }
     if (M.accepted) {
       for (int k = tid; k < K; k += blockDim.x) Sk[k] = Sn[k];
-      const int ns = M.ns;
+      const int ns = M.ns, mtype = M.mtype;
       if (mtype == kDelete) {
         const int lo = M.commit_lo, end = M.seg_end;
         for (int base = lo; base < end - ns; base += blockDim.x) {

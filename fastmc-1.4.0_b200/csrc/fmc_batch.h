@@ -33,6 +33,7 @@ struct SysConst {
   double steadd[kBatchMaxTab + 1];
   int numfrz[kBatchMaxTypes + 1];
   double engunit, volm, statvolm;
+  const double2* sk_fw;  // S(k) of the framework alone (periodic FP64 recompute)
 };
 
 // Per-chain parameters and mutable state (device memory).
@@ -60,6 +61,9 @@ struct ChainDev {
   // SM clock cycles spent per phase when the launch is profiled: begin (thread 0), phase
   // tables, k-space + real space + reduction, end (thread 0), commit
   long long prof[12];
+  // mixed precision: FP64 re-evaluations of the acceptance, moves since the last FP64 S(k)
+  // recompute, recomputes done
+  long long rechecks, since_recompute, recomputes;
   // buffers
   double2* sk;
   double4* gsite;
@@ -74,6 +78,11 @@ struct BatchLaunch {
   MoveRecord* trace;  // [nchains][moves] or null
   int kmax_smem;      // largest K in the batch rounded up to a multiple of 4 (smem sizing)
   int profile;        // accumulate per-phase clock counters into ChainDev::prof
+  int mixed;          // FP32 component mask (0 = all FP64): 1 reciprocal phases, 2 real-space
+                      // Coulomb, 4 vdW; S(k), totals and dE assembly stay FP64
+  long long recompute_every;  // mixed: moves between FP64 recomputes of S(k) (0: never)
+  double* shadow;     // mixed, optional [nchains][moves][4]: FP64 {ewld1, ewld2, vdw, dE} of every
+                      // move on the same state
 };
 
 cudaError_t launch_batch(const BatchLaunch& L, int smem_bytes, int tab_stride, cudaStream_t st);
@@ -94,12 +103,16 @@ class Batch {
   MoveRecord* d_trace = nullptr;
   size_t trace_cap = 0;
   int kmax_all = 0, tab_sites = 0, tab_stride = 0, smem = 0;
+  int mixed = 0;
+  long long recompute_every = 0;
+  double* d_shadow = nullptr;
+  size_t shadow_cap = 0;
   int nchains = 0;
   ~Batch();
   int open(const std::vector<std::string>& dirs, const std::vector<int>& seeds, int device, std::string& err);
   // One step: control blocks host->device, `moves` moves of every chain, control blocks (and
   // the optional per-move trace) device->host.  *ms: CUDA-event time of the kernel alone.
-  int run(int moves, MoveRecord* trace_host, float* ms, std::string& err);
+  int run(int moves, MoveRecord* trace_host, float* ms, std::string& err, double* shadow_host = nullptr);
   int profile = 0;
 };
 

@@ -35,6 +35,7 @@ Batch::~Batch() {
     cudaStreamSynchronize(st);
     for (void* p : allocations) cudaFree(p);
     if (d_trace) cudaFree(d_trace);
+    if (d_shadow) cudaFree(d_shadow);
     if (h_chains) cudaFreeHost(h_chains);
     cudaStreamDestroy(st);
   }
@@ -120,6 +121,17 @@ int Batch::open(const std::vector<std::string>& dirs, const std::vector<int>& se
     Y.engunit = H.engunit;
     Y.volm = H.cell.volm;
     Y.statvolm = H.statvolm;
+    {
+      double2* fw = nullptr;
+      cudaError_t e = cudaMalloc(&fw, sizeof(double2) * std::max(H.K, 1));
+      if (e == cudaSuccess) allocations.push_back(fw);
+      if (e == cudaSuccess) e = cudaMemcpy(fw, ch.sk, sizeof(double2) * H.K, cudaMemcpyDeviceToDevice);
+      if (e != cudaSuccess) {
+        err = std::string("framework S(k) copy failed: ") + cudaGetErrorString(e);
+        return -100 - (int)e;
+      }
+      Y.sk_fw = fw;
+    }
     kmax_all = std::max(kmax_all, H.K);
     tab_stride = std::max(tab_stride, H.deck.kmax[0] + H.deck.kmax[1] + H.deck.kmax[2] + 3);
   }
@@ -215,7 +227,7 @@ int Batch::open(const std::vector<std::string>& dirs, const std::vector<int>& se
   return 0;
 }
 
-int Batch::run(int moves, MoveRecord* trace_host, float* ms, std::string& err) {
+int Batch::run(int moves, MoveRecord* trace_host, float* ms, std::string& err, double* shadow_host) {
   cudaSetDevice(device);
   BatchLaunch L;
   L.chains = d_chains;
@@ -224,8 +236,21 @@ int Batch::run(int moves, MoveRecord* trace_host, float* ms, std::string& err) {
   L.moves = moves;
   L.kmax_smem = kmax_all;
   L.profile = profile;
+  L.mixed = mixed;
+  L.recompute_every = recompute_every;
   L.trace = nullptr;
+  L.shadow = nullptr;
   cudaError_t e = cudaSuccess;
+  if (shadow_host && mixed) {
+    size_t need = (size_t)nchains * moves;
+    if (need > shadow_cap) {
+      if (d_shadow) cudaFree(d_shadow);
+      d_shadow = nullptr;
+      e = cudaMalloc(&d_shadow, sizeof(double) * 4 * need);
+      shadow_cap = e == cudaSuccess ? need : 0;
+    }
+    L.shadow = d_shadow;
+  }
   if (trace_host) {
     size_t need = (size_t)nchains * moves;
     if (need > trace_cap) {
@@ -246,6 +271,9 @@ int Batch::run(int moves, MoveRecord* trace_host, float* ms, std::string& err) {
   if (e == cudaSuccess) e = cudaEventRecord(b, st);
   if (e == cudaSuccess && trace_host)
     e = cudaMemcpyAsync(trace_host, d_trace, sizeof(MoveRecord) * (size_t)nchains * moves, cudaMemcpyDeviceToHost,
+                        st);
+  if (e == cudaSuccess && L.shadow)
+    e = cudaMemcpyAsync(shadow_host, d_shadow, sizeof(double) * 4 * (size_t)nchains * moves, cudaMemcpyDeviceToHost,
                         st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(h_chains, d_chains, cb, cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
@@ -307,6 +335,37 @@ int fmc_batch_profile(fmc_batch* b, int enable) {
   return 0;
 }
 
+int fmc_batch_set_precision(fmc_batch* b, int mixed, long long recompute_every) {
+  if (!b || recompute_every < 0) {
+    fmc::set_last_error("bad batch handle or recompute interval");
+    return -1;
+  }
+  b->impl.mixed = mixed & 7;
+  b->impl.recompute_every = recompute_every;
+  return 0;
+}
+
+int fmc_batch_run_shadow(fmc_batch* b, int moves, fmc_move_record* trace, double* shadow, float* device_ms) {
+  if (!b || moves < 0) {
+    fmc::set_last_error("bad batch handle or move count");
+    return -1;
+  }
+  std::string err;
+  int rc = b->impl.run(moves, reinterpret_cast<fmc::MoveRecord*>(trace), device_ms, err, shadow);
+  if (rc) {
+    fmc::set_last_error(err);
+    return rc;
+  }
+  for (int i = 0; i < b->impl.nchains; i++) {
+    const fmc::ChainDev& c = b->impl.h_chains[i];
+    if (c.status) {
+      fmc::set_last_error(c.status == 75 ? "too many atoms in specified system" : "unsupported move drawn");
+      return c.status;
+    }
+  }
+  return 0;
+}
+
 int fmc_batch_run(fmc_batch* b, int moves, fmc_move_record* trace, float* device_ms) {
   if (!b || moves < 0) {
     fmc::set_last_error("bad batch handle or move count");
@@ -356,6 +415,8 @@ int fmc_batch_chain_state(fmc_batch* b, int chain, double* out) {
   v[26] = C.press[0];
   for (int k = 0; k < 5; k++) v[27 + k] = (double)C.prof[k];
   for (int k = 5; k < 9; k++) v[k + 27] = (double)C.prof[k];
+  v[36] = (double)C.rechecks;
+  v[37] = (double)C.recomputes;
   std::memcpy(out, v, sizeof(v));
   return 0;
 }

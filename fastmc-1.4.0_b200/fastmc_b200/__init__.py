@@ -184,7 +184,24 @@ class Batch:
     _STATE = ["status", "moves", "gcmccount", "nmol0", "nmol1", "nmol2", "nmol3", "energy0", "energy1", "energy2",
               "energy3", "elrc", "accept_ins", "accept_del", "ins_count", "del_count", "prodcount", "N", "E", "EN",
               "N2", "E2", "system", "K", "nframework", "temp", "press0", "cyc_begin", "cyc_phase", "cyc_sums",
-              "cyc_end", "cyc_commit", "cyc_t0_kspace", "cyc_t0_real", "cyc_select", "cyc_trial"]
+              "cyc_end", "cyc_commit", "cyc_t0_kspace", "cyc_t0_real", "cyc_select", "cyc_trial", "rechecks",
+              "recomputes"]
+
+    # FP32 component masks of set_precision
+    FP32_RECIP, FP32_COULOMB, FP32_VDW = 1, 2, 4
+
+    def set_precision(self, mixed, recompute_every=0):
+        """mixed: mask of FP32 components (True = all three); 0/False = FP64."""
+        m = 7 if mixed is True else int(mixed)
+        check(lib().fmc_batch_set_precision(self.h, m, int(recompute_every)))
+
+    def run_shadow(self, moves):
+        """Mixed precision run that also returns the FP64 dE of every move on the same state."""
+        rec = np.zeros((self.n, moves), dtype=MOVE_DTYPE)
+        sh = np.zeros((self.n, moves, 4))
+        ms = ctypes.c_float(0)
+        check(lib().fmc_batch_run_shadow(self.h, int(moves), rec.ctypes.data, sh.ctypes.data, ctypes.byref(ms)))
+        return rec, sh, float(ms.value)
 
     def profile(self, enable=True):
         check(lib().fmc_batch_profile(self.h, int(bool(enable))))

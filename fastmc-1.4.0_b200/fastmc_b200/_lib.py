@@ -47,6 +47,8 @@ SIGNATURES = {
     "fmc_batch_close": (None, [_vp]),
     "fmc_batch_run": (_ci, [_vp, _ci, _vp, ctypes.POINTER(ctypes.c_float)]),
     "fmc_batch_profile": (_ci, [_vp, _ci]),
+    "fmc_batch_set_precision": (_ci, [_vp, _ci, ctypes.c_longlong]),
+    "fmc_batch_run_shadow": (_ci, [_vp, _ci, _vp, _vp, ctypes.POINTER(ctypes.c_float)]),
     "fmc_batch_chain_state": (_ci, [_vp, _ci, _dp]),
     "fmc_batch_guest_coords": (_ci, [_vp, _ci, _ci, _dp, _ip, _ip]),
     "fmc_deck_inspect": (_ci, [ctypes.c_char_p, _ip, _dp, _ip, _dp, _dp, _dp, _ip, _ip]),

@@ -113,6 +113,17 @@ void fmc_batch_close(fmc_batch* b);
 /* Advances every chain by `moves` trial moves in one launch; trace (nullable) receives
  * nchains*moves records, chain-major; *device_ms is the launch's CUDA-event time. */
 int fmc_batch_run(fmc_batch* b, int moves, fmc_move_record* trace, float* device_ms);
+/* Precision of later runs.  `mixed` is a mask of the components evaluated in FP32: 1 the
+ * reciprocal-space phases and dS, 2 the real-space Coulomb pair terms, 4 the vdW pair terms
+ * (0 = all FP64).  S(k), the energy totals and the dE assembly (2Re(S* dS) + |dS|^2) stay
+ * FP64; a move whose acceptance margin lies inside the FP32 error band is re-evaluated in
+ * FP64; S(k) is recomputed in FP64 from the framework's S(k) and the guest sites every
+ * `recompute_every` moves (0: never). */
+int fmc_batch_set_precision(fmc_batch* b, int mixed, long long recompute_every);
+/* fmc_batch_run that also stores, for mixed precision, the FP64 {ewld1, ewld2, vdw, dE} of every
+ * move evaluated on the same state (shadow[nchains*moves*4], chain-major) to measure the
+ * mixed-precision error. */
+int fmc_batch_run_shadow(fmc_batch* b, int moves, fmc_move_record* trace, double* shadow, float* device_ms);
 /* enable != 0: later runs accumulate SM clock cycles per phase of the move (see
  * fmc_batch_chain_state out[27..31]). */
 int fmc_batch_profile(fmc_batch* b, int enable);
@@ -120,7 +131,8 @@ int fmc_batch_profile(fmc_batch* b, int enable);
  * insertions, accepted deletions, insert attempts, delete attempts, production moves,
  * species-0 <N>,<E>,<EN>,<N^2>,<E^2>, system index, K, framework atoms, T, P(species 0),
  * profiled cycles of: trial set-up, phase tables, energy sums, acceptance, commit, then
- * (thread 0's share) k-space, + real space, move selection, trial generation. */
+ * (thread 0's share) k-space, + real space, move selection, trial generation, then FP64
+ * re-evaluations and S(k) recomputes (mixed precision). */
 int fmc_batch_chain_state(fmc_batch* b, int chain, double* out);
 int fmc_batch_guest_coords(fmc_batch* b, int chain, int iguest, double* xyz, int* nmol, int* nsite);
 
