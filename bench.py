@@ -32,7 +32,14 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="batched", choices=["plain", "batched"])
+    ap.add_argument("--workload", default="batched", choices=["plain", "batched", "serve"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--serve-requests", type=int, default=400)
+    ap.add_argument("--serve-slots", type=int, default=296)
+    ap.add_argument("--serve-moves", type=int, default=1000, help="moves per slot per serving step")
+    ap.add_argument("--serve-kcap", type=int, default=0, help="0: the largest request's K")
+    ap.add_argument("--serve-cycle-scale", type=float, default=0.01,
+                    help="scale of the U(2k,20k) cycle budgets so that requests finish within the run")
     ap.add_argument("--moves", type=int, default=2000, help="trial moves per chain per step")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="bounded CPU baseline sample")
     return ap.parse_args()
@@ -200,6 +207,12 @@ def cpu_sample(deck, seed, guest_xyz, seconds, threads=1):
     return sum(done) / dt, n, dt
 
 
+PLAIN_METRIC = "MC trial moves/s (plain FP64 single-chain GPU path)"
+PLAIN_WORKLOAD = ("plain FP64 GPU drop-in: 3392-atom cubic framework a=51.664 A, CO2 1 bar, kmax 12 (K=4192), "
+                  "host move loop")
+BATCHED_METRIC = "MC trial moves/s on 1 B200 (batched vs plain)"
+
+
 def run_plain(args, dist):
     import numpy as np
 
@@ -248,7 +261,7 @@ def run_plain(args, dist):
     h2d = int(h2d_total / args.steps)
     d2h = int(prof["passes"] * 24 / args.steps)
     result = {
-        "metric": "MC trial moves/s (plain FP64 single-chain GPU path)",
+        "metric": PLAIN_METRIC,
         "value": total_moves / t_dev,
         "unit": "moves/s",
         "n_gpus": dist.world,
@@ -260,8 +273,7 @@ def run_plain(args, dist):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic (seeded framework generator, FastMC input formats)",
-        "config": {"workload": "plain FP64 GPU drop-in: 3392-atom cubic framework a=51.664 A, CO2 1 bar, "
-                               "kmax 12 (K=4192), host move loop", "moves_per_step": args.moves,
+        "config": {"workload": PLAIN_WORKLOAD, "moves_per_step": args.moves,
                    "chains_per_gpu": 1, "guests_mean": float(np.mean(tr["nmols_after"])),
                    "l2": "working set (S(k) 67 KB + framework 130 KB) is L2-resident; no flush between moves",
                    "parallelism": f"replicas{dist.world}"},
@@ -343,7 +355,7 @@ def run_batched(args, dist):
     from fastmc_b200._lib import lib as _l  # noqa: F401
     cb = 1512  # bytes of one chain control block moved each way per step (sizeof(ChainDev))
     result = {
-        "metric": "MC trial moves/s on 1 B200 (batched vs plain)",
+        "metric": BATCHED_METRIC,
         "value": total_moves / t_dev,
         "unit": "moves/s",
         "n_gpus": dist.world,
@@ -414,29 +426,158 @@ def run_batched(args, dist):
     return result
 
 
-def run_reference(args, dist):
-    """The reference algorithm (oracle restatement; the Fortran reference cannot be built here)
-    on all host cores: one independent chain per core, like the reference's MPI replicas."""
-    if dist.rank != 0:
-        return None
+def _write_request(job):
+    from fastmc_b200 import synth
+
+    path, req = job
+    return synth.write_request(path, req)
+
+
+def write_requests(root, reqs):
+    """Request decks are client-side inputs: written before any GPU work, in a spawn pool."""
+    import multiprocessing as mp
+
+    jobs = [(os.path.join(root, f"req_{r['id']:05d}"), r) for r in reqs]
+    with mp.get_context("spawn").Pool(max(1, min(len(jobs), os.cpu_count() or 1))) as pool:
+        return pool.map(_write_request, jobs, chunksize=4)
+
+
+SERVE_WORKLOAD = ("serving: Poisson stream of isotherm-point requests, each a fresh cubic framework of 400-6000 "
+                  "atoms (rho 0.025 A^-3), gas CO2 / N2 / CH4, T U(273,348) K, P log-U(0.01,10) bar, cycle budget "
+                  "U(2k,20k) x {scale} per phase (a cycle = N_guests+1 moves), continuous batching over {slots} slots")
+
+
+def run_serve(args, dist):
+    """Continuous-batching server on a Poisson request stream; time-to-completion p50/p99."""
     import numpy as np
 
+    from fastmc_b200 import synth
+
+    tmp = tempfile.mkdtemp(prefix="fmcserve")
+    n_pilot, n_req = 64, args.serve_requests
+    reqs = synth.serving_requests(n_pilot + n_req, seed=7 + 1000 * dist.rank)
+    for r in reqs:
+        r["cycles"] = max(1, int(round(r["cycles"] * args.serve_cycle_scale)))
+    t0 = time.perf_counter()
+    dirs = write_requests(tmp, reqs)  # before the first CUDA call (spawned pool)
+    gen_s = time.perf_counter() - t0
+    import fastmc_b200 as fm
+
+    # k capacity: the largest request's K (cubic cells: K grows with the edge)
+    kcap = args.serve_kcap or int(fm.deck_inspect(dirs[int(np.argmax([r["edge"] for r in reqs]))])["K"])
+    srv = fm.Server(slots=args.serve_slots, device=dist.local, k_capacity=kcap)
+    if args.precision == "mixed":
+        srv.set_precision(7, recompute_every=1000)
+    # pilot (warm-up): a closed batch of requests measures moves per request and throughput
+    ids = [srv.submit(d, (12, 34, 56, r["id"] % 169)) for d, r in zip(dirs[:n_pilot], reqs[:n_pilot])]
+    p_ms, p_wall = 0.0, time.perf_counter()
+    while True:
+        a, q, ms = srv.step(args.serve_moves)
+        p_ms += ms
+        if not a and not q:
+            break
+    p_wall = time.perf_counter() - p_wall
+    pil = [srv.poll(i) for i in ids]
+    moves_per_req = float(np.mean([r["moves"] for r in pil]))
+    # offered load: 90% of the throughput the pilot reached with all its requests resident
+    rate = 0.9 * sum(r["moves"] for r in pil) / max(p_wall, 1e-9) / moves_per_req
+    rate = max(rate, 1.0)
+    rng = np.random.default_rng(99 + dist.rank)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, n_req))
+    dist.barrier()
+    live = {}
+    done_t = {}
+    nxt = 0
+    dev_ms, steps, moves_total = 0.0, 0, 0
+    moves_seen = {}
+    wall0 = time.perf_counter()
+    with ClockSampler(dist.local) as clk:
+        while len(done_t) < n_req:
+            now = time.perf_counter() - wall0
+            while nxt < n_req and arrivals[nxt] <= now:
+                rid = srv.submit(dirs[n_pilot + nxt], (12, 34, 56, reqs[n_pilot + nxt]["id"] % 169))
+                live[rid] = nxt
+                nxt += 1
+            if not live:
+                time.sleep(max(0.0, min(arrivals[nxt] - now, 0.05)))
+                continue
+            a, q, ms = srv.step(args.serve_moves)
+            dev_ms += ms
+            steps += 1
+            now = time.perf_counter() - wall0
+            for rid in list(live):
+                res = srv.poll(rid)
+                if res["state"] in (srv.DONE, srv.REJECTED, srv.CANCELLED):
+                    done_t[live[rid]] = (now - arrivals[live[rid]], res)
+                    moves_total += int(res["moves"])
+                    del live[rid]
+    wall = time.perf_counter() - wall0
+    dist.barrier()
+    lat = np.array([v[0] for v in done_t.values()])
+    rejected = sum(1 for v in done_t.values() if v[1]["state"] != srv.DONE)
+    t_dev = dist.max(dev_ms / 1000.0)
+    t_wall = dist.max(wall)
+    total = dist.sum(moves_total)
+    used, budget = srv.memory()
+    srv.close()
+    # host<->device bytes per step: slot control blocks (SysConst + ChainDev) each way
+    return {
+        "metric": "MC trial moves/s on 1 B200 (continuous-batching serving); p50/p99 time-to-completion",
+        "value": total / t_dev, "unit": "moves/s", "n_gpus": dist.world, "steps": steps, "warmup": 1,
+        "ms_per_step": t_dev * 1000.0 / max(steps, 1), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
+        "data": "synthetic (seeded request generator, FastMC input formats)",
+        "config": {"workload": SERVE_WORKLOAD.format(scale=args.serve_cycle_scale, slots=args.serve_slots),
+                   "requests": n_req, "pilot_requests": n_pilot, "arrival_rate_hz": rate,
+                   "moves_per_request_mean": moves_per_req, "moves_per_step": args.serve_moves,
+                   "precision": args.precision, "deck_generation_s": gen_s, "k_capacity": kcap,
+                   "l2": "per-chain S(k) shared-memory resident; frameworks + voxel lists exceed L2 (no flush)",
+                   "parallelism": f"replicas{dist.world}"},
+        "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                      "mean": float(lat.mean()), "max": float(lat.max())},
+        "rejected": rejected,
+        "gpu_launches": steps,
+        "e2e": {"value": total / t_wall, "unit": "moves/s",
+                "h2d_bytes_per_step": args.serve_slots * 2 * 1512, "d2h_bytes_per_step": args.serve_slots * 1512},
+        "clocks": clk.summary(),
+        "memory": {"slots_bytes_at_end": used, "budget_bytes": budget},
+    }
+
+
+def run_reference(args, dist):
+    """The reference algorithm (oracle restatement; the Fortran reference cannot be built here)
+    on all host cores, on the default arm's workload: one chain per thread at a time, like the
+    reference's independent MPI replicas."""
+    if dist.rank != 0:
+        return None
     tmp = tempfile.mkdtemp(prefix="fmcref")
-    deck = make_plain_deck(tmp)
     threads = os.cpu_count() or 1
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
 
     oracle.build()
-    chains = [oracle.Chain(deck, seed=(12, 34, 56, (78 + t) % 169)) for t in range(threads)]
-    # bounded sample per step, sized so the whole run stays within a few minutes
+    if args.workload == "plain":
+        dirs = [make_plain_deck(tmp)] * threads
+        metric = PLAIN_METRIC
+        workload = PLAIN_WORKLOAD
+    else:
+        dirs = make_batched_decks(tmp)
+        metric = BATCHED_METRIC
+        workload = BATCHED_WORKLOAD
+    n = len(dirs)
+    seeds = [(12, 34, 56, (78 + 7 * i) % 169) for i in range(n)]
+    chains = [oracle.Chain(d, seed=s) for d, s in zip(dirs, seeds)]
+    # bounded sample per step: ~4 s of moves per thread, on chains taken round-robin
     t0 = time.perf_counter()
     chains[0].run(100, trace=False)
     per = (time.perf_counter() - t0) / 100
-    n = max(50, int(6.0 / max(per, 1e-7)))
+    m = max(50, int(4.0 / max(per, 1e-7)))
+    state = {"next": 0}
 
     def step():
-        ths = [threading.Thread(target=lambda c=c: c.run(n, trace=False)) for c in chains]
+        pick = [(state["next"] + t) % n for t in range(threads)]
+        state["next"] = (state["next"] + threads) % n
+        ths = [threading.Thread(target=lambda c=chains[i]: c.run(m, trace=False)) for i in pick]
         for th in ths:
             th.start()
         for th in ths:
@@ -448,18 +589,17 @@ def run_reference(args, dist):
     for _ in range(args.steps):
         step()
     dt = time.perf_counter() - t0
-    v = args.steps * n * threads / dt
+    v = args.steps * m * threads / dt
     return {
-        "metric": "MC trial moves/s (plain FP64 single-chain GPU path)", "value": v, "unit": "moves/s",
+        "metric": metric, "value": v, "unit": "moves/s",
         "n_gpus": dist.world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1000 / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded framework generator, FastMC input formats)",
-        "config": {"workload": "plain FP64 GPU drop-in: 3392-atom cubic framework a=51.664 A, CO2 1 bar, "
-                               "kmax 12 (K=4192), host move loop", "moves_per_step": n, "chains": threads},
+        "config": {"workload": workload, "chains": n, "moves_per_thread_per_step": m, "threads": threads},
         "impl": "reference",
         "cpu_baseline": {"value": v, "unit": "moves/s", "cores": threads, "kind": "port",
-                         "sample": f"{n} moves per chain per step, {threads} independent chains on "
-                                   f"{threads} threads (oracle FP64 restatement of the reference)"},
+                         "sample": f"{m} moves per thread per step, {threads} threads each on one of the {n} "
+                                   f"chains (round-robin over steps), oracle FP64 restatement of the reference"},
         "e2e": {"value": v, "unit": "moves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
@@ -472,6 +612,8 @@ def main():
             res = run_reference(args, dist)
         elif args.workload == "plain":
             res = run_plain(args, dist)
+        elif args.workload == "serve":
+            res = run_serve(args, dist)
         else:
             res = run_batched(args, dist)
         if dist.rank == 0 and res is not None:

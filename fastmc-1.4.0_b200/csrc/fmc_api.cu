@@ -267,7 +267,7 @@ int fmc_chain_profile(fmc_chain* c, int enable, double* out) {
     out[2] = (double)C.pass_timed;
     out[3] = C.pass_ms;
     out[4] = (double)S.K;
-    out[5] = nv ? (double)S.vox_atoms.size() / nv : 0.0;
+    out[5] = nv ? (double)C.dsys.vox_entries / nv : 0.0;
   }
   return 0;
 }
@@ -304,7 +304,7 @@ int fmc_deck_inspect(const char* dir, int* ints, double* dbls, int* lmn, double*
   int natoms = S.nf;
   for (auto& g : deck.guests) natoms += g.nmols * g.nsite;
   int iv[16] = {S.cell.imcon, deck.kmax[0], deck.kmax[1], deck.kmax[2], S.K, natoms, (int)deck.guests.size(),
-                S.ntypes, S.mxgrid, S.nf, 0, nv, 0, (int)S.vox_atoms.size(), 0, 0};
+                S.ntypes, S.mxgrid, S.nf, 0, nv, 0, 0, 0, 0};
   double dv[16] = {S.alpha, S.rcut, deck.delr, S.cell.volm, S.engunit, deck.temp, S.beta, S.drewd, S.dlrpot,
                    0, 0, 0, 0, 0, S.statvolm, 0};
   if (ints) std::memcpy(ints, iv, sizeof(iv));

@@ -597,6 +597,7 @@ __global__ void __launch_bounds__(kBatchThreads, 2) fmc_batch_kernel(BatchLaunch
   DevSystem& S = Ysm.S;
   const int tid = threadIdx.x, cidx = blockIdx.x, warp = tid >> 5, lane = tid & 31;
   if (cidx >= L.nchains) return;
+  if (!L.chains[cidx].active) return;
   {
     const int* src = reinterpret_cast<const int*>(&L.chains[cidx]);
     int* dst = reinterpret_cast<int*>(&C);
@@ -629,7 +630,11 @@ __global__ void __launch_bounds__(kBatchThreads, 2) fmc_batch_kernel(BatchLaunch
   __syncthreads();
   long long t0 = 0, t1 = 0;
   const bool prof = L.profile != 0;
-  for (int mv = 0; mv < L.moves; mv++) {
+  // a chain ends after the move on which its deck's equilibration + production budget ran
+  // out (the reference's do-while(lgchk) loop, gcmc.f:589-736), or at its move budget
+  long long nmoves = C.lgchk ? L.moves : 0;
+  if (C.budget > 0) nmoves = min(nmoves, C.budget - C.moves_done);
+  for (int mv = 0; mv < nmoves; mv++) {
     if (mixed && L.recompute_every > 0 && C.since_recompute >= L.recompute_every) {
       recompute_sk(S, Y, C, nseg, kp, Sk);
       __syncthreads();
@@ -647,6 +652,7 @@ __global__ void __launch_bounds__(kBatchThreads, 2) fmc_batch_kernel(BatchLaunch
       t0 = t1;
     }
     if (C.status) break;
+    const bool last = !C.lgchk;  // thread 0 writes lgchk only in move_begin
     const int nsite = M.nold + M.nnew;
     if (warp == 0) {
       if (mixed && (L.mixed & 1))
@@ -771,6 +777,7 @@ __global__ void __launch_bounds__(kBatchThreads, 2) fmc_batch_kernel(BatchLaunch
     }
     __syncthreads();
     if (prof && tid == 0) C.prof[4] += clock64() - t0;
+    if (last) break;
   }
   for (int k = tid; k < K; k += blockDim.x) C.sk[k] = Sk[k];
   __syncthreads();

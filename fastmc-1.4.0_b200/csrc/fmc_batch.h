@@ -40,6 +40,8 @@ struct SysConst {
 struct ChainDev {
   int sys;
   int status;  // 0 ok; 75 guest capacity exhausted; 3 unsupported move drawn
+  int active;  // 0: an empty serving slot (the launch skips it)
+  long long budget;  // total moves this chain is to run (0: unlimited)
   // parameters (CONTROL)
   double temp, beta, press[kMaxGuestTypes], mvcum[kMaxGuestTypes][9];
   double disp_ratio[kMaxGuestTypes], tran_ratio[kMaxGuestTypes], rota_ratio;
@@ -88,6 +90,10 @@ struct BatchLaunch {
 cudaError_t launch_batch(const BatchLaunch& L, int smem_bytes, int tab_stride, cudaStream_t st);
 int batch_smem_bytes(int kmax_K, int tab_sites, int tab_stride);
 cudaError_t configure_batch_kernel(int smem_bytes);
+
+int make_sysconst(const Chain& ch, SysConst& Y, std::vector<void*>& allocations, int* tab_sites, std::string& err);
+int init_chain(const InputDeck& d, const Chain& ch, int sys, const int* seed, ChainDev& C,
+               std::vector<void*>& allocations, cudaStream_t st, std::string& err);
 
 class Batch {
  public:

@@ -29,6 +29,126 @@ std::string system_key(const std::string& dir, const InputDeck& d) {
 
 }  // namespace
 
+// Per-system constants of an opened system chain (its HostSystem, device arrays and the
+// framework S(k), which the chain holds while it has no guests).
+int make_sysconst(const Chain& ch, SysConst& Y, std::vector<void*>& allocations, int* tab_sites, std::string& err) {
+  const HostSystem& H = ch.sys;
+  std::memset(&Y, 0, sizeof(Y));
+  Y.S = ch.dsys.view;
+  Y.nspecies = (int)H.deck.guests.size();
+  Y.ntypes = H.ntypes;
+  Y.lrc_on = H.lrc_on;
+  if (Y.ntypes > kBatchMaxTypes) {
+    err = "more atom types than the batched path supports";
+    return -5;
+  }
+  for (int g = 0; g < Y.nspecies; g++) {
+    const GuestSpecies& G = H.deck.guests[g];
+    if (G.nsite > kBatchMaxSites) {
+      err = "guest with more sites than the batched path supports";
+      return -5;
+    }
+    SpeciesConst& P = Y.sp[g];
+    P.nsite = G.nsite;
+    for (int s = 0; s < G.nsite; s++) {
+      P.tx[s] = G.tx[s];
+      P.ty[s] = G.ty[s];
+      P.tz[s] = G.tz[s];
+      P.q[s] = G.charge[s];
+      P.mass[s] = G.mass[s];
+      P.type[s] = G.type[s];
+    }
+    P.engsic = H.engsic[g];
+    P.ewald3en = H.ewald3en[g];
+    *tab_sites = std::max(*tab_sites, 2 * G.nsite);
+  }
+  for (int t = 1; t < (int)H.steadd.size() && t <= kBatchMaxTab; t++) Y.steadd[t] = H.steadd[t];
+  for (int j = 0; j < H.nf; j++)
+    if (H.ffrz[j]) Y.numfrz[H.ftype[j]]++;
+  Y.engunit = H.engunit;
+  Y.volm = H.cell.volm;
+  Y.statvolm = H.statvolm;
+  {
+    double2* fw = nullptr;
+    cudaError_t e = cudaMalloc(&fw, sizeof(double2) * std::max(H.K, 1));
+    if (e == cudaSuccess) allocations.push_back(fw);
+    if (e == cudaSuccess) e = cudaMemcpy(fw, ch.sk, sizeof(double2) * H.K, cudaMemcpyDeviceToDevice);
+    if (e != cudaSuccess) {
+      err = std::string("framework S(k) copy failed: ") + cudaGetErrorString(e);
+      return -100 - (int)e;
+    }
+    Y.sk_fw = fw;
+  }
+  return 0;
+}
+
+// Parameters (from the chain's own deck) and initial state of one chain of system `sys`;
+// allocates its S(k) (initialised to the framework's) and guest-site segments.
+int init_chain(const InputDeck& d, const Chain& ch, int sys, const int* seed, ChainDev& C,
+             std::vector<void*>& allocations, cudaStream_t st, std::string& err) {
+  const HostSystem& H = ch.sys;
+  std::memset(&C, 0, sizeof(C));
+  C.sys = sys;
+  C.temp = d.temp;
+  C.beta = 1.0 / (kKboltz * d.temp);
+  const int ng = (int)d.guests.size();
+  for (int g = 0; g < ng; g++) {
+    C.press[g] = d.press[g];
+    std::array<double, 9> f = d.movefreq[g];
+    double nrm = 0;
+    for (double v : f) nrm += v;
+    if (nrm == 0) {
+      nrm = 1;
+      f = {1.0 / 3.0, 1.0 / 3.0, 1.0 / 3.0, 0, 0, 0, 0, 0, 0};
+    }
+    if (f[3] != 0 || f[4] != 0 || f[5] != 0 || f[8] != 0) {
+      err = "jump, flex, swap and multi-jump moves are outside the GCMC trial-move path";
+      return -3;
+    }
+    C.mvcum[g][0] = f[0] / nrm;
+    for (int k = 1; k < 9; k++) C.mvcum[g][k] = C.mvcum[g][k - 1] + (f[k] / nrm);
+    C.disp_ratio[g] = d.disp_ratio[g];
+    C.tran_ratio[g] = d.tran_ratio[g];
+    C.delrdisp[g] = d.delr;
+    C.tran_delr[g] = d.delr;
+    C.energy[g] = ch.spenergy;
+  }
+  C.rota_ratio = d.rota_ratio;
+  C.maxguest = d.maxguest;
+  C.mcsteps = d.mcsteps;
+  C.eqsteps = d.eqsteps;
+  C.laccsample = d.laccsample;
+  duni_seed(C.rng, seed[0], seed[1], seed[2], seed[3]);
+  duni_next(C.rng);  // gcmc.f:335-336
+  C.totatm = C.framatm = H.nf;
+  for (int j = 0; j < H.nf; j++) C.numtyp[H.ftype[j]]++;
+  C.rotangle = kPi / 3.0;
+  C.rota_rotangle = kPi / 3.0;
+  C.production = d.eqsteps == 0;
+  C.lgchk = 1;
+  C.active = 1;
+  C.budget = 0;
+  // buffers: S(k) starts as the framework's (empty framework), guest segments per species
+  cudaError_t e = cudaMalloc(&C.sk, sizeof(double2) * std::max(H.K, 1));
+  if (e == cudaSuccess) allocations.push_back(C.sk);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(C.sk, ch.sk, sizeof(double2) * H.K, cudaMemcpyDeviceToDevice, st);
+  int off = 0;
+  for (int g = 0; g < ng; g++) {
+    C.seg_off[g] = off;
+    C.seg_cap[g] = d.maxguest;
+    off += d.maxguest;
+  }
+  if (e == cudaSuccess) e = cudaMalloc(&C.gsite, sizeof(double4) * std::max(off, 1));
+  if (e == cudaSuccess) allocations.push_back(C.gsite);
+  if (e == cudaSuccess) e = cudaMalloc(&C.gtype, sizeof(int) * std::max(off, 1));
+  if (e == cudaSuccess) allocations.push_back(C.gtype);
+  if (e != cudaSuccess) {
+    err = std::string("batch allocation failed: ") + cudaGetErrorString(e);
+    return -100 - (int)e;
+  }
+  return 0;
+}
+
 Batch::~Batch() {
   if (st) {
     cudaSetDevice(device);
@@ -83,55 +203,9 @@ int Batch::open(const std::vector<std::string>& dirs, const std::vector<int>& se
   // ---- per-system constants
   h_sys.assign(sys_chains.size(), SysConst());
   for (size_t i = 0; i < sys_chains.size(); i++) {
-    const Chain& ch = *sys_chains[i];
-    const HostSystem& H = ch.sys;
-    SysConst& Y = h_sys[i];
-    std::memset(&Y, 0, sizeof(Y));
-    Y.S = ch.dsys.view;
-    Y.nspecies = (int)H.deck.guests.size();
-    Y.ntypes = H.ntypes;
-    Y.lrc_on = H.lrc_on;
-    if (Y.ntypes > kBatchMaxTypes) {
-      err = "more atom types than the batched path supports";
-      return -5;
-    }
-    for (int g = 0; g < Y.nspecies; g++) {
-      const GuestSpecies& G = H.deck.guests[g];
-      if (G.nsite > kBatchMaxSites) {
-        err = "guest with more sites than the batched path supports";
-        return -5;
-      }
-      SpeciesConst& P = Y.sp[g];
-      P.nsite = G.nsite;
-      for (int s = 0; s < G.nsite; s++) {
-        P.tx[s] = G.tx[s];
-        P.ty[s] = G.ty[s];
-        P.tz[s] = G.tz[s];
-        P.q[s] = G.charge[s];
-        P.mass[s] = G.mass[s];
-        P.type[s] = G.type[s];
-      }
-      P.engsic = H.engsic[g];
-      P.ewald3en = H.ewald3en[g];
-      tab_sites = std::max(tab_sites, 2 * G.nsite);
-    }
-    for (int t = 1; t < (int)H.steadd.size() && t <= kBatchMaxTab; t++) Y.steadd[t] = H.steadd[t];
-    for (int j = 0; j < H.nf; j++)
-      if (H.ffrz[j]) Y.numfrz[H.ftype[j]]++;
-    Y.engunit = H.engunit;
-    Y.volm = H.cell.volm;
-    Y.statvolm = H.statvolm;
-    {
-      double2* fw = nullptr;
-      cudaError_t e = cudaMalloc(&fw, sizeof(double2) * std::max(H.K, 1));
-      if (e == cudaSuccess) allocations.push_back(fw);
-      if (e == cudaSuccess) e = cudaMemcpy(fw, ch.sk, sizeof(double2) * H.K, cudaMemcpyDeviceToDevice);
-      if (e != cudaSuccess) {
-        err = std::string("framework S(k) copy failed: ") + cudaGetErrorString(e);
-        return -100 - (int)e;
-      }
-      Y.sk_fw = fw;
-    }
+    int rc = make_sysconst(*sys_chains[i], h_sys[i], allocations, &tab_sites, err);
+    if (rc) return rc;
+    const HostSystem& H = sys_chains[i]->sys;
     kmax_all = std::max(kmax_all, H.K);
     tab_stride = std::max(tab_stride, H.deck.kmax[0] + H.deck.kmax[1] + H.deck.kmax[2] + 3);
   }
@@ -151,67 +225,9 @@ int Batch::open(const std::vector<std::string>& dirs, const std::vector<int>& se
     return -100;
   }
   for (int c = 0; c < nchains; c++) {
-    const InputDeck& d = decks[c];
-    const Chain& ch = *sys_chains[chain_sys[c]];
-    const HostSystem& H = ch.sys;
-    ChainDev& C = h_chains[c];
-    std::memset(&C, 0, sizeof(C));
-    C.sys = chain_sys[c];
-    C.temp = d.temp;
-    C.beta = 1.0 / (kKboltz * d.temp);
-    const int ng = (int)d.guests.size();
-    for (int g = 0; g < ng; g++) {
-      C.press[g] = d.press[g];
-      std::array<double, 9> f = d.movefreq[g];
-      double nrm = 0;
-      for (double v : f) nrm += v;
-      if (nrm == 0) {
-        nrm = 1;
-        f = {1.0 / 3.0, 1.0 / 3.0, 1.0 / 3.0, 0, 0, 0, 0, 0, 0};
-      }
-      if (f[3] != 0 || f[4] != 0 || f[5] != 0 || f[8] != 0) {
-        err = "jump, flex, swap and multi-jump moves are outside the GCMC trial-move path";
-        return -3;
-      }
-      C.mvcum[g][0] = f[0] / nrm;
-      for (int k = 1; k < 9; k++) C.mvcum[g][k] = C.mvcum[g][k - 1] + (f[k] / nrm);
-      C.disp_ratio[g] = d.disp_ratio[g];
-      C.tran_ratio[g] = d.tran_ratio[g];
-      C.delrdisp[g] = d.delr;
-      C.tran_delr[g] = d.delr;
-      C.energy[g] = ch.spenergy;
-    }
-    C.rota_ratio = d.rota_ratio;
-    C.maxguest = d.maxguest;
-    C.mcsteps = d.mcsteps;
-    C.eqsteps = d.eqsteps;
-    C.laccsample = d.laccsample;
-    duni_seed(C.rng, seeds[4 * c], seeds[4 * c + 1], seeds[4 * c + 2], seeds[4 * c + 3]);
-    duni_next(C.rng);  // gcmc.f:335-336
-    C.totatm = C.framatm = H.nf;
-    for (int j = 0; j < H.nf; j++) C.numtyp[H.ftype[j]]++;
-    C.rotangle = kPi / 3.0;
-    C.rota_rotangle = kPi / 3.0;
-    C.production = d.eqsteps == 0;
-    C.lgchk = 1;
-    // buffers: S(k) starts as the framework's (empty framework), guest segments per species
-    cudaError_t e = cudaMalloc(&C.sk, sizeof(double2) * std::max(H.K, 1));
-    if (e == cudaSuccess) allocations.push_back(C.sk);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(C.sk, ch.sk, sizeof(double2) * H.K, cudaMemcpyDeviceToDevice, st);
-    int off = 0;
-    for (int g = 0; g < ng; g++) {
-      C.seg_off[g] = off;
-      C.seg_cap[g] = d.maxguest;
-      off += d.maxguest;
-    }
-    if (e == cudaSuccess) e = cudaMalloc(&C.gsite, sizeof(double4) * std::max(off, 1));
-    if (e == cudaSuccess) allocations.push_back(C.gsite);
-    if (e == cudaSuccess) e = cudaMalloc(&C.gtype, sizeof(int) * std::max(off, 1));
-    if (e == cudaSuccess) allocations.push_back(C.gtype);
-    if (e != cudaSuccess) {
-      err = std::string("batch allocation failed: ") + cudaGetErrorString(e);
-      return -100 - (int)e;
-    }
+    int rc = init_chain(decks[c], *sys_chains[chain_sys[c]], chain_sys[c], &seeds[4 * c], h_chains[c], allocations,
+                        st, err);
+    if (rc) return rc;
   }
   cudaError_t e = cudaMalloc(&d_sys, sizeof(SysConst) * h_sys.size());
   if (e == cudaSuccess) allocations.push_back(d_sys);
@@ -417,6 +433,7 @@ int fmc_batch_chain_state(fmc_batch* b, int chain, double* out) {
   for (int k = 5; k < 9; k++) v[k + 27] = (double)C.prof[k];
   v[36] = (double)C.rechecks;
   v[37] = (double)C.recomputes;
+  v[38] = C.lgchk ? 0.0 : 1.0;
   std::memcpy(out, v, sizeof(v));
   return 0;
 }

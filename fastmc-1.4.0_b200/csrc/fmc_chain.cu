@@ -52,23 +52,35 @@ int upload_system(const HostSystem& h, DeviceSystem& d, std::string& err) {
   if ((e = upload(d.allocations, &v.fw, fw)) != cudaSuccess) goto fail;
   if ((e = upload(d.allocations, &v.fw_type, h.ftype)) != cudaSuccess) goto fail;
   for (int a = 0; a < 3; a++) v.nvox[a] = h.nvox[a];
-  if ((e = upload(d.allocations, &v.vox_off, h.vox_off)) != cudaSuccess) goto fail;
-  if ((e = upload(d.allocations, &v.vox_atoms, h.vox_atoms)) != cudaSuccess) goto fail;
-  v.vox_atoms16 = nullptr;
-  if (h.nf <= 65535) {
-    std::vector<unsigned short> v16(h.vox_atoms.begin(), h.vox_atoms.end());
-    if ((e = upload(d.allocations, &v.vox_atoms16, v16)) != cudaSuccess) goto fail;
-  }
   {
-    std::vector<double4> vx(h.vox_atoms.size());
-    std::vector<unsigned char> vt(h.vox_atoms.size());
-    for (size_t i = 0; i < h.vox_atoms.size(); i++) {
-      int j = h.vox_atoms[i];
-      vx[i] = make_double4(h.fx[j], h.fy[j], h.fz[j], h.fq[j]);
-      vt[i] = (unsigned char)h.ftype[j];
-    }
-    if ((e = upload(d.allocations, &v.vox_xyzq, vx)) != cudaSuccess) goto fail;
-    if ((e = upload(d.allocations, &v.vox_type, vt)) != cudaSuccess) goto fail;
+    // voxel lists built on the device: count per voxel, prefix sum, ordered fill
+    const int nv = h.nvox[0] * h.nvox[1] * h.nvox[2];
+    int* counts = nullptr;
+    if ((e = cudaMalloc(&counts, sizeof(int) * nv)) != cudaSuccess) goto fail;
+    e = launch_voxel_count(h.cell, h.nvox, v.fw, h.nf, h.vox_lim2, counts, 0);
+    std::vector<int> cnt(nv), offv(nv + 1, 0);
+    if (e == cudaSuccess) e = cudaMemcpy(cnt.data(), counts, sizeof(int) * nv, cudaMemcpyDeviceToHost);
+    cudaFree(counts);
+    if (e != cudaSuccess) goto fail;
+    for (int i = 0; i < nv; i++) offv[i + 1] = offv[i] + cnt[i];
+    const size_t ne = (size_t)offv[nv];
+    d.vox_entries = (long long)ne;
+    int* atoms = nullptr;
+    unsigned short* a16 = nullptr;
+    double4* xyzq = nullptr;
+    unsigned char* vt = nullptr;
+    if ((e = upload(d.allocations, &v.vox_off, offv)) != cudaSuccess) goto fail;
+    if ((e = dalloc(d.allocations, &atoms, ne)) != cudaSuccess) goto fail;
+    if (h.nf <= 65535 && (e = dalloc(d.allocations, &a16, ne)) != cudaSuccess) goto fail;
+    if ((e = dalloc(d.allocations, &xyzq, ne)) != cudaSuccess) goto fail;
+    if ((e = dalloc(d.allocations, &vt, ne)) != cudaSuccess) goto fail;
+    e = launch_voxel_fill(h.cell, h.nvox, v.fw, v.fw_type, h.nf, h.vox_lim2, v.vox_off, atoms, a16, xyzq, vt, 0);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) goto fail;
+    v.vox_atoms = atoms;
+    v.vox_atoms16 = a16;
+    v.vox_xyzq = xyzq;
+    v.vox_type = vt;
   }
   v.rcut2 = h.rcut * h.rcut;
   v.rdr_e = 1.0 / h.drewd;

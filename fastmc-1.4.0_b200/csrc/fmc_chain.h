@@ -22,6 +22,7 @@ struct DeviceSystem {
   DevSystem view{};
   std::vector<void*> allocations;
   int device = 0;
+  long long vox_entries = 0;
   ~DeviceSystem();
 };
 

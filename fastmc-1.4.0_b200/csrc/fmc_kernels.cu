@@ -306,4 +306,113 @@ cudaError_t launch_single_point_rs(const DevSystem& S, const GuestView& G, int n
   return cudaGetLastError();
 }
 
+// ------------------------------------------------------------------------------ voxel lists
+// Every framework atom whose true minimum-image distance to a voxel's centre is below
+// sqrt(lim2) (rcut + the voxel's circumradius), in ascending atom order.
+__device__ __forceinline__ double true_dist2_dev(const CellGeom& c, double dx, double dy, double dz) {
+  min_image(c, dx, dy, dz);
+  double best = dx * dx + dy * dy + dz * dz;
+  if (c.imcon == 3) {
+    for (int i = -1; i <= 1; i++)
+      for (int j = -1; j <= 1; j++)
+        for (int k = -1; k <= 1; k++) {
+          double x = dx + i * c.h[0] + j * c.h[3] + k * c.h[6];
+          double y = dy + i * c.h[1] + j * c.h[4] + k * c.h[7];
+          double z = dz + i * c.h[2] + j * c.h[5] + k * c.h[8];
+          best = fmin(best, x * x + y * y + z * z);
+        }
+  }
+  return best;
+}
+
+__device__ __forceinline__ void voxel_centre(const CellGeom& c, int v, int n0, int n1, int n2, double* p) {
+  int a = v / (n1 * n2), b = (v / n2) % n1, cc = v % n2;
+  double fa = (a + 0.5) / n0, fb = (b + 0.5) / n1, fc = (cc + 0.5) / n2;
+  p[0] = fa * c.h[0] + fb * c.h[3] + fc * c.h[6];
+  p[1] = fa * c.h[1] + fb * c.h[4] + fc * c.h[7];
+  p[2] = fa * c.h[2] + fb * c.h[5] + fc * c.h[8];
+}
+
+constexpr int kVoxThreads = 128;
+
+__global__ void __launch_bounds__(kVoxThreads) fmc_voxel_count_kernel(CellGeom cell, int n0, int n1, int n2,
+                                                                      const double4* __restrict__ fw, int nf,
+                                                                      double lim2, int* counts) {
+  __shared__ int ws[kVoxThreads / 32];
+  double p[3];
+  voxel_centre(cell, blockIdx.x, n0, n1, n2, p);
+  int cnt = 0;
+  for (int j = threadIdx.x; j < nf; j += blockDim.x) {
+    double4 a = fw[j];
+    if (true_dist2_dev(cell, p[0] - a.x, p[1] - a.y, p[2] - a.z) < lim2) cnt++;
+  }
+  for (int o = 16; o > 0; o >>= 1) cnt += __shfl_down_sync(0xffffffffu, cnt, o);
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = cnt;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int t = 0;
+    for (int w = 0; w < kVoxThreads / 32; w++) t += ws[w];
+    counts[blockIdx.x] = t;
+  }
+}
+
+__global__ void __launch_bounds__(kVoxThreads) fmc_voxel_fill_kernel(CellGeom cell, int n0, int n1, int n2,
+                                                                     const double4* __restrict__ fw,
+                                                                     const int* __restrict__ ftype, int nf, double lim2,
+                                                                     const int* __restrict__ off, int* atoms,
+                                                                     unsigned short* atoms16, double4* xyzq,
+                                                                     unsigned char* vtype) {
+  __shared__ int woff[kVoxThreads / 32 + 1];
+  __shared__ int running;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double p[3];
+  voxel_centre(cell, blockIdx.x, n0, n1, n2, p);
+  if (threadIdx.x == 0) running = 0;
+  const int base = off[blockIdx.x];
+  __syncthreads();
+  for (int chunk = 0; chunk < nf; chunk += blockDim.x) {
+    int j = chunk + threadIdx.x;
+    bool flag = false;
+    double4 a = make_double4(0, 0, 0, 0);
+    if (j < nf) {
+      a = fw[j];
+      flag = true_dist2_dev(cell, p[0] - a.x, p[1] - a.y, p[2] - a.z) < lim2;
+    }
+    unsigned mask = __ballot_sync(0xffffffffu, flag);
+    if (lane == 0) woff[warp + 1] = __popc(mask);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      woff[0] = 0;
+      for (int w = 1; w <= kVoxThreads / 32; w++) woff[w] += woff[w - 1];
+    }
+    __syncthreads();
+    if (flag) {
+      int pos = base + running + woff[warp] + __popc(mask & ((1u << lane) - 1u));
+      atoms[pos] = j;
+      if (atoms16) atoms16[pos] = (unsigned short)j;
+      xyzq[pos] = a;
+      vtype[pos] = (unsigned char)ftype[j];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) running += woff[kVoxThreads / 32];
+    __syncthreads();
+  }
+}
+
+cudaError_t launch_voxel_count(const CellGeom& cell, const int* nvox, const double4* fw, int nf, double lim2,
+                               int* counts, cudaStream_t st) {
+  int nv = nvox[0] * nvox[1] * nvox[2];
+  fmc_voxel_count_kernel<<<nv, kVoxThreads, 0, st>>>(cell, nvox[0], nvox[1], nvox[2], fw, nf, lim2, counts);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_voxel_fill(const CellGeom& cell, const int* nvox, const double4* fw, const int* ftype, int nf,
+                              double lim2, const int* off, int* atoms, unsigned short* atoms16, double4* xyzq,
+                              unsigned char* vtype, cudaStream_t st) {
+  int nv = nvox[0] * nvox[1] * nvox[2];
+  fmc_voxel_fill_kernel<<<nv, kVoxThreads, 0, st>>>(cell, nvox[0], nvox[1], nvox[2], fw, ftype, nf, lim2, off, atoms,
+                                                    atoms16, xyzq, vtype);
+  return cudaGetLastError();
+}
+
 }  // namespace fmc

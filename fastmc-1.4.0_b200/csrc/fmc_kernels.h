@@ -54,4 +54,10 @@ double recip_energy_from_parts(const DevSystem& S, const double* host_parts);
 cudaError_t launch_single_point_rs(const DevSystem& S, const GuestView& G, int nsites, const int* sites, const int* lo,
                                    const int* hi, double* out, cudaStream_t st);
 
+cudaError_t launch_voxel_count(const CellGeom& cell, const int* nvox, const double4* fw, int nf, double lim2,
+                               int* counts, cudaStream_t st);
+cudaError_t launch_voxel_fill(const CellGeom& cell, const int* nvox, const double4* fw, const int* ftype, int nf,
+                              double lim2, const int* off, int* atoms, unsigned short* atoms16, double4* xyzq,
+                              unsigned char* vtype, cudaStream_t st);
+
 }  // namespace fmc

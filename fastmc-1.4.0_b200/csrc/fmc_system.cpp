@@ -337,7 +337,7 @@ int build_host_system(const InputDeck& d, HostSystem& s, std::string& err, doubl
   s.fq = d.fq;
   s.ftype = d.ftype;
   s.ffrz = d.ffrz;
-  // ---- voxel neighbour lists over the framework
+  // ---- voxel grid over the framework (lists are built on the device)
   {
     double w[3];
     widths(s.cell.h, w);
@@ -353,26 +353,30 @@ int build_host_system(const InputDeck& d, HostSystem& s, std::string& err, doubl
         circ = std::max(circ, 0.5 * std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]));
       }
     double lim = s.rcut + circ + 1e-6;
-    double lim2 = lim * lim;
-    int nv = s.nvox[0] * s.nvox[1] * s.nvox[2];
-    s.vox_off.assign(nv + 1, 0);
-    s.vox_atoms.clear();
-    for (int a = 0; a < s.nvox[0]; a++)
-      for (int b = 0; b < s.nvox[1]; b++)
-        for (int c = 0; c < s.nvox[2]; c++) {
-          double fa = (a + 0.5) / s.nvox[0], fb = (b + 0.5) / s.nvox[1], fc = (c + 0.5) / s.nvox[2];
-          const double* h = s.cell.h;
-          double cx = fa * h[0] + fb * h[3] + fc * h[6];
-          double cy = fa * h[1] + fb * h[4] + fc * h[7];
-          double cz = fa * h[2] + fb * h[5] + fc * h[8];
-          int v = (a * s.nvox[1] + b) * s.nvox[2] + c;
-          for (int j = 0; j < s.nf; j++)
-            if (true_dist2(s.cell, cx - s.fx[j], cy - s.fy[j], cz - s.fz[j]) < lim2) s.vox_atoms.push_back(j);
-          s.vox_off[v + 1] = (int)s.vox_atoms.size();
-        }
+    s.vox_lim2 = lim * lim;
   }
   (void)nint_image_dist2;
   return 0;
+}
+
+void build_host_voxels(HostSystem& s) {
+  int nv = s.nvox[0] * s.nvox[1] * s.nvox[2];
+  s.vox_off.assign(nv + 1, 0);
+  s.vox_atoms.clear();
+  const double* h = s.cell.h;
+  for (int a = 0; a < s.nvox[0]; a++)
+    for (int b = 0; b < s.nvox[1]; b++)
+      for (int c = 0; c < s.nvox[2]; c++) {
+        double fa = (a + 0.5) / s.nvox[0], fb = (b + 0.5) / s.nvox[1], fc = (c + 0.5) / s.nvox[2];
+        double cx = fa * h[0] + fb * h[3] + fc * h[6];
+        double cy = fa * h[1] + fb * h[4] + fc * h[7];
+        double cz = fa * h[2] + fb * h[5] + fc * h[8];
+        int v = (a * s.nvox[1] + b) * s.nvox[2] + c;
+        for (int j = 0; j < s.nf; j++)
+          if (true_dist2(s.cell, cx - s.fx[j], cy - s.fy[j], cz - s.fz[j]) < s.vox_lim2) s.vox_atoms.push_back(j);
+        s.vox_off[v + 1] = (int)s.vox_atoms.size();
+      }
+  s.vox_entries = (long long)s.vox_atoms.size();
 }
 
 }  // namespace fmc

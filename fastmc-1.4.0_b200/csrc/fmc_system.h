@@ -40,10 +40,16 @@ struct HostSystem {
   std::vector<double> fx, fy, fz, fq;
   std::vector<int> ftype, ffrz;
   // voxel neighbour lists: every framework atom whose minimum-image distance to the voxel
-  // centre is below rcut + the voxel's circumradius
+  // centre is below rcut + the voxel's circumradius (built on the device by upload_system;
+  // build_host_voxels fills the host copies for inspection)
   int nvox[3] = {1, 1, 1};
+  double vox_lim2 = 0;
+  long long vox_entries = 0;
   std::vector<int> vox_off, vox_atoms;
 };
+
+// Host construction of the voxel lists (the device builds the same lists in upload_system).
+void build_host_voxels(HostSystem& sys);
 
 // Builds everything above from a deck.  Returns 0 or an error code; fills err.
 int build_host_system(const InputDeck& deck, HostSystem& sys, std::string& err, double voxel_edge = 2.0);

@@ -12,7 +12,7 @@ import numpy as np
 from . import _lib
 from ._lib import DELETE, DISPLACE, INSERT, MOVE_DTYPE, ROTATE, TRANSLATE, FastMCError, check, dp, ip, lib
 
-__all__ = ["Chain", "Batch", "deck_inspect", "FastMCError", "INSERT", "DELETE", "DISPLACE", "TRANSLATE", "ROTATE",
+__all__ = ["Chain", "Batch", "Server", "deck_inspect", "FastMCError", "INSERT", "DELETE", "DISPLACE", "TRANSLATE", "ROTATE",
            "MOVE_DTYPE"]
 
 _INFO_INTS = ["imcon", "kmax1", "kmax2", "kmax3", "K", "natoms", "nspecies", "ntypes", "mxgrid", "nframework",
@@ -175,7 +175,10 @@ class Batch:
             pass
 
     def run(self, moves, trace=False):
-        """Advance every chain by `moves`; returns (trace[n, moves] or None, device ms)."""
+        """Advance every chain by `moves`; returns (trace[n, moves] or None, device ms).
+
+        A chain whose deck's equilibration + production budget runs out stops after that move
+        (state()["finished"]); its remaining trace records stay zero."""
         rec = np.zeros((self.n, moves), dtype=MOVE_DTYPE) if trace else None
         ms = ctypes.c_float(0)
         check(lib().fmc_batch_run(self.h, int(moves), rec.ctypes.data if trace else None, ctypes.byref(ms)))
@@ -185,7 +188,7 @@ class Batch:
               "energy3", "elrc", "accept_ins", "accept_del", "ins_count", "del_count", "prodcount", "N", "E", "EN",
               "N2", "E2", "system", "K", "nframework", "temp", "press0", "cyc_begin", "cyc_phase", "cyc_sums",
               "cyc_end", "cyc_commit", "cyc_t0_kspace", "cyc_t0_real", "cyc_select", "cyc_trial", "rechecks",
-              "recomputes"]
+              "recomputes", "finished"]
 
     # FP32 component masks of set_precision
     FP32_RECIP, FP32_COULOMB, FP32_VDW = 1, 2, 4
@@ -218,3 +221,62 @@ class Batch:
         check(lib().fmc_batch_guest_coords(self.h, int(chain), int(iguest), dp(buf), ctypes.byref(n),
                                            ctypes.byref(ns)))
         return buf[: n.value]
+
+
+class Server:
+    """Continuous-batching server of isotherm-point requests on one GPU."""
+
+    QUEUED, RUNNING, DONE, REJECTED, CANCELLED = 0, 1, 2, -1, -2
+    _OUT = ["moves", "status", "nmol0", "nmol1", "nmol2", "nmol3", "energy0", "energy1", "energy2", "energy3",
+            "prodcount", "N", "E", "EN", "N2", "E2", "accept_ins", "accept_del", "rechecks", "K", "nframework",
+            "temp", "press0", "budget", "finished", "N_1", "E_1", "EN_1", "N2_1", "E2_1", "gcmccount", "_"]
+
+    def __init__(self, slots=296, device=0, mem_budget=0, k_capacity=2400):
+        self.h = ctypes.c_void_p()
+        check(lib().fmc_server_open(int(slots), int(device), int(mem_budget), int(k_capacity), ctypes.byref(self.h)))
+
+    def close(self):
+        if self.h:
+            lib().fmc_server_close(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_precision(self, mixed, recompute_every=0):
+        m = 7 if mixed is True else int(mixed)
+        check(lib().fmc_server_set_precision(self.h, m, int(recompute_every)))
+
+    def submit(self, directory, seed, moves=0):
+        """Queue one request; moves=0 runs the deck's own equilibration + production cycles."""
+        rid = ctypes.c_int(0)
+        s = np.asarray(seed, dtype=np.int32)
+        check(lib().fmc_server_submit(self.h, str(directory).encode(), ip(s), int(moves), ctypes.byref(rid)))
+        return rid.value
+
+    def cancel(self, rid):
+        check(lib().fmc_server_cancel(self.h, int(rid)))
+
+    def step(self, moves):
+        """One continuous-batching step; returns (active, queued, device ms)."""
+        a, q, ms = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_float(0)
+        check(lib().fmc_server_step(self.h, int(moves), ctypes.byref(a), ctypes.byref(q), ctypes.byref(ms)))
+        return a.value, q.value, float(ms.value)
+
+    def poll(self, rid):
+        st = ctypes.c_int(0)
+        out = np.zeros(32)
+        check(lib().fmc_server_poll(self.h, int(rid), ctypes.byref(st), dp(out)))
+        res = dict(zip(self._OUT, out.tolist()))
+        res["state"] = st.value
+        if st.value == self.REJECTED:
+            res["error"] = lib().fmc_last_error().decode()
+        return res
+
+    def memory(self):
+        u, b = ctypes.c_longlong(0), ctypes.c_longlong(0)
+        check(lib().fmc_server_memory(self.h, ctypes.byref(u), ctypes.byref(b)))
+        return u.value, b.value

@@ -51,6 +51,14 @@ SIGNATURES = {
     "fmc_batch_run_shadow": (_ci, [_vp, _ci, _vp, _vp, ctypes.POINTER(ctypes.c_float)]),
     "fmc_batch_chain_state": (_ci, [_vp, _ci, _dp]),
     "fmc_batch_guest_coords": (_ci, [_vp, _ci, _ci, _dp, _ip, _ip]),
+    "fmc_server_open": (_ci, [_ci, _ci, ctypes.c_longlong, _ci, ctypes.POINTER(_vp)]),
+    "fmc_server_close": (None, [_vp]),
+    "fmc_server_set_precision": (_ci, [_vp, _ci, ctypes.c_longlong]),
+    "fmc_server_submit": (_ci, [_vp, ctypes.c_char_p, _ip, ctypes.c_longlong, _ip]),
+    "fmc_server_cancel": (_ci, [_vp, _ci]),
+    "fmc_server_step": (_ci, [_vp, _ci, _ip, _ip, ctypes.POINTER(ctypes.c_float)]),
+    "fmc_server_poll": (_ci, [_vp, _ci, _ip, _dp]),
+    "fmc_server_memory": (_ci, [_vp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
     "fmc_deck_inspect": (_ci, [ctypes.c_char_p, _ip, _dp, _ip, _dp, _dp, _dp, _ip, _ip]),
 }
 

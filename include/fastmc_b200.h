@@ -111,7 +111,9 @@ typedef struct fmc_batch fmc_batch;
 int fmc_batch_open(int nchains, const char* const* dirs, const int* seeds, int device, fmc_batch** out);
 void fmc_batch_close(fmc_batch* b);
 /* Advances every chain by `moves` trial moves in one launch; trace (nullable) receives
- * nchains*moves records, chain-major; *device_ms is the launch's CUDA-event time. */
+ * nchains*moves records, chain-major; *device_ms is the launch's CUDA-event time.  A chain
+ * stops after the move on which its deck's equilibration + production cycles end (the
+ * reference's loop test, gcmc.f:594-736); its later records stay as the caller left them. */
 int fmc_batch_run(fmc_batch* b, int moves, fmc_move_record* trace, float* device_ms);
 /* Precision of later runs.  `mixed` is a mask of the components evaluated in FP32: 1 the
  * reciprocal-space phases and dS, 2 the real-space Coulomb pair terms, 4 the vdW pair terms
@@ -132,9 +134,34 @@ int fmc_batch_profile(fmc_batch* b, int enable);
  * species-0 <N>,<E>,<EN>,<N^2>,<E^2>, system index, K, framework atoms, T, P(species 0),
  * profiled cycles of: trial set-up, phase tables, energy sums, acceptance, commit, then
  * (thread 0's share) k-space, + real space, move selection, trial generation, then FP64
- * re-evaluations and S(k) recomputes (mixed precision). */
+ * re-evaluations and S(k) recomputes (mixed precision), then 1 once the chain has finished. */
 int fmc_batch_chain_state(fmc_batch* b, int chain, double* out);
 int fmc_batch_guest_coords(fmc_batch* b, int chain, int iguest, double* xyz, int* nmol, int* nsite);
+
+/* ---------------------------------------------------------------- serving
+ * Isotherm-point requests (an input-deck directory, a duni seed and a budget) served with
+ * continuous batching on one GPU: fmc_server_step admits queued requests into free slots while
+ * the device-memory budget allows (mem_budget 0: 80% of the free memory), advances every
+ * running request by up to `moves` moves in one persistent launch, and retires finished ones,
+ * freeing their slots for the next step.  k_capacity bounds the k-vectors of any request
+ * (with guests of up to 4 sites and kmax <= 32 per axis; larger requests are rejected).
+ * A request's budget is `moves` trial moves, or with moves = 0 its deck's own equilibration +
+ * production cycles (CONTROL `equilibration` / `steps`). */
+typedef struct fmc_server fmc_server;
+int fmc_server_open(int slots, int device, long long mem_budget, int k_capacity, fmc_server** out);
+void fmc_server_close(fmc_server* s);
+int fmc_server_set_precision(fmc_server* s, int mixed, long long recompute_every);
+int fmc_server_submit(fmc_server* s, const char* dir, const int* seed, long long moves, int* request_id);
+int fmc_server_cancel(fmc_server* s, int request_id);
+/* *active: requests advanced by this step's launch; *queued: requests still waiting. */
+int fmc_server_step(fmc_server* s, int moves, int* active, int* queued, float* device_ms);
+/* *state: 0 queued, 1 running, 2 done, -1 rejected (message in fmc_last_error), -2 cancelled.
+ * out[0..31]: moves done, status, nmol[4], energy[4] (kcal/mol), production moves,
+ * species-0 <N>,<E>,<EN>,<N^2>,<E^2>, accepted insertions, accepted deletions, FP64 re-checks,
+ * K, framework atoms, T, P(species 0), move budget, 1 if the deck's cycles finished,
+ * species-1 <N>,<E>,<EN>,<N^2>,<E^2>, gcmccount, 0. */
+int fmc_server_poll(fmc_server* s, int request_id, int* state, double* out);
+int fmc_server_memory(fmc_server* s, long long* used, long long* budget);
 
 /* Launch accounting and timing of the plain path.  enable != 0 turns on CUDA-event timing of
  * every trial-pass kernel on the chain's stream (enable < 0 also clears the counters).

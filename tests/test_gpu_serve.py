@@ -1,0 +1,126 @@
+"""Serving with continuous batching: requests admitted into free slots as others retire.
+
+A served request must end in exactly the state the same deck and seed reach in a batch of
+their own (FP64: nmol, energies and production statistics bitwise), whatever the other
+requests in the launches were and however the move budget was cut into steps."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+REQS = [("small", (12, 34, 56, 78), 1700), ("ortho0", (1, 2, 3, 4), 900), ("mixture", (9, 10, 11, 12), 2300),
+        ("ortho1", (5, 6, 7, 8), 600), ("small", (31, 41, 59, 26), 1250), ("ortho2", (17, 19, 23, 29), 1000),
+        ("ortho0", (2, 7, 1, 8), 400)]
+
+
+def _alone(fmc, d, seed, moves):
+    b = fmc.Batch([d], [seed])
+    b.run(moves)
+    return b.state(0)
+
+
+def _same(res, st):
+    assert res["moves"] == st["moves"]
+    for g in range(4):
+        assert res[f"nmol{g}"] == st[f"nmol{g}"]
+        assert res[f"energy{g}"] == st[f"energy{g}"]
+    for k in ("prodcount", "N", "E", "EN", "N2", "E2", "accept_ins", "accept_del"):
+        assert res[k] == st[k], k
+
+
+def test_continuous_batching_matches_isolated_runs(fmc, decks):
+    srv = fmc.Server(slots=3, k_capacity=2400)
+    ids = [srv.submit(decks[n], s, m) for n, s, m in REQS]
+    seen_active, steps = [], 0
+    while True:
+        active, queued, ms = srv.step(250)
+        steps += 1
+        seen_active.append(active)
+        assert active <= 3
+        if active == 0 and queued == 0:
+            break
+        assert steps < 100
+    # more requests than slots: later requests waited for retirements
+    assert max(seen_active) == 3
+    for rid, (n, s, m) in zip(ids, REQS):
+        res = srv.poll(rid)
+        assert res["state"] == srv.DONE, res
+        assert res["moves"] == m and res["budget"] == m
+        _same(res, _alone(fmc, decks[n], s, m))
+    used, budget = srv.memory()
+    assert used == 0 and budget > 0
+
+
+def test_serve_cancel_and_reject(fmc, decks, tmp_path):
+    # k capacity below the small deck's K: that request is rejected at admission
+    k_cap = fmc.deck_inspect(decks["ortho0"])["K"]
+    assert fmc.deck_inspect(decks["small"])["K"] > k_cap
+    srv = fmc.Server(slots=2, k_capacity=k_cap)
+    big = srv.submit(decks["small"], (1, 2, 3, 4), 100)
+    missing = srv.submit(str(tmp_path / "no_such_deck"), (1, 1, 1, 1), 100)
+    a = srv.submit(decks["ortho0"], (12, 34, 56, 78), 800)
+    b = srv.submit(decks["ortho0"], (31, 41, 59, 26), 5000)
+    c = srv.submit(decks["ortho0"], (5, 5, 5, 5), 300)
+    srv.cancel(c)  # cancelled while queued: never runs
+    srv.step(200)
+    assert srv.poll(missing)["state"] == srv.REJECTED
+    r = srv.poll(big)
+    assert r["state"] == srv.REJECTED and "k-vector" in r["error"]
+    assert srv.poll(a)["state"] == srv.RUNNING and srv.poll(b)["state"] == srv.RUNNING
+    srv.cancel(b)  # cancelled while running: slot freed, partial result kept
+    rb = srv.poll(b)
+    assert rb["state"] == srv.CANCELLED and rb["moves"] == 200
+    while srv.step(200)[0]:
+        pass
+    assert srv.poll(c)["state"] == srv.CANCELLED and srv.poll(c)["moves"] == 0
+    ra = srv.poll(a)
+    assert ra["state"] == srv.DONE
+    _same(ra, _alone(fmc, decks["ortho0"], (12, 34, 56, 78), 800))
+
+
+def test_serve_memory_budget_limits_admission(fmc, decks):
+    """A budget that holds one slot (plus the admission estimate) admits one request at a time."""
+    probe = fmc.Server(slots=1)
+    probe.submit(decks["small"], (1, 2, 3, 4), 10**6)
+    probe.step(1)
+    slot_bytes, _ = probe.memory()
+    probe.close()
+    assert slot_bytes > 0
+    srv = fmc.Server(slots=4, mem_budget=(64 << 20) + slot_bytes // 2)
+    ids = [srv.submit(decks["small"], (i + 1, 2, 3, 4), 300) for i in range(3)]
+    active_seen = []
+    for _ in range(20):
+        active, queued, _ = srv.step(300)
+        active_seen.append(active)
+        used, budget = srv.memory()
+        assert used <= budget
+        if not active and not queued:
+            break
+    assert all(srv.poll(i)["state"] == srv.DONE for i in ids)
+    assert max(active_seen) == 1
+
+
+def test_serve_deck_cycle_budget_matches_oracle(fmc, oracle_mod, tmp_path):
+    """moves=0: a request runs until its deck's own equilibration + production cycles end, on
+    the same move as the reference loop (gcmc.f:594-736), with the same statistics."""
+    from fastmc_b200 import synth
+
+    d = synth.write_plain_small(str(tmp_path / "short"), cycles=3)
+    seed = (12, 34, 56, 78)
+    orc = oracle_mod.Chain(d, seed=seed)
+    n_ref = orc.run_to_completion(10**6)
+    assert 2000 < n_ref < 10**6
+    srv = fmc.Server(slots=2)
+    rid = srv.submit(d, seed)
+    other = srv.submit(d, (1, 2, 3, 4), 700)
+    for _ in range(200):
+        if not srv.step(900)[0]:
+            break
+    res = srv.poll(rid)
+    assert res["state"] == srv.DONE and res["finished"] == 1.0
+    assert res["moves"] == n_ref
+    ref = orc.stats(0)
+    assert res["prodcount"] == ref["prodcount"]
+    for k in ("N", "E", "EN", "N2", "E2"):
+        assert abs(res[k] - ref[k]) <= 1e-8 * max(abs(ref[k]), 1.0), k
+    assert srv.poll(other)["moves"] == 700 and srv.poll(other)["finished"] == 0.0
