@@ -34,14 +34,16 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="batched", choices=["plain", "batched", "serve"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
-    ap.add_argument("--serve-requests", type=int, default=400)
+    ap.add_argument("--serve-requests", type=int, default=1500)
     ap.add_argument("--serve-slots", type=int, default=296)
     ap.add_argument("--serve-moves", type=int, default=1000, help="moves per slot per serving step")
     ap.add_argument("--serve-kcap", type=int, default=0, help="0: the largest request's K")
-    ap.add_argument("--serve-cycle-scale", type=float, default=0.01,
+    ap.add_argument("--serve-cycle-scale", type=float, default=0.1,
                     help="scale of the U(2k,20k) cycle budgets so that requests finish within the run")
     ap.add_argument("--moves", type=int, default=2000, help="trial moves per chain per step")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="bounded CPU baseline sample")
+    ap.add_argument("--skip-baselines", action="store_true",
+                    help="omit the plain-path and CPU samples (profiling runs of the batched kernel)")
     return ap.parse_args()
 
 
@@ -143,13 +145,13 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def profiled_traffic(kernel):
-    """Per-launch DRAM bytes of `kernel` from the committed ncu summary, or None."""
+def profiled_traffic(kernel, key="traffic_bytes_per_launch"):
+    """A DRAM-bytes figure of `kernel` from its committed ncu summary, or None."""
     p = os.path.join(ROOT, "profiles", f"{kernel}.md")
     if not os.path.exists(p):
         return None
     for line in open(p):
-        if line.strip().startswith("traffic_bytes_per_launch:"):
+        if line.strip().startswith(key + ":"):
             try:
                 return float(line.split(":", 1)[1].split()[0])
             except ValueError:
@@ -351,6 +353,9 @@ def run_batched(args, dist):
         per_launch += args.moves * (inf["K"] * 40 + 4.5 * nrc * 36)
     avg_launch_s = t_dev / args.steps
     achieved = per_launch / avg_launch_s / 1e9
+    # ncu DRAM bytes per chain-move (captured on a 200-move launch), scaled to this launch
+    tpm = profiled_traffic("batch_kernel_batched", "traffic_bytes_per_chain_move")
+    traffic = tpm * n * args.moves if tpm else None
     peak, peak_kind = peaks()
     from fastmc_b200._lib import lib as _l  # noqa: F401
     cb = 1512  # bytes of one chain control block moved each way per step (sizeof(ChainDev))
@@ -374,7 +379,7 @@ def run_batched(args, dist):
                    "l2": "per-chain S(k) is shared-memory resident; frameworks + voxel lists exceed L2 (no flush)",
                    "parallelism": f"replicas{dist.world}"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": profiled_traffic("batch_kernel_batched"), "kernel": "fmc_batch_kernel",
+                     "traffic": traffic, "kernel": "fmc_batch_kernel",
                      "bytes_per_launch": per_launch, "avg_launch_us": avg_launch_s * 1e6,
                      "peak_kind": f"{peak_kind} (hbm_gbs)"},
         "gpu_launches": args.steps,
@@ -382,7 +387,7 @@ def run_batched(args, dist):
                 "d2h_bytes_per_step": n * cb},
         "clocks": clk.summary(),
     }
-    if dist.rank == 0 and dist.world == 1:
+    if dist.rank == 0 and dist.world == 1 and not args.skip_baselines:
         # the plain single-chain GPU path on a sample of the same chains
         sample = list(range(0, n, max(1, n // 8)))[:8]
         pm, pt = 0, 0.0
@@ -454,7 +459,7 @@ def run_serve(args, dist):
     from fastmc_b200 import synth
 
     tmp = tempfile.mkdtemp(prefix="fmcserve")
-    n_pilot, n_req = 64, args.serve_requests
+    n_pilot, n_req = args.serve_slots + 64, args.serve_requests
     reqs = synth.serving_requests(n_pilot + n_req, seed=7 + 1000 * dist.rank)
     for r in reqs:
         r["cycles"] = max(1, int(round(r["cycles"] * args.serve_cycle_scale)))
@@ -468,67 +473,80 @@ def run_serve(args, dist):
     srv = fm.Server(slots=args.serve_slots, device=dist.local, k_capacity=kcap)
     if args.precision == "mixed":
         srv.set_precision(7, recompute_every=1000)
-    # pilot (warm-up): a closed batch of requests measures moves per request and throughput
-    ids = [srv.submit(d, (12, 34, 56, r["id"] % 169)) for d, r in zip(dirs[:n_pilot], reqs[:n_pilot])]
-    p_ms, p_wall = 0.0, time.perf_counter()
+    # pilot (warm-up): more requests than slots at once; the launches that ran with every
+    # slot busy give the server's capacity in moves/s
+    ids = [srv.submit(d, (12, 34, 56, 1 + r["id"] % 168)) for d, r in zip(dirs[:n_pilot], reqs[:n_pilot])]
+    full_ms = []
     while True:
         a, q, ms = srv.step(args.serve_moves)
-        p_ms += ms
+        if a == args.serve_slots:
+            full_ms.append(ms)
         if not a and not q:
             break
-    p_wall = time.perf_counter() - p_wall
     pil = [srv.poll(i) for i in ids]
     moves_per_req = float(np.mean([r["moves"] for r in pil]))
-    # offered load: 90% of the throughput the pilot reached with all its requests resident
-    rate = 0.9 * sum(r["moves"] for r in pil) / max(p_wall, 1e-9) / moves_per_req
-    rate = max(rate, 1.0)
+    capacity = args.serve_slots * args.serve_moves / (float(np.median(full_ms)) / 1000.0) if full_ms else None
+    # offered load: 90% of that capacity
+    rate = 0.9 * capacity / moves_per_req if capacity else 50.0
     rng = np.random.default_rng(99 + dist.rank)
     arrivals = np.cumsum(rng.exponential(1.0 / rate, n_req))
     dist.barrier()
     live = {}
     done_t = {}
     nxt = 0
-    dev_ms, steps, moves_total = 0.0, 0, 0
-    moves_seen = {}
+    dev_ms, steps, occ = 0.0, 0, 0.0
+    log = []  # per step: wall start, wall end, device ms, moves run, active slots
     wall0 = time.perf_counter()
     with ClockSampler(dist.local) as clk:
         while len(done_t) < n_req:
             now = time.perf_counter() - wall0
             while nxt < n_req and arrivals[nxt] <= now:
-                rid = srv.submit(dirs[n_pilot + nxt], (12, 34, 56, reqs[n_pilot + nxt]["id"] % 169))
+                rid = srv.submit(dirs[n_pilot + nxt], (12, 34, 56, 1 + reqs[n_pilot + nxt]["id"] % 168))
                 live[rid] = nxt
                 nxt += 1
             if not live:
                 time.sleep(max(0.0, min(arrivals[nxt] - now, 0.05)))
                 continue
             a, q, ms = srv.step(args.serve_moves)
+            end = time.perf_counter() - wall0
+            log.append((now, end, ms, int(srv.stats()["last_moves"]), a))
             dev_ms += ms
+            occ += a * ms
             steps += 1
-            now = time.perf_counter() - wall0
             for rid in list(live):
                 res = srv.poll(rid)
                 if res["state"] in (srv.DONE, srv.REJECTED, srv.CANCELLED):
-                    done_t[live[rid]] = (now - arrivals[live[rid]], res)
-                    moves_total += int(res["moves"])
+                    done_t[live[rid]] = (end - arrivals[live[rid]], res)
                     del live[rid]
     wall = time.perf_counter() - wall0
     dist.barrier()
     lat = np.array([v[0] for v in done_t.values()])
     rejected = sum(1 for v in done_t.values() if v[1]["state"] != srv.DONE)
-    t_dev = dist.max(dev_ms / 1000.0)
-    t_wall = dist.max(wall)
-    total = dist.sum(moves_total)
+    # loaded window: the steps that started while requests were still arriving; the drain of
+    # the last (longest) requests afterwards is reported separately
+    t_last = float(arrivals[-1])
+    win = [x for x in log if x[0] <= t_last]
+    w_moves = sum(x[3] for x in win)
+    w_dev = sum(x[2] for x in win) / 1000.0
+    w_wall = win[-1][1] if win else 0.0
+    w_occ = sum(x[4] * x[2] for x in win) / max(sum(x[2] for x in win), 1e-9) / args.serve_slots
+    all_moves = sum(x[3] for x in log)
+    t_dev = dist.max(w_dev)
+    t_wall = dist.max(w_wall)
+    total = dist.sum(w_moves)
     used, budget = srv.memory()
+    sstats = srv.stats()
     srv.close()
     # host<->device bytes per step: slot control blocks (SysConst + ChainDev) each way
     return {
         "metric": "MC trial moves/s on 1 B200 (continuous-batching serving); p50/p99 time-to-completion",
-        "value": total / t_dev, "unit": "moves/s", "n_gpus": dist.world, "steps": steps, "warmup": 1,
-        "ms_per_step": t_dev * 1000.0 / max(steps, 1), "higher_is_better": True, "scaling": "weak",
+        "value": total / t_dev, "unit": "moves/s", "n_gpus": dist.world, "steps": len(win), "warmup": 1,
+        "ms_per_step": t_dev * 1000.0 / max(len(win), 1), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
         "data": "synthetic (seeded request generator, FastMC input formats)",
         "config": {"workload": SERVE_WORKLOAD.format(scale=args.serve_cycle_scale, slots=args.serve_slots),
                    "requests": n_req, "pilot_requests": n_pilot, "arrival_rate_hz": rate,
+                   "capacity_moves_per_s": capacity, "offered_load": 0.9,
                    "moves_per_request_mean": moves_per_req, "moves_per_step": args.serve_moves,
                    "precision": args.precision, "deck_generation_s": gen_s, "k_capacity": kcap,
                    "l2": "per-chain S(k) shared-memory resident; frameworks + voxel lists exceed L2 (no flush)",
@@ -536,11 +554,19 @@ def run_serve(args, dist):
         "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                       "mean": float(lat.mean()), "max": float(lat.max())},
         "rejected": rejected,
-        "gpu_launches": steps,
+        "window": {"what": "value/e2e cover the steps started before the last arrival",
+                   "steps": len(win), "moves": w_moves, "device_s": w_dev, "wall_s": w_wall,
+                   "slot_occupancy": w_occ},
+        "whole_run": {"steps": steps, "moves": all_moves, "device_s": dev_ms / 1000.0, "wall_s": wall,
+                      "moves_per_device_s": all_moves / max(dev_ms / 1000.0, 1e-9),
+                      "moves_per_wall_s": all_moves / max(wall, 1e-9),
+                      "slot_occupancy": occ / max(dev_ms, 1e-9) / args.serve_slots},
+        "gpu_launches": len(win),
         "e2e": {"value": total / t_wall, "unit": "moves/s",
                 "h2d_bytes_per_step": args.serve_slots * 2 * 1512, "d2h_bytes_per_step": args.serve_slots * 1512},
         "clocks": clk.summary(),
         "memory": {"slots_bytes_at_end": used, "budget_bytes": budget},
+        "server": sstats,
     }
 
 

@@ -2,6 +2,7 @@
 // chain, the whole move loop of gcmc.f:589-1380 on the device.  Chains that share a framework
 // deck (same FIELD / CONFIG / cut-offs / Ewald parameters) share one device system.
 #pragma once
+#include <functional>
 #include <cuda_runtime.h>
 
 #include <memory>
@@ -91,9 +92,30 @@ cudaError_t launch_batch(const BatchLaunch& L, int smem_bytes, int tab_stride, c
 int batch_smem_bytes(int kmax_K, int tab_sites, int tab_stride);
 cudaError_t configure_batch_kernel(int smem_bytes);
 
+using DevAllocFn = std::function<cudaError_t(void**, size_t)>;
+int fill_sysconst(const HostSystem& H, const DevSystem& S, SysConst& Y, int* tab_sites, std::string& err);
 int make_sysconst(const Chain& ch, SysConst& Y, std::vector<void*>& allocations, int* tab_sites, std::string& err);
+int init_chain_state(const InputDeck& d, const HostSystem& H, const double2* sk_src, double energy0, int sys,
+                     const int* seed, ChainDev& C, const DevAllocFn& alloc, cudaStream_t st, std::string& err);
 int init_chain(const InputDeck& d, const Chain& ch, int sys, const int* seed, ChainDev& C,
                std::vector<void*>& allocations, cudaStream_t st, std::string& err);
+
+// Device memory of one serving slot.  Every allocation comes from a memory pool on the
+// slot's stream, so admitting and retiring slots needs no device-wide synchronisation.
+struct SlotMemory {
+  cudaStream_t st = nullptr;
+  cudaMemPool_t pool = nullptr;
+  std::vector<void*> ptrs;
+  size_t bytes = 0;
+  cudaError_t alloc(void** p, size_t n);
+  void release();  // stream-ordered frees of every allocation
+};
+
+// A serving slot built from a prepared host system: the device system (framework, voxel
+// lists, tables), the framework S(k), the per-system constants and an empty chain, all on
+// mem.st.  Waits once on mem.st for the voxel-list size.
+int build_slot(const HostSystem& h, int slot, const int seed[4], SlotMemory& mem, SysConst& Y, ChainDev& C,
+               std::string& err);
 
 class Batch {
  public:

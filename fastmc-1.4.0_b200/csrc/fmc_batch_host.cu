@@ -29,12 +29,10 @@ std::string system_key(const std::string& dir, const InputDeck& d) {
 
 }  // namespace
 
-// Per-system constants of an opened system chain (its HostSystem, device arrays and the
-// framework S(k), which the chain holds while it has no guests).
-int make_sysconst(const Chain& ch, SysConst& Y, std::vector<void*>& allocations, int* tab_sites, std::string& err) {
-  const HostSystem& H = ch.sys;
+// Per-system constants from the host tables and the device arrays (Y.sk_fw left unset).
+int fill_sysconst(const HostSystem& H, const DevSystem& S, SysConst& Y, int* tab_sites, std::string& err) {
   std::memset(&Y, 0, sizeof(Y));
-  Y.S = ch.dsys.view;
+  Y.S = S;
   Y.nspecies = (int)H.deck.guests.size();
   Y.ntypes = H.ntypes;
   Y.lrc_on = H.lrc_on;
@@ -68,6 +66,15 @@ int make_sysconst(const Chain& ch, SysConst& Y, std::vector<void*>& allocations,
   Y.engunit = H.engunit;
   Y.volm = H.cell.volm;
   Y.statvolm = H.statvolm;
+  return 0;
+}
+
+// Per-system constants of an opened system chain (its HostSystem, device arrays and the
+// framework S(k), which the chain holds while it has no guests).
+int make_sysconst(const Chain& ch, SysConst& Y, std::vector<void*>& allocations, int* tab_sites, std::string& err) {
+  const HostSystem& H = ch.sys;
+  int rc = fill_sysconst(H, ch.dsys.view, Y, tab_sites, err);
+  if (rc) return rc;
   {
     double2* fw = nullptr;
     cudaError_t e = cudaMalloc(&fw, sizeof(double2) * std::max(H.K, 1));
@@ -83,10 +90,9 @@ int make_sysconst(const Chain& ch, SysConst& Y, std::vector<void*>& allocations,
 }
 
 // Parameters (from the chain's own deck) and initial state of one chain of system `sys`;
-// allocates its S(k) (initialised to the framework's) and guest-site segments.
-int init_chain(const InputDeck& d, const Chain& ch, int sys, const int* seed, ChainDev& C,
-             std::vector<void*>& allocations, cudaStream_t st, std::string& err) {
-  const HostSystem& H = ch.sys;
+// allocates its S(k) (a copy of sk_src, the framework's) and guest-site segments.
+int init_chain_state(const InputDeck& d, const HostSystem& H, const double2* sk_src, double energy0, int sys,
+                     const int* seed, ChainDev& C, const DevAllocFn& alloc, cudaStream_t st, std::string& err) {
   std::memset(&C, 0, sizeof(C));
   C.sys = sys;
   C.temp = d.temp;
@@ -111,7 +117,7 @@ int init_chain(const InputDeck& d, const Chain& ch, int sys, const int* seed, Ch
     C.tran_ratio[g] = d.tran_ratio[g];
     C.delrdisp[g] = d.delr;
     C.tran_delr[g] = d.delr;
-    C.energy[g] = ch.spenergy;
+    C.energy[g] = energy0;
   }
   C.rota_ratio = d.rota_ratio;
   C.maxguest = d.maxguest;
@@ -129,24 +135,31 @@ int init_chain(const InputDeck& d, const Chain& ch, int sys, const int* seed, Ch
   C.active = 1;
   C.budget = 0;
   // buffers: S(k) starts as the framework's (empty framework), guest segments per species
-  cudaError_t e = cudaMalloc(&C.sk, sizeof(double2) * std::max(H.K, 1));
-  if (e == cudaSuccess) allocations.push_back(C.sk);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(C.sk, ch.sk, sizeof(double2) * H.K, cudaMemcpyDeviceToDevice, st);
+  cudaError_t e = alloc((void**)&C.sk, sizeof(double2) * std::max(H.K, 1));
+  if (e == cudaSuccess) e = cudaMemcpyAsync(C.sk, sk_src, sizeof(double2) * H.K, cudaMemcpyDeviceToDevice, st);
   int off = 0;
   for (int g = 0; g < ng; g++) {
     C.seg_off[g] = off;
     C.seg_cap[g] = d.maxguest;
     off += d.maxguest;
   }
-  if (e == cudaSuccess) e = cudaMalloc(&C.gsite, sizeof(double4) * std::max(off, 1));
-  if (e == cudaSuccess) allocations.push_back(C.gsite);
-  if (e == cudaSuccess) e = cudaMalloc(&C.gtype, sizeof(int) * std::max(off, 1));
-  if (e == cudaSuccess) allocations.push_back(C.gtype);
+  if (e == cudaSuccess) e = alloc((void**)&C.gsite, sizeof(double4) * std::max(off, 1));
+  if (e == cudaSuccess) e = alloc((void**)&C.gtype, sizeof(int) * std::max(off, 1));
   if (e != cudaSuccess) {
     err = std::string("batch allocation failed: ") + cudaGetErrorString(e);
     return -100 - (int)e;
   }
   return 0;
+}
+
+int init_chain(const InputDeck& d, const Chain& ch, int sys, const int* seed, ChainDev& C,
+               std::vector<void*>& allocations, cudaStream_t st, std::string& err) {
+  DevAllocFn alloc = [&allocations](void** p, size_t n) {
+    cudaError_t e = cudaMalloc(p, n);
+    if (e == cudaSuccess) allocations.push_back(*p);
+    return e;
+  };
+  return init_chain_state(d, ch.sys, ch.sk, ch.spenergy, sys, seed, C, alloc, st, err);
 }
 
 Batch::~Batch() {

@@ -141,7 +141,7 @@ GuestView Chain::guest_view() const {
   return G;
 }
 
-int Chain::open(const std::string& dir, const int seed[4], int dev, std::string& err) {
+int prepare_system(const std::string& dir, HostSystem& sys, std::string& err) {
   InputDeck deck;
   int rc = read_input_deck(dir, deck, err);
   if (rc) return rc;
@@ -154,8 +154,20 @@ int Chain::open(const std::string& dir, const int seed[4], int dev, std::string&
       err = "framework atoms must be frozen (rigid framework)";
       return -6;
     }
-  rc = build_host_system(deck, sys, err);
+  return build_host_system(deck, sys, err);
+}
+
+int Chain::open(const std::string& dir, const int seed[4], int dev, std::string& err) {
+  HostSystem h;
+  int rc = prepare_system(dir, h, err);
   if (rc) return rc;
+  return open_prepared(std::move(h), seed, dev, err);
+}
+
+int Chain::open_prepared(HostSystem&& prepared, const int seed[4], int dev, std::string& err) {
+  sys = std::move(prepared);
+  const InputDeck& deck = sys.deck;
+  int rc = 0;
   device = dev;
   dsys.device = dev;
   FMC_CUDA(cudaSetDevice(dev));

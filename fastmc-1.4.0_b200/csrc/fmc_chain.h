@@ -33,6 +33,10 @@ struct Species {
   std::vector<double> xyz;  // 3*nmol*nsite, molecule-major (framwkxxx of the reference)
 };
 
+// Host part of opening a chain: reads the deck, checks what the GPU path supports and
+// builds the host tables.  Thread-safe (no device calls).
+int prepare_system(const std::string& dir, HostSystem& sys, std::string& err);
+
 class Chain {
  public:
   HostSystem sys;
@@ -80,6 +84,8 @@ class Chain {
 
   ~Chain();
   int open(const std::string& dir, const int seed[4], int device, std::string& err);
+  // open from a system already built on the host by prepare_system (the device part only)
+  int open_prepared(HostSystem&& prepared, const int seed[4], int device, std::string& err);
   GuestView guest_view() const;
   // Energies of one trial pass.  old_xyz/new_xyz are interleaved xyz of the molecule's sites.
   int pass(int move, int g, int mol, const double* old_xyz, const double* new_xyz, double out[3]);

@@ -388,7 +388,7 @@ __global__ void __launch_bounds__(kVoxThreads) fmc_voxel_fill_kernel(CellGeom ce
     __syncthreads();
     if (flag) {
       int pos = base + running + woff[warp] + __popc(mask & ((1u << lane) - 1u));
-      atoms[pos] = j;
+      if (atoms) atoms[pos] = j;
       if (atoms16) atoms16[pos] = (unsigned short)j;
       xyzq[pos] = a;
       vtype[pos] = (unsigned char)ftype[j];

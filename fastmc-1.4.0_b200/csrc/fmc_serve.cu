@@ -1,13 +1,23 @@
 // Serving: isotherm-point requests (a FastMC input deck + seed + budget) run as chains of
-// the persistent batched kernel with continuous batching.  Each step admits queued requests
-// into free slots while the device-memory budget allows (every slot holds its own framework
-// system and chain state), advances every active slot by up to `moves` moves in one launch,
-// and retires the chains that have used their budget (a move count, or with 0 the deck's own
-// equilibration + production cycles), freeing their slots and memory for the next step.  The reference runs one such isotherm point per MPI rank (gcmc.f:334-417).
+// the persistent batched kernel with continuous batching.  Host worker threads parse each
+// queued request's deck and build its host tables ahead of time; each step admits prepared
+// requests from the front of the queue into free slots while the device-memory budget allows
+// (every slot holds its own framework system and chain state), advances every active slot by
+// up to `moves` moves in one launch, and retires the chains that have used their budget (a
+// move count, or with 0 the deck's own equilibration + production cycles), freeing their
+// slots and memory for the next step.  The reference runs one such isotherm point per MPI
+// rank (gcmc.f:334-417).
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
 #include <cstring>
 #include <deque>
 #include <memory>
+#include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/fastmc_b200.h"
@@ -15,6 +25,12 @@
 
 namespace fmc {
 void set_last_error(const std::string& msg);
+
+namespace {
+double now_ms() {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+}  // namespace
 
 class Server {
  public:
@@ -26,36 +42,62 @@ class Server {
     int state = kQueued, slot = -1;
     double result[32] = {0};
     std::string err;
+    // host preparation (worker threads): 0 pending, 1 ready
+    std::atomic<int> prepared{0};
+    int prep_rc = 0;
+    std::string prep_err;
+    std::unique_ptr<HostSystem> host;
+    size_t bytes_estimate = 0;
   };
   struct Slot {
     int request = -1;
-    std::unique_ptr<Chain> sys;
-    std::vector<void*> allocs;
-    size_t bytes = 0;
+    SlotMemory mem;
   };
 
-  int device = 0;
-  cudaStream_t st = nullptr;
   // phase tables in shared memory hold the old + new sites of one trial of up to
   // kServeMaxSites-site guests with kmax <= 32 per axis
   static constexpr int kServeMaxSites = 4;
+  int device = 0;
+  cudaStream_t st = nullptr;
   int nslots = 0, kcap = 0, tab_sites = 2 * kServeMaxSites, tab_stride = 0, smem = 0;
-  size_t budget = 0, used = 0, slot_estimate = 64u << 20;
+  size_t budget = 0, used = 0;
+  cudaMemPool_t pool = nullptr;
   int mixed = 0;
   long long recompute_every = 0;
   std::vector<Slot> slots;
-  std::vector<Request> reqs;
-  std::deque<int> queue;
+  std::vector<std::unique_ptr<Request>> reqs;  // the vector is guarded by mu; entries are stable
+  std::deque<int> queue;                       // admission order (caller's thread only)
   SysConst* h_sys = nullptr;
   SysConst* d_sys = nullptr;
   ChainDev* h_chains = nullptr;
   ChainDev* d_chains = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // worker pool
+  std::mutex mu;
+  std::condition_variable cv;
+  std::deque<int> prep_queue;
+  std::vector<std::thread> workers;
+  bool stopping = false;
+  // accounting
+  long long admitted = 0, retired = 0, launches = 0, moves_run = 0, last_moves = 0;
+  double admit_ms = 0, launch_ms = 0, wait_ms = 0;
+  std::atomic<long long> prep_us{0};
 
   ~Server() {
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      stopping = true;
+    }
+    cv.notify_all();
+    for (auto& t : workers) t.join();
     if (!st) return;
     cudaSetDevice(device);
     cudaStreamSynchronize(st);
     for (int i = 0; i < nslots; i++) release(i);
+    cudaStreamSynchronize(st);
+    if (pool) cudaMemPoolDestroy(pool);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
     if (d_sys) cudaFree(d_sys);
     if (d_chains) cudaFree(d_chains);
     if (h_sys) cudaFreeHost(h_sys);
@@ -63,7 +105,7 @@ class Server {
     cudaStreamDestroy(st);
   }
 
-  int open(int n, int dev, size_t mem_budget, int k_cap, std::string& err) {
+  int open(int n, int dev, size_t mem_budget, int k_cap, int nworkers, std::string& err) {
     device = dev;
     nslots = n;
     kcap = (k_cap + 3) & ~3;
@@ -80,37 +122,125 @@ class Server {
       err = "k-vector capacity exceeds the shared-memory budget of one CTA";
       return -9;
     }
-    if (configure_batch_kernel(smem) != cudaSuccess) {
-      err = "cannot configure the batched kernel";
+    if (configure_batch_kernel(smem) != cudaSuccess || configure_kernels() != cudaSuccess ||
+        configure_recip_kernels() != cudaSuccess) {
+      err = "cannot configure the kernels";
       return -100;
     }
+    // slot memory: a pool of its own that keeps freed blocks for the next admissions
+    cudaMemPoolProps props;
+    std::memset(&props, 0, sizeof(props));
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
+      err = "cannot create the slot memory pool";
+      return -100;
+    }
+    unsigned long long keep = ~0ull;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
     slots.resize(n);
+    for (auto& sl : slots) {
+      sl.mem.st = st;
+      sl.mem.pool = pool;
+    }
     cudaError_t e = cudaMallocHost(&h_sys, sizeof(SysConst) * n);
     if (e == cudaSuccess) e = cudaMallocHost(&h_chains, sizeof(ChainDev) * n);
     if (e == cudaSuccess) e = cudaMalloc(&d_sys, sizeof(SysConst) * n);
     if (e == cudaSuccess) e = cudaMalloc(&d_chains, sizeof(ChainDev) * n);
+    if (e == cudaSuccess) e = cudaEventCreate(&ev0);
+    if (e == cudaSuccess) e = cudaEventCreate(&ev1);
     if (e != cudaSuccess) {
       err = std::string("server allocation failed: ") + cudaGetErrorString(e);
       return -100 - (int)e;
     }
     std::memset(h_sys, 0, sizeof(SysConst) * n);
     std::memset(h_chains, 0, sizeof(ChainDev) * n);
+    for (int w = 0; w < nworkers; w++) workers.emplace_back([this] { worker(); });
     return 0;
   }
 
+  // Host preparation of one request: deck, host tables and the serving capacity checks.
+  void prepare(Request& r) {
+    const double t0 = now_ms();
+    auto h = std::make_unique<HostSystem>();
+    std::string err;
+    int rc = prepare_system(r.dir, *h, err);
+    if (!rc)
+      for (auto& g : h->deck.guests)
+        if (g.nmols) {
+          rc = -8;
+          err = "serving starts chains from an empty framework (NUMMOLS 0 for guests)";
+        }
+    if (!rc && h->K > kcap) {
+      rc = -9;
+      err = "the request's k-vector count exceeds the server's capacity";
+    }
+    if (!rc && h->deck.kmax[0] + h->deck.kmax[1] + h->deck.kmax[2] + 3 > tab_stride) {
+      rc = -9;
+      err = "the request's kmax exceeds the server's phase-table capacity";
+    }
+    if (!rc)
+      for (auto& g : h->deck.guests)
+        if (g.nsite > kServeMaxSites) {
+          rc = -9;
+          err = "a guest of the request has more sites than the server's capacity";
+        }
+    r.prep_rc = rc;
+    r.prep_err = err;
+    if (!rc) {
+      r.bytes_estimate = slot_bytes_estimate(*h);
+      r.host = std::move(h);
+    }
+    prep_us += (long long)((now_ms() - t0) * 1000.0);
+    r.prepared.store(1, std::memory_order_release);
+  }
+
+  // Worker threads: host preparation of queued requests, in submission order.
+  void worker() {
+    for (;;) {
+      Request* r = nullptr;
+      {
+        std::unique_lock<std::mutex> lk(mu);
+        cv.wait(lk, [this] { return stopping || !prep_queue.empty(); });
+        if (stopping) return;
+        r = reqs[prep_queue.front()].get();
+        prep_queue.pop_front();
+      }
+      prepare(*r);
+    }
+  }
+
+  Request& req(int id) {
+    std::lock_guard<std::mutex> lk(mu);
+    return *reqs[id];
+  }
+
+  int nreqs() {
+    std::lock_guard<std::mutex> lk(mu);
+    return (int)reqs.size();
+  }
+
   int submit(const std::string& dir, const int* seed, long long moves) {
-    Request r;
-    r.dir = dir;
-    std::memcpy(r.seed, seed, sizeof(r.seed));
-    r.moves = moves;
-    reqs.push_back(r);
-    queue.push_back((int)reqs.size() - 1);
-    return (int)reqs.size() - 1;
+    auto r = std::make_unique<Request>();
+    r->dir = dir;
+    std::memcpy(r->seed, seed, sizeof(r->seed));
+    r->moves = moves;
+    int id;
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      reqs.push_back(std::move(r));
+      id = (int)reqs.size() - 1;
+      if (!workers.empty()) prep_queue.push_back(id);
+    }
+    cv.notify_one();
+    queue.push_back(id);
+    return id;
   }
 
   int cancel(int id) {
-    if (id < 0 || id >= (int)reqs.size()) return -1;
-    Request& r = reqs[id];
+    if (id < 0 || id >= nreqs()) return -1;
+    Request& r = req(id);
     if (r.state == kQueued) {
       for (auto it = queue.begin(); it != queue.end(); ++it)
         if (*it == id) {
@@ -128,13 +258,22 @@ class Server {
 
   void release(int i) {
     Slot& s = slots[i];
-    for (void* p : s.allocs) cudaFree(p);
-    s.allocs.clear();
-    s.sys.reset();
-    used -= std::min(used, s.bytes);
-    s.bytes = 0;
+    used -= std::min(used, s.mem.bytes);
+    s.mem.release();
     s.request = -1;
     h_chains[i].active = 0;
+  }
+
+  // Device bytes of a slot for admission: voxel entries from the framework's mean density
+  // (+15%), plus atoms, tables, k-vector tables and guest segments.
+  static size_t slot_bytes_estimate(const HostSystem& h) {
+    const double lim = std::sqrt(h.vox_lim2);
+    const double per_vox = std::min((double)h.nf, h.nf * (4.0 / 3.0 * kPi * lim * lim * lim) / h.cell.volm);
+    const double nv = (double)h.nvox[0] * h.nvox[1] * h.nvox[2];
+    double b = 1.15 * nv * per_vox * (sizeof(double4) + 1) + 4.0 * (nv + 1) + 36.0 * h.nf;
+    b += 12.0 * (h.erc.size() + h.vvv.size()) + 4.0 * h.pair_row.size() + 60.0 * h.K;
+    b += 36.0 * h.deck.maxguest * h.deck.guests.size();
+    return (size_t)b + (64u << 10);
   }
 
   void snapshot(int i, Request& r) {
@@ -161,78 +300,78 @@ class Server {
     v[30] = (double)C.gcmccount;
   }
 
-  // Opens request `id` into free slot `i`; returns bytes used, or 0 (and marks the request
-  // rejected) on failure.
+  void reject(Request& r, int rc, const std::string& err) {
+    r.state = kRejected;
+    r.err = err;
+    r.result[1] = rc;
+    r.host.reset();
+  }
+
+  // Builds prepared request `id` into free slot `i` (stream-ordered, one wait for the voxel
+  // list size); returns the slot's device bytes, or 0 (and marks the request rejected).
   size_t admit(int id, int i) {
-    Request& r = reqs[id];
+    Request& r = req(id);
     Slot& s = slots[i];
-    size_t f0 = 0, f1 = 0, tot = 0;
-    cudaMemGetInfo(&f0, &tot);
+    if (r.prep_rc) {
+      reject(r, r.prep_rc, r.prep_err);
+      return 0;
+    }
     std::string err;
-    InputDeck deck;
-    int rc = read_input_deck(r.dir, deck, err);
-    if (!rc)
-      for (auto& g : deck.guests)
-        if (g.nmols) {
-          rc = -8;
-          err = "serving starts chains from an empty framework (NUMMOLS 0 for guests)";
-        }
-    if (!rc) {
-      s.sys = std::make_unique<Chain>();
-      rc = s.sys->open(r.dir, r.seed, device, err);
-    }
-    if (!rc && s.sys->sys.K > kcap) {
-      rc = -9;
-      err = "the request's k-vector count exceeds the server's capacity";
-    }
-    if (!rc && s.sys->sys.deck.kmax[0] + s.sys->sys.deck.kmax[1] + s.sys->sys.deck.kmax[2] + 3 > tab_stride) {
-      rc = -9;
-      err = "the request's kmax exceeds the server's phase-table capacity";
-    }
-    if (!rc)
-      for (auto& g : deck.guests)
-        if (g.nsite > kServeMaxSites) {
-          rc = -9;
-          err = "a guest of the request has more sites than the server's capacity";
-        }
-    int ts = 0;
-    if (!rc) rc = make_sysconst(*s.sys, h_sys[i], s.allocs, &ts, err);
-    if (!rc) rc = init_chain(deck, *s.sys, i, r.seed, h_chains[i], s.allocs, st, err);
+    int rc = build_slot(*r.host, i, r.seed, s.mem, h_sys[i], h_chains[i], err);
+    r.host.reset();
     if (rc) {
-      for (void* p : s.allocs) cudaFree(p);
-      s.allocs.clear();
-      s.sys.reset();
+      s.mem.release();
       std::memset(&h_chains[i], 0, sizeof(ChainDev));
-      r.state = kRejected;
-      r.err = err;
-      r.result[1] = rc;
+      reject(r, rc, err);
       return 0;
     }
     h_chains[i].budget = r.moves;
-    cudaStreamSynchronize(st);
-    cudaMemGetInfo(&f1, &tot);
-    s.bytes = f0 > f1 ? f0 - f1 : 0;
     s.request = id;
     r.state = kRunning;
     r.slot = i;
-    slot_estimate = std::max(slot_estimate, s.bytes);
-    return s.bytes;
+    admitted++;
+    return s.mem.bytes;
   }
 
   int step(int moves, int* n_active, int* n_queued, float* ms, std::string& err) {
     cudaSetDevice(device);
-    // admission: FIFO, while a slot is free and the memory budget holds
-    for (int i = 0; i < nslots && !queue.empty(); i++) {
-      if (slots[i].request >= 0) continue;
-      if (used + slot_estimate > budget) break;
-      int id = queue.front();
-      queue.pop_front();
-      used += admit(id, i);
-      if (reqs[id].state != kRunning) i--;  // slot still free
-    }
     int active = 0;
     for (int i = 0; i < nslots; i++) active += slots[i].request >= 0;
+    // admission: FIFO, while a slot is free, the front request is prepared and the memory
+    // budget holds.  With nothing running, wait for the front request's preparation.
+    const double t0 = now_ms();
+    for (int i = 0; i < nslots && !queue.empty(); i++) {
+      if (slots[i].request >= 0) continue;
+      const int id = queue.front();
+      Request& r = req(id);
+      if (workers.empty()) {
+        prepare(r);
+      } else if (!r.prepared.load(std::memory_order_acquire)) {
+        if (active) break;
+        const double w0 = now_ms();
+        while (!r.prepared.load(std::memory_order_acquire)) std::this_thread::sleep_for(std::chrono::microseconds(200));
+        wait_ms += now_ms() - w0;
+      }
+      if (!r.prep_rc && used + r.bytes_estimate > budget) {
+        if (r.bytes_estimate > budget) {
+          queue.pop_front();
+          reject(r, -10, "the request's device footprint exceeds the server's memory budget");
+          i--;
+          continue;
+        }
+        break;  // wait for retirements
+      }
+      queue.pop_front();
+      used += admit(id, i);
+      if (r.state == kRunning) active++;
+      else i--;  // slot still free
+    }
+    admit_ms += now_ms() - t0;
     float t = 0.f;
+    long long before = 0;
+    for (int i = 0; i < nslots; i++)
+      if (slots[i].request >= 0) before += h_chains[i].moves_done;
+    last_moves = 0;
     if (active) {
       cudaError_t e = cudaMemcpyAsync(d_sys, h_sys, sizeof(SysConst) * nslots, cudaMemcpyHostToDevice, st);
       if (e == cudaSuccess)
@@ -246,22 +385,24 @@ class Server {
       L.kmax_smem = kcap;
       L.mixed = mixed;
       L.recompute_every = recompute_every;
-      cudaEvent_t a, b;
-      cudaEventCreate(&a);
-      cudaEventCreate(&b);
-      if (e == cudaSuccess) e = cudaEventRecord(a, st);
+      if (e == cudaSuccess) e = cudaEventRecord(ev0, st);
       if (e == cudaSuccess) e = launch_batch(L, smem, tab_stride, st);
-      if (e == cudaSuccess) e = cudaEventRecord(b, st);
+      if (e == cudaSuccess) e = cudaEventRecord(ev1, st);
       if (e == cudaSuccess)
         e = cudaMemcpyAsync(h_chains, d_chains, sizeof(ChainDev) * nslots, cudaMemcpyDeviceToHost, st);
       if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-      if (e == cudaSuccess) cudaEventElapsedTime(&t, a, b);
-      cudaEventDestroy(a);
-      cudaEventDestroy(b);
+      if (e == cudaSuccess) cudaEventElapsedTime(&t, ev0, ev1);
       if (e != cudaSuccess) {
         err = std::string("serving launch failed: ") + cudaGetErrorString(e);
         return -100 - (int)e;
       }
+      launches++;
+      launch_ms += t;
+      long long after = 0;
+      for (int i = 0; i < nslots; i++)
+        if (slots[i].request >= 0) after += h_chains[i].moves_done;
+      last_moves = after - before;
+      moves_run += last_moves;
     }
     // retirement
     for (int i = 0; i < nslots; i++) {
@@ -269,11 +410,12 @@ class Server {
       if (id < 0) continue;
       const ChainDev& C = h_chains[i];
       if ((C.budget > 0 && C.moves_done >= C.budget) || !C.lgchk || C.status) {
-        Request& r = reqs[id];
+        Request& r = req(id);
         snapshot(i, r);
         r.state = C.status ? kRejected : kDone;
         if (C.status) r.err = C.status == 75 ? "too many atoms in specified system" : "unsupported move drawn";
         release(i);
+        retired++;
       }
     }
     if (n_active) *n_active = active;
@@ -298,7 +440,9 @@ int fmc_server_open(int slots, int device, long long mem_budget, int k_capacity,
   }
   fmc_server* s = new fmc_server();
   std::string err;
-  int rc = s->impl.open(slots, device, (size_t)mem_budget, k_capacity, err);
+  unsigned hw = std::thread::hardware_concurrency();
+  int nworkers = (int)std::max(1u, std::min(8u, hw > 1 ? hw - 1 : 1u));
+  int rc = s->impl.open(slots, device, (size_t)mem_budget, k_capacity, nworkers, err);
   if (rc) {
     delete s;
     *out = nullptr;
@@ -350,11 +494,11 @@ int fmc_server_step(fmc_server* s, int moves, int* active, int* queued, float* d
 }
 
 int fmc_server_poll(fmc_server* s, int request_id, int* state, double* out) {
-  if (!s || request_id < 0 || request_id >= (int)s->impl.reqs.size()) {
+  if (!s || request_id < 0 || request_id >= s->impl.nreqs()) {
     fmc::set_last_error("bad server handle or request id");
     return -1;
   }
-  const fmc::Server::Request& r = s->impl.reqs[request_id];
+  const fmc::Server::Request& r = s->impl.req(request_id);
   if (state) *state = r.state;
   if (out) std::memcpy(out, r.result, sizeof(r.result));
   if (r.state == fmc::Server::kRejected) fmc::set_last_error(r.err);
@@ -368,6 +512,25 @@ int fmc_server_memory(fmc_server* s, long long* used, long long* budget) {
   }
   if (used) *used = (long long)s->impl.used;
   if (budget) *budget = (long long)s->impl.budget;
+  return 0;
+}
+
+int fmc_server_stats(fmc_server* s, double* out) {
+  if (!s || !out) {
+    fmc::set_last_error("bad server handle");
+    return -1;
+  }
+  const fmc::Server& v = s->impl;
+  out[0] = (double)v.admitted;
+  out[1] = (double)v.retired;
+  out[2] = (double)v.launches;
+  out[3] = v.admit_ms;
+  out[4] = v.launch_ms;
+  out[5] = v.wait_ms;
+  out[6] = (double)v.prep_us.load() / 1000.0;
+  out[7] = (double)v.workers.size();
+  out[8] = (double)v.moves_run;
+  out[9] = (double)v.last_moves;
   return 0;
 }
 

@@ -276,6 +276,12 @@ class Server:
             res["error"] = lib().fmc_last_error().decode()
         return res
 
+    def stats(self):
+        out = np.zeros(10)
+        check(lib().fmc_server_stats(self.h, dp(out)))
+        return dict(zip(["admitted", "retired", "launches", "admit_ms", "launch_ms", "prep_wait_ms", "prep_ms",
+                         "workers", "moves", "last_moves"], out.tolist()))
+
     def memory(self):
         u, b = ctypes.c_longlong(0), ctypes.c_longlong(0)
         check(lib().fmc_server_memory(self.h, ctypes.byref(u), ctypes.byref(b)))

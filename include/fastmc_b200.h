@@ -162,6 +162,12 @@ int fmc_server_step(fmc_server* s, int moves, int* active, int* queued, float* d
  * species-1 <N>,<E>,<EN>,<N^2>,<E^2>, gcmccount, 0. */
 int fmc_server_poll(fmc_server* s, int request_id, int* state, double* out);
 int fmc_server_memory(fmc_server* s, long long* used, long long* budget);
+/* out[0..9]: requests admitted, retired, launches, host ms spent admitting (device set-up of
+ * new slots, incl. waits), device ms of the launches, ms waited for host preparation with
+ * nothing running, worker ms preparing decks (summed over threads), worker threads, trial
+ * moves run in all launches, trial moves run in the last step's launch.  Deck parsing and
+ * host tables run on worker threads ahead of admission. */
+int fmc_server_stats(fmc_server* s, double* out);
 
 /* Launch accounting and timing of the plain path.  enable != 0 turns on CUDA-event timing of
  * every trial-pass kernel on the chain's stream (enable < 0 also clears the counters).

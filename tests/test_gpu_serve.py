@@ -79,14 +79,15 @@ def test_serve_cancel_and_reject(fmc, decks, tmp_path):
 
 
 def test_serve_memory_budget_limits_admission(fmc, decks):
-    """A budget that holds one slot (plus the admission estimate) admits one request at a time."""
+    """A budget that holds one slot admits one request at a time; a request larger than the
+    whole budget is rejected."""
     probe = fmc.Server(slots=1)
     probe.submit(decks["small"], (1, 2, 3, 4), 10**6)
     probe.step(1)
     slot_bytes, _ = probe.memory()
     probe.close()
     assert slot_bytes > 0
-    srv = fmc.Server(slots=4, mem_budget=(64 << 20) + slot_bytes // 2)
+    srv = fmc.Server(slots=4, mem_budget=int(1.5 * slot_bytes))
     ids = [srv.submit(decks["small"], (i + 1, 2, 3, 4), 300) for i in range(3)]
     active_seen = []
     for _ in range(20):
@@ -98,6 +99,11 @@ def test_serve_memory_budget_limits_admission(fmc, decks):
             break
     assert all(srv.poll(i)["state"] == srv.DONE for i in ids)
     assert max(active_seen) == 1
+    tiny = fmc.Server(slots=2, mem_budget=1 << 20)
+    rid = tiny.submit(decks["small"], (1, 2, 3, 4), 100)
+    tiny.step(100)
+    r = tiny.poll(rid)
+    assert r["state"] == tiny.REJECTED and "memory budget" in r["error"]
 
 
 def test_serve_deck_cycle_budget_matches_oracle(fmc, oracle_mod, tmp_path):
