@@ -587,6 +587,9 @@ __device__ __forceinline__ void recompute_sk(const DevSystem& S, const SysConst&
   }
 }
 
+// kMixed: the mixed-precision build (FP32 components per L.mixed, FP64 re-checks); the FP64
+// build carries none of that code.
+template <bool kMixed>
 __global__ void __launch_bounds__(kBatchThreads, 2) fmc_batch_kernel(BatchLaunch L, int tab_stride) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ ChainDev C;
@@ -613,7 +616,7 @@ __global__ void __launch_bounds__(kBatchThreads, 2) fmc_batch_kernel(BatchLaunch
   const SysConst& Y = Ysm;
   const int K = S.K, Kmax = L.kmax_smem, nseg = Y.nspecies;
   const int nt1 = S.ntypes + 1;
-  const bool mixed = L.mixed != 0;
+  constexpr bool mixed = kMixed;
   for (int i = tid; i < nt1 * nt1; i += blockDim.x) prow_s[i] = S.pair_row[i];
   double2* Sk = reinterpret_cast<double2*>(smem_raw);
   double2* Sn = Sk + Kmax;
@@ -796,11 +799,17 @@ int batch_smem_bytes(int kmax_K, int tab_sites, int tab_stride) {
 }
 
 cudaError_t configure_batch_kernel(int smem_bytes) {
-  return cudaFuncSetAttribute(fmc_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
+  cudaError_t e = cudaFuncSetAttribute(fmc_batch_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(fmc_batch_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
+  return e;
 }
 
 cudaError_t launch_batch(const BatchLaunch& L, int smem_bytes, int tab_stride, cudaStream_t st) {
-  fmc_batch_kernel<<<L.nchains, kBatchThreads, smem_bytes, st>>>(L, tab_stride);
+  if (L.mixed)
+    fmc_batch_kernel<true><<<L.nchains, kBatchThreads, smem_bytes, st>>>(L, tab_stride);
+  else
+    fmc_batch_kernel<false><<<L.nchains, kBatchThreads, smem_bytes, st>>>(L, tab_stride);
   return cudaGetLastError();
 }
 
