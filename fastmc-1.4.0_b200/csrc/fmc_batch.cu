@@ -45,10 +45,41 @@ __device__ double lrc_device(const SysConst& Y, const int* numtyp) {
   return e;
 }
 
+// duni (gcmc.f:2712-2805) with ir, jr and c held in registers across a run of draws; the
+// arithmetic is duni_next's, draw for draw.
+struct DuniLocal {
+  float* u;
+  float c;
+  int ir, jr;
+  __device__ explicit DuniLocal(Duni& d) : u(d.u), c(d.c), ir(d.ir), jr(d.jr) {}
+  __device__ void store(Duni& d) const {
+    d.c = c;
+    d.ir = ir;
+    d.jr = jr;
+  }
+  __device__ double next() {
+    const float cd = 7654321.0f / 16777216.0f, cm = 16777213.0f / 16777216.0f;
+    float uni = u[ir - 1] - u[jr - 1];
+    if (uni < 0.0f) uni = uni + 1.0f;
+    u[ir - 1] = uni;
+    ir = ir - 1;
+    if (ir == 0) ir = 97;
+    jr = jr - 1;
+    if (jr == 0) jr = 97;
+    c = c - cd;
+    if (c < 0.0f) c = c + cm;
+    uni = uni - c;
+    if (uni < 0.0f) uni = uni + 1.0f;
+    return (double)uni;
+  }
+};
+
 // Thread 0: bookkeeping of gcmc.f:594-736 (production / termination every 400 moves),
 // random choices and the trial sites.
+template <bool kProf>
 __device__ __noinline__ void move_begin(ChainDev& C, const SysConst& Y, const DevSystem& S, MoveSmem& M) {
-  C.prof[7] -= clock64();
+  if (kProf) C.prof[7] -= clock64();
+  DuniLocal R(C.rng);  // written back before every return
   C.gcmccount++;
   if (C.gcmccount % 400 == 0) {
     int totalguests = 0;
@@ -78,8 +109,8 @@ __device__ __noinline__ void move_begin(ChainDev& C, const SysConst& Y, const De
   }
   const int ng = Y.nspecies;
   int g = 0;
-  if (ng > 1) g = (int)floor(duni_next(C.rng) * ng);
-  double randmov = duni_next(C.rng);
+  if (ng > 1) g = (int)floor(R.next() * ng);
+  double randmov = R.next();
   const double* c = C.mvcum[g];
   int mtype;
   if (randmov < c[0]) mtype = kInsert;
@@ -111,7 +142,7 @@ __device__ __noinline__ void move_begin(ChainDev& C, const SysConst& Y, const De
     else if (C.rota_rotangle > kMinAngle) C.rota_rotangle = C.rota_rotangle * 0.95;
   }
   if (nmols == 0) mtype = kInsert;
-  C.prof[7] += clock64();  // minus the stamp taken at entry: selection + adaptation
+  if (kProf) C.prof[7] += clock64();  // minus the stamp taken at entry: selection + adaptation
   M.mtype = mtype;
   M.g = g;
   M.ns = ns;
@@ -126,27 +157,29 @@ __device__ __noinline__ void move_begin(ChainDev& C, const SysConst& Y, const De
   M.recheck = 0;
   if (mtype < 0) {
     C.status = 3;
+    R.store(C.rng);
     return;
   }
   double* x = M.x;
   double* y = M.y;
   double* z = M.z;
-  C.prof[8] -= clock64();  // trial generation and site loads
+  if (kProf) C.prof[8] -= clock64();  // trial generation and site loads
   if (mtype == kInsert) {
     C.ins_count++;
     if ((C.totatm - C.framatm) + ns >= C.maxguest || (nmols + 1) * ns > C.seg_cap[g]) {
       C.status = 75;
+      R.store(C.rng);
       return;
     }
     double r[7];
-    for (int i = 0; i < 7; i++) r[i] = duni_next(C.rng);
+    for (int i = 0; i < 7; i++) r[i] = R.next();
     trial_insert(S.cell, P.tx, P.ty, P.tz, ns, r, x, y, z);
     M.nnew = ns;
     for (int i = 0; i < ns; i++) C.numtyp[P.type[i]]++;
     M.need_lrc = 1;
   } else if (mtype == kDelete) {
     C.del_count++;
-    int randchoice = (int)floor(duni_next(C.rng) * nmols) + 1;
+    int randchoice = (int)floor(R.next() * nmols) + 1;
     M.randchoice = randchoice;
     M.mol = randchoice - 1;
     M.ex_lo = C.seg_off[g] + M.mol * ns;
@@ -164,25 +197,25 @@ __device__ __noinline__ void move_begin(ChainDev& C, const SysConst& Y, const De
     double r[7], dis_delr, dis_rot;
     if (mtype == kTranslate) {
       C.tran_count[g]++;
-      r[0] = duni_next(C.rng);
-      r[1] = duni_next(C.rng);
-      r[2] = duni_next(C.rng);
+      r[0] = R.next();
+      r[1] = R.next();
+      r[2] = R.next();
       r[3] = r[4] = r[5] = r[6] = 0.0;
       dis_delr = C.tran_delr[g];
       dis_rot = 0.0;
     } else if (mtype == kRotate) {
       C.rota_count++;
       r[0] = r[1] = r[2] = 0.5;
-      for (int i = 3; i < 7; i++) r[i] = duni_next(C.rng);
+      for (int i = 3; i < 7; i++) r[i] = R.next();
       dis_delr = 0.0;
       dis_rot = C.rota_rotangle;
     } else {
       C.disp_count[g]++;
-      for (int i = 0; i < 7; i++) r[i] = duni_next(C.rng);
+      for (int i = 0; i < 7; i++) r[i] = R.next();
       dis_delr = C.delrdisp[g];
       dis_rot = C.rotangle;
     }
-    int randchoice = (int)floor(duni_next(C.rng) * nmols) + 1;
+    int randchoice = (int)floor(R.next() * nmols) + 1;
     M.randchoice = randchoice;
     M.mol = randchoice - 1;
     M.ex_lo = C.seg_off[g] + M.mol * ns;
@@ -205,7 +238,8 @@ __device__ __noinline__ void move_begin(ChainDev& C, const SysConst& Y, const De
     M.q[i] = P.q[s];
     M.type[i] = P.type[s];
   }
-  C.prof[8] += clock64();
+  R.store(C.rng);
+  if (kProf) C.prof[8] += clock64();
 }
 
 // Thread 0: energy assembly of the move (gcmc.f:946, 1112, 1328).  v = {sum akk*d|S|^2,
@@ -365,6 +399,8 @@ __device__ __forceinline__ void lrc_warp(const ChainDev& C, const SysConst& Y, M
 }
 
 // One real-space candidate: a framework atom from a site's voxel list or a guest site.
+constexpr int kRealDepth = 1;  // candidates a thread takes per loop trip (1-8 measured; 1 is fastest)
+
 struct Cand {
   double4 a;
   int type, site;
@@ -441,6 +477,73 @@ __device__ __forceinline__ void build_phases(const DevSystem& S, const MoveSmem&
 // All threads: this thread's share of the reciprocal sum and of the real-space pairs.
 // v[0] sum akk*d|S|^2, v[1] ewld2, v[2] vdw, v[3] and v[4] the absolute sums that bound the
 // rounding error of v[0] and v[1]+v[2] (mixed precision).  S_new goes to Sn when write_sn.
+// Real-space sums of one pass: every (site, candidate) pair, kRealDepth candidates in flight per
+// thread, compiled per boundary condition so the hot loop holds one minimum-image form.
+template <bool kMixed, int kImcon>
+__device__ __noinline__ void real_space(const DevSystem& S, const ChainDev& C, const MoveSmem& M, int nseg,
+                                        const int* prow_s, int nt1, int fp32_mask, double* vout) {
+  const int tid = threadIdx.x, nsite = M.nold + M.nnew, nold = M.nold, mtype = M.mtype;
+  double v[5] = {0.0, vout[1], vout[2], 0.0, vout[4]};
+  const bool sub_old = (mtype != kInsert && mtype != kDelete);
+  const int T = M.pre[nsite];
+  const float rdrf_e = (float)S.rdr_e, rdrf_v = (float)S.rdr_v;
+  // a thread takes candidates tid, tid + 256, tid + 512, ... in that order whatever the depth
+  int sc[kRealDepth];
+#pragma unroll
+  for (int u = 0; u < kRealDepth; u++) sc[u] = 0;
+  for (int base = tid; base < T; base += kRealDepth * kBatchThreads) {
+    Cand c[kRealDepth];
+#pragma unroll
+    for (int u = 0; u < kRealDepth; u++) c[u] = fetch_candidate(S, C, M, nseg, base + u * kBatchThreads, sc[u]);
+#pragma unroll
+    for (int u = 0; u < kRealDepth; u++) {
+      if (!c[u].live) continue;
+      const int st = c[u].site;
+      const int row = prow_s[M.type[st] * nt1 + c[u].type];
+      double ec = 0.0, ev = 0.0;
+      if (kMixed && (fp32_mask & 6)) {
+        // FP32 for the components selected by fp32_mask (bit 1 Coulomb, bit 2 vdW); the
+        // separation and minimum image stay FP64
+        double dx = M.x[st] - c[u].a.x, dy = M.y[st] - c[u].a.y, dz = M.z[st] - c[u].a.z;
+        min_image_t<kImcon>(S.cell, dx, dy, dz);
+        double rsq = dx * dx + dy * dy + dz * dz;
+        if (rsq < S.rcut2) {
+          const bool need64 = (fp32_mask & 6) != 6;
+          double r = need64 ? sqrt(rsq) : 0.0;
+          float rf = need64 ? (float)r : sqrtf((float)rsq);
+          double chgprd = M.q[st] * kR4pie0 * c[u].a.w;
+          if (fabs(chgprd) > 1e-10) {
+            if (fp32_mask & 2)
+              ec = (double)(interp3f(S.erc_f, rf, rdrf_e) * (float)chgprd);
+            else
+              ec = interp3(S.erc, r, S.rdr_e) * chgprd;
+          }
+          if (row >= 0) {
+            if (fp32_mask & 4)
+              ev = (double)interp3f(S.vvv_f + (size_t)row * S.tab_stride, rf, rdrf_v);
+            else
+              ev = interp3(S.vvv + (size_t)row * S.tab_stride, r, S.rdr_v);
+          }
+        }
+        v[4] += ((fp32_mask & 2) ? fabs(ec) : 0.0) + ((fp32_mask & 4) ? fabs(ev) : 0.0);
+      } else {
+        pair_energy<kImcon>(S, M.x[st] - c[u].a.x, M.y[st] - c[u].a.y, M.z[st] - c[u].a.z, M.q[st] * kR4pie0, c[u].a.w,
+                    row, ec, ev);
+      }
+      if (sub_old && st < nold) {
+        v[1] -= ec;
+        v[2] -= ev;
+      } else {
+        v[1] += ec;
+        v[2] += ev;
+      }
+    }
+  }
+  vout[1] = v[1];
+  vout[2] = v[2];
+  vout[4] = v[4];
+}
+
 template <bool kMixed>
 __device__ __noinline__ void sums(const DevSystem& S, const ChainDev& C, const MoveSmem& M, int nseg,
                                      const int* prow_s, int nt1, const int* kp, const double* ak,
@@ -504,61 +607,11 @@ __device__ __noinline__ void sums(const DevSystem& S, const ChainDev& C, const M
     }
     if (write_sn) Sn[k] = sn;
   }
-  // real space: every (site, candidate) pair, four candidates in flight per thread
-  const bool sub_old = (mtype != kInsert && mtype != kDelete);
-  const int T = M.pre[nsite];
-  const float rdrf_e = (float)S.rdr_e, rdrf_v = (float)S.rdr_v;
-  int s0 = 0, s1 = 0, s2 = 0, s3 = 0;
-  for (int base = tid; base < T; base += 4 * kBatchThreads) {
-    Cand c[4];
-    c[0] = fetch_candidate(S, C, M, nseg, base, s0);
-    c[1] = fetch_candidate(S, C, M, nseg, base + kBatchThreads, s1);
-    c[2] = fetch_candidate(S, C, M, nseg, base + 2 * kBatchThreads, s2);
-    c[3] = fetch_candidate(S, C, M, nseg, base + 3 * kBatchThreads, s3);
-#pragma unroll
-    for (int u = 0; u < 4; u++) {
-      if (!c[u].live) continue;
-      const int st = c[u].site;
-      const int row = prow_s[M.type[st] * nt1 + c[u].type];
-      double ec = 0.0, ev = 0.0;
-      if (kMixed && (fp32_mask & 6)) {
-        // FP32 for the components selected by fp32_mask (bit 1 Coulomb, bit 2 vdW); the
-        // separation and minimum image stay FP64
-        double dx = M.x[st] - c[u].a.x, dy = M.y[st] - c[u].a.y, dz = M.z[st] - c[u].a.z;
-        min_image(S.cell, dx, dy, dz);
-        double rsq = dx * dx + dy * dy + dz * dz;
-        if (rsq < S.rcut2) {
-          const bool need64 = (fp32_mask & 6) != 6;
-          double r = need64 ? sqrt(rsq) : 0.0;
-          float rf = need64 ? (float)r : sqrtf((float)rsq);
-          double chgprd = M.q[st] * kR4pie0 * c[u].a.w;
-          if (fabs(chgprd) > 1e-10) {
-            if (fp32_mask & 2)
-              ec = (double)(interp3f(S.erc_f, rf, rdrf_e) * (float)chgprd);
-            else
-              ec = interp3(S.erc, r, S.rdr_e) * chgprd;
-          }
-          if (row >= 0) {
-            if (fp32_mask & 4)
-              ev = (double)interp3f(S.vvv_f + (size_t)row * S.tab_stride, rf, rdrf_v);
-            else
-              ev = interp3(S.vvv + (size_t)row * S.tab_stride, r, S.rdr_v);
-          }
-        }
-        v[4] += ((fp32_mask & 2) ? fabs(ec) : 0.0) + ((fp32_mask & 4) ? fabs(ev) : 0.0);
-      } else {
-        pair_energy(S, M.x[st] - c[u].a.x, M.y[st] - c[u].a.y, M.z[st] - c[u].a.z, M.q[st] * kR4pie0, c[u].a.w,
-                    row, ec, ev);
-      }
-      if (sub_old && st < nold) {
-        v[1] -= ec;
-        v[2] -= ev;
-      } else {
-        v[1] += ec;
-        v[2] += ev;
-      }
-    }
-  }
+  // real space, per boundary condition
+  if (S.cell.imcon == 1) real_space<kMixed, 1>(S, C, M, nseg, prow_s, nt1, fp32_mask, v);
+  else if (S.cell.imcon == 2) real_space<kMixed, 2>(S, C, M, nseg, prow_s, nt1, fp32_mask, v);
+  else if (S.cell.imcon == 3) real_space<kMixed, 3>(S, C, M, nseg, prow_s, nt1, fp32_mask, v);
+  else real_space<kMixed, 0>(S, C, M, nseg, prow_s, nt1, fp32_mask, v);
 }
 
 // All threads: FP64 recompute of S(k) = S_framework(k) + sum over guest sites (bounds the drift
@@ -589,7 +642,7 @@ __device__ __forceinline__ void recompute_sk(const DevSystem& S, const SysConst&
 
 // kMixed: the mixed-precision build (FP32 components per L.mixed, FP64 re-checks); the FP64
 // build carries none of that code.
-template <bool kMixed>
+template <bool kMixed, bool kProf>
 __global__ void __launch_bounds__(kBatchThreads, 2) fmc_batch_kernel(BatchLaunch L, int tab_stride) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ ChainDev C;
@@ -632,7 +685,7 @@ __global__ void __launch_bounds__(kBatchThreads, 2) fmc_batch_kernel(BatchLaunch
   (void)tab_stride;
   __syncthreads();
   long long t0 = 0, t1 = 0;
-  const bool prof = L.profile != 0;
+  constexpr bool prof = kProf;
   // a chain ends after the move on which its deck's equilibration + production budget ran
   // out (the reference's do-while(lgchk) loop, gcmc.f:589-736), or at its move budget
   long long nmoves = C.lgchk ? L.moves : 0;
@@ -647,7 +700,7 @@ __global__ void __launch_bounds__(kBatchThreads, 2) fmc_batch_kernel(BatchLaunch
       }
     }
     if (prof && tid == 0) t0 = clock64();
-    if (tid == 0) move_begin(C, Y, S, M);
+    if (tid == 0) move_begin<kProf>(C, Y, S, M);
     __syncthreads();
     if (prof && tid == 0) {
       t1 = clock64();
@@ -799,17 +852,26 @@ int batch_smem_bytes(int kmax_K, int tab_sites, int tab_stride) {
 }
 
 cudaError_t configure_batch_kernel(int smem_bytes) {
-  cudaError_t e = cudaFuncSetAttribute(fmc_batch_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
+  cudaError_t e = cudaFuncSetAttribute(fmc_batch_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       smem_bytes);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(fmc_batch_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
+    e = cudaFuncSetAttribute(fmc_batch_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(fmc_batch_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(fmc_batch_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
   return e;
 }
 
 cudaError_t launch_batch(const BatchLaunch& L, int smem_bytes, int tab_stride, cudaStream_t st) {
-  if (L.mixed)
-    fmc_batch_kernel<true><<<L.nchains, kBatchThreads, smem_bytes, st>>>(L, tab_stride);
+  if (L.mixed && L.profile)
+    fmc_batch_kernel<true, true><<<L.nchains, kBatchThreads, smem_bytes, st>>>(L, tab_stride);
+  else if (L.mixed)
+    fmc_batch_kernel<true, false><<<L.nchains, kBatchThreads, smem_bytes, st>>>(L, tab_stride);
+  else if (L.profile)
+    fmc_batch_kernel<false, true><<<L.nchains, kBatchThreads, smem_bytes, st>>>(L, tab_stride);
   else
-    fmc_batch_kernel<false><<<L.nchains, kBatchThreads, smem_bytes, st>>>(L, tab_stride);
+    fmc_batch_kernel<false, false><<<L.nchains, kBatchThreads, smem_bytes, st>>>(L, tab_stride);
   return cudaGetLastError();
 }
 

@@ -89,18 +89,20 @@ inline void cell_reciprocals(CellGeom& c) {
 // Fortran nint: nearest integer, halves away from zero.
 FMC_HD double fnint(double x) { return round(x); }
 
-// Minimum image of one separation vector for imcon 1, 2, 3 (images, utility_pack.f:1138-1202).
-FMC_HD void min_image(const CellGeom& c, double& x, double& y, double& z) {
-  if (c.imcon == 1) {
+// Minimum image of one separation vector for imcon 1, 2, 3 (images, utility_pack.f:1138-1202),
+// for a boundary condition known at compile time (other values: no image).
+template <int kImcon>
+FMC_HD void min_image_t(const CellGeom& c, double& x, double& y, double& z) {
+  if (kImcon == 1) {
     const double a = c.h[0], ra = c.inv[0];
     x = x - a * fnint(ra * x);
     y = y - a * fnint(ra * y);
     z = z - a * fnint(ra * z);
-  } else if (c.imcon == 2) {
+  } else if (kImcon == 2) {
     x = x - c.h[0] * fnint(c.inv[0] * x);
     y = y - c.h[4] * fnint(c.inv[1] * y);
     z = z - c.h[8] * fnint(c.inv[2] * z);
-  } else if (c.imcon == 3) {
+  } else if (kImcon == 3) {
     const double* r = c.rh;
     double sx = r[0] * x + r[3] * y + r[6] * z;
     double sy = r[1] * x + r[4] * y + r[7] * z;
@@ -112,6 +114,13 @@ FMC_HD void min_image(const CellGeom& c, double& x, double& y, double& z) {
     y = c.h[1] * sx + c.h[4] * sy + c.h[7] * sz;
     z = c.h[2] * sx + c.h[5] * sy + c.h[8] * sz;
   }
+}
+
+// The same with the boundary condition read from the cell.
+FMC_HD void min_image(const CellGeom& c, double& x, double& y, double& z) {
+  if (c.imcon == 1) min_image_t<1>(c, x, y, z);
+  else if (c.imcon == 2) min_image_t<2>(c, x, y, z);
+  else if (c.imcon == 3) min_image_t<3>(c, x, y, z);
 }
 
 // ------------------------------------------------------------------ trial generators

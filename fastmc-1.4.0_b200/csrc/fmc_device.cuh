@@ -88,9 +88,12 @@ __device__ __forceinline__ void frac_coords(const CellGeom& c, double x, double 
 }
 
 // Pair energy of one site with charge factor chgea = q_i*r4pie0 and table row lookup base.
+// kImcon < 0: the boundary condition is read from the cell.
+template <int kImcon = -1>
 __device__ __forceinline__ void pair_energy(const DevSystem& S, double dx, double dy, double dz, double chgea,
                                             double qj, int row, double& ec, double& ev) {
-  min_image(S.cell, dx, dy, dz);
+  if (kImcon < 0) min_image(S.cell, dx, dy, dz);
+  else min_image_t<kImcon>(S.cell, dx, dy, dz);
   double rsq = dx * dx + dy * dy + dz * dz;
   if (rsq < S.rcut2) {
     double r = sqrt(rsq);
