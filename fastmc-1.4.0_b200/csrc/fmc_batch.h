@@ -111,11 +111,27 @@ struct SlotMemory {
   void release();  // stream-ordered frees of every allocation
 };
 
-// A serving slot built from a prepared host system: the device system (framework, voxel
-// lists, tables), the framework S(k), the per-system constants and an empty chain, all on
-// mem.st.  Waits once on mem.st for the voxel-list size.
-int build_slot(const HostSystem& h, int slot, const int seed[4], SlotMemory& mem, SysConst& Y, ChainDev& C,
-               std::string& err);
+// Pinned host staging for slot uploads: a bump allocator over one pinned buffer; its owner
+// resets `used` once the stream that reads the staged bytes has drained.
+struct Staging {
+  unsigned char* base = nullptr;
+  size_t cap = 0, used = 0;
+  void* take(size_t n);  // 256-byte aligned; nullptr when the buffer is full
+};
+
+// Pinned bytes build_slot stages for a system.
+size_t slot_staging_bytes(const HostSystem& h);
+// Voxel-list entries of a system estimated from its framework density (+15% and 4096).
+long long slot_voxel_capacity(const HostSystem& h);
+
+// A serving slot built from a prepared host system: the device system (framework, voxel lists,
+// tables), the framework S(k), the per-system constants and an empty chain, all enqueued on
+// mem.st without waiting (one staged host-to-device copy; voxel lists sized by vox_cap entries,
+// the exact count copied to *vox_total, pinned, for the caller to check once mem.st has
+// drained: a total above vox_cap means the lists are cut and the slot must be rebuilt with
+// vox_cap = total).
+int build_slot(const HostSystem& h, int slot, const int seed[4], SlotMemory& mem, Staging& stg, long long vox_cap,
+               int* vox_total, SysConst& Y, ChainDev& C, std::string& err);
 
 class Batch {
  public:

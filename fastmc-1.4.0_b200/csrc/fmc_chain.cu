@@ -74,7 +74,8 @@ int upload_system(const HostSystem& h, DeviceSystem& d, std::string& err) {
     if (h.nf <= 65535 && (e = dalloc(d.allocations, &a16, ne)) != cudaSuccess) goto fail;
     if ((e = dalloc(d.allocations, &xyzq, ne)) != cudaSuccess) goto fail;
     if ((e = dalloc(d.allocations, &vt, ne)) != cudaSuccess) goto fail;
-    e = launch_voxel_fill(h.cell, h.nvox, v.fw, v.fw_type, h.nf, h.vox_lim2, v.vox_off, atoms, a16, xyzq, vt, 0);
+    e = launch_voxel_fill(h.cell, h.nvox, v.fw, v.fw_type, h.nf, h.vox_lim2, v.vox_off, atoms, a16, xyzq, vt,
+                          (long long)ne, 0);
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) goto fail;
     v.vox_atoms = atoms;

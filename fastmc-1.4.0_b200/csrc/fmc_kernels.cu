@@ -361,7 +361,7 @@ __global__ void __launch_bounds__(kVoxThreads) fmc_voxel_fill_kernel(CellGeom ce
                                                                      const int* __restrict__ ftype, int nf, double lim2,
                                                                      const int* __restrict__ off, int* atoms,
                                                                      unsigned short* atoms16, double4* xyzq,
-                                                                     unsigned char* vtype) {
+                                                                     unsigned char* vtype, long long cap) {
   __shared__ int woff[kVoxThreads / 32 + 1];
   __shared__ int running;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -388,10 +388,12 @@ __global__ void __launch_bounds__(kVoxThreads) fmc_voxel_fill_kernel(CellGeom ce
     __syncthreads();
     if (flag) {
       int pos = base + running + woff[warp] + __popc(mask & ((1u << lane) - 1u));
-      if (atoms) atoms[pos] = j;
-      if (atoms16) atoms16[pos] = (unsigned short)j;
-      xyzq[pos] = a;
-      vtype[pos] = (unsigned char)ftype[j];
+      if (pos < cap) {  // beyond the capacity: the caller compares off[nv] with cap and rebuilds
+        if (atoms) atoms[pos] = j;
+        if (atoms16) atoms16[pos] = (unsigned short)j;
+        xyzq[pos] = a;
+        vtype[pos] = (unsigned char)ftype[j];
+      }
     }
     __syncthreads();
     if (threadIdx.x == 0) running += woff[kVoxThreads / 32];
@@ -408,10 +410,54 @@ cudaError_t launch_voxel_count(const CellGeom& cell, const int* nvox, const doub
 
 cudaError_t launch_voxel_fill(const CellGeom& cell, const int* nvox, const double4* fw, const int* ftype, int nf,
                               double lim2, const int* off, int* atoms, unsigned short* atoms16, double4* xyzq,
-                              unsigned char* vtype, cudaStream_t st) {
+                              unsigned char* vtype, long long cap, cudaStream_t st) {
   int nv = nvox[0] * nvox[1] * nvox[2];
   fmc_voxel_fill_kernel<<<nv, kVoxThreads, 0, st>>>(cell, nvox[0], nvox[1], nvox[2], fw, ftype, nf, lim2, off, atoms,
-                                                    atoms16, xyzq, vtype);
+                                                    atoms16, xyzq, vtype, cap);
+  return cudaGetLastError();
+}
+
+namespace {
+constexpr int kScanThreads = 1024;
+
+// Exclusive prefix sum of n counts into off[0..n] (off[n] = total) by one CTA: each thread sums
+// a contiguous chunk, the chunk sums are scanned across the block, then each thread writes its
+// chunk's offsets.
+__global__ void __launch_bounds__(kScanThreads) fmc_exclusive_scan_kernel(const int* __restrict__ counts, int n,
+                                                                          int* __restrict__ off) {
+  __shared__ int wsum[kScanThreads / 32];
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const int chunk = (n + kScanThreads - 1) / kScanThreads;
+  const int lo = min(n, t * chunk), hi = min(n, lo + chunk);
+  int sum = 0;
+  for (int i = lo; i < hi; i++) sum += counts[i];
+  int incl = sum;
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) wsum[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    int w = wsum[lane];
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    wsum[lane] = w;
+  }
+  __syncthreads();
+  int run = incl - sum + (warp ? wsum[warp - 1] : 0);
+  for (int i = lo; i < hi; i++) {
+    off[i] = run;
+    run += counts[i];
+  }
+  if (t == kScanThreads - 1) off[n] = wsum[kScanThreads / 32 - 1];
+}
+}  // namespace
+
+cudaError_t launch_exclusive_scan(const int* counts, int n, int* off, cudaStream_t st) {
+  fmc_exclusive_scan_kernel<<<1, kScanThreads, 0, st>>>(counts, n, off);
   return cudaGetLastError();
 }
 

@@ -58,6 +58,8 @@ cudaError_t launch_voxel_count(const CellGeom& cell, const int* nvox, const doub
                                int* counts, cudaStream_t st);
 cudaError_t launch_voxel_fill(const CellGeom& cell, const int* nvox, const double4* fw, const int* ftype, int nf,
                               double lim2, const int* off, int* atoms, unsigned short* atoms16, double4* xyzq,
-                              unsigned char* vtype, cudaStream_t st);
+                              unsigned char* vtype, long long cap, cudaStream_t st);  // entries >= cap not written
+// off[0..n]: exclusive prefix sum of counts[0..n-1], off[n] the total (one CTA)
+cudaError_t launch_exclusive_scan(const int* counts, int n, int* off, cudaStream_t st);
 
 }  // namespace fmc

@@ -52,6 +52,8 @@ class Server {
   struct Slot {
     int request = -1;
     SlotMemory mem;
+    long long vox_cap = 0;  // voxel-list entries allocated
+    bool fresh = false;     // admitted in this step; capacity not checked yet
   };
 
   // phase tables in shared memory hold the old + new sites of one trial of up to
@@ -71,7 +73,12 @@ class Server {
   SysConst* d_sys = nullptr;
   ChainDev* h_chains = nullptr;
   ChainDev* d_chains = nullptr;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  ChainDev* h_out = nullptr;      // pinned: control blocks as the last launch left them
+  int* h_vox_total = nullptr;     // pinned: exact voxel-list size of each slot's last build
+  std::vector<char> launched;     // slots in the current launch
+  cudaStream_t st2 = nullptr;     // admission stream (slot set-up beside the running launch)
+  Staging stage;                  // pinned staging of slot uploads
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_h2d = nullptr;
   // worker pool
   std::mutex mu;
   std::condition_variable cv;
@@ -93,11 +100,17 @@ class Server {
     if (!st) return;
     cudaSetDevice(device);
     cudaStreamSynchronize(st);
+    if (st2) cudaStreamSynchronize(st2);
     for (int i = 0; i < nslots; i++) release(i);
-    cudaStreamSynchronize(st);
+    if (st2) cudaStreamSynchronize(st2);
     if (pool) cudaMemPoolDestroy(pool);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
+    if (ev_h2d) cudaEventDestroy(ev_h2d);
+    if (h_out) cudaFreeHost(h_out);
+    if (h_vox_total) cudaFreeHost(h_vox_total);
+    if (stage.base) cudaFreeHost(stage.base);
+    if (st2) cudaStreamDestroy(st2);
     if (d_sys) cudaFree(d_sys);
     if (d_chains) cudaFree(d_chains);
     if (h_sys) cudaFreeHost(h_sys);
@@ -139,12 +152,22 @@ class Server {
     }
     unsigned long long keep = ~0ull;
     cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    if (cudaStreamCreateWithFlags(&st2, cudaStreamNonBlocking) != cudaSuccess) {
+      err = "cannot create the admission stream";
+      return -100;
+    }
     slots.resize(n);
+    launched.assign(n, 0);
     for (auto& sl : slots) {
-      sl.mem.st = st;
+      sl.mem.st = st2;
       sl.mem.pool = pool;
     }
-    cudaError_t e = cudaMallocHost(&h_sys, sizeof(SysConst) * n);
+    stage.cap = 64u << 20;
+    cudaError_t e = cudaMallocHost(&stage.base, stage.cap);
+    if (e == cudaSuccess) e = cudaMallocHost(&h_out, sizeof(ChainDev) * n);
+    if (e == cudaSuccess) e = cudaMallocHost(&h_vox_total, sizeof(int) * n);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_h2d, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaMallocHost(&h_sys, sizeof(SysConst) * n);
     if (e == cudaSuccess) e = cudaMallocHost(&h_chains, sizeof(ChainDev) * n);
     if (e == cudaSuccess) e = cudaMalloc(&d_sys, sizeof(SysConst) * n);
     if (e == cudaSuccess) e = cudaMalloc(&d_chains, sizeof(ChainDev) * n);
@@ -307,8 +330,8 @@ class Server {
     r.host.reset();
   }
 
-  // Builds prepared request `id` into free slot `i` (stream-ordered, one wait for the voxel
-  // list size); returns the slot's device bytes, or 0 (and marks the request rejected).
+  // Enqueues the slot set-up of prepared request `id` into free slot `i` on the admission
+  // stream; returns the slot's device bytes, or 0 (and marks the request rejected).
   size_t admit(int id, int i) {
     Request& r = req(id);
     Slot& s = slots[i];
@@ -316,9 +339,22 @@ class Server {
       reject(r, r.prep_rc, r.prep_err);
       return 0;
     }
+    const size_t need = slot_staging_bytes(*r.host);
+    if (stage.used + need > stage.cap) {  // the staged bytes of earlier admissions are read by now
+      cudaStreamSynchronize(st2);
+      stage.used = 0;
+      if (need > stage.cap) {
+        cudaFreeHost(stage.base);
+        stage.cap = need;
+        if (cudaMallocHost(&stage.base, stage.cap) != cudaSuccess) {
+          stage.base = nullptr;
+          stage.cap = 0;
+        }
+      }
+    }
     std::string err;
-    int rc = build_slot(*r.host, i, r.seed, s.mem, h_sys[i], h_chains[i], err);
-    r.host.reset();
+    s.vox_cap = slot_voxel_capacity(*r.host);
+    int rc = build_slot(*r.host, i, r.seed, s.mem, stage, s.vox_cap, &h_vox_total[i], h_sys[i], h_chains[i], err);
     if (rc) {
       s.mem.release();
       std::memset(&h_chains[i], 0, sizeof(ChainDev));
@@ -327,18 +363,16 @@ class Server {
     }
     h_chains[i].budget = r.moves;
     s.request = id;
+    s.fresh = true;
     r.state = kRunning;
     r.slot = i;
     admitted++;
     return s.mem.bytes;
   }
 
-  int step(int moves, int* n_active, int* n_queued, float* ms, std::string& err) {
-    cudaSetDevice(device);
-    int active = 0;
-    for (int i = 0; i < nslots; i++) active += slots[i].request >= 0;
-    // admission: FIFO, while a slot is free, the front request is prepared and the memory
-    // budget holds.  With nothing running, wait for the front request's preparation.
+  // Admission: FIFO, while a slot is free, the front request is prepared and the memory budget
+  // holds.  With nothing running, waits for the front request's preparation.
+  void admit_queued(int running) {
     const double t0 = now_ms();
     for (int i = 0; i < nslots && !queue.empty(); i++) {
       if (slots[i].request >= 0) continue;
@@ -347,7 +381,7 @@ class Server {
       if (workers.empty()) {
         prepare(r);
       } else if (!r.prepared.load(std::memory_order_acquire)) {
-        if (active) break;
+        if (running) break;
         const double w0 = now_ms();
         while (!r.prepared.load(std::memory_order_acquire)) std::this_thread::sleep_for(std::chrono::microseconds(200));
         wait_ms += now_ms() - w0;
@@ -363,19 +397,72 @@ class Server {
       }
       queue.pop_front();
       used += admit(id, i);
-      if (r.state == kRunning) active++;
-      else i--;  // slot still free
+      if (r.state != kRunning) i--;  // slot still free
     }
     admit_ms += now_ms() - t0;
+  }
+
+  // Once the admission stream has drained: slots whose voxel lists outgrew the estimate are
+  // rebuilt at their exact size (rare; the estimate carries 15% headroom).
+  int settle_admissions(std::string& err) {
+    cudaError_t e = cudaStreamSynchronize(st2);
+    if (e != cudaSuccess) {
+      err = std::string("slot set-up failed: ") + cudaGetErrorString(e);
+      return -100 - (int)e;
+    }
+    stage.used = 0;
+    for (int i = 0; i < nslots; i++) {
+      Slot& s = slots[i];
+      if (s.request < 0 || !s.fresh) continue;
+      s.fresh = false;
+      Request& r = req(s.request);
+      if ((long long)h_vox_total[i] > s.vox_cap) {
+        used -= std::min(used, s.mem.bytes);
+        s.mem.release();
+        s.vox_cap = h_vox_total[i];
+        std::string e2;
+        int rc = build_slot(*r.host, i, r.seed, s.mem, stage, s.vox_cap, &h_vox_total[i], h_sys[i], h_chains[i], e2);
+        if (rc == 0 && cudaStreamSynchronize(st2) != cudaSuccess) rc = -100;
+        stage.used = 0;
+        if (rc || (long long)h_vox_total[i] > s.vox_cap) {
+          s.mem.release();
+          s.request = -1;
+          std::memset(&h_chains[i], 0, sizeof(ChainDev));
+          reject(r, rc ? rc : -12, rc ? e2 : "voxel lists changed size between builds");
+          continue;
+        }
+        h_chains[i].budget = r.moves;
+        used += s.mem.bytes;
+      }
+      r.host.reset();
+    }
+    return 0;
+  }
+
+  int step(int moves, int* n_active, int* n_queued, float* ms, std::string& err) {
+    cudaSetDevice(device);
+    int running = 0;
+    for (int i = 0; i < nslots; i++) {
+      launched[i] = slots[i].request >= 0;
+      running += launched[i];
+    }
+    if (!running) {  // nothing on the device: admit first, then launch what was admitted
+      admit_queued(0);
+      int rc = settle_admissions(err);
+      if (rc) return rc;
+      for (int i = 0; i < nslots; i++) {
+        launched[i] = slots[i].request >= 0;
+        running += launched[i];
+      }
+    }
     float t = 0.f;
-    long long before = 0;
-    for (int i = 0; i < nslots; i++)
-      if (slots[i].request >= 0) before += h_chains[i].moves_done;
     last_moves = 0;
-    if (active) {
-      cudaError_t e = cudaMemcpyAsync(d_sys, h_sys, sizeof(SysConst) * nslots, cudaMemcpyHostToDevice, st);
+    cudaError_t e = cudaSuccess;
+    if (running) {
+      e = cudaMemcpyAsync(d_sys, h_sys, sizeof(SysConst) * nslots, cudaMemcpyHostToDevice, st);
       if (e == cudaSuccess)
         e = cudaMemcpyAsync(d_chains, h_chains, sizeof(ChainDev) * nslots, cudaMemcpyHostToDevice, st);
+      if (e == cudaSuccess) e = cudaEventRecord(ev_h2d, st);
       BatchLaunch L;
       std::memset(&L, 0, sizeof(L));
       L.chains = d_chains;
@@ -389,25 +476,32 @@ class Server {
       if (e == cudaSuccess) e = launch_batch(L, smem, tab_stride, st);
       if (e == cudaSuccess) e = cudaEventRecord(ev1, st);
       if (e == cudaSuccess)
-        e = cudaMemcpyAsync(h_chains, d_chains, sizeof(ChainDev) * nslots, cudaMemcpyDeviceToHost, st);
+        e = cudaMemcpyAsync(h_out, d_chains, sizeof(ChainDev) * nslots, cudaMemcpyDeviceToHost, st);
+      // requests admitted now set up on the admission stream while the launch runs; their host
+      // control blocks change only after the launch's copy of them has been read
+      if (e == cudaSuccess) e = cudaEventSynchronize(ev_h2d);
+      if (e == cudaSuccess) admit_queued(running);
       if (e == cudaSuccess) e = cudaStreamSynchronize(st);
       if (e == cudaSuccess) cudaEventElapsedTime(&t, ev0, ev1);
       if (e != cudaSuccess) {
         err = std::string("serving launch failed: ") + cudaGetErrorString(e);
         return -100 - (int)e;
       }
+      int rc = settle_admissions(err);
+      if (rc) return rc;
       launches++;
       launch_ms += t;
-      long long after = 0;
       for (int i = 0; i < nslots; i++)
-        if (slots[i].request >= 0) after += h_chains[i].moves_done;
-      last_moves = after - before;
+        if (launched[i]) {
+          last_moves += h_out[i].moves_done - h_chains[i].moves_done;
+          h_chains[i] = h_out[i];
+        }
       moves_run += last_moves;
     }
-    // retirement
+    // retirement of the chains that ran
     for (int i = 0; i < nslots; i++) {
       int id = slots[i].request;
-      if (id < 0) continue;
+      if (id < 0 || !launched[i]) continue;
       const ChainDev& C = h_chains[i];
       if ((C.budget > 0 && C.moves_done >= C.budget) || !C.lgchk || C.status) {
         Request& r = req(id);
@@ -418,7 +512,7 @@ class Server {
         retired++;
       }
     }
-    if (n_active) *n_active = active;
+    if (n_active) *n_active = running;
     if (n_queued) *n_queued = (int)queue.size();
     if (ms) *ms = t;
     return 0;

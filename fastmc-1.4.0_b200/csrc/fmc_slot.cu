@@ -1,9 +1,10 @@
-// Serving slots: the device side of admitting one request, stream-ordered on the server's
-// stream with allocations from its memory pool.  The slot holds only what the batched kernel
-// reads: framework atoms, inlined voxel lists, erfc / vdW tables (FP64 and FP32), the k-vector
-// tables, the framework S(k) (ewald1 over the framework, ewald.f:368-630) and the chain's S(k)
-// and guest segments.
+// Serving slots: the device side of admitting one request, enqueued on the admission stream with
+// allocations from the server's memory pool and every host array staged into pinned memory, so
+// admitting needs no wait.  The slot holds only what the batched kernel reads: framework atoms,
+// inlined voxel lists, erfc / vdW tables (FP64 and FP32), the k-vector tables, the framework S(k)
+// (ewald1 over the framework, ewald.f:368-630) and the chain's S(k) and guest segments.
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 
 #include "fmc_batch.h"
@@ -26,80 +27,132 @@ void SlotMemory::release() {
   bytes = 0;
 }
 
+void* Staging::take(size_t n) {
+  size_t at = (used + 255) & ~size_t(255);
+  if (at + n > cap) return nullptr;
+  used = at + n;
+  return base + at;
+}
+
 namespace {
 
-template <class T>
-cudaError_t put(SlotMemory& m, const T** out, const T* src, size_t n) {
-  T* p = nullptr;
-  cudaError_t e = m.alloc((void**)&p, n * sizeof(T));
-  if (e == cudaSuccess && n) e = cudaMemcpyAsync(p, src, n * sizeof(T), cudaMemcpyHostToDevice, m.st);
-  *out = p;
-  return e;
-}
+size_t al(size_t n) { return (n + 255) & ~size_t(255); }
 
-template <class T>
-cudaError_t put(SlotMemory& m, const T** out, const std::vector<T>& v) {
-  return put(m, out, v.data(), v.size());
-}
+// Host arrays of a system in the order they are staged, with their byte sizes.
+struct Parts {
+  size_t fw, ftype, erc, vvv, erc_f, vvv_f, prow, kp, akk;
+  explicit Parts(const HostSystem& h)
+      : fw(sizeof(double4) * h.nf),
+        ftype(sizeof(int) * h.nf),
+        erc(sizeof(double) * h.erc.size()),
+        vvv(sizeof(double) * h.vvv.size()),
+        erc_f(sizeof(float) * h.erc.size()),
+        vvv_f(sizeof(float) * h.vvv.size()),
+        prow(sizeof(int) * h.pair_row.size()),
+        kp(sizeof(int) * h.K),
+        akk(sizeof(double) * h.K) {}
+  size_t total() const {
+    return al(fw) + al(ftype) + al(erc) + al(vvv) + al(erc_f) + al(vvv_f) + al(prow) + al(kp) + al(akk);
+  }
+};
 
 }  // namespace
 
-int build_slot(const HostSystem& h, int slot, const int seed[4], SlotMemory& mem, SysConst& Y, ChainDev& C,
-               std::string& err) {
+size_t slot_staging_bytes(const HostSystem& h) { return Parts(h).total() + 256; }
+
+long long slot_voxel_capacity(const HostSystem& h) {
+  // every atom appears in the lists of the voxels whose centres lie within lim of it
+  const double lim = std::sqrt(h.vox_lim2);
+  const double nv = (double)h.nvox[0] * h.nvox[1] * h.nvox[2];
+  const double per_atom = std::min(nv, 4.0 / 3.0 * kPi * lim * lim * lim / (h.cell.volm / nv));
+  return (long long)(1.15 * h.nf * per_atom) + 4096;
+}
+
+int build_slot(const HostSystem& h, int slot, const int seed[4], SlotMemory& mem, Staging& stg, long long vox_cap,
+               int* vox_total, SysConst& Y, ChainDev& C, std::string& err) {
   DevSystem v;
   std::memset(&v, 0, sizeof(v));
   v.cell = h.cell;
   v.nf = h.nf;
   cudaStream_t st = mem.st;
-  cudaError_t e;
-  std::vector<double4> fw(h.nf);
-  for (int i = 0; i < h.nf; i++) fw[i] = make_double4(h.fx[i], h.fy[i], h.fz[i], h.fq[i]);
-  std::vector<float> ef(h.erc.begin(), h.erc.end()), vf(h.vvv.begin(), h.vvv.end());
-  std::vector<int> kp(h.K);
-  for (int k = 0; k < h.K; k++) kp[k] = kpack(h.kl[k], h.km[k], h.kn[k]);
+  cudaError_t e = cudaSuccess;
+  const Parts P(h);
+  const size_t total = P.total();
+  unsigned char* hs = (unsigned char*)stg.take(total);
+  if (!hs) {
+    err = "slot staging buffer full";
+    return -11;
+  }
+  // stage every host array, then one copy into one device block with the same layout
+  size_t o = 0;
+  auto place = [&](size_t n) {
+    size_t at = o;
+    o += al(n);
+    return at;
+  };
+  const size_t o_fw = place(P.fw), o_ft = place(P.ftype), o_erc = place(P.erc), o_vvv = place(P.vvv),
+               o_ercf = place(P.erc_f), o_vvvf = place(P.vvv_f), o_prow = place(P.prow), o_kp = place(P.kp),
+               o_akk = place(P.akk);
+  {
+    double4* fw = (double4*)(hs + o_fw);
+    for (int i = 0; i < h.nf; i++) fw[i] = make_double4(h.fx[i], h.fy[i], h.fz[i], h.fq[i]);
+    std::memcpy(hs + o_ft, h.ftype.data(), P.ftype);
+    std::memcpy(hs + o_erc, h.erc.data(), P.erc);
+    std::memcpy(hs + o_vvv, h.vvv.data(), P.vvv);
+    float* ef = (float*)(hs + o_ercf);
+    for (size_t i = 0; i < h.erc.size(); i++) ef[i] = (float)h.erc[i];
+    float* vf = (float*)(hs + o_vvvf);
+    for (size_t i = 0; i < h.vvv.size(); i++) vf[i] = (float)h.vvv[i];
+    std::memcpy(hs + o_prow, h.pair_row.data(), P.prow);
+    int* kp = (int*)(hs + o_kp);
+    for (int k = 0; k < h.K; k++) kp[k] = kpack(h.kl[k], h.km[k], h.kn[k]);
+    std::memcpy(hs + o_akk, h.akk.data(), P.akk);
+  }
+  unsigned char* d = nullptr;
   const int nv = h.nvox[0] * h.nvox[1] * h.nvox[2];
-  std::vector<int> cnt(nv), offv(nv + 1, 0);
+  if (vox_cap <= 0) vox_cap = slot_voxel_capacity(h);
   int* counts = nullptr;
+  int* off = nullptr;
+  double4* xyzq = nullptr;
+  unsigned char* vt = nullptr;
   double2* skfw = nullptr;
   double* scratch = nullptr;
   double* parts = nullptr;
-  if ((e = put(mem, &v.fw, fw)) != cudaSuccess) goto fail;
-  if ((e = put(mem, &v.fw_type, h.ftype)) != cudaSuccess) goto fail;
+  if ((e = mem.alloc((void**)&d, total)) != cudaSuccess) goto fail;
+  if ((e = cudaMemcpyAsync(d, hs, total, cudaMemcpyHostToDevice, st)) != cudaSuccess) goto fail;
+  v.fw = (const double4*)(d + o_fw);
+  v.fw_type = (const int*)(d + o_ft);
+  v.erc = (const double*)(d + o_erc);
+  v.vvv = (const double*)(d + o_vvv);
+  v.erc_f = (const float*)(d + o_ercf);
+  v.vvv_f = (const float*)(d + o_vvvf);
+  v.pair_row = (const int*)(d + o_prow);
+  v.kpack = (const int*)(d + o_kp);
+  v.akk = (const double*)(d + o_akk);
   for (int a = 0; a < 3; a++) v.nvox[a] = h.nvox[a];
-  // voxel lists: count per voxel on the device, prefix on the host (one wait), ordered fill
+  // voxel lists: count, device prefix sum, fill up to the capacity
   if ((e = cudaMallocFromPoolAsync((void**)&counts, sizeof(int) * nv, mem.pool, st)) != cudaSuccess) goto fail;
+  if ((e = mem.alloc((void**)&off, sizeof(int) * (nv + 1))) != cudaSuccess) goto fail;
+  if ((e = mem.alloc((void**)&xyzq, sizeof(double4) * vox_cap)) != cudaSuccess) goto fail;
+  if ((e = mem.alloc((void**)&vt, vox_cap)) != cudaSuccess) goto fail;
   e = launch_voxel_count(h.cell, h.nvox, v.fw, h.nf, h.vox_lim2, counts, st);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(cnt.data(), counts, sizeof(int) * nv, cudaMemcpyDeviceToHost, st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  cudaFreeAsync(counts, st);
+  if (e == cudaSuccess) e = launch_exclusive_scan(counts, nv, off, st);
+  if (e == cudaSuccess) cudaFreeAsync(counts, st);
+  if (e == cudaSuccess)
+    e = launch_voxel_fill(h.cell, h.nvox, v.fw, v.fw_type, h.nf, h.vox_lim2, off, nullptr, nullptr, xyzq, vt, vox_cap,
+                          st);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(vox_total, off + nv, sizeof(int), cudaMemcpyDeviceToHost, st);
   if (e != cudaSuccess) goto fail;
-  for (int i = 0; i < nv; i++) offv[i + 1] = offv[i] + cnt[i];
-  {
-    const size_t ne = (size_t)offv[nv];
-    double4* xyzq = nullptr;
-    unsigned char* vt = nullptr;
-    if ((e = put(mem, &v.vox_off, offv)) != cudaSuccess) goto fail;
-    if ((e = mem.alloc((void**)&xyzq, sizeof(double4) * ne)) != cudaSuccess) goto fail;
-    if ((e = mem.alloc((void**)&vt, ne)) != cudaSuccess) goto fail;
-    e = launch_voxel_fill(h.cell, h.nvox, v.fw, v.fw_type, h.nf, h.vox_lim2, v.vox_off, nullptr, nullptr, xyzq, vt, st);
-    if (e != cudaSuccess) goto fail;
-    v.vox_xyzq = xyzq;
-    v.vox_type = vt;
-  }
+  v.vox_off = off;
+  v.vox_xyzq = xyzq;
+  v.vox_type = vt;
   v.rcut2 = h.rcut * h.rcut;
   v.rdr_e = 1.0 / h.drewd;
   v.rdr_v = 1.0 / h.dlrpot;
-  if ((e = put(mem, &v.erc, h.erc)) != cudaSuccess) goto fail;
-  if ((e = put(mem, &v.vvv, h.vvv)) != cudaSuccess) goto fail;
-  if ((e = put(mem, &v.erc_f, ef)) != cudaSuccess) goto fail;
-  if ((e = put(mem, &v.vvv_f, vf)) != cudaSuccess) goto fail;
   v.tab_stride = h.mxgrid + 1;
   v.ntypes = h.ntypes;
-  if ((e = put(mem, &v.pair_row, h.pair_row)) != cudaSuccess) goto fail;
   v.K = h.K;
   for (int a = 0; a < 3; a++) v.kmax[a] = h.deck.kmax[a];
-  if ((e = put(mem, &v.kpack, kp)) != cudaSuccess) goto fail;
-  if ((e = put(mem, &v.akk, h.akk)) != cudaSuccess) goto fail;
   v.recip_pref = h.recip_pref;
   // framework S(k); the scratch goes back to the pool once the kernels have run
   if ((e = mem.alloc((void**)&skfw, sizeof(double2) * std::max(h.K, 1))) != cudaSuccess) goto fail;
