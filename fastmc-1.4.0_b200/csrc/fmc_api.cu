@@ -4,6 +4,7 @@
 
 #include "../../include/fastmc_b200.h"
 #include "fmc_chain.h"
+#include "fmc_restart.h"
 
 struct fmc_chain {
   fmc::Chain impl;
@@ -240,6 +241,80 @@ int fmc_guest_coords(fmc_chain* c, int iguest, double* xyz, int* nmol, int* nsit
   if (nsite) *nsite = C.sp[iguest].nsite;
   if (xyz) std::memcpy(xyz, C.sp[iguest].xyz.data(), sizeof(double) * C.sp[iguest].xyz.size());
   return 0;
+}
+
+int fmc_revive_write_state(const char* deck_dir, const char* outdir, int production, const int* nmol,
+                           const double* guest_xyz, const double* chainstats, const double* energy, double eng) {
+  if (!deck_dir || !outdir || !nmol) return fail(-1, "bad arguments");
+  fmc::InputDeck d;
+  std::string err;
+  int rc = fmc::read_input_deck(deck_dir, d, err);
+  if (rc) return fail(rc, err);
+  const int ng = (int)d.guests.size();
+  std::vector<std::vector<double>> xyz(ng);
+  size_t off = 0;
+  for (int g = 0; g < ng; g++) {
+    const size_t n = 3 * (size_t)nmol[g] * d.guests[g].nsite;
+    if (n && !guest_xyz) return fail(-1, "guest coordinates missing");
+    xyz[g].assign(guest_xyz + off, guest_xyz + off + n);
+    off += n;
+  }
+  std::vector<double> cs(1 + 14 * ng, 0.0), en(ng, 0.0);
+  if (chainstats) cs.assign(chainstats, chainstats + cs.size());
+  if (energy) en.assign(energy, energy + ng);
+  fmc::Revive r = fmc::revive_state(d, production != 0, xyz, cs, en);
+  rc = fmc::write_revive(std::string(outdir) + "/REVIVE", r, err);
+  if (!rc) rc = fmc::write_revcon(std::string(outdir) + "/REVCON", d, r, eng, err);
+  return rc ? fail(rc, err) : 0;
+}
+
+int fmc_revive_read(const char* path, const char* deck_dir, int* production, int* nmol, double* guest_xyz,
+                    double* chainstats, double* energy, int* natms) {
+  if (!path || !deck_dir) return fail(-1, "bad arguments");
+  fmc::InputDeck d;
+  std::string err;
+  int rc = fmc::read_input_deck(deck_dir, d, err);
+  if (rc) return fail(rc, err);
+  fmc::Revive r;
+  rc = fmc::read_revive(path, d, r, err);
+  if (rc) return fail(rc, err);
+  const auto xyz = fmc::revive_guest_xyz(d, r);
+  const int ng = (int)d.guests.size();
+  if (production) *production = r.production ? 1 : 0;
+  if (natms) *natms = r.natms;
+  size_t off = 0;
+  for (int g = 0; g < ng; g++) {
+    if (nmol) nmol[g] = (int)(xyz[g].size() / (3 * d.guests[g].nsite));
+    if (guest_xyz) std::memcpy(guest_xyz + off, xyz[g].data(), sizeof(double) * xyz[g].size());
+    off += xyz[g].size();
+  }
+  if (chainstats) std::memcpy(chainstats, r.chainstats.data(), sizeof(double) * r.chainstats.size());
+  if (energy) std::memcpy(energy, r.energy.data(), sizeof(double) * r.energy.size());
+  return 0;
+}
+
+int fmc_chain_write_revive(fmc_chain* c, const char* outdir) {
+  CHECK_CHAIN(c);
+  if (!outdir) return fail(-1, "bad arguments");
+  fmc::Chain& C = c->impl;
+  std::vector<std::vector<double>> xyz;
+  for (auto& s : C.sp) xyz.push_back(std::vector<double>(s.xyz.begin(), s.xyz.begin() + 3 * s.nmol * s.nsite));
+  fmc::Revive r = fmc::revive_state(C.sys.deck, C.production, xyz, C.chainstats, C.energy);
+  std::string err;
+  int rc = fmc::write_revive(std::string(outdir) + "/REVIVE", r, err);
+  const double eng = C.delE.empty() ? 0.0 : C.delE[C.last_guest];
+  if (!rc) rc = fmc::write_revcon(std::string(outdir) + "/REVCON", C.sys.deck, r, eng, err);
+  return rc ? fail(rc, err) : 0;
+}
+
+int fmc_chain_restart(fmc_chain* c, const char* revive_path) {
+  CHECK_CHAIN(c);
+  if (!revive_path) return fail(-1, "bad arguments");
+  fmc::Revive r;
+  std::string err;
+  int rc = fmc::read_revive(revive_path, c->impl.sys.deck, r, err);
+  if (!rc) rc = c->impl.restart(r, err);
+  return rc ? fail(rc, err) : 0;
 }
 
 int fmc_stats(fmc_chain* c, int iguest, double* out) {

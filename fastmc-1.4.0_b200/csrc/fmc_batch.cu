@@ -354,6 +354,7 @@ __device__ __noinline__ void bookkeep(ChainDev& C, const SysConst& Y, MoveSmem& 
       cs[4] = cs[4] + (e2 - cs[4]) / pc;
     }
   }
+  C.last_dE = accepted ? estep : 0.0;
   C.moves_done++;
   C.since_recompute++;
   if (rec) {

@@ -57,6 +57,7 @@ struct ChainDev {
   int rota_count, accept_rota, ins_count, del_count, accept_ins, accept_del;
   double delrdisp[kMaxGuestTypes], tran_delr[kMaxGuestTypes], rotangle, rota_rotangle;
   double elrc, energy[kMaxGuestTypes];
+  double last_dE;  // energy change of the last move if accepted, else 0 (the reference's delE)
   int production, lgchk, tick[5];
   long long prodcount;
   double stats[kMaxGuestTypes][5];  // rolling <N>, <E>, <EN>, <N^2>, <E^2>
@@ -154,6 +155,10 @@ class Batch {
   int nchains = 0;
   ~Batch();
   int open(const std::vector<std::string>& dirs, const std::vector<int>& seeds, int device, std::string& err);
+  // REVIVE + REVCON of chain c into outdir; restart of chain c from a REVIVE (call before
+  // the chain's first run to match the reference's restart, which re-seeds duni).
+  int write_revive(int c, const std::string& outdir, std::string& err);
+  int restart(int c, const std::string& revive_path, std::string& err);
   // One step: control blocks host->device, `moves` moves of every chain, control blocks (and
   // the optional per-move trace) device->host.  *ms: CUDA-event time of the kernel alone.
   int run(int moves, MoveRecord* trace_host, float* ms, std::string& err, double* shadow_host = nullptr);

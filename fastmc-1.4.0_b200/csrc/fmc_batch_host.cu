@@ -5,6 +5,7 @@
 #include <sstream>
 
 #include "fmc_batch.h"
+#include "fmc_restart.h"
 
 namespace fmc {
 
@@ -256,6 +257,100 @@ int Batch::open(const std::vector<std::string>& dirs, const std::vector<int>& se
   return 0;
 }
 
+int Batch::write_revive(int c, const std::string& outdir, std::string& err) {
+  const ChainDev& C = h_chains[c];
+  const Chain& S = *sys_chains[chain_sys[c]];
+  const InputDeck& d = S.sys.deck;
+  const int ng = (int)d.guests.size();
+  std::vector<std::vector<double>> xyz(ng);
+  cudaSetDevice(device);
+  for (int g = 0; g < ng; g++) {
+    const int n = C.nmol[g] * d.guests[g].nsite;
+    std::vector<double4> a(std::max(n, 1));
+    if (n) {
+      cudaError_t e = cudaMemcpy(a.data(), C.gsite + C.seg_off[g], sizeof(double4) * n, cudaMemcpyDeviceToHost);
+      if (e != cudaSuccess) {
+        err = cudaGetErrorString(e);
+        return -100 - (int)e;
+      }
+    }
+    for (int i = 0; i < n; i++) {
+      xyz[g].push_back(a[i].x);
+      xyz[g].push_back(a[i].y);
+      xyz[g].push_back(a[i].z);
+    }
+  }
+  std::vector<double> cs(1 + 14 * ng, 0.0), en(ng);
+  cs[0] = (double)C.prodcount;
+  for (int g = 0; g < ng; g++) {
+    for (int k = 0; k < 5; k++) cs[1 + 14 * g + k] = C.stats[g][k];
+    en[g] = C.energy[g];
+  }
+  Revive r = revive_state(d, C.production != 0, xyz, cs, en);
+  int rc = fmc::write_revive(outdir + "/REVIVE", r, err);
+  if (!rc) rc = fmc::write_revcon(outdir + "/REVCON", d, r, C.last_dE, err);
+  return rc;
+}
+
+int Batch::restart(int c, const std::string& path, std::string& err) {
+  ChainDev& C = h_chains[c];
+  Chain& S = *sys_chains[chain_sys[c]];
+  const InputDeck& d = S.sys.deck;
+  const int ng = (int)d.guests.size();
+  Revive r;
+  int rc = read_revive(path, d, r, err);
+  if (rc) return rc;
+  const std::vector<std::vector<double>> xyz = revive_guest_xyz(d, r);
+  for (int g = 0; g < ng; g++)
+    if ((int)(xyz[g].size() / 3) > C.seg_cap[g]) {
+      err = "REVIVE holds more guests than the chain's capacity (max guest atoms)";
+      return -75;
+    }
+  // the system's own chain computes the single point and S(k) of the restart state
+  cudaSetDevice(device);
+  rc = S.restart(r, err);
+  if (rc) return rc;
+  cudaError_t e = cudaMemcpy(C.sk, S.sk, sizeof(double2) * S.sys.K, cudaMemcpyDeviceToDevice);
+  for (int g = 0; g < ng && e == cudaSuccess; g++) {
+    const GuestSpecies& G = d.guests[g];
+    const int n = (int)(xyz[g].size() / 3);
+    std::vector<double4> a(std::max(n, 1));
+    std::vector<int> t(std::max(n, 1));
+    for (int i = 0; i < n; i++) {
+      a[i] = make_double4(xyz[g][3 * i], xyz[g][3 * i + 1], xyz[g][3 * i + 2], G.charge[i % G.nsite]);
+      t[i] = G.type[i % G.nsite];
+    }
+    if (n) e = cudaMemcpy(C.gsite + C.seg_off[g], a.data(), sizeof(double4) * n, cudaMemcpyHostToDevice);
+    if (n && e == cudaSuccess) e = cudaMemcpy(C.gtype + C.seg_off[g], t.data(), sizeof(int) * n, cudaMemcpyHostToDevice);
+  }
+  if (e != cudaSuccess) {
+    err = std::string("restart upload failed: ") + cudaGetErrorString(e);
+    return -100 - (int)e;
+  }
+  const HostSystem& H = S.sys;
+  std::memset(C.numtyp, 0, sizeof(C.numtyp));
+  for (int j = 0; j < H.nf; j++) C.numtyp[H.ftype[j]]++;
+  C.totatm = H.nf;
+  for (int g = 0; g < ng; g++) {
+    const GuestSpecies& G = d.guests[g];
+    C.nmol[g] = (int)(xyz[g].size() / (3 * G.nsite));
+    C.totatm += C.nmol[g] * G.nsite;
+    for (int m = 0; m < C.nmol[g]; m++)
+      for (int i = 0; i < G.nsite; i++) C.numtyp[G.type[i]]++;
+    C.energy[g] = S.spenergy;  // gcmc.f:547-556
+    for (int k = 0; k < 5; k++) C.stats[g][k] = r.chainstats[1 + 14 * g + k];
+  }
+  C.framatm = H.nf;
+  C.prodcount = 0;
+  C.last_dE = 0.0;
+  C.production = r.production;
+  if (C.production && C.eqsteps > 0) C.production = 0;  // gcmc.f:396-409
+  if (C.eqsteps == 0) C.production = 1;                 // gcmc.f:553-554
+  // the system chain goes back to the empty framework for the next restart or inspection
+  for (int g = 0; g < ng; g++) S.set_guests(g, 0, nullptr);
+  return 0;
+}
+
 int Batch::run(int moves, MoveRecord* trace_host, float* ms, std::string& err, double* shadow_host) {
   cudaSetDevice(device);
   BatchLaunch L;
@@ -449,6 +544,28 @@ int fmc_batch_chain_state(fmc_batch* b, int chain, double* out) {
   v[38] = C.lgchk ? 0.0 : 1.0;
   std::memcpy(out, v, sizeof(v));
   return 0;
+}
+
+int fmc_batch_write_revive(fmc_batch* b, int chain, const char* outdir) {
+  if (!b || chain < 0 || chain >= b->impl.nchains || !outdir) {
+    fmc::set_last_error("bad batch handle, chain index or directory");
+    return -1;
+  }
+  std::string err;
+  int rc = b->impl.write_revive(chain, outdir, err);
+  if (rc) fmc::set_last_error(err);
+  return rc;
+}
+
+int fmc_batch_restart(fmc_batch* b, int chain, const char* revive_path) {
+  if (!b || chain < 0 || chain >= b->impl.nchains || !revive_path) {
+    fmc::set_last_error("bad batch handle, chain index or path");
+    return -1;
+  }
+  std::string err;
+  int rc = b->impl.restart(chain, revive_path, err);
+  if (rc) fmc::set_last_error(err);
+  return rc;
 }
 
 int fmc_batch_guest_coords(fmc_batch* b, int chain, int iguest, double* xyz, int* nmol, int* nsite) {

@@ -1,5 +1,6 @@
 // Chain: device upload, single-point set-up and the plain-path host move loop.
 #include "fmc_chain.h"
+#include "fmc_restart.h"
 
 #include <algorithm>
 #include <cmath>
@@ -263,6 +264,30 @@ int Chain::set_guests(int g, int nmol, const double* xyz) {
   if (e != cudaSuccess) return sync_error(e);
   totatm = sys.nf;
   for (auto& x : sp) totatm += x.nmol * x.nsite;
+  return 0;
+}
+
+int Chain::restart(const Revive& r, std::string& err) {
+  const std::vector<std::vector<double>> xyz = revive_guest_xyz(sys.deck, r);
+  for (int g = 0; g < (int)sp.size(); g++) {
+    const int nmol = (int)(xyz[g].size() / (3 * sp[g].nsite));
+    if (set_guests(g, nmol, xyz[g].data())) {
+      err = "REVIVE holds more guests than the chain's capacity (max guest atoms)";
+      return -75;
+    }
+  }
+  int rc = single_point();
+  if (rc) {
+    err = "single point of the restart state failed on the device";
+    return rc;
+  }
+  energy.assign(sp.size(), spenergy);  // gcmc.f:547-556: every species starts at spenergy
+  delE.assign(sp.size(), 0.0);
+  if (r.chainstats.size() == chainstats.size()) chainstats = r.chainstats;
+  prodcount = 0;
+  production = r.production;
+  if (production && sys.deck.eqsteps > 0) production = false;  // gcmc.f:396-409
+  if (sys.deck.eqsteps == 0) production = true;                 // gcmc.f:553-554
   return 0;
 }
 
@@ -562,6 +587,7 @@ int Chain::step(MoveRecord* rec) {
   double e[3] = {0, 0, 0}, ewld3 = 0, delrc = 0, estep = 0, rande = -1;
   double oldx[3 * kMaxGuestSites], newx[3 * kMaxGuestSites];
   delE[g] = 0.0;
+  last_guest = g;
   int rc = 0;
   if (mtype == kInsert) {
     ins_count++;

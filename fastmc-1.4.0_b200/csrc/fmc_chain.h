@@ -94,6 +94,10 @@ class Chain {
   int single_point();
   int step(MoveRecord* rec);
   int set_guests(int g, int nmol, const double* xyz);  // replace species g (condense equivalent)
+  // Restart from a REVIVE (gcmc.f:353-418, revread): the stored guests, a fresh single point,
+  // every species' energy set to it, the production flag and chain statistics.
+  int restart(const struct Revive& r, std::string& err);
+  int last_guest = 0;  // species of the last move (the reference's REVCON energy is its delE)
   int sync_error(cudaError_t e, std::string* err = nullptr);
 };
 

@@ -506,6 +506,7 @@ void read_field(const std::string& dir, InputDeck& d, const Scan& s, std::vector
               d.fq.push_back(chg[k]);
               d.ftype.push_back(typ[k]);
               d.ffrz.push_back(frz[k]);
+              d.fname.push_back(names[k]);
             }
         }
         blocks.push_back(b);
@@ -735,6 +736,13 @@ int read_input_deck(const std::string& dir, InputDeck& d, std::string& err) {
     read_field(dir, d, s, blocks);
     read_config(dir, d, blocks);
     read_control(dir, d);
+    for (const MolBlock& b : blocks)
+      d.mols.push_back({b.guest ? b.index : -1, b.guest ? 0 : b.index, b.nummols, b.numatoms});
+    {
+      std::ifstream f(dir + "/CONFIG");
+      std::getline(f, d.title);
+      if (!d.title.empty() && d.title.back() == '\r') d.title.pop_back();
+    }
     return 0;
   } catch (const InputError& e) {
     err = e.msg;

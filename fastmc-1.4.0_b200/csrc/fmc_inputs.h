@@ -19,6 +19,13 @@ struct GuestSpecies {
   std::vector<double> xyz;         // 3*nmols*nsite, interleaved, molecule-major
 };
 
+// One FIELD molecule type in FIELD order (the layout of REVIVE records).
+struct MolLayout {
+  int guest;      // index into InputDeck::guests, or -1 for a framework type
+  int fw_offset;  // framework types: first atom in the condensed framework arrays
+  int nummols, numatoms;
+};
+
 struct InputDeck {
   // initscan
   int imcon = 0, keyfce = 0, kmax[3] = {0, 0, 0};
@@ -32,6 +39,9 @@ struct InputDeck {
   // framework atoms in condensed order (all non-guest molecules, FIELD order)
   std::vector<double> fx, fy, fz, fq;
   std::vector<int> ftype, ffrz;
+  std::vector<std::string> fname;  // framework site names, condensed order
+  std::vector<MolLayout> mols;     // FIELD molecule types in FIELD order
+  std::string title;               // CONFIG's first record, as written
   int ntpvdw = 0, maxvdw = 0, mxgrid = 0;
   std::vector<int> ltpvdw, lstvdw;           // [1..maxvdw+1]
   std::vector<std::array<double, 5>> prmvdw;  // [1..maxvdw+1], energies in internal units

@@ -6,6 +6,7 @@ ewald1_guest, guest real space = guestlistgen + ewald2 + srfrce, single_point) a
 loop, all evaluated on the GPU through libfastmc_b200.so.
 """
 import ctypes
+import os
 
 import numpy as np
 
@@ -143,6 +144,14 @@ class Chain:
         check(lib().fmc_guest_coords(self.h, int(iguest), dp(buf), ctypes.byref(n), ctypes.byref(ns)))
         return buf[: n.value]
 
+    def write_revive(self, outdir):
+        """REVIVE + REVCON of the chain's state in outdir (revive, utility_pack.f:1772-1817)."""
+        check(lib().fmc_chain_write_revive(self.h, str(outdir).encode()))
+
+    def restart(self, revive_path):
+        """Load a REVIVE: guests, fresh single point, production flag and statistics."""
+        check(lib().fmc_chain_restart(self.h, str(revive_path).encode()))
+
     def stats(self, iguest=0):
         out = np.zeros(6)
         check(lib().fmc_stats(self.h, int(iguest), dp(out)))
@@ -213,6 +222,13 @@ class Batch:
         out = np.zeros(40)
         check(lib().fmc_batch_chain_state(self.h, int(chain), dp(out)))
         return dict(zip(self._STATE, out.tolist()))
+
+    def write_revive(self, chain, outdir):
+        check(lib().fmc_batch_write_revive(self.h, int(chain), str(outdir).encode()))
+
+    def restart(self, chain, revive_path):
+        """Restart chain `chain` from a REVIVE (before its first run, like the reference)."""
+        check(lib().fmc_batch_restart(self.h, int(chain), str(revive_path).encode()))
 
     def guest_coords(self, chain, iguest=0):
         n, ns = ctypes.c_int(0), ctypes.c_int(0)
@@ -286,3 +302,66 @@ class Server:
         u, b = ctypes.c_longlong(0), ctypes.c_longlong(0)
         check(lib().fmc_server_memory(self.h, ctypes.byref(u), ctypes.byref(b)))
         return u.value, b.value
+
+
+# ------------------------------------------------------------------ checkpoint / restart
+def write_revive_state(deck_dir, outdir, guests, production=False, chainstats=None, energy=None, eng=0.0):
+    """Write outdir/REVIVE and outdir/REVCON (the reference's formats) for a deck and a host
+    state: `guests` is one (nmol, nsite, 3) array per guest species."""
+    gs = [np.asarray(g, dtype=np.float64).reshape(-1, 3) for g in guests]
+    info = deck_inspect(deck_dir)
+    ng = info["nspecies"]
+    nmol = np.zeros(max(ng, 1), dtype=np.int32)
+    for i in range(ng):
+        ns = _species_sites(deck_dir, i)
+        nmol[i] = len(gs[i]) // ns if ns else 0
+    xyz = np.ascontiguousarray(np.concatenate([g.reshape(-1) for g in gs]) if gs else np.zeros(1))
+    cs = np.ascontiguousarray(chainstats if chainstats is not None else np.zeros(1 + 14 * ng), dtype=np.float64)
+    en = np.ascontiguousarray(energy if energy is not None else np.zeros(ng), dtype=np.float64)
+    check(lib().fmc_revive_write_state(str(deck_dir).encode(), str(outdir).encode(), int(bool(production)), ip(nmol),
+                                       dp(xyz), dp(cs), dp(en), float(eng)))
+
+
+def _species_sites(deck_dir, g):
+    """Sites per molecule of guest species g of a deck."""
+    return _SITES_CACHE.setdefault((str(deck_dir), g), _read_sites(deck_dir, g))
+
+
+_SITES_CACHE = {}
+
+
+def _read_sites(deck_dir, g):
+    # the FIELD guest blocks in order: the first ATOMS record after the g-th &guest header
+    lines = open(os.path.join(str(deck_dir), "FIELD")).read().lower().splitlines()
+    k = -1
+    for i, line in enumerate(lines):
+        if "&guest" in line:
+            k += 1
+            if k == g:
+                for l2 in lines[i + 1:]:
+                    if l2.strip().startswith("atoms"):
+                        return int(l2.split()[1])
+    raise ValueError("guest species not found in FIELD")
+
+
+def read_revive(path, deck_dir):
+    """A REVIVE as a dict: production, natms, chainstats, energy, guests (one (nmol, nsite, 3)
+    array per species)."""
+    info = deck_inspect(deck_dir)
+    ng = info["nspecies"]
+    nmol = np.zeros(max(ng, 1), dtype=np.int32)
+    prod, natms = ctypes.c_int(0), ctypes.c_int(0)
+    d, p = str(deck_dir).encode(), str(path).encode()
+    check(lib().fmc_revive_read(p, d, None, ip(nmol), None, None, None, None))
+    ns = [_read_sites(deck_dir, g) for g in range(ng)]
+    xyz = np.zeros(max(1, sum(int(nmol[g]) * ns[g] * 3 for g in range(ng))))
+    cs = np.zeros(1 + 14 * ng)
+    en = np.zeros(max(ng, 1))
+    check(lib().fmc_revive_read(p, d, ctypes.byref(prod), ip(nmol), dp(xyz), dp(cs), dp(en), ctypes.byref(natms)))
+    guests, off = [], 0
+    for g in range(ng):
+        n = int(nmol[g]) * ns[g] * 3
+        guests.append(xyz[off:off + n].reshape(int(nmol[g]), ns[g], 3))
+        off += n
+    return {"production": bool(prod.value), "natms": natms.value, "chainstats": cs, "energy": en[:ng],
+            "guests": guests}

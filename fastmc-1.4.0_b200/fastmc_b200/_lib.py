@@ -51,6 +51,12 @@ SIGNATURES = {
     "fmc_batch_run_shadow": (_ci, [_vp, _ci, _vp, _vp, ctypes.POINTER(ctypes.c_float)]),
     "fmc_batch_chain_state": (_ci, [_vp, _ci, _dp]),
     "fmc_batch_guest_coords": (_ci, [_vp, _ci, _ci, _dp, _ip, _ip]),
+    "fmc_revive_write_state": (_ci, [ctypes.c_char_p, ctypes.c_char_p, _ci, _ip, _dp, _dp, _dp, ctypes.c_double]),
+    "fmc_revive_read": (_ci, [ctypes.c_char_p, ctypes.c_char_p, _ip, _ip, _dp, _dp, _dp, _ip]),
+    "fmc_chain_write_revive": (_ci, [_vp, ctypes.c_char_p]),
+    "fmc_chain_restart": (_ci, [_vp, ctypes.c_char_p]),
+    "fmc_batch_write_revive": (_ci, [_vp, _ci, ctypes.c_char_p]),
+    "fmc_batch_restart": (_ci, [_vp, _ci, ctypes.c_char_p]),
     "fmc_server_open": (_ci, [_ci, _ci, ctypes.c_longlong, _ci, ctypes.POINTER(_vp)]),
     "fmc_server_close": (None, [_vp]),
     "fmc_server_set_precision": (_ci, [_vp, _ci, ctypes.c_longlong]),

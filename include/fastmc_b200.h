@@ -101,6 +101,23 @@ int fmc_guest_coords(fmc_chain* c, int iguest, double* xyz, int* nmol, int* nsit
  * out[0..5] = <N>, <E>, <EN>, <N^2>, <E^2>, production moves counted. */
 int fmc_stats(fmc_chain* c, int iguest, double* out);
 
+/* ---------------------------------------------------------------- checkpoint / restart
+ * REVIVE and REVCON in the reference's formats (revive, utility_pack.f:1772-1817; revread,
+ * 1840-1878): REVIVE is Fortran unformatted sequential (4-byte little-endian record markers):
+ * production flag, nummols per FIELD molecule type, chainstats(1+14*nguest), natms, x/y/z per
+ * molecule type, energy per guest species.  A restart (gcmc.f:353-418) loads the guests,
+ * recomputes the single point and sets every species' energy to it, keeps the production flag
+ * unless a positive equilibration count follows, restores chainstats and restarts prodcount. */
+/* Writes outdir/REVIVE and outdir/REVCON for a deck and a state given on the host (no GPU):
+ * nmol[nguest]; guest_xyz = every species' interleaved xyz, species after species. */
+int fmc_revive_write_state(const char* deck_dir, const char* outdir, int production, const int* nmol,
+                           const double* guest_xyz, const double* chainstats, const double* energy, double eng);
+/* Reads a REVIVE against the deck's FIELD; any output may be NULL (nmol first to size guest_xyz). */
+int fmc_revive_read(const char* path, const char* deck_dir, int* production, int* nmol, double* guest_xyz,
+                    double* chainstats, double* energy, int* natms);
+int fmc_chain_write_revive(fmc_chain* c, const char* outdir);  /* replaces revive */
+int fmc_chain_restart(fmc_chain* c, const char* revive_path);   /* replaces revread + restart */
+
 /* ---------------------------------------------------------------- batched path
  * Many independent chains (isotherm points) advanced by one persistent kernel, one CTA per
  * chain, the whole move loop of gcmc.f:589-1380 on the device (no counterpart in the
@@ -137,6 +154,10 @@ int fmc_batch_profile(fmc_batch* b, int enable);
  * re-evaluations and S(k) recomputes (mixed precision), then 1 once the chain has finished. */
 int fmc_batch_chain_state(fmc_batch* b, int chain, double* out);
 int fmc_batch_guest_coords(fmc_batch* b, int chain, int iguest, double* xyz, int* nmol, int* nsite);
+/* Checkpoint / restart of one chain of a batch (formats as fmc_chain_write_revive).  A restart
+ * before the chain's first run matches the reference's restart, which re-seeds duni. */
+int fmc_batch_write_revive(fmc_batch* b, int chain, const char* outdir);
+int fmc_batch_restart(fmc_batch* b, int chain, const char* revive_path);
 
 /* ---------------------------------------------------------------- serving
  * Isotherm-point requests (an input-deck directory, a duni seed and a budget) served with

@@ -2570,6 +2570,18 @@ int orc_load_guests(void* p, int g, int nmol, const double* xyz) {
   C.energy.assign(C.ntpguest, C.spenergy);
   return C.totatm;
 }
+// State a restart takes from REVIVE besides the coordinates (gcmc.f:353-418 with revread,
+// utility_pack.f:1840-1878): the production flag, kept only when no positive equilibration
+// count follows (gcmc.f:396-409) and forced when there is none at all (gcmc.f:553-554), and
+// the chain statistics; prodcount starts again at zero (gcmc.f:143).
+void orc_restart_flags(void* p, int production, const double* chainstats) {
+  Chain& C = ((OrcHandle*)p)->C;
+  C.production = production != 0;
+  if (C.production && C.eqsteps > 0) C.production = false;
+  if (C.eqsteps == 0) C.production = true;
+  for (size_t i = 0; i < C.chainstats.size(); i++) C.chainstats[i] = chainstats[i];
+  C.prodcount = 0;
+}
 // Rolling statistics of guest type g: <N>,<E>,<EN>,<N^2>,<E^2>, prodcount
 void orc_stats(void* p, int g, double* out) {
   Chain& C = ((OrcHandle*)p)->C;

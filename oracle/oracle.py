@@ -67,6 +67,7 @@ def lib():
         L.orc_guest_coords.argtypes = [vp, ctypes.c_int, dp]
         L.orc_load_guests.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp]
         L.orc_stats.argtypes = [vp, ctypes.c_int, dp]
+        L.orc_restart_flags.argtypes = [vp, ctypes.c_int, dp]
         assert L.orc_sizeof_moverec() == MOVE_DTYPE.itemsize
         _lib = L
     return _lib
@@ -212,6 +213,11 @@ class Chain:
 
     def duni(self):
         return lib().orc_duni(self.h)
+
+    def restart_flags(self, production, chainstats):
+        """Production flag and chain statistics of a restart from REVIVE (after load_guests)."""
+        cs = np.ascontiguousarray(chainstats, dtype=np.float64)
+        lib().orc_restart_flags(self.h, int(production), _dp(cs))
 
     def stats(self, g=0):
         out = np.zeros(6)

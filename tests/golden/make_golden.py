@@ -13,7 +13,11 @@ expected.json come from that example's OUTPUT and REVIVE:
 * OUTPUT:108  duni seed "103 112 53 153"
 * OUTPUT:113  "Energy reported by DL_POLY: -11190.606165" (empty framework, recip + self)
 * REVIVE      energy(1) = -731.5072668178669 kcal/mol for the 90-CO2 state it stores
+* REVIVE      its production flag, chainstats and natms, and the SHA-256 of REVIVE and REVCON,
+              so that a writer restating revive (utility_pack.f:1772-1817) can be checked
+              byte for byte without the files themselves
 """
+import hashlib
 import json
 import os
 import shutil
@@ -50,6 +54,11 @@ def main(ref):
     gx, gy, gz = (np.frombuffer(recs[4 + i], "<f8") for i in range(3))
     guests = np.stack([gx, gy, gz], axis=1).reshape(nco2, 3, 3)
     energy = float(np.frombuffer(recs[-1], "<f8")[0])
+    production = int(np.frombuffer(recs[0], "<i4")[0])
+    chainstats = [float(v) for v in np.frombuffer(recs[2], "<f8")]
+    natms = int(np.frombuffer(recs[3], "<i4")[0])
+    sha = {f: hashlib.sha256(open(os.path.join(src, "branch01", f), "rb").read()).hexdigest()
+           for f in ("REVIVE", "REVCON")}
     np.save(os.path.join(out, "revive_guests.npy"), guests)
     expected = {
         "seed": [103, 112, 53, 153],
@@ -59,6 +68,11 @@ def main(ref):
         "K": 870,
         "revive_nummols": [int(v) for v in nummols],
         "revive_energy_kcal": energy,
+        "revive_production": production,
+        "revive_chainstats": chainstats,
+        "revive_natms": natms,
+        "revive_sha256": sha["REVIVE"],
+        "revcon_sha256": sha["REVCON"],
         "source": EXAMPLE + " (OUTPUT lines 108, 113; branch01/REVIVE)",
     }
     with open(os.path.join(out, "expected.json"), "w") as f:
