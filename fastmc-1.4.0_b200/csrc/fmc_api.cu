@@ -365,6 +365,23 @@ int fmc_run_timed(fmc_chain* c, int nmoves, fmc_move_record* trace, float* devic
   return rc;
 }
 
+int fmc_deck_vdw(const char* dir, int k, double* out, int* ntables) {
+  if (!dir) return fail(-1, "null argument");
+  fmc::InputDeck deck;
+  std::string err;
+  int rc = fmc::read_input_deck(dir, deck, err);
+  if (rc) return fail(rc, err);
+  fmc::HostSystem S;
+  rc = fmc::build_host_system(deck, S, err);
+  if (rc) return fail(rc, err);
+  if (ntables) *ntables = S.ntables;
+  if (out) {
+    if (k < 1 || k > S.ntables) return fail(-1, "table index out of range");
+    for (int i = 0; i <= S.mxgrid; i++) out[i] = S.vvv[(size_t)k * (S.mxgrid + 1) + i];
+  }
+  return 0;
+}
+
 int fmc_deck_inspect(const char* dir, int* ints, double* dbls, int* lmn, double* akk, double* erc, double* charges,
                      int* K, int* nerc) {
   if (!dir) return fail(-1, "null argument");

@@ -400,8 +400,6 @@ __device__ __forceinline__ void lrc_warp(const ChainDev& C, const SysConst& Y, M
 }
 
 // One real-space candidate: a framework atom from a site's voxel list or a guest site.
-constexpr int kRealDepth = 1;  // candidates a thread takes per loop trip (1-8 measured; 1 is fastest)
-
 struct Cand {
   double4 a;
   int type, site;
@@ -478,8 +476,9 @@ __device__ __forceinline__ void build_phases(const DevSystem& S, const MoveSmem&
 // All threads: this thread's share of the reciprocal sum and of the real-space pairs.
 // v[0] sum akk*d|S|^2, v[1] ewld2, v[2] vdw, v[3] and v[4] the absolute sums that bound the
 // rounding error of v[0] and v[1]+v[2] (mixed precision).  S_new goes to Sn when write_sn.
-// Real-space sums of one pass: every (site, candidate) pair, kRealDepth candidates in flight per
-// thread, compiled per boundary condition so the hot loop holds one minimum-image form.
+// Real-space sums of one pass: every (site, candidate) pair, compiled per boundary condition so
+// the hot loop holds one minimum-image form.  Deeper unrolling (2-8 candidates per trip) was
+// measured slower: the larger loop costs more in instruction fetch than it hides in latency.
 template <bool kMixed, int kImcon>
 __device__ __noinline__ void real_space(const DevSystem& S, const ChainDev& C, const MoveSmem& M, int nseg,
                                         const int* prow_s, int nt1, int fp32_mask, double* vout) {
@@ -488,16 +487,16 @@ __device__ __noinline__ void real_space(const DevSystem& S, const ChainDev& C, c
   const bool sub_old = (mtype != kInsert && mtype != kDelete);
   const int T = M.pre[nsite];
   const float rdrf_e = (float)S.rdr_e, rdrf_v = (float)S.rdr_v;
-  // a thread takes candidates tid, tid + 256, tid + 512, ... in that order whatever the depth
-  int sc[kRealDepth];
+  // a thread takes candidates tid, tid + 256, tid + 512, ... in that order
+  // one candidate per loop trip, the next one's loads issued before this one is evaluated
+  int s_next = 0;
+  Cand pre = fetch_candidate(S, C, M, nseg, tid, s_next);
+  for (int base = tid; base < T; base += kBatchThreads) {
+    Cand c[1];
+    c[0] = pre;
+    pre = fetch_candidate(S, C, M, nseg, base + kBatchThreads, s_next);
 #pragma unroll
-  for (int u = 0; u < kRealDepth; u++) sc[u] = 0;
-  for (int base = tid; base < T; base += kRealDepth * kBatchThreads) {
-    Cand c[kRealDepth];
-#pragma unroll
-    for (int u = 0; u < kRealDepth; u++) c[u] = fetch_candidate(S, C, M, nseg, base + u * kBatchThreads, sc[u]);
-#pragma unroll
-    for (int u = 0; u < kRealDepth; u++) {
+    for (int u = 0; u < 1; u++) {
       if (!c[u].live) continue;
       const int st = c[u].site;
       const int row = prow_s[M.type[st] * nt1 + c[u].type];

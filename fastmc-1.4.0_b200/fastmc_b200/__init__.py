@@ -41,6 +41,20 @@ def deck_inspect(directory):
     return info
 
 
+def deck_vdw(directory):
+    """The deck's vdW tables (host, no GPU): list of arrays, table 1 first."""
+    n = ctypes.c_int(0)
+    d = str(directory).encode()
+    check(lib().fmc_deck_vdw(d, 0, None, ctypes.byref(n)))
+    npts = deck_inspect(directory)["mxgrid"] + 1
+    out = []
+    for k in range(1, n.value + 1):
+        a = np.zeros(npts)
+        check(lib().fmc_deck_vdw(d, k, dp(a), None))
+        out.append(a)
+    return out
+
+
 class Chain:
     """One GCMC chain on one GPU (the plain FP64 path)."""
 

@@ -66,6 +66,7 @@ SIGNATURES = {
     "fmc_server_poll": (_ci, [_vp, _ci, _ip, _dp]),
     "fmc_server_stats": (_ci, [_vp, _dp]),
     "fmc_server_memory": (_ci, [_vp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
+    "fmc_deck_vdw": (_ci, [ctypes.c_char_p, _ci, _dp, _ip]),
     "fmc_deck_inspect": (_ci, [ctypes.c_char_p, _ip, _dp, _ip, _dp, _dp, _dp, _ip, _ip]),
 }
 

@@ -112,8 +112,38 @@ def _fmt(x):
     return f"{x:.10f}"
 
 
+def _pair_line(a, b, eps, sig, form):
+    """A FIELD vdW line of the given functional form whose well matches LJ(eps, sig)."""
+    r6 = sig ** 6
+    rm = 2.0 ** (1.0 / 6.0) * sig
+    if form == "lj" or eps == 0.0:
+        body = f"lj {eps:.6f} {sig:.6f}"
+    elif form == "12-6":
+        body = f"12-6 {4 * eps * r6 * r6:.6f} {4 * eps * r6:.6f}"
+    elif form == "nm":
+        body = f"nm {eps:.6f} 12.0 6.0 {rm:.6f}"
+    elif form == "buck":
+        body = f"buck {eps * 1.0e7:.6f} {sig / 10.0:.6f} {4 * eps * r6:.6f}"
+    elif form == "bhm":
+        body = f"bhm {eps * 50.0:.6f} {12.0 / sig:.6f} {rm:.6f} {4 * eps * r6:.6f} {eps * sig ** 8:.6f}"
+    elif form == "hbnd":
+        body = f"hbnd {4 * eps * r6 * r6:.6f} {4 * eps * sig ** 10:.6f}"
+    elif form == "snm":
+        body = f"snm {eps:.6f} 12.0 6.0 {rm:.6f} 0.0"
+    elif form == "mors":
+        body = f"mors {eps:.6f} {rm:.6f} {6.0 / sig:.6f}"
+    elif form == "wca":
+        body = f"wca {eps:.6f} {sig:.6f} 0.0"
+    else:
+        raise ValueError(form)
+    return f"{a:<8s} {b:<8s} {body}"
+
+
+VDW_FORMS = ("lj", "12-6", "nm", "buck", "bhm", "hbnd", "snm", "mors", "wca")
+
+
 def write_inputs(path, fw, gases, pressures_bar, temp, kmax, moves=None, eq_cycles=-5000, prod_cycles=-5000,
-                 imcon=None, title="synthetic framework", rcut=RCUT, alpha=ALPHA, delr=1.0):
+                 imcon=None, title="synthetic framework", rcut=RCUT, alpha=ALPHA, delr=1.0, vdw_forms=("lj",)):
     """Write CONTROL, FIELD and CONFIG for one chain into directory `path`."""
     os.makedirs(path, exist_ok=True)
     if imcon is None:
@@ -160,7 +190,7 @@ def write_inputs(path, fw, gases, pressures_bar, temp, kmax, moves=None, eq_cycl
             eb, sb = lj[b]
             eps = math.sqrt(ea * eb)
             sig = 0.5 * (sa + sb) if eps > 0 else 0.0
-            pairs.append(f"{a:<8s} {b:<8s} lj {eps:.6f} {sig:.6f}")
+            pairs.append(_pair_line(a, b, eps, sig, vdw_forms[len(pairs) % len(vdw_forms)]))
     lines.append(f"VDW {len(pairs)}")
     lines += pairs
     lines.append("close")

@@ -221,6 +221,9 @@ int fmc_ewald1_guest_noalloc(int K, const int* kmax, const double* cell, const i
 /* Host-only (no GPU needed): parse a deck and build its tables.  ints/dbls as in
  * fmc_chain_info (entries that need the device are zero).  Any of lmn[3K], akk[K], erc[mxgrid+1],
  * charges[framework atoms] may be NULL; *K and *nerc return the sizes. */
+/* vdW table k (1-based, FIELD pair order; forgen, vdw_terms.f:190-396) of a deck: mxgrid+1
+ * values; *ntables = tables including the zero table for undefined pairs. */
+int fmc_deck_vdw(const char* dir, int k, double* out, int* ntables);
 int fmc_deck_inspect(const char* dir, int* ints, double* dbls, int* lmn, double* akk, double* erc, double* charges,
                      int* K, int* nerc);
 

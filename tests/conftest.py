@@ -51,6 +51,9 @@ def decks(tmp_path_factory):
         L = [fw.cell[j, j] for j in range(3)]
         out[f"ortho{i}"] = synth.write_inputs(str(root / f"ortho{i}"), fw, ["CO2"], [1.0], 298.0,
                                               tuple(synth.kmax_for(x) for x in L))
+    L = [fws[1].cell[j, j] for j in range(3)]
+    out["forms"] = synth.write_inputs(str(root / "forms"), fws[1], ["CO2"], [1.0], 298.0,
+                                      tuple(synth.kmax_for(x) for x in L), vdw_forms=synth.VDW_FORMS)
     fw = fws[0]
     out["mixture"] = synth.write_inputs(str(root / "mixture"), fw, ["CO2", "N2"], [0.15, 0.85], 298.0,
                                         tuple(synth.kmax_for(fw.cell[j, j]) for j in range(3)))

@@ -44,3 +44,12 @@ def test_batch_isolation_alone_vs_mixed(fmc, decks):
     for key in ("mtype", "randchoice", "accepted", "nmols_after"):
         assert np.array_equal(ta[0][key], tm[1][key])
     assert np.array_equal(ta[0]["estep"], tm[1]["estep"])
+
+
+def test_batch_every_vdw_form_replays_oracle(fmc, oracle_mod, decks):
+    """All nine pair forms of forgen in one deck (each pair of types uses one of them)."""
+    seeds = [(2, 4, 6, 8), (3, 5, 7, 9)]
+    b = fmc.Batch([decks["forms"]] * 2, seeds)
+    tr, _ = b.run(1500, trace=True)
+    for i, s in enumerate(seeds):
+        _compare_traces(tr[i], oracle_mod.Chain(decks["forms"], seed=s).run(1500))

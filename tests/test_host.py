@@ -46,6 +46,19 @@ def test_deck_tables_match_oracle_bit_exact(fmc, oracle_mod, decks, name):
     assert np.array_equal(info["charges"], q[len(q) - info["nframework"]:])
 
 
+def test_every_vdw_form_tabulates_like_the_oracle(fmc, oracle_mod, decks):
+    """The nine pair forms of forgen (vdw_terms.f:190-396), each used by some pair of the deck."""
+    field = open(decks["forms"] + "/FIELD").read().lower()
+    for form in ("12-6", " lj ", " nm ", "buck", " bhm ", "hbnd", " snm ", "mors", " wca "):
+        assert form in field, form
+    tabs = fmc.deck_vdw(decks["forms"])
+    orc = oracle_mod.Chain(decks["forms"])
+    ntpvdw = int(next(l for l in field.splitlines() if l.startswith("vdw")).split()[1])
+    assert ntpvdw >= 9 and len(tabs) >= ntpvdw
+    for k in range(1, ntpvdw + 1):
+        assert np.array_equal(tabs[k - 1], orc.vvv(k)), k
+
+
 def _copy_deck(src, dst):
     shutil.copytree(src, dst)
     return dst
