@@ -1,4 +1,5 @@
 // extern "C" boundary (include/fastmc_b200.h) over fmc::Chain.
+#include <cstdio>
 #include <cstring>
 #include <string>
 
@@ -317,6 +318,54 @@ int fmc_chain_restart(fmc_chain* c, const char* revive_path) {
   return rc ? fail(rc, err) : 0;
 }
 
+int fmc_atomic_number(double mass) { return fmc::atomic_number(mass); }
+
+int fmc_write_prob_cube(const char* deck_dir, const char* path, const double* grid, long long steps) {
+  if (!deck_dir || !path || !grid || steps < 1) return fail(-1, "bad arguments");
+  fmc::InputDeck d;
+  std::string err;
+  int rc = fmc::read_input_deck(deck_dir, d, err);
+  if (!rc && d.plots.empty()) {
+    rc = -1;
+    err = "the deck requests no probability plots";
+  }
+  if (!rc) rc = fmc::write_prob_cube(path, d, grid, steps, err);
+  return rc ? fail(rc, err) : 0;
+}
+
+int fmc_chain_prob(fmc_chain* c, int plot, int* dims, double* out) {
+  CHECK_CHAIN(c);
+  const fmc::Chain& C = c->impl;
+  const fmc::InputDeck& d = C.sys.deck;
+  if (dims) {
+    dims[0] = (int)C.prob.size();
+    for (int a = 0; a < 3; a++) dims[1 + a] = d.ngrid[a];
+  }
+  if (out) {
+    if (plot < 0 || plot >= (int)C.prob.size()) return fail(-1, "plot index out of range");
+    std::memcpy(out, C.prob[plot].data(), sizeof(double) * C.prob[plot].size());
+  }
+  return 0;
+}
+
+int fmc_chain_write_prob(fmc_chain* c, const char* outdir) {
+  CHECK_CHAIN(c);
+  if (!outdir) return fail(-1, "bad arguments");
+  const fmc::Chain& C = c->impl;
+  const fmc::InputDeck& d = C.sys.deck;
+  if (C.prodcount <= 0) return 0;  // gcmc.f:2213: nothing is written before production
+  std::vector<int> per(d.guests.size(), 0);
+  for (size_t ip = 0; ip < d.plots.size(); ip++) {
+    const int g = d.plots[ip].guest;
+    char name[64];
+    std::snprintf(name, sizeof(name), "/prob_guest%02d_prob_%02d.cube", g + 1, ++per[g]);
+    std::string err;
+    int rc = fmc::write_prob_cube(std::string(outdir) + name, d, C.prob[ip].data(), C.prodcount, err);
+    if (rc) return fail(rc, err);
+  }
+  return 0;
+}
+
 int fmc_stats(fmc_chain* c, int iguest, double* out) {
   CHECK_CHAIN(c);
   fmc::Chain& C = c->impl;
@@ -396,7 +445,7 @@ int fmc_deck_inspect(const char* dir, int* ints, double* dbls, int* lmn, double*
   int natoms = S.nf;
   for (auto& g : deck.guests) natoms += g.nmols * g.nsite;
   int iv[16] = {S.cell.imcon, deck.kmax[0], deck.kmax[1], deck.kmax[2], S.K, natoms, (int)deck.guests.size(),
-                S.ntypes, S.mxgrid, S.nf, 0, nv, 0, 0, 0, 0};
+                S.ntypes, S.mxgrid, S.nf, 0, nv, (int)deck.plots.size(), deck.ngrid[0], deck.ngrid[1], deck.ngrid[2]};
   double dv[16] = {S.alpha, S.rcut, deck.delr, S.cell.volm, S.engunit, deck.temp, S.beta, S.drewd, S.dlrpot,
                    0, 0, 0, 0, 0, S.statvolm, 0};
   if (ints) std::memcpy(ints, iv, sizeof(iv));

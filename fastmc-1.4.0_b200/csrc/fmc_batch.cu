@@ -614,6 +614,50 @@ __device__ __noinline__ void sums(const DevSystem& S, const ChainDev& C, const M
   else real_space<kMixed, 0>(S, C, M, nseg, prow_s, nt1, fp32_mask, v);
 }
 
+// All threads, in production: storeprob (utility_pack.f:496-561) for the chain's state after the
+// move, one guest molecule per thread, weights added to the plots' fixed-point grids.
+__device__ __noinline__ void prob_store(const SysConst& Y, const ChainDev& C) {
+  const int na = Y.ngrid[0], nb = Y.ngrid[1], nc = Y.ngrid[2];
+  const long long cells = (long long)na * nb * nc;
+  int base = 0;
+  for (int g = 0; g < Y.nspecies; g++) {
+    const SpeciesConst& P = Y.sp[g];
+    const int ns = P.nsite, nmol = C.nmol[g];
+    for (int m = threadIdx.x; m < nmol; m += blockDim.x) {
+      double x[kBatchMaxSites], y[kBatchMaxSites], z[kBatchMaxSites];
+      const double4* site = C.gsite + C.seg_off[g] + m * ns;
+      for (int i = 0; i < ns; i++) {
+        double4 a = site[i];
+        x[i] = a.x;
+        y[i] = a.y;
+        z[i] = a.z;
+      }
+      double c[3], fc[3];
+      centre_of_mass(P.mass, ns, x, y, z, 1, c);
+      frac_wrap(Y.S.cell.rh, c[0], c[1], c[2], fc);
+      for (int ip = 0; ip < Y.nplots; ip++) {
+        if (Y.plot_guest[ip] != g) continue;
+        unsigned long long* grid = C.prob + ip * cells;
+        auto add = [grid](long long i, double w) {
+          atomicAdd(grid + i, (unsigned long long)llrint(w * 4294967296.0));
+        };
+        for (int j = 0; j < Y.plot_nsite[ip]; j++) {
+          const int s = Y.plot_site[ip][j];
+          if (s == 0) {
+            equitable_bin(na, nb, nc, fc[0], fc[1], fc[2], add);
+          } else {
+            double f[3];
+            frac_wrap(Y.S.cell.rh, x[s - 1], y[s - 1], z[s - 1], f);
+            equitable_bin(na, nb, nc, f[0], f[1], f[2], add);
+          }
+        }
+      }
+    }
+    base += nmol;
+  }
+  (void)base;
+}
+
 // All threads: FP64 recompute of S(k) = S_framework(k) + sum over guest sites (bounds the drift
 // of the mixed-precision running sums).  Each thread owns its k-vectors.
 __device__ __forceinline__ void recompute_sk(const DevSystem& S, const SysConst& Y, const ChainDev& C, int nseg,
@@ -831,8 +875,11 @@ __global__ void __launch_bounds__(kBatchThreads, 2) fmc_batch_kernel(BatchLaunch
         C.gtype[M.commit_lo + tid] = M.type[st];
       }
     }
+    // read before the barrier: thread 0 may change the production flag in the next move_begin
+    const bool store = Y.nplots && C.production;
     __syncthreads();
     if (prof && tid == 0) C.prof[4] += clock64() - t0;
+    if (store) prob_store(Y, C);  // every production move (gcmc.f:1929-1931)
     if (last) break;
   }
   for (int k = tid; k < K; k += blockDim.x) C.sk[k] = Sk[k];

@@ -17,6 +17,8 @@ constexpr int kBatchMaxSites = 16;  // sites per guest species on the batched pa
 constexpr int kBatchMaxTypes = 16;  // unique atom types
 constexpr int kBatchMaxTab = kBatchMaxTypes * (kBatchMaxTypes + 1) / 2;
 constexpr int kBatchThreads = 256;
+constexpr int kMaxPlots = 8;      // probability plots per system
+constexpr int kMaxPlotSites = 8;  // sites per plot (0 = centre of mass)
 
 struct SpeciesConst {
   int nsite;
@@ -35,6 +37,9 @@ struct SysConst {
   int numfrz[kBatchMaxTypes + 1];
   double engunit, volm, statvolm;
   const double2* sk_fw;  // S(k) of the framework alone (periodic FP64 recompute)
+  // probability plots (storeprob): grid cells per axis, and per plot its species and sites
+  int nplots, ngrid[3];
+  int plot_guest[kMaxPlots], plot_nsite[kMaxPlots], plot_site[kMaxPlots][kMaxPlotSites];
 };
 
 // Per-chain parameters and mutable state (device memory).
@@ -73,6 +78,9 @@ struct ChainDev {
   double4* gsite;
   int* gtype;
   int seg_off[kMaxGuestTypes], seg_cap[kMaxGuestTypes];
+  // probability plots: nplots grids of weights in fixed point (units of 2^-32), summed with
+  // integer atomics so the totals do not depend on the order of the adds
+  unsigned long long* prob;
 };
 
 struct BatchLaunch {

@@ -1,4 +1,5 @@
 // Host side of the batched path: deduplicated device systems, per-chain state, launches.
+#include <cstdio>
 #include <cstring>
 #include <fstream>
 #include <map>
@@ -67,6 +68,22 @@ int fill_sysconst(const HostSystem& H, const DevSystem& S, SysConst& Y, int* tab
   Y.engunit = H.engunit;
   Y.volm = H.cell.volm;
   Y.statvolm = H.statvolm;
+  const InputDeck& d = H.deck;
+  if ((int)d.plots.size() > kMaxPlots) {
+    err = "more probability plots than the batched path supports";
+    return -5;
+  }
+  Y.nplots = (int)d.plots.size();
+  for (int a = 0; a < 3; a++) Y.ngrid[a] = d.ngrid[a];
+  for (int ip = 0; ip < Y.nplots; ip++) {
+    if ((int)d.plots[ip].sites.size() > kMaxPlotSites) {
+      err = "a probability plot lists more sites than the batched path supports";
+      return -5;
+    }
+    Y.plot_guest[ip] = d.plots[ip].guest;
+    Y.plot_nsite[ip] = (int)d.plots[ip].sites.size();
+    for (size_t j = 0; j < d.plots[ip].sites.size(); j++) Y.plot_site[ip][j] = d.plots[ip].sites[j];
+  }
   return 0;
 }
 
@@ -146,6 +163,11 @@ int init_chain_state(const InputDeck& d, const HostSystem& H, const double2* sk_
   }
   if (e == cudaSuccess) e = alloc((void**)&C.gsite, sizeof(double4) * std::max(off, 1));
   if (e == cudaSuccess) e = alloc((void**)&C.gtype, sizeof(int) * std::max(off, 1));
+  if (e == cudaSuccess && !H.deck.plots.empty()) {
+    const size_t n = H.deck.plots.size() * (size_t)H.deck.ngrid[0] * H.deck.ngrid[1] * H.deck.ngrid[2];
+    e = alloc((void**)&C.prob, sizeof(unsigned long long) * n);
+    if (e == cudaSuccess) e = cudaMemsetAsync(C.prob, 0, sizeof(unsigned long long) * n, st);
+  }
   if (e != cudaSuccess) {
     err = std::string("batch allocation failed: ") + cudaGetErrorString(e);
     return -100 - (int)e;
@@ -543,6 +565,65 @@ int fmc_batch_chain_state(fmc_batch* b, int chain, double* out) {
   v[37] = (double)C.recomputes;
   v[38] = C.lgchk ? 0.0 : 1.0;
   std::memcpy(out, v, sizeof(v));
+  return 0;
+}
+
+int fmc_batch_prob(fmc_batch* b, int chain, int plot, int* dims, double* out) {
+  if (!b || chain < 0 || chain >= b->impl.nchains) {
+    fmc::set_last_error("bad batch handle or chain index");
+    return -1;
+  }
+  const fmc::Batch& B = b->impl;
+  const fmc::ChainDev& C = B.h_chains[chain];
+  const fmc::InputDeck& d = B.sys_chains[B.chain_sys[chain]]->sys.deck;
+  const size_t cells = (size_t)d.ngrid[0] * d.ngrid[1] * d.ngrid[2];
+  if (dims) {
+    dims[0] = (int)d.plots.size();
+    for (int a = 0; a < 3; a++) dims[1 + a] = d.ngrid[a];
+  }
+  if (out) {
+    if (plot < 0 || plot >= (int)d.plots.size()) {
+      fmc::set_last_error("plot index out of range");
+      return -1;
+    }
+    std::vector<unsigned long long> q(cells);
+    cudaSetDevice(B.device);
+    cudaError_t e = cudaMemcpy(q.data(), C.prob + plot * cells, sizeof(unsigned long long) * cells,
+                               cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) {
+      fmc::set_last_error(cudaGetErrorString(e));
+      return -100 - (int)e;
+    }
+    for (size_t i = 0; i < cells; i++) out[i] = (double)q[i] / 4294967296.0;
+  }
+  return 0;
+}
+
+int fmc_batch_write_prob(fmc_batch* b, int chain, const char* outdir) {
+  if (!b || chain < 0 || chain >= b->impl.nchains || !outdir) {
+    fmc::set_last_error("bad batch handle, chain index or directory");
+    return -1;
+  }
+  const fmc::Batch& B = b->impl;
+  const fmc::ChainDev& C = B.h_chains[chain];
+  const fmc::InputDeck& d = B.sys_chains[B.chain_sys[chain]]->sys.deck;
+  if (C.prodcount <= 0) return 0;
+  const size_t cells = (size_t)d.ngrid[0] * d.ngrid[1] * d.ngrid[2];
+  std::vector<double> grid(cells);
+  std::vector<int> per(d.guests.size(), 0);
+  for (size_t ip = 0; ip < d.plots.size(); ip++) {
+    int rc = fmc_batch_prob(b, chain, (int)ip, nullptr, grid.data());
+    if (rc) return rc;
+    const int g = d.plots[ip].guest;
+    char name[64];
+    std::snprintf(name, sizeof(name), "/prob_guest%02d_prob_%02d.cube", g + 1, ++per[g]);
+    std::string err;
+    rc = fmc::write_prob_cube(std::string(outdir) + name, d, grid.data(), C.prodcount, err);
+    if (rc) {
+      fmc::set_last_error(err);
+      return rc;
+    }
+  }
   return 0;
 }
 

@@ -238,6 +238,7 @@ int Chain::open_prepared(HostSystem&& prepared, const int seed[4], int dev, std:
   rotangle = kPi / 3.0;
   rota_rotangle = rotangle;
   chainstats.assign(1 + 14 * ng, 0.0);
+  prob.assign(deck.plots.size(), std::vector<double>((size_t)deck.ngrid[0] * deck.ngrid[1] * deck.ngrid[2], 0.0));
   production = (deck.eqsteps == 0);
   return 0;
 }
@@ -265,6 +266,38 @@ int Chain::set_guests(int g, int nmol, const double* xyz) {
   totatm = sys.nf;
   for (auto& x : sp) totatm += x.nmol * x.nsite;
   return 0;
+}
+
+// storeprob (utility_pack.f:496-561): every guest molecule's centre of mass and sites in
+// fractional coordinates, binned into its species' plots in the reference's order.
+void Chain::store_prob() {
+  const InputDeck& d = sys.deck;
+  const int na = d.ngrid[0], nb = d.ngrid[1], nc = d.ngrid[2];
+  for (int g = 0; g < (int)sp.size(); g++) {
+    const GuestSpecies& G = d.guests[g];
+    const int ns = sp[g].nsite;
+    for (int m = 0; m < sp[g].nmol; m++) {
+      const double* x = sp[g].xyz.data() + 3 * m * ns;
+      double c[3], fc[3];
+      centre_of_mass(G.mass.data(), ns, x, x + 1, x + 2, 3, c);
+      frac_wrap(sys.cell.rh, c[0], c[1], c[2], fc);
+      for (size_t ip = 0; ip < d.plots.size(); ip++) {
+        if (d.plots[ip].guest != g) continue;
+        std::vector<double>& grid = prob[ip];
+        auto add = [&grid](long long i, double w) { grid[i] += w; };
+        for (int site : d.plots[ip].sites) {
+          if (site == 0) {
+            equitable_bin(na, nb, nc, fc[0], fc[1], fc[2], add);
+          } else {
+            double f[3];
+            const double* a = x + 3 * (site - 1);
+            frac_wrap(sys.cell.rh, a[0], a[1], a[2], f);
+            equitable_bin(na, nb, nc, f[0], f[1], f[2], add);
+          }
+        }
+      }
+    }
+  }
 }
 
 int Chain::restart(const Revive& r, std::string& err) {
@@ -708,6 +741,7 @@ int Chain::step(MoveRecord* rec) {
       cs[5] = cs[5] + (e2 - cs[5]) / pc;
     }
   }
+  if (production && !prob.empty()) store_prob();  // gcmc.f:1929-1931, every production move
   R.accepted = accepted;
   R.nmols_after = s.nmol;
   R.ewld1 = e[0];

@@ -238,6 +238,71 @@ FMC_HD bool accept_move(double eng, double rande, double volm_m3, double press, 
   return rande < test;
 }
 
+// ------------------------------------------------------------------ probability plots
+// One axis of equitable_bin (utility_pack.f:1880-1990): the two grid cells (0-based) whose
+// centres bracket fractional position f on an n-cell axis, and their linear weights.
+FMC_HD void equitable_axis(int n, double f, int& lo, int& hi, double& wl, double& wr) {
+  double gp = n * f;
+  int idx = (int)ceil(gp);
+  double part = gp - floor(gp);
+  if (part > 0.5) {
+    lo = idx >= n ? n - 1 : idx - 1;
+    hi = idx >= n ? 0 : idx;
+    wl = 1.5 - part;
+    wr = part - 0.5;
+  } else {
+    lo = idx <= 1 ? n - 1 : idx - 2;
+    hi = idx <= 1 ? 0 : idx - 1;
+    wl = 0.5 - part;
+    wr = 0.5 + part;
+  }
+}
+
+// The unit weight of fractional position (fa, fb, fc) spread over the 8 surrounding cells of an
+// na x nb x nc grid (index a*nb*nc + b*nc + c), in the reference's order; add(index, weight).
+template <class Add>
+FMC_HD void equitable_bin(int na, int nb, int nc, double fa, double fb, double fc, Add add) {
+  int al, ar, bl, br, cl, cr;
+  double wal, war, wbl, wbr, wcl, wcr;
+  equitable_axis(na, fa, al, ar, wal, war);
+  equitable_axis(nb, fb, bl, br, wbl, wbr);
+  equitable_axis(nc, fc, cl, cr, wcl, wcr);
+  auto at = [&](int a, int b, int c) { return ((long long)a * nb + b) * nc + c; };
+  add(at(al, bl, cl), wal * wbl * wcl);
+  add(at(ar, bl, cl), war * wbl * wcl);
+  add(at(al, br, cl), wal * wbr * wcl);
+  add(at(al, bl, cr), wal * wbl * wcr);
+  add(at(ar, br, cl), war * wbr * wcl);
+  add(at(ar, bl, cr), war * wbl * wcr);
+  add(at(al, br, cr), wal * wbr * wcr);
+  add(at(ar, br, cr), war * wbr * wcr);
+}
+
+// Centre of mass of n sites (com, utility_pack.f:3003-3034); stride between sites' x values.
+FMC_HD void centre_of_mass(const double* mass, int n, const double* x, const double* y, const double* z, int stride,
+                           double* c) {
+  double w = 0.0, sx = 0.0, sy = 0.0, sz = 0.0;
+  for (int i = 0; i < n; i++) {
+    w = w + mass[i];
+    sx = sx + x[i * stride] * mass[i];
+    sy = sy + y[i * stride] * mass[i];
+    sz = sz + z[i * stride] * mass[i];
+  }
+  c[0] = sx / w;
+  c[1] = sy / w;
+  c[2] = sz / w;
+}
+
+// Fractional coordinates, wrapped into [0, 1) (frac / frac2, utility_pack.f:650-704).
+FMC_HD void frac_wrap(const double* rh, double x, double y, double z, double* f) {
+  double sx = x * rh[0] + y * rh[3] + z * rh[6];
+  double sy = x * rh[1] + y * rh[4] + z * rh[7];
+  double sz = x * rh[2] + y * rh[5] + z * rh[8];
+  f[0] = sx - floor(sx);
+  f[1] = sy - floor(sy);
+  f[2] = sz - floor(sz);
+}
+
 // 3-point interpolation of a tabulated function on r_l = l*dr (ewald.f:670-684,
 // vdw_terms.f:476-489).  tab[0] is defined as tab[1].
 FMC_HD double interp3(const double* tab, double rrr, double rdr) {

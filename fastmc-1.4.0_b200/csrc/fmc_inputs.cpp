@@ -329,6 +329,13 @@ void prescan(const std::string& dir, InputDeck& d, Scan& s) {
       } else if (r.has("rvdw")) {
         d.rvdw = r.take_double();
         lrvdw = true;
+      } else if (r.has("grid")) {
+        // probability grid parameters (utility_pack.f:403-411)
+        if (r.has("spa")) {
+          d.griddim = r.take_double();
+        } else if (r.has("fac")) {
+          for (int i = 0; i < 3; i++) d.gridfactor[i] = r.take_int();
+        }
       }
     }
   }
@@ -507,6 +514,7 @@ void read_field(const std::string& dir, InputDeck& d, const Scan& s, std::vector
               d.ftype.push_back(typ[k]);
               d.ffrz.push_back(frz[k]);
               d.fname.push_back(names[k]);
+              d.fmass.push_back(mass[k]);
             }
         }
         blocks.push_back(b);
@@ -636,11 +644,19 @@ void read_control(const std::string& dir, InputDeck& d) {
         } else if (q.has("press")) {
           d.press[g] = q.take_double() * 1.0e5;
         } else if (q.has("probability")) {
+          // probability plots of this guest: per plot, a site count then the sites (0: the
+          // molecule's centre of mass) (readinputs.f:638-660)
           int n = q.take_int(), seen = 0;
           while (seen < n) {
             Record p = f.next();
             p.strip();
-            if (!p.blank_or_comment()) seen++;
+            if (p.blank_or_comment()) continue;
+            seen++;
+            ProbPlot plot;
+            plot.guest = g;
+            int ns = p.take_int();
+            for (int j = 0; j < ns; j++) plot.sites.push_back(p.take_int());
+            d.plots.push_back(plot);
           }
         } else if (q.has("move")) {
           own_moves[g] = 1;
@@ -738,6 +754,15 @@ int read_input_deck(const std::string& dir, InputDeck& d, std::string& err) {
     read_control(dir, d);
     for (const MolBlock& b : blocks)
       d.mols.push_back({b.guest ? b.index : -1, b.guest ? 0 : b.index, b.nummols, b.numatoms});
+    if (!d.plots.empty()) {  // gcmc.f:246-256
+      double cp[10];
+      cell_props(d.cell, cp);
+      for (int i = 0; i < 3; i++)
+        d.ngrid[i] = d.gridfactor[i] * (int)std::ceil(cp[i] / (d.griddim * d.gridfactor[i]));
+      for (const ProbPlot& pl : d.plots)
+        for (int site : pl.sites)
+          if (site < 0 || site > d.guests[pl.guest].nsite) raise(-4, "probability plot names a site the guest lacks");
+    }
     {
       std::ifstream f(dir + "/CONFIG");
       std::getline(f, d.title);

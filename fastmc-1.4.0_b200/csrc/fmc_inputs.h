@@ -26,6 +26,12 @@ struct MolLayout {
   int nummols, numatoms;
 };
 
+// One probability plot of a guest species: the sites binned (0 = the centre of mass).
+struct ProbPlot {
+  int guest = 0;
+  std::vector<int> sites;
+};
+
 struct InputDeck {
   // initscan
   int imcon = 0, keyfce = 0, kmax[3] = {0, 0, 0};
@@ -40,8 +46,14 @@ struct InputDeck {
   std::vector<double> fx, fy, fz, fq;
   std::vector<int> ftype, ffrz;
   std::vector<std::string> fname;  // framework site names, condensed order
+  std::vector<double> fmass;       // framework site masses, condensed order
   std::vector<MolLayout> mols;     // FIELD molecule types in FIELD order
   std::string title;               // CONFIG's first record, as written
+  // probability plots (CONTROL &guest `probability`, `grid spacing`, `grid factors`)
+  std::vector<ProbPlot> plots;     // in guest order, then the order given
+  double griddim = 0.1;            // gcmc.f:136
+  int gridfactor[3] = {1, 1, 1};   // gcmc.f:138
+  int ngrid[3] = {0, 0, 0};        // grid cells along a, b, c when plots are requested
   int ntpvdw = 0, maxvdw = 0, mxgrid = 0;
   std::vector<int> ltpvdw, lstvdw;           // [1..maxvdw+1]
   std::vector<std::array<double, 5>> prmvdw;  // [1..maxvdw+1], energies in internal units

@@ -211,6 +211,89 @@ int write_revcon(const std::string& path, const InputDeck& d, const Revive& r, d
   return 0;
 }
 
+int atomic_number(double mass) {
+  // mass windows -> atomic number, the same windows as the reference's atmnumber so that the
+  // cube files label framework atoms alike (first matching window wins; 0 when none matches)
+  struct Win {
+    double lo, hi;
+    int z;
+  };
+  static const Win win[] = {
+      {0, 1.5, 1}, {3.9, 4.5, 2}, {6.5, 7.1, 3}, {8.9, 9.5, 4}, {10.5, 11.1, 5}, {11.9, 12.5, 6}, {13.9, 14.5, 7},
+      {15.5, 16.1, 8}, {18.5, 19.1, 9}, {19.9, 20.5, 10}, {22.5, 23.1, 11}, {23.9, 24.5, 12}, {26.5, 27.1, 13},
+      {27.9, 28.5, 14}, {30.5, 31.1, 15}, {31.9, 32.5, 16}, {34.9, 36.1, 17}, {39.5, 39.9999, 18},
+      {38.9, 39.4, 19}, {40, 40.5, 20}, {44.5, 45.1, 21}, {47.5, 48.1, 22}, {50.5, 51.1, 23}, {51.5, 52.1, 24},
+      {54.5, 55.1, 25}, {55.5, 56.1, 26}, {58.76, 59.1, 27}, {58.5, 59.75, 28}, {62.9, 64.1, 29}, {64.9, 66.1, 30},
+      {69.5, 70.1, 31}, {72.5, 73.1, 32}, {74.5, 75.1, 33}, {78.5, 79.1, 34}, {79.5, 80.1, 35}, {83.5, 84.1, 36},
+      {84.9, 86.1, 37}, {87.5, 88.1, 38}, {88.5, 89.1, 39}, {90.9, 91.5, 40}, {92.5, 93.1, 41}, {95.5, 96.1, 42},
+      {97.9, 98.1, 43}, {109.9, 101.5, 44}, {102.5, 103.1, 45}, {105.9, 106.5, 46}, {107.5, 108.1, 47},
+      {111.9, 112.5, 48}, {114.5, 115.1, 49}, {118.5, 119.1, 50}, {121.5, 122.1, 51}, {127.5, 128.1, 52},
+      {126.5, 127.1, 53}, {130.9, 131.5, 54}, {132.5, 133.1, 55}, {136.9, 137.5, 56}, {138.5, 139.1, 57},
+      {139.9, 140.5, 58}, {140.6, 141.1, 59}, {144, 144.5, 60}, {144.9, 145.1, 61}, {150, 150.6, 62},
+      {151.5, 152.1, 63}, {156.9, 157.5, 64}, {158.5, 159.1, 65}, {162, 163.1, 66}, {164.5, 165.1, 67},
+      {166.5, 167.9, 68}, {168, 169.1, 69}, {172.9, 173.5, 70}, {174, 175.1, 71}, {178, 179.1, 72},
+      {180, 181.1, 73}, {183, 184.1, 74}, {185.9, 186.5, 75}, {189.9, 190.5, 76}, {191.9, 192.5, 77},
+      {194.9, 195.5, 78}, {196.5, 197.1, 79}, {200, 201.1, 80}, {203.9, 204.6, 81}, {206.9, 207.6, 82},
+      {208.5, 209.1, 83}, {209.9, 210.1, 85}, {221.9, 222.1, 86}, {222.9, 223.1, 87}, {225.9, 226.1, 88},
+      {226.9, 227.1, 89}, {231.9, 232.1, 90}, {230.9, 231.1, 91}, {237.9, 238.1, 92}, {243.9, 244.1, 94},
+      {242.9, 243.1, 95}, {246.9, 247.1, 96}, {250.9, 251.1, 98}, {251.9, 252.1, 99}, {256.9, 257.1, 100},
+      {257.9, 258.1, 101}, {258.9, 259.1, 102}, {261.9, 262.1, 103}, {266.9, 267.1, 104}, {267.9, 268.1, 105},
+      {270.9, 271.1, 106}, {269.9, 270.1, 107}, {268.9, 269.1, 108}, {277.9, 278.1, 109}, {280.9, 281.1, 110},
+      {284.9, 285.1, 112}, {285.9, 286.1, 113}, {288.9, 289.1, 114}, {292.9, 293.1, 116}, {293.9, 294.1, 117}};
+  for (const Win& v : win)
+    if (mass >= v.lo && mass <= v.hi) return v.z;
+  return 0;
+}
+
+int write_prob_cube(const std::string& path, const InputDeck& d, const double* grid, long long steps,
+                    std::string& err) {
+  std::ofstream f(path, std::ios::trunc);
+  if (!f) {
+    err = "cannot write " + path;
+    return -1;
+  }
+  const double a2b = 1.889725989;  // Angstrom -> Bohr (utility_pack.f:82)
+  double c[9];
+  for (int i = 0; i < 9; i++) c[i] = d.cell[i] * a2b;
+  const int na = d.ngrid[0], nb = d.ngrid[1], nc = d.ngrid[2];
+  // volume of one grid cell (writeprob), in Bohr^3
+  const double vol = (c[1] * c[5] - c[2] * c[4]) / (na * nb) * c[6] / nc +
+                     (c[2] * c[3] - c[0] * c[5]) / (na * nb) * c[7] / nc +
+                     (c[0] * c[4] - c[1] * c[3]) / (na * nb) * c[8] / nc;
+  char buf[160];
+  // the second line keeps the blanks the reference's fixed-form continuation puts in it
+  f << "probability cube file\n" << "outer loop a, middle loop     b, inner loop c\n";
+  const int nf = (int)d.fq.size();
+  std::snprintf(buf, sizeof(buf), "%6d%12.6f%12.6f%12.6f\n", nf, 0.0, 0.0, 0.0);
+  f << buf;
+  const int n[3] = {na, nb, nc};
+  for (int a = 0; a < 3; a++) {
+    std::snprintf(buf, sizeof(buf), "%6d%12.6f%12.6f%12.6f\n", n[a], c[3 * a] / n[a], c[3 * a + 1] / n[a],
+                  c[3 * a + 2] / n[a]);
+    f << buf;
+  }
+  for (int i = 0; i < nf; i++) {
+    std::snprintf(buf, sizeof(buf), "%6d%12.6f%12.6f%12.6f%12.6f\n", atomic_number(d.fmass[i]), 0.0, d.fx[i] * a2b,
+                  d.fy[i] * a2b, d.fz[i] * a2b);
+    f << buf;
+  }
+  const long long total = (long long)na * nb * nc;
+  int ip = 0;
+  for (long long j = 1; j <= total; j++) {
+    ip++;
+    f << fortran_e(grid[j - 1] / vol / (double)steps, 15, 6);
+    if (j % nc == 0 || ip == 6) {
+      f << '\n';
+      ip = 0;
+    }
+  }
+  if (!f) {
+    err = "write failed: " + path;
+    return -1;
+  }
+  return 0;
+}
+
 std::vector<std::vector<double>> revive_guest_xyz(const InputDeck& d, const Revive& r) {
   std::vector<std::vector<double>> out(d.guests.size());
   for (size_t i = 0; i < d.mols.size(); i++) {

@@ -36,6 +36,16 @@ int write_revive(const std::string& path, const Revive& r, std::string& err);
 // Fortran g20.10 coordinates.
 int write_revcon(const std::string& path, const InputDeck& d, const Revive& r, double eng, std::string& err);
 
+// Atomic number of a framework atom's mass for the probability cube files, by the mass windows
+// of the reference's atmnumber (utility_pack.f:1992-2237); 0 when no window holds the mass.
+int atomic_number(double mass);
+
+// Writes one probability plot as a Gaussian cube file (writeprob, utility_pack.f:563-648):
+// header, the framework atoms in Bohr, then grid / (cell volume in Bohr^3) / steps, six values
+// a line and a new line after every c row.  `grid` is na*nb*nc values, c fastest.
+int write_prob_cube(const std::string& path, const InputDeck& d, const double* grid, long long steps,
+                    std::string& err);
+
 // Per-species interleaved guest coordinates of a REVIVE.
 std::vector<std::vector<double>> revive_guest_xyz(const InputDeck& d, const Revive& r);
 

@@ -29,8 +29,9 @@ def deck_inspect(directory):
     K, nerc = ctypes.c_int(0), ctypes.c_int(0)
     d = str(directory).encode()
     check(lib().fmc_deck_inspect(d, ip(ints), dp(dbls), None, None, None, None, ctypes.byref(K), ctypes.byref(nerc)))
-    info = dict(zip(_INFO_INTS, ints.tolist()))
+    info = dict(zip(_INFO_INTS[:12], ints.tolist()))
     info.update(zip(_INFO_DBLS, dbls.tolist()))
+    info.update(nplots=int(ints[12]), ngrid=(int(ints[13]), int(ints[14]), int(ints[15])))
     lmn = np.zeros((K.value, 3), dtype=np.int32)
     akk = np.zeros(K.value)
     erc = np.zeros(nerc.value)
@@ -52,6 +53,29 @@ def deck_vdw(directory):
         a = np.zeros(npts)
         check(lib().fmc_deck_vdw(d, k, dp(a), None))
         out.append(a)
+    return out
+
+
+def atomic_number(mass):
+    """Atomic number the probability cube files give a framework mass."""
+    return int(lib().fmc_atomic_number(float(mass)))
+
+
+def write_prob_cube(deck_dir, path, grid, steps):
+    """Write one plot's grid (na, nb, nc) as a cube file, as the reference's writeprob does."""
+    g = np.ascontiguousarray(grid, dtype=np.float64)
+    check(lib().fmc_write_prob_cube(str(deck_dir).encode(), str(path).encode(), dp(g), int(steps)))
+
+
+def _prob(call):
+    dims = np.zeros(4, dtype=np.int32)
+    check(call(0, ip(dims), None))
+    n, na, nb, nc = (int(v) for v in dims)
+    out = np.zeros((n, na, nb, nc))
+    for k in range(n):
+        buf = np.zeros(max(na * nb * nc, 1))
+        check(call(k, None, dp(buf)))
+        out[k] = buf[: na * nb * nc].reshape(na, nb, nc)
     return out
 
 
@@ -158,6 +182,13 @@ class Chain:
         check(lib().fmc_guest_coords(self.h, int(iguest), dp(buf), ctypes.byref(n), ctypes.byref(ns)))
         return buf[: n.value]
 
+    def prob(self):
+        """Probability plots: array [plots, na, nb, nc] of binned weights (storeprob)."""
+        return _prob(lambda k, dims, out: lib().fmc_chain_prob(self.h, k, dims, out))
+
+    def write_prob(self, outdir):
+        check(lib().fmc_chain_write_prob(self.h, str(outdir).encode()))
+
     def write_revive(self, outdir):
         """REVIVE + REVCON of the chain's state in outdir (revive, utility_pack.f:1772-1817)."""
         check(lib().fmc_chain_write_revive(self.h, str(outdir).encode()))
@@ -236,6 +267,12 @@ class Batch:
         out = np.zeros(40)
         check(lib().fmc_batch_chain_state(self.h, int(chain), dp(out)))
         return dict(zip(self._STATE, out.tolist()))
+
+    def prob(self, chain):
+        return _prob(lambda k, dims, out: lib().fmc_batch_prob(self.h, int(chain), k, dims, out))
+
+    def write_prob(self, chain, outdir):
+        check(lib().fmc_batch_write_prob(self.h, int(chain), str(outdir).encode()))
 
     def write_revive(self, chain, outdir):
         check(lib().fmc_batch_write_revive(self.h, int(chain), str(outdir).encode()))

@@ -57,6 +57,12 @@ SIGNATURES = {
     "fmc_chain_restart": (_ci, [_vp, ctypes.c_char_p]),
     "fmc_batch_write_revive": (_ci, [_vp, _ci, ctypes.c_char_p]),
     "fmc_batch_restart": (_ci, [_vp, _ci, ctypes.c_char_p]),
+    "fmc_chain_prob": (_ci, [_vp, _ci, _ip, _dp]),
+    "fmc_write_prob_cube": (_ci, [ctypes.c_char_p, ctypes.c_char_p, _dp, ctypes.c_longlong]),
+    "fmc_atomic_number": (_ci, [ctypes.c_double]),
+    "fmc_chain_write_prob": (_ci, [_vp, ctypes.c_char_p]),
+    "fmc_batch_prob": (_ci, [_vp, _ci, _ci, _ip, _dp]),
+    "fmc_batch_write_prob": (_ci, [_vp, _ci, ctypes.c_char_p]),
     "fmc_server_open": (_ci, [_ci, _ci, ctypes.c_longlong, _ci, ctypes.POINTER(_vp)]),
     "fmc_server_close": (None, [_vp]),
     "fmc_server_set_precision": (_ci, [_vp, _ci, ctypes.c_longlong]),

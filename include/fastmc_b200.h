@@ -118,6 +118,20 @@ int fmc_revive_read(const char* path, const char* deck_dir, int* production, int
 int fmc_chain_write_revive(fmc_chain* c, const char* outdir);  /* replaces revive */
 int fmc_chain_restart(fmc_chain* c, const char* revive_path);   /* replaces revread + restart */
 
+/* ---------------------------------------------------------------- probability plots
+ * CONTROL `probability` plots (per guest: sites binned, 0 = centre of mass), `grid spacing`,
+ * `grid factors`.  Every production move bins each guest molecule's sites into its species'
+ * plots by equitable_bin (storeprob, utility_pack.f:496-561, 1880-1990).  dims[4]: plots, then
+ * grid cells along a, b, c; out: one plot's na*nb*nc summed weights, c fastest.  The cube
+ * writers emit prob_guestGG_prob_PP.cube per plot (writeprob, utility_pack.f:563-648), density
+ * per Bohr^3 per production move, nothing before production. */
+int fmc_chain_prob(fmc_chain* c, int plot, int* dims, double* out);
+/* Host only: one plot's grid written as a cube file for a deck; the atomic number the cube
+ * files give a mass (the reference's atmnumber mass windows, utility_pack.f:1992-2237). */
+int fmc_write_prob_cube(const char* deck_dir, const char* path, const double* grid, long long steps);
+int fmc_atomic_number(double mass);
+int fmc_chain_write_prob(fmc_chain* c, const char* outdir);
+
 /* ---------------------------------------------------------------- batched path
  * Many independent chains (isotherm points) advanced by one persistent kernel, one CTA per
  * chain, the whole move loop of gcmc.f:589-1380 on the device (no counterpart in the
@@ -158,6 +172,10 @@ int fmc_batch_guest_coords(fmc_batch* b, int chain, int iguest, double* xyz, int
  * before the chain's first run matches the reference's restart, which re-seeds duni. */
 int fmc_batch_write_revive(fmc_batch* b, int chain, const char* outdir);
 int fmc_batch_restart(fmc_batch* b, int chain, const char* revive_path);
+/* Probability plots of one chain of a batch (as fmc_chain_prob; the device sums weights in
+ * fixed point, 2^-32 units, so the grids do not depend on the order of the adds). */
+int fmc_batch_prob(fmc_batch* b, int chain, int plot, int* dims, double* out);
+int fmc_batch_write_prob(fmc_batch* b, int chain, const char* outdir);
 
 /* ---------------------------------------------------------------- serving
  * Isotherm-point requests (an input-deck directory, a duni seed and a budget) served with

@@ -384,7 +384,18 @@ struct MoveRec {
   double ewld1, ewld2, ewld3, vdw, delrc, estep, rande, energy_after;
 };
 
+struct ProbPlotO {
+  int guest = 0;
+  std::vector<int> sites;  // 0: centre of mass
+};
+
 struct Chain {
+  // ---- probability plots (readinputs.f:638-660, gcmc.f:246-265, storeprob utility_pack.f:496-561)
+  std::vector<ProbPlotO> plots;
+  double griddim = 0.1;            // gcmc.f:136
+  int gridfactor[3] = {1, 1, 1};   // gcmc.f:138
+  int ngrid[3] = {0, 0, 0};
+  std::vector<std::vector<double>> grid;  // [plot][a*nb*nc + b*nc + c]
   // ---- initscan (utility_pack.f:176-457)
   int imcon = 0, keyfce = 0, kmax1 = 0, kmax2 = 0, kmax3 = 0, ntpvdw = 0, mxatm = 0, mxatyp = 0;
   int maxguest = 3000, maxatm = 15000;
@@ -586,6 +597,14 @@ static void initscan(Chain& C, const std::string& dir) {
       } else if (findstring("rvdw", r.c)) {
         C.rvdw = dblstr(r.c, LENREC);
         C.lrvdw = true;
+      } else if (findstring("grid", r.c)) {  // utility_pack.f:403-411
+        if (findstring("spa", r.c)) {
+          C.griddim = dblstr(r.c, LENREC);
+        } else if (findstring("fac", r.c)) {
+          C.gridfactor[0] = intstr(r.c, LENREC, nullptr);
+          C.gridfactor[1] = intstr(r.c, LENREC, nullptr);
+          C.gridfactor[2] = intstr(r.c, LENREC, nullptr);
+        }
       }
     }
   }
@@ -1015,7 +1034,14 @@ static void readcontrol(Chain& C, const std::string& dir) {
           while (cprob < n) {
             if (!f.getrec(r)) fail(53, "end of CONTROL file encountered");
             strip(r.c, LENREC);
-            if (!(r.c[0] == '#' || r.c[0] == ' ')) cprob++;
+            if (!(r.c[0] == '#' || r.c[0] == ' ')) {
+              cprob++;
+              ProbPlotO pl;
+              pl.guest = g;
+              int ns = intstr(r.c, LENREC, nullptr);
+              for (int j = 0; j < ns; j++) pl.sites.push_back(intstr(r.c, LENREC, nullptr));
+              C.plots.push_back(pl);
+            }
           }
         } else if (findstring("move", r.c)) {
           mvspefid[g] = 1;
@@ -1812,6 +1838,88 @@ static void com(const MolType& M, int natms, const double* x, const double* y, c
   *cy = sy / w;
   *cz = sz / w;
 }
+// equitable_bin (utility_pack.f:1880-1990): the unit weight of fractional position (fa, fb, fc)
+// spread over the 8 grid cells around it, linear in each direction between cell centres.
+static void equitable_axis(int n, double f, int* lo, int* hi, double* wl, double* wr) {
+  double gp = n * f;
+  int idx = (int)std::ceil(gp);
+  double part = gp - std::floor(gp);
+  if (part > 0.5) {
+    if (idx >= n) {
+      *lo = n - 1;
+      *hi = 0;
+    } else {
+      *lo = idx - 1;
+      *hi = idx;
+    }
+    *wl = 1.5 - part;
+    *wr = part - 0.5;
+  } else {
+    if (idx <= 1) {
+      *lo = n - 1;
+      *hi = 0;
+    } else {
+      *lo = idx - 2;
+      *hi = idx - 1;
+    }
+    *wl = 0.5 - part;
+    *wr = 0.5 + part;
+  }
+}
+static void equitable_bin(Chain& C, double fa, double fb, double fc, std::vector<double>& g) {
+  const int na = C.ngrid[0], nb = C.ngrid[1], nc = C.ngrid[2];
+  int al, ar, bl, br, cl, cr;
+  double wal, war, wbl, wbr, wcl, wcr;
+  equitable_axis(na, fa, &al, &ar, &wal, &war);
+  equitable_axis(nb, fb, &bl, &br, &wbl, &wbr);
+  equitable_axis(nc, fc, &cl, &cr, &wcl, &wcr);
+  auto at = [&](int a, int b, int c) -> double& { return g[((size_t)a * nb + b) * nc + c]; };
+  at(al, bl, cl) += wal * wbl * wcl;
+  at(ar, bl, cl) += war * wbl * wcl;
+  at(al, br, cl) += wal * wbr * wcl;
+  at(al, bl, cr) += wal * wbl * wcr;
+  at(ar, br, cl) += war * wbr * wcl;
+  at(ar, bl, cr) += war * wbl * wcr;
+  at(al, br, cr) += wal * wbr * wcr;
+  at(ar, br, cr) += war * wbr * wcr;
+}
+static double frac_mod(double x) { return x - std::floor(x); }  // modulo(x, 1.0)
+static void com(const MolType& M, int natms, const double* x, const double* y, const double* z, double* cx,
+                double* cy, double* cz);
+// storeprob (utility_pack.f:496-561): every guest molecule's centre of mass and sites in
+// fractional coordinates, binned into the plots of its species.
+static void storeprob(Chain& C) {
+  double rcell[9], det;
+  invert(C.cell, rcell, &det);
+  for (int g = 0; g < C.ntpguest; g++) {
+    const MolType& M = C.mols[C.locguest[g]];
+    const int natms = M.numatoms;
+    for (int m = 0; m < M.nummols; m++) {
+      const double* x = M.fx.data() + m * natms;
+      const double* y = M.fy.data() + m * natms;
+      const double* z = M.fz.data() + m * natms;
+      double cx, cy, cz;
+      com(M, natms, x, y, z, &cx, &cy, &cz);
+      double fc[3] = {frac_mod(cx * rcell[0] + cy * rcell[3] + cz * rcell[6]),
+                      frac_mod(cx * rcell[1] + cy * rcell[4] + cz * rcell[7]),
+                      frac_mod(cx * rcell[2] + cy * rcell[5] + cz * rcell[8])};
+      for (size_t ip = 0; ip < C.plots.size(); ip++) {
+        if (C.plots[ip].guest != g) continue;
+        for (int site : C.plots[ip].sites) {
+          if (site == 0) {
+            equitable_bin(C, fc[0], fc[1], fc[2], C.grid[ip]);
+          } else {
+            const int j = site - 1;
+            double fa = frac_mod(x[j] * rcell[0] + y[j] * rcell[3] + z[j] * rcell[6]);
+            double fb = frac_mod(x[j] * rcell[1] + y[j] * rcell[4] + z[j] * rcell[7]);
+            double fz = frac_mod(x[j] * rcell[2] + y[j] * rcell[5] + z[j] * rcell[8]);
+            equitable_bin(C, fa, fb, fz, C.grid[ip]);
+          }
+        }
+      }
+    }
+  }
+}
 // random_disp utility_pack.f:2679-2763 + random_rot 2929-3000
 static void random_disp(Chain& C, const MolType& M, int natms, double delr, const double* rcell, double rotangle,
                         double ra, double rb, double rcc, double r1, double r2, double r3, double r4) {
@@ -1968,6 +2076,11 @@ static void setup(Chain& C, const std::string& dir, int si, int sj, int sk, int 
   C.accept_tran.assign(C.ntpguest, 0);
   C.tran_count.assign(C.ntpguest, 0);
   C.chainstats.assign(1 + 14 * C.ntpguest, 0.0);
+  if (!C.plots.empty()) {  // gcmc.f:246-265
+    for (int i = 0; i < 3; i++)
+      C.ngrid[i] = C.gridfactor[i] * (int)std::ceil(C.celprp[i] / (C.griddim * C.gridfactor[i]));
+    C.grid.assign(C.plots.size(), std::vector<double>((size_t)C.ngrid[0] * C.ngrid[1] * C.ngrid[2], 0.0));
+  }
   C.production = (C.eqsteps == 0);
   int maxs = 64;
   C.ind.assign(maxs, -1);
@@ -2322,6 +2435,7 @@ static void gcmc_step(Chain& C, MoveRec* rec) {
         cs[is + 5] = cs[is + 5] + delta / pc;
       }
     }
+    if (!C.plots.empty()) storeprob(C);  // gcmc.f:1929-1931, every production move
   }
   R.accepted = accepted ? 1 : 0;
   R.nmols_after = M.nummols;
@@ -2581,6 +2695,18 @@ void orc_restart_flags(void* p, int production, const double* chainstats) {
   if (C.eqsteps == 0) C.production = true;
   for (size_t i = 0; i < C.chainstats.size(); i++) C.chainstats[i] = chainstats[i];
   C.prodcount = 0;
+}
+// Probability plots: dims[0..3] = plots, na, nb, nc; grid of plot ip when out is non-null.
+int orc_prob(void* p, int ip, int* dims, double* out) {
+  Chain& C = ((OrcHandle*)p)->C;
+  if (dims) {
+    dims[0] = (int)C.plots.size();
+    dims[1] = C.ngrid[0];
+    dims[2] = C.ngrid[1];
+    dims[3] = C.ngrid[2];
+  }
+  if (out && ip >= 0 && ip < (int)C.grid.size()) std::memcpy(out, C.grid[ip].data(), sizeof(double) * C.grid[ip].size());
+  return 0;
 }
 // Rolling statistics of guest type g: <N>,<E>,<EN>,<N^2>,<E^2>, prodcount
 void orc_stats(void* p, int g, double* out) {

@@ -68,6 +68,7 @@ def lib():
         L.orc_load_guests.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp]
         L.orc_stats.argtypes = [vp, ctypes.c_int, dp]
         L.orc_restart_flags.argtypes = [vp, ctypes.c_int, dp]
+        L.orc_prob.argtypes = [vp, ctypes.c_int, ip, dp]
         assert L.orc_sizeof_moverec() == MOVE_DTYPE.itemsize
         _lib = L
     return _lib
@@ -213,6 +214,18 @@ class Chain:
 
     def duni(self):
         return lib().orc_duni(self.h)
+
+    def prob(self):
+        """Probability grids (storeprob): array [plots, na, nb, nc] of binned weights."""
+        dims = np.zeros(4, dtype=np.int32)
+        lib().orc_prob(self.h, 0, _ip(dims), None)
+        n, na, nb, nc = (int(v) for v in dims)
+        out = np.zeros((n, na, nb, nc))
+        for k in range(n):
+            buf = np.zeros(na * nb * nc)
+            lib().orc_prob(self.h, k, None, _dp(buf))
+            out[k] = buf.reshape(na, nb, nc)
+        return out
 
     def restart_flags(self, production, chainstats):
         """Production flag and chain statistics of a restart from REVIVE (after load_guests)."""

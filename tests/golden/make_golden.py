@@ -13,6 +13,7 @@ expected.json come from that example's OUTPUT and REVIVE:
 * OUTPUT:108  duni seed "103 112 53 153"
 * OUTPUT:113  "Energy reported by DL_POLY: -11190.606165" (empty framework, recip + self)
 * REVIVE      energy(1) = -731.5072668178669 kcal/mol for the 90-CO2 state it stores
+* examples/advance/1_probability_plot_unary inputs, and atmnumber's mass windows as data
 * REVIVE      its production flag, chainstats and natms, and the SHA-256 of REVIVE and REVCON,
               so that a writer restating revive (utility_pack.f:1772-1817) can be checked
               byte for byte without the files themselves
@@ -78,6 +79,22 @@ def main(ref):
     with open(os.path.join(out, "expected.json"), "w") as f:
         json.dump(expected, f, indent=1)
     print("wrote", out)
+    # the probability-plot example's inputs (two plots of CO2: site 1; sites 2 and 3)
+    pp = os.path.join(HERE, "probplot")
+    os.makedirs(pp, exist_ok=True)
+    for f in ("CONTROL", "FIELD", "CONFIG"):
+        shutil.copyfile(os.path.join(ref, "examples/advance/1_probability_plot_unary", f), os.path.join(pp, f))
+    print("wrote", pp)
+    # the mass windows of atmnumber (utility_pack.f:1992-2237) as data, to check the writer's
+    # atomic numbers against them
+    import re
+    src = open(os.path.join(ref, "fastmc", "utility_pack.f")).read()
+    body = src[src.index("integer function atmnumber"):src.index("end function atmnumber")]
+    wins = [[float(lo), float(hi), int(z)] for lo, hi, z in
+            re.findall(r"\(i\.ge\.([0-9.]+)\)\.and\.\(i\.le\.([0-9.]+)\)\)then\s*\n\s*atmnumber=(\d+)", body)]
+    with open(os.path.join(HERE, "atmnumber_windows.json"), "w") as f:
+        json.dump(wins, f)
+    print("wrote", len(wins), "atmnumber windows")
 
 
 if __name__ == "__main__":
