@@ -116,7 +116,8 @@ __device__ __noinline__ void move_begin(ChainDev& C, const SysConst& Y, const De
   if (randmov < c[0]) mtype = kInsert;
   else if (randmov < c[1]) mtype = kDelete;
   else if (randmov < c[2]) mtype = kDisplace;
-  else if (randmov < c[5]) mtype = -1;
+  else if (randmov < c[3]) mtype = kJump;
+  else if (randmov < c[5]) mtype = kNoop;  // flex, swap (gcmc.f:1789-1795)
   else if (randmov < c[6]) mtype = kTranslate;
   else if (randmov < c[7]) mtype = kRotate;
   else if (randmov < c[8]) mtype = -1;
@@ -193,6 +194,30 @@ __device__ __noinline__ void move_begin(ChainDev& C, const SysConst& Y, const De
     M.nold = ns;
     for (int i = 0; i < ns; i++) C.numtyp[P.type[i]]--;
     M.need_lrc = 1;
+  } else if (mtype == kJump) {
+    // long jump (gcmc.f:1389-1547): the choice first, then the seven draws of random_jump
+    C.jump_count++;
+    int randchoice = (int)floor(R.next() * nmols) + 1;
+    M.randchoice = randchoice;
+    M.mol = randchoice - 1;
+    M.ex_lo = C.seg_off[g] + M.mol * ns;
+    M.ex_hi = M.ex_lo + ns;
+    double r[7];
+    for (int i = 0; i < 7; i++) r[i] = R.next();
+    for (int i = 0; i < ns; i++) {
+      double4 a = C.gsite[M.ex_lo + i];
+      x[i] = a.x;
+      y[i] = a.y;
+      z[i] = a.z;
+      x[ns + i] = a.x;
+      y[ns + i] = a.y;
+      z[ns + i] = a.z;
+    }
+    trial_jump(S.cell, P.mass, ns, r, x + ns, y + ns, z + ns);
+    M.nold = ns;
+    M.nnew = ns;
+  } else if (mtype == kNoop) {
+    // nothing moves; no sites, no draws beyond the move choice
   } else {
     double r[7], dis_delr, dis_rot;
     if (mtype == kTranslate) {
@@ -270,6 +295,10 @@ __device__ __forceinline__ void assemble(const SysConst& Y, MoveSmem& M, const d
 __device__ __forceinline__ int decide(ChainDev& C, const SysConst& Y, MoveSmem& M, double band) {
   const int g = M.g, mtype = M.mtype, nmols = C.nmol[g];
   const double e = M.estep;
+  if (mtype == kNoop) {  // nothing to accept or reject; no draw
+    M.accepted = 0;
+    return 0;
+  }
   if (mtype == kInsert || mtype == kDelete) {
     if (!M.rande_drawn) {
       M.rande = duni_next(C.rng);
@@ -332,16 +361,20 @@ __device__ __noinline__ void bookkeep(ChainDev& C, const SysConst& Y, MoveSmem& 
     } else {
       for (int i = 0; i < ns; i++) C.numtyp[P.type[i]]++;
     }
-  } else {
+  } else if (mtype != kNoop) {
     M.commit_lo = M.ex_lo;
     if (accepted) {
       if (mtype == kTranslate) C.accept_tran[g]++;
       else if (mtype == kRotate) C.accept_rota++;
+      else if (mtype == kJump) C.accept_jump++;
       else C.accept_disp[g]++;
       C.energy[g] += estep;
     }
   }
-  if (C.production && ((C.laccsample && accepted) || !C.laccsample)) {
+  // flex / swap leave the reference's `accepted` as the previous move set it
+  const bool counted = mtype == kNoop ? (C.last_accepted != 0) : accepted;
+  if (mtype != kNoop) C.last_accepted = accepted;
+  if (C.production && ((C.laccsample && counted) || !C.laccsample)) {
     C.prodcount++;
     double pc = (double)C.prodcount;
     for (int i = 0; i < Y.nspecies; i++) {
@@ -362,7 +395,7 @@ __device__ __noinline__ void bookkeep(ChainDev& C, const SysConst& Y, MoveSmem& 
     rec->iguest = g;
     rec->mtype = mtype;
     rec->randchoice = M.randchoice;
-    rec->accepted = accepted;
+    rec->accepted = counted;  // as the reference's `accepted` reads after the move
     rec->nmols_after = C.nmol[g];
     rec->pad0 = M.recheck;
     rec->pad1 = 0;

@@ -60,6 +60,7 @@ struct ChainDev {
   int disp_count[kMaxGuestTypes], accept_disp[kMaxGuestTypes];
   int tran_count[kMaxGuestTypes], accept_tran[kMaxGuestTypes];
   int rota_count, accept_rota, ins_count, del_count, accept_ins, accept_del;
+  int jump_count, accept_jump, last_accepted;
   double delrdisp[kMaxGuestTypes], tran_delr[kMaxGuestTypes], rotangle, rota_rotangle;
   double elrc, energy[kMaxGuestTypes];
   double last_dE;  // energy change of the last move if accepted, else 0 (the reference's delE)

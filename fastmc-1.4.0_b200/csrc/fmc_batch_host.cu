@@ -125,8 +125,8 @@ int init_chain_state(const InputDeck& d, const HostSystem& H, const double2* sk_
       nrm = 1;
       f = {1.0 / 3.0, 1.0 / 3.0, 1.0 / 3.0, 0, 0, 0, 0, 0, 0};
     }
-    if (f[3] != 0 || f[4] != 0 || f[5] != 0 || f[8] != 0) {
-      err = "jump, flex, swap and multi-jump moves are outside the GCMC trial-move path";
+    if (f[8] != 0) {
+      err = "multi-jump moves are outside the GCMC trial-move path";
       return -3;
     }
     C.mvcum[g][0] = f[0] / nrm;

@@ -583,7 +583,8 @@ int Chain::step(MoveRecord* rec) {
   if (randmov < c[0]) mtype = kInsert;
   else if (randmov < c[1]) mtype = kDelete;
   else if (randmov < c[2]) mtype = kDisplace;
-  else if (randmov < c[5]) return -3;  // jump/flex/swap (rejected at set-up)
+  else if (randmov < c[3]) mtype = kJump;
+  else if (randmov < c[5]) mtype = kNoop;  // flex, swap (gcmc.f:1789-1795)
   else if (randmov < c[6]) mtype = kTranslate;
   else if (randmov < c[7]) mtype = kRotate;
   else if (randmov < c[8]) return -3;
@@ -672,6 +673,43 @@ int Chain::step(MoveRecord* rec) {
     } else {
       for (int i = 0; i < natms; i++) numtyp[G.type[i]]++;
     }
+  } else if (mtype == kJump) {
+    // long jump (gcmc.f:1389-1547): choice first, then the seven draws of random_jump
+    jump_count++;
+    int randchoice = (int)std::floor(duni_next(rng) * nmols) + 1;
+    R.randchoice = randchoice;
+    int mol = randchoice - 1;
+    std::copy(s.xyz.begin() + (size_t)mol * 3 * natms, s.xyz.begin() + (size_t)(mol + 1) * 3 * natms, oldx);
+    double r[7];
+    for (int i = 0; i < 7; i++) r[i] = duni_next(rng);
+    double x[kMaxGuestSites], y[kMaxGuestSites], z[kMaxGuestSites];
+    for (int i = 0; i < natms; i++) {
+      x[i] = oldx[3 * i];
+      y[i] = oldx[3 * i + 1];
+      z[i] = oldx[3 * i + 2];
+    }
+    trial_jump(sys.cell, G.mass.data(), natms, r, x, y, z);
+    for (int i = 0; i < natms; i++) {
+      newx[3 * i] = x[i];
+      newx[3 * i + 1] = y[i];
+      newx[3 * i + 2] = z[i];
+    }
+    if ((rc = pass(kDisplace, g, mol, oldx, newx, e))) return rc;
+    estep = (e[0] + e[1] + e[2]) / sys.engunit;
+    if (estep < 0.0) {
+      accepted = true;
+    } else {
+      rande = duni_next(rng);
+      accepted = accept_move(estep, rande, sys.statvolm, d.press[g], nmols, d.temp, sys.beta, kDisplace);
+    }
+    if (accepted) {
+      delE[g] = estep;
+      accept_jump++;
+      if ((rc = commit(kDisplace, g, mol, newx))) return rc;
+      energy[g] += delE[g];
+    }
+  } else if (mtype == kNoop) {
+    accepted = last_accepted;  // the reference leaves `accepted` as the last move set it
   } else {
     double r[7], dis_delr, dis_rot;
     if (mtype == kTranslate) {
@@ -727,6 +765,7 @@ int Chain::step(MoveRecord* rec) {
       energy[g] += delE[g];
     }
   }
+  last_accepted = accepted;
   if (production && ((d.laccsample && accepted) || !d.laccsample)) {
     prodcount++;
     chainstats[0] = (double)prodcount;

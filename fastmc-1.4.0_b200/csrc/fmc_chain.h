@@ -98,6 +98,8 @@ class Chain {
   // every species' energy set to it, the production flag and chain statistics.
   int restart(const struct Revive& r, std::string& err);
   int last_guest = 0;  // species of the last move (the reference's REVCON energy is its delE)
+  bool last_accepted = false;  // flex / swap moves report the previous move's flag
+  int jump_count = 0, accept_jump = 0;
   // probability plots (storeprob): one grid per plot of the deck, weights summed in FP64
   std::vector<std::vector<double>> prob;
   void store_prob();

@@ -25,7 +25,9 @@ constexpr double kDelrMin = 0.1;             // utility_pack.f:90
 constexpr int kMaxGuestSites = 50;           // mxguestsite, utility_pack.f:76
 constexpr int kMaxGuestTypes = 4;
 
-enum MoveType : int { kInsert = 1, kDelete = 2, kDisplace = 3, kTranslate = 4, kRotate = 5 };
+// kJump: long jump (gcmc.f:1389-1547); kNoop: flex and swap, which the reference selects but
+// does not implement (gcmc.f:1789-1795)
+enum MoveType : int { kInsert = 1, kDelete = 2, kDisplace = 3, kTranslate = 4, kRotate = 5, kJump = 6, kNoop = 7 };
 
 // ------------------------------------------------------------------ duni
 // Marsaglia-Zaman-Tsang universal generator in IEEE single precision, as duni in
@@ -301,6 +303,42 @@ FMC_HD void frac_wrap(const double* rh, double x, double y, double z, double* f)
   f[0] = sx - floor(sx);
   f[1] = sy - floor(sy);
   f[2] = sz - floor(sz);
+}
+
+// random_jump (utility_pack.f:2766-2813) + random_rot (2929-3000), rotangle = 8 atan(1): the
+// centre of mass moves to fractional (r0, r1, r2) of the cell, then the molecule turns about it
+// by r3 * 2 pi around the axis (2 r4 - 1, 2 r5 - 1, 2 r6 - 1).  x, y, z: current sites in,
+// trial sites out.
+FMC_HD void trial_jump(const CellGeom& c, const double* mass, int n, const double r[7], double* x, double* y,
+                       double* z) {
+  const double* h = c.h;
+  double xd = r[0] * h[0] + r[1] * h[3] + r[2] * h[6];
+  double yd = r[0] * h[1] + r[1] * h[4] + r[2] * h[7];
+  double zd = r[0] * h[2] + r[1] * h[5] + r[2] * h[8];
+  double cm[3];
+  centre_of_mass(mass, n, x, y, z, 1, cm);
+  xd = xd - cm[0];
+  yd = yd - cm[1];
+  zd = zd - cm[2];
+  for (int i = 0; i < n; i++) {
+    x[i] = xd + x[i];
+    y[i] = yd + y[i];
+    z[i] = zd + z[i];
+  }
+  centre_of_mass(mass, n, x, y, z, 1, cm);
+  for (int i = 0; i < n; i++) {
+    x[i] = x[i] - cm[0];
+    y[i] = y[i] - cm[1];
+    z[i] = z[i] - cm[2];
+  }
+  double q[4];
+  axis_angle_quat(r[3] * (8.0 * atan(1.0)), r[4], r[5], r[6], q);
+  rotate_sites(x, y, z, n, q);
+  for (int i = 0; i < n; i++) {
+    x[i] = x[i] + cm[0];
+    y[i] = y[i] + cm[1];
+    z[i] = z[i] + cm[2];
+  }
 }
 
 // 3-point interpolation of a tabulated function on r_l = l*dr (ewald.f:670-684,

@@ -320,8 +320,8 @@ int build_host_system(const InputDeck& d, HostSystem& s, std::string& err, doubl
       nrm = 1;
       f = {1.0 / 3.0, 1.0 / 3.0, 1.0 / 3.0, 0, 0, 0, 0, 0, 0};
     }
-    if (f[3] != 0 || f[4] != 0 || f[5] != 0 || f[8] != 0) {
-      err = "jump, flex, swap and multi-jump moves are outside the GCMC trial-move path";
+    if (f[8] != 0) {
+      err = "multi-jump moves are outside the GCMC trial-move path";
       return -3;
     }
     std::array<double, 9> c;

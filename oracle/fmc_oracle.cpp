@@ -449,6 +449,8 @@ struct Chain {
   // production statistics (gcmc.f:1814-1860, chainstats(1+14*(i-1)+1..5))
   bool production = false;
   long long prodcount = 0;
+  bool last_accepted = false;
+  int jump_count = 0, accept_jump = 0;
   std::vector<double> chainstats;
   bool tick_tock[5] = {false, false, false, false, false};
   bool lgchk = true;
@@ -1969,6 +1971,44 @@ static void random_disp(Chain& C, const MolType& M, int natms, double delr, cons
     z[i] = z[i] + cz;
   }
 }
+// random_jump (utility_pack.f:2766-2813) + random_rot (2929-3000) with rotangle = 8 atan(1):
+// the centre of mass moves to the cell point of fractional (ra, rb, rc), then the molecule
+// turns about it.
+static void random_jump(Chain& C, const MolType& M, int natms, double ra, double rb, double rcc, double r1,
+                        double r2, double r3, double r4) {
+  double* x = C.newx.data();
+  double* y = C.newy.data();
+  double* z = C.newz.data();
+  const double* cell = C.cell;
+  double xd = ra * cell[0] + rb * cell[3] + rcc * cell[6];
+  double yd = ra * cell[1] + rb * cell[4] + rcc * cell[7];
+  double zd = ra * cell[2] + rb * cell[5] + rcc * cell[8];
+  double cx, cy, cz;
+  com(M, natms, x, y, z, &cx, &cy, &cz);
+  xd = xd - cx;
+  yd = yd - cy;
+  zd = zd - cz;
+  for (int i = 0; i < natms; i++) {
+    x[i] = xd + x[i];
+    y[i] = yd + y[i];
+    z[i] = zd + z[i];
+  }
+  com(M, natms, x, y, z, &cx, &cy, &cz);
+  for (int i = 0; i < natms; i++) {
+    x[i] = x[i] - cx;
+    y[i] = y[i] - cy;
+    z[i] = z[i] - cz;
+  }
+  const double jumpangle = 8.0 * std::atan(1.0);
+  double theta = r1 * jumpangle, q[4];
+  quat_from(theta, r2, r3, r4, q);
+  rotation(x, y, z, natms, q[0], q[1], q[2], q[3]);
+  for (int i = 0; i < natms; i++) {
+    x[i] = x[i] + cx;
+    y[i] = y[i] + cy;
+    z[i] = z[i] + cz;
+  }
+}
 // energy_eval utility_pack.f:3049-3095
 static bool energy_eval(double eng, double rande, double volm, double press, int ngsts, double temp, double beta,
                         int move) {
@@ -2018,8 +2058,7 @@ static void setup(Chain& C, const std::string& dir, int si, int sj, int sk, int 
       C.mcdisf[i] = 1.0 / 3.0;
       C.mcjmpf[i] = C.mcflxf[i] = C.mcswpf[i] = C.mctraf[i] = C.mcrotf[i] = C.mcmjpf[i] = 0.0;
     }
-    if (C.mcjmpf[i] != 0 || C.mcflxf[i] != 0 || C.mcswpf[i] != 0 || C.mcmjpf[i] != 0)
-      fail(-3, "jump/flex/swap/multi-jump moves are not part of this restatement");
+    if (C.mcmjpf[i] != 0) fail(-3, "multi-jump moves are not part of this restatement");
     C.mcinsf[i] = C.mcinsf[i] / nrm;
     C.mcdelf[i] = C.mcinsf[i] + (C.mcdelf[i] / nrm);
     C.mcdisf[i] = C.mcdelf[i] + (C.mcdisf[i] / nrm);
@@ -2135,15 +2174,17 @@ static void gcmc_step(Chain& C, MoveRec* rec) {
   int iguest = 0;
   if (C.ntpguest > 1) iguest = (int)std::floor(C.rng.next() * C.ntpguest);
   double randmov = C.rng.next();
-  bool insert = false, del = false, displace = false, tran = false, rota = false;
+  bool insert = false, del = false, displace = false, tran = false, rota = false, jump = false, noop = false;
   if (randmov < C.mcinsf[iguest])
     insert = true;
   else if (randmov < C.mcdelf[iguest])
     del = true;
   else if (randmov < C.mcdisf[iguest])
     displace = true;
-  else if (randmov < C.mcjmpf[iguest] || randmov < C.mcflxf[iguest] || randmov < C.mcswpf[iguest])
-    fail(-3, "jump/flex/swap selected");
+  else if (randmov < C.mcjmpf[iguest])
+    jump = true;
+  else if (randmov < C.mcflxf[iguest] || randmov < C.mcswpf[iguest])
+    noop = true;  // flex and swap are not implemented by the reference (gcmc.f:1789-1795)
   else if (randmov < C.mctraf[iguest]) {
     displace = true;
     tran = true;
@@ -2185,7 +2226,7 @@ static void gcmc_step(Chain& C, MoveRec* rec) {
   }
   if (nmols == 0) {
     insert = true;
-    del = displace = tran = rota = false;
+    del = displace = tran = rota = jump = noop = false;
   }
   MoveRec R;
   std::memset(&R, 0, sizeof(R));
@@ -2411,7 +2452,79 @@ static void gcmc_step(Chain& C, MoveRec* rec) {
       condense(C);
       C.energy[iguest] += C.delE[iguest];
     }
+  } else if (jump) {
+    // long jump gcmc.f:1389-1547: the molecule leaves its place (pass 1) and reappears anywhere
+    // in the cell with a random orientation (random_jump, pass 2)
+    R.mtype = 6;
+    C.jump_count++;
+    int randchoice = (int)std::floor(C.rng.next() * nmols) + 1;
+    R.randchoice = randchoice;
+    int atmadd = guest_offset(C, iguest);
+    int at = (randchoice - 1) * natms;
+    for (int k = 0; k < natms; k++) {
+      C.ind[k] = atmadd + at + k;
+      C.newx[k] = M.fx[at + k];
+      C.newy[k] = M.fy[at + k];
+      C.newz[k] = M.fz[at + k];
+    }
+    ewald1_guest(C, iguest, natms, C.newx.data(), C.newy.data(), C.newz.data(), MV_DISPLACE, 1);
+    for (int i = 0; i < natms; i++) {
+      chg[i] = C.atmcharge[C.ind[i]];
+      styp[i] = C.ltype[C.ind[i]];
+    }
+    {
+      std::vector<double> se(natms), sv(natms);
+      double a, b;
+      guest_realspace(C, natms, C.newx.data(), C.newy.data(), C.newz.data(), C.ind.data(), chg.data(),
+                      styp.data(), &a, &b, se.data(), sv.data());
+      ewld2sum = 0.0;
+      vdwsum = 0.0;
+      for (int i = 0; i < natms; i++) {
+        ewld2sum = ewld2sum - se[i];
+        vdwsum = vdwsum - sv[i];
+      }
+    }
+    double ra = C.rng.next(), rb = C.rng.next(), rc_ = C.rng.next();
+    double r1 = C.rng.next(), r2 = C.rng.next(), r3 = C.rng.next(), r4 = C.rng.next();
+    random_jump(C, M, natms, ra, rb, rc_, r1, r2, r3, r4);
+    ewld1eng = ewald1_guest(C, iguest, natms, C.newx.data(), C.newy.data(), C.newz.data(), MV_DISPLACE, 2);
+    {
+      std::vector<double> se(natms), sv(natms);
+      double a, b;
+      guest_realspace(C, natms, C.newx.data(), C.newy.data(), C.newz.data(), C.ind.data(), chg.data(),
+                      styp.data(), &a, &b, se.data(), sv.data());
+      for (int i = 0; i < natms; i++) {
+        ewld2sum = ewld2sum + se[i];
+        vdwsum = vdwsum + sv[i];
+      }
+    }
+    estep = (ewld1eng + ewld2sum + vdwsum) / C.engunit;
+    if (estep < 0.0) {
+      accepted = true;
+    } else {
+      rande = C.rng.next();
+      accepted = energy_eval(estep, rande, C.statvolm, C.gstpress[iguest], M.nummols, C.temp, C.beta, MV_DISPLACE);
+    }
+    if (accepted) {
+      C.delE[iguest] = estep;
+      C.accept_jump++;
+      for (int j = 0; j < natms; j++) {
+        M.fx[at + j] = C.newx[j];
+        M.fy[at + j] = C.newy[j];
+        M.fz[at + j] = C.newz[j];
+      }
+      for (int i = 0; i < C.newld; i++) {
+        C.ckcsum[i] = C.ckcsnew[i];
+        C.ckssum[i] = C.ckssnew[i];
+      }
+      condense(C);
+      C.energy[iguest] += C.delE[iguest];
+    }
+  } else if (noop) {
+    R.mtype = 7;
+    accepted = C.last_accepted;  // the reference leaves `accepted` as the last move set it
   }
+  C.last_accepted = accepted;
   // production statistics gcmc.f:1814-1860 (rolling <N>,<E>,<EN>,<N^2>,<E^2>)
   if (C.production) {
     if ((C.laccsample && accepted) || !C.laccsample) {

@@ -54,6 +54,11 @@ def decks(tmp_path_factory):
     L = [fws[1].cell[j, j] for j in range(3)]
     out["forms"] = synth.write_inputs(str(root / "forms"), fws[1], ["CO2"], [1.0], 298.0,
                                       tuple(synth.kmax_for(x) for x in L), vdw_forms=synth.VDW_FORMS)
+    L = [fws[2].cell[j, j] for j in range(3)]
+    out["jumps"] = synth.write_inputs(str(root / "jumps"), fws[2], ["CO2"], [1.0], 298.0,
+                                      tuple(synth.kmax_for(x) for x in L),
+                                      moves={"insert": 0.3, "delete": 0.25, "displace": 0.15, "jump": 0.15,
+                                             "flex": 0.05, "swap": 0.05, "rotate": 0.05})
     fw = fws[0]
     out["mixture"] = synth.write_inputs(str(root / "mixture"), fw, ["CO2", "N2"], [0.15, 0.85], 298.0,
                                         tuple(synth.kmax_for(fw.cell[j, j]) for j in range(3)))

@@ -53,3 +53,18 @@ def test_batch_every_vdw_form_replays_oracle(fmc, oracle_mod, decks):
     tr, _ = b.run(1500, trace=True)
     for i, s in enumerate(seeds):
         _compare_traces(tr[i], oracle_mod.Chain(decks["forms"], seed=s).run(1500))
+
+
+def test_batch_jump_flex_swap_replay_oracle(fmc, oracle_mod, decks):
+    """Long jumps (gcmc.f:1389-1547) and the flex / swap moves the reference selects but does not
+    implement, mixed with insertions, deletions, displacements and rotations."""
+    seeds = [(4, 8, 15, 16), (23, 42, 4, 8)]
+    b = fmc.Batch([decks["jumps"]] * 2, seeds)
+    tr, _ = b.run(2500, trace=True)
+    accepted_jumps = 0
+    for i, s in enumerate(seeds):
+        ref = oracle_mod.Chain(decks["jumps"], seed=s).run(2500)
+        _compare_traces(tr[i], ref)
+        assert np.any(ref["mtype"] == fmc.JUMP) and np.any(ref["mtype"] == fmc.NOOP)
+        accepted_jumps += int(np.sum((ref["mtype"] == fmc.JUMP) & (ref["accepted"] == 1)))
+    assert accepted_jumps > 0
