@@ -333,6 +333,22 @@ int fmc_write_prob_cube(const char* deck_dir, const char* path, const double* gr
   return rc ? fail(rc, err) : 0;
 }
 
+int fmc_write_report(const char* deck_dir, const double* final_stats, const double* seltot, const char* path) {
+  if (!deck_dir || !final_stats || !path) return fail(-1, "bad arguments");
+  fmc::InputDeck d;
+  std::string err;
+  int rc = fmc::read_input_deck(deck_dir, d, err);
+  if (rc) return fail(rc, err);
+  const int ng = (int)d.guests.size();
+  if (ng > 4) return fail(-1, "more than 4 guest species");
+  fmc::WindowStats W{};
+  if (seltot)
+    for (int i = 0; i < ng; i++)
+      for (int j = 0; j < ng; j++) W.seltot[i][j] = seltot[i * ng + j];
+  rc = fmc::write_report(path, d, final_stats, W, d.temp, err);
+  return rc ? fail(rc, err) : 0;
+}
+
 int fmc_chain_prob(fmc_chain* c, int plot, int* dims, double* out) {
   CHECK_CHAIN(c);
   const fmc::Chain& C = c->impl;
@@ -364,6 +380,32 @@ int fmc_chain_write_prob(fmc_chain* c, const char* outdir) {
     if (rc) return fail(rc, err);
   }
   return 0;
+}
+
+int fmc_chain_window_stats(fmc_chain* c, double* out) {
+  CHECK_CHAIN(c);
+  fmc::window_stats_out(c->impl.win, (int)c->impl.sp.size(), out);
+  return 0;
+}
+
+int fmc_chain_final_stats(fmc_chain* c, double* out) {
+  CHECK_CHAIN(c);
+  const fmc::Chain& C = c->impl;
+  fmc::final_stats((int)C.sp.size(), C.sys.deck.temp, C.chainstats.data(), C.win, C.gasmol.data(), C.gaseng.data(),
+                   out);
+  return 0;
+}
+
+int fmc_chain_write_report(fmc_chain* c, const char* path) {
+  CHECK_CHAIN(c);
+  if (!path) return fail(-1, "bad arguments");
+  const fmc::Chain& C = c->impl;
+  std::vector<double> cs(C.chainstats.size());
+  fmc::final_stats((int)C.sp.size(), C.sys.deck.temp, C.chainstats.data(), C.win, C.gasmol.data(), C.gaseng.data(),
+                   cs.data());
+  std::string err;
+  int rc = fmc::write_report(path, C.sys.deck, cs.data(), C.win, C.sys.deck.temp, err);
+  return rc ? fail(rc, err) : 0;
 }
 
 int fmc_stats(fmc_chain* c, int iguest, double* out) {

@@ -332,6 +332,33 @@ __device__ __forceinline__ int decide(ChainDev& C, const SysConst& Y, MoveSmem& 
 
 // Thread 0: counters, running energy, statistics and the trace record (gcmc.f:954-1380,
 // 1814-1860) once the move is decided.
+// Thread 0, production moves: the rolling averages, the stored samples and the averaging
+// windows of gcmc.f:1814-1928.  ins_g: species of an accepted insertion (-1: none).
+__device__ __noinline__ void production_sample(ChainDev& C, const SysConst& Y, int ins_g, bool counted,
+                                               double estep) {
+  if ((C.laccsample && counted) || !C.laccsample) {
+    C.prodcount++;
+    C.win.rollcount++;
+    const double pc = (double)C.prodcount;
+    for (int i = 0; i < Y.nspecies; i++) {
+      double dm = (double)(float)C.nmol[i], m2 = dm * dm, en = C.energy[i], e2 = en * en;
+      if (C.gasmol && C.prodcount <= kSampleCap + 1) {
+        C.gasmol[(size_t)i * kSampleCap + C.prodcount - 1] = dm;
+        C.gaseng[(size_t)i * kSampleCap + C.prodcount - 1] = en;
+      }
+      double* cs = C.stats[i];
+      cs[0] = cs[0] + (dm - cs[0]) / pc;
+      cs[1] = cs[1] + (en - cs[1]) / pc;
+      cs[2] = cs[2] + (en * dm - cs[2]) / pc;
+      cs[3] = cs[3] + (m2 - cs[3]) / pc;
+      cs[4] = cs[4] + (e2 - cs[4]) / pc;
+      window_sample(C.win, i, dm, en, ins_g == i, estep, C.temp, C.accept_ins, cs);
+    }
+  }
+  if (C.prodcount % C.nwind == 0 || !C.lgchk)
+    window_close(C.win, Y.nspecies, C.nwind, C.temp, [&C](int i) { return (const double*)C.stats[i]; });
+}
+
 __device__ __noinline__ void bookkeep(ChainDev& C, const SysConst& Y, MoveSmem& M, MoveRecord* rec) {
   const int g = M.g, ns = M.ns, mtype = M.mtype;
   const SpeciesConst& P = Y.sp[g];
@@ -374,19 +401,7 @@ __device__ __noinline__ void bookkeep(ChainDev& C, const SysConst& Y, MoveSmem& 
   // flex / swap leave the reference's `accepted` as the previous move set it
   const bool counted = mtype == kNoop ? (C.last_accepted != 0) : accepted;
   if (mtype != kNoop) C.last_accepted = accepted;
-  if (C.production && ((C.laccsample && counted) || !C.laccsample)) {
-    C.prodcount++;
-    double pc = (double)C.prodcount;
-    for (int i = 0; i < Y.nspecies; i++) {
-      double dm = (double)C.nmol[i], m2 = dm * dm, en = C.energy[i], e2 = en * en;
-      double* cs = C.stats[i];
-      cs[0] = cs[0] + (dm - cs[0]) / pc;
-      cs[1] = cs[1] + (en - cs[1]) / pc;
-      cs[2] = cs[2] + (en * dm - cs[2]) / pc;
-      cs[3] = cs[3] + (m2 - cs[3]) / pc;
-      cs[4] = cs[4] + (e2 - cs[4]) / pc;
-    }
-  }
+  if (C.production) production_sample(C, Y, mtype == kInsert && accepted ? g : -1, counted, estep);
   C.last_dE = accepted ? estep : 0.0;
   C.moves_done++;
   C.since_recompute++;

@@ -66,7 +66,11 @@ struct ChainDev {
   double last_dE;  // energy change of the last move if accepted, else 0 (the reference's delE)
   int production, lgchk, tick[5];
   long long prodcount;
-  double stats[kMaxGuestTypes][5];  // rolling <N>, <E>, <EN>, <N^2>, <E^2>
+  double stats[kMaxGuestTypes][6];  // rolling <N>, <E>, <EN>, <N^2>, <E^2>, <exp(-dE/kT)> of insertions
+  WindowStats win;                  // the reference's averaging windows
+  int nwind;                        // production samples per window (CONTROL `averaging window`)
+  double* gasmol;                   // first production samples of N and E per species
+  double* gaseng;                   // ([nspecies * 500000 + 1]; null: not recorded)
   long long moves_done;
   // SM clock cycles spent per phase when the launch is profiled: begin (thread 0), phase
   // tables, k-space + real space + reduction, end (thread 0), commit
@@ -105,8 +109,11 @@ cudaError_t configure_batch_kernel(int smem_bytes);
 using DevAllocFn = std::function<cudaError_t(void**, size_t)>;
 int fill_sysconst(const HostSystem& H, const DevSystem& S, SysConst& Y, int* tab_sites, std::string& err);
 int make_sysconst(const Chain& ch, SysConst& Y, std::vector<void*>& allocations, int* tab_sites, std::string& err);
+// record_samples: allocate the first production samples of N and E (gasmol / gaseng, 16 MB a
+// species) that the final report's blocked errors need up to 500,000 production moves.
 int init_chain_state(const InputDeck& d, const HostSystem& H, const double2* sk_src, double energy0, int sys,
-                     const int* seed, ChainDev& C, const DevAllocFn& alloc, cudaStream_t st, std::string& err);
+                     const int* seed, ChainDev& C, const DevAllocFn& alloc, cudaStream_t st, std::string& err,
+                     bool record_samples);
 int init_chain(const InputDeck& d, const Chain& ch, int sys, const int* seed, ChainDev& C,
                std::vector<void*>& allocations, cudaStream_t st, std::string& err);
 

@@ -110,7 +110,8 @@ int make_sysconst(const Chain& ch, SysConst& Y, std::vector<void*>& allocations,
 // Parameters (from the chain's own deck) and initial state of one chain of system `sys`;
 // allocates its S(k) (a copy of sk_src, the framework's) and guest-site segments.
 int init_chain_state(const InputDeck& d, const HostSystem& H, const double2* sk_src, double energy0, int sys,
-                     const int* seed, ChainDev& C, const DevAllocFn& alloc, cudaStream_t st, std::string& err) {
+                     const int* seed, ChainDev& C, const DevAllocFn& alloc, cudaStream_t st, std::string& err,
+                     bool record_samples) {
   std::memset(&C, 0, sizeof(C));
   C.sys = sys;
   C.temp = d.temp;
@@ -141,6 +142,7 @@ int init_chain_state(const InputDeck& d, const HostSystem& H, const double2* sk_
   C.maxguest = d.maxguest;
   C.mcsteps = d.mcsteps;
   C.eqsteps = d.eqsteps;
+  C.nwind = d.nwind;
   C.laccsample = d.laccsample;
   duni_seed(C.rng, seed[0], seed[1], seed[2], seed[3]);
   duni_next(C.rng);  // gcmc.f:335-336
@@ -163,6 +165,13 @@ int init_chain_state(const InputDeck& d, const HostSystem& H, const double2* sk_
   }
   if (e == cudaSuccess) e = alloc((void**)&C.gsite, sizeof(double4) * std::max(off, 1));
   if (e == cudaSuccess) e = alloc((void**)&C.gtype, sizeof(int) * std::max(off, 1));
+  if (e == cudaSuccess && record_samples) {  // gasmol / gaseng of the final report
+    const size_t n = (size_t)ng * kSampleCap + 1;
+    e = alloc((void**)&C.gasmol, sizeof(double) * n);
+    if (e == cudaSuccess) e = alloc((void**)&C.gaseng, sizeof(double) * n);
+    if (e == cudaSuccess) e = cudaMemsetAsync(C.gasmol, 0, sizeof(double) * n, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(C.gaseng, 0, sizeof(double) * n, st);
+  }
   if (e == cudaSuccess && !H.deck.plots.empty()) {
     const size_t n = H.deck.plots.size() * (size_t)H.deck.ngrid[0] * H.deck.ngrid[1] * H.deck.ngrid[2];
     e = alloc((void**)&C.prob, sizeof(unsigned long long) * n);
@@ -182,7 +191,7 @@ int init_chain(const InputDeck& d, const Chain& ch, int sys, const int* seed, Ch
     if (e == cudaSuccess) allocations.push_back(*p);
     return e;
   };
-  return init_chain_state(d, ch.sys, ch.sk, ch.spenergy, sys, seed, C, alloc, st, err);
+  return init_chain_state(d, ch.sys, ch.sk, ch.spenergy, sys, seed, C, alloc, st, err, true);
 }
 
 Batch::~Batch() {
@@ -305,7 +314,7 @@ int Batch::write_revive(int c, const std::string& outdir, std::string& err) {
   std::vector<double> cs(1 + 14 * ng, 0.0), en(ng);
   cs[0] = (double)C.prodcount;
   for (int g = 0; g < ng; g++) {
-    for (int k = 0; k < 5; k++) cs[1 + 14 * g + k] = C.stats[g][k];
+    for (int k = 0; k < 6; k++) cs[1 + 14 * g + k] = C.stats[g][k];
     en[g] = C.energy[g];
   }
   Revive r = revive_state(d, C.production != 0, xyz, cs, en);
@@ -360,7 +369,7 @@ int Batch::restart(int c, const std::string& path, std::string& err) {
     for (int m = 0; m < C.nmol[g]; m++)
       for (int i = 0; i < G.nsite; i++) C.numtyp[G.type[i]]++;
     C.energy[g] = S.spenergy;  // gcmc.f:547-556
-    for (int k = 0; k < 5; k++) C.stats[g][k] = r.chainstats[1 + 14 * g + k];
+    for (int k = 0; k < 6; k++) C.stats[g][k] = r.chainstats[1 + 14 * g + k];
   }
   C.framatm = H.nf;
   C.prodcount = 0;
@@ -625,6 +634,76 @@ int fmc_batch_write_prob(fmc_batch* b, int chain, const char* outdir) {
     }
   }
   return 0;
+}
+
+namespace {
+// The chainstats layout of a batched chain, with its stored samples copied to the host.
+int batch_chain_stats(fmc_batch* b, int chain, std::vector<double>& cs, std::vector<double>& gm,
+                      std::vector<double>& ge) {
+  const fmc::Batch& B = b->impl;
+  const fmc::ChainDev& C = B.h_chains[chain];
+  const fmc::InputDeck& d = B.sys_chains[B.chain_sys[chain]]->sys.deck;
+  const int ng = (int)d.guests.size();
+  cs.assign(1 + 14 * ng, 0.0);
+  cs[0] = (double)C.prodcount;
+  for (int g = 0; g < ng; g++)
+    for (int k = 0; k < 6; k++) cs[1 + 14 * g + k] = C.stats[g][k];
+  if (C.gasmol && C.prodcount > 0 && C.prodcount <= fmc::kSampleCap) {
+    const size_t n = (size_t)ng * fmc::kSampleCap + 1;
+    gm.resize(n);
+    ge.resize(n);
+    cudaSetDevice(B.device);
+    cudaError_t e = cudaMemcpy(gm.data(), C.gasmol, sizeof(double) * n, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(ge.data(), C.gaseng, sizeof(double) * n, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) {
+      fmc::set_last_error(cudaGetErrorString(e));
+      return -100 - (int)e;
+    }
+  }
+  return 0;
+}
+}  // namespace
+
+int fmc_batch_window_stats(fmc_batch* b, int chain, double* out) {
+  if (!b || chain < 0 || chain >= b->impl.nchains || !out) {
+    fmc::set_last_error("bad batch handle or chain index");
+    return -1;
+  }
+  const fmc::Batch& B = b->impl;
+  const int ng = (int)B.sys_chains[B.chain_sys[chain]]->sys.deck.guests.size();
+  fmc::window_stats_out(B.h_chains[chain].win, ng, out);
+  return 0;
+}
+
+int fmc_batch_final_stats(fmc_batch* b, int chain, double* out) {
+  if (!b || chain < 0 || chain >= b->impl.nchains || !out) {
+    fmc::set_last_error("bad batch handle or chain index");
+    return -1;
+  }
+  std::vector<double> cs, gm, ge;
+  int rc = batch_chain_stats(b, chain, cs, gm, ge);
+  if (rc) return rc;
+  const fmc::Batch& B = b->impl;
+  const fmc::ChainDev& C = B.h_chains[chain];
+  fmc::final_stats((int)(cs.size() - 1) / 14, C.temp, cs.data(), C.win, gm.empty() ? nullptr : gm.data(),
+                   ge.empty() ? nullptr : ge.data(), out);
+  return 0;
+}
+
+int fmc_batch_write_report(fmc_batch* b, int chain, const char* path) {
+  if (!b || chain < 0 || chain >= b->impl.nchains || !path) {
+    fmc::set_last_error("bad batch handle, chain index or path");
+    return -1;
+  }
+  const fmc::Batch& B = b->impl;
+  const fmc::InputDeck& d = B.sys_chains[B.chain_sys[chain]]->sys.deck;
+  std::vector<double> out(1 + 14 * d.guests.size());
+  int rc = fmc_batch_final_stats(b, chain, out.data());
+  if (rc) return rc;
+  std::string err;
+  rc = fmc::write_report(path, d, out.data(), B.h_chains[chain].win, B.h_chains[chain].temp, err);
+  if (rc) fmc::set_last_error(err);
+  return rc;
 }
 
 int fmc_batch_write_revive(fmc_batch* b, int chain, const char* outdir) {

@@ -238,6 +238,9 @@ int Chain::open_prepared(HostSystem&& prepared, const int seed[4], int dev, std:
   rotangle = kPi / 3.0;
   rota_rotangle = rotangle;
   chainstats.assign(1 + 14 * ng, 0.0);
+  std::memset(&win, 0, sizeof(win));
+  gasmol.assign((size_t)ng * kSampleCap + 1, 0.0);
+  gaseng.assign((size_t)ng * kSampleCap + 1, 0.0);
   prob.assign(deck.plots.size(), std::vector<double>((size_t)deck.ngrid[0] * deck.ngrid[1] * deck.ngrid[2], 0.0));
   production = (deck.eqsteps == 0);
   return 0;
@@ -768,18 +771,26 @@ int Chain::step(MoveRecord* rec) {
   last_accepted = accepted;
   if (production && ((d.laccsample && accepted) || !d.laccsample)) {
     prodcount++;
+    win.rollcount++;
     chainstats[0] = (double)prodcount;
     double pc = (double)prodcount;
     for (int i = 0; i < ng; i++) {
-      double dm = (double)sp[i].nmol, m2 = dm * dm, en = energy[i], e2 = en * en;
+      double dm = (double)(float)sp[i].nmol, m2 = dm * dm, en = energy[i], e2 = en * en;
+      if (prodcount <= kSampleCap + 1) {  // gasmol / gaseng (gcmc.f:1824-1827)
+        gasmol[(size_t)i * kSampleCap + prodcount - 1] = dm;
+        gaseng[(size_t)i * kSampleCap + prodcount - 1] = en;
+      }
       double* cs = chainstats.data() + 14 * i;
       cs[1] = cs[1] + (dm - cs[1]) / pc;
       cs[2] = cs[2] + (en - cs[2]) / pc;
       cs[3] = cs[3] + (en * dm - cs[3]) / pc;
       cs[4] = cs[4] + (m2 - cs[4]) / pc;
       cs[5] = cs[5] + (e2 - cs[5]) / pc;
+      window_sample(win, i, dm, en, mtype == kInsert && g == i && accepted, delE[i], d.temp, accept_ins, cs + 1);
     }
   }
+  if (production && (prodcount % d.nwind == 0 || !lgchk))
+    window_close(win, ng, d.nwind, d.temp, [this](int i) { return (const double*)chainstats.data() + 14 * i + 1; });
   if (production && !prob.empty()) store_prob();  // gcmc.f:1929-1931, every production move
   R.accepted = accepted;
   R.nmols_after = s.nmol;

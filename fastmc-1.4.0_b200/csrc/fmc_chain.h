@@ -99,6 +99,8 @@ class Chain {
   int restart(const struct Revive& r, std::string& err);
   int last_guest = 0;  // species of the last move (the reference's REVCON energy is its delE)
   bool last_accepted = false;  // flex / swap moves report the previous move's flag
+  WindowStats win;                      // the reference's averaging windows
+  std::vector<double> gasmol, gaseng;   // first production samples of N and E per species
   int jump_count = 0, accept_jump = 0;
   // probability plots (storeprob): one grid per plot of the deck, weights summed in FP64
   std::vector<std::vector<double>> prob;

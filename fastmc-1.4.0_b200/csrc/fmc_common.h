@@ -341,6 +341,85 @@ FMC_HD void trial_jump(const CellGeom& c, const double* mass, int n, const doubl
   }
 }
 
+// ------------------------------------------------------------------ windowed statistics
+constexpr double kRgas = 8.314472 / 4184.0;  // kcal/mol/K (utility_pack.f:109)
+constexpr int kSampleCap = 500000;           // stored production samples per species (gcmc.f)
+
+// calc_Qst and calc_Cv (utility_pack.f:2280-2316)
+FMC_HD double calc_qst(double E2, double E, double N, double N2, double EN, double temp) {
+  (void)E2;
+  return -1.0 * (EN - E * N) / (N2 - N * N) + kRgas * temp;
+}
+FMC_HD double calc_cv(double E2, double E, double N, double N2, double EN, double temp) {
+  const double d = EN - E * N;
+  return (3.0 / 2.0 * kRgas) + (E2 - (E * E) - d * d / (N2 - N * N)) / (N * kKboltz * temp * temp);
+}
+
+// The reference's averaging windows (gcmc.f:1814-1928): rolling window means of N, E, EN, N^2,
+// E^2 (and <exp(-dE/kT)> of insertions), closed every `nwind` production samples into weighted
+// running means and variances, with the selectivities between species.
+struct WindowStats {
+  int rollcount, ins_rollcount, avcount;
+  double avg[kMaxGuestTypes][8], sum[kMaxGuestTypes][8], var[kMaxGuestTypes][8];
+  double seltot[kMaxGuestTypes][kMaxGuestTypes], selwin[kMaxGuestTypes][kMaxGuestTypes];
+};
+
+// One counted production sample of species i, after its cumulative averages cs[0..4] (<N>,
+// <E>, <EN>, <N^2>, <E^2>) were updated; cs[5] is the rolling <exp(-dE/kT)> of accepted
+// insertions.  rollcount must already count this sample.
+FMC_HD void window_sample(WindowStats& W, int i, double dm, double e, bool ins_accepted, double delE, double temp,
+                          int accept_ins, double* cs) {
+  double* aw = W.avg[i];
+  if (ins_accepted) {
+    double h = exp(-1.0 * delE / kKboltz / temp);
+    W.ins_rollcount++;
+    double delta = h - cs[5];
+    h = cs[5] + delta / accept_ins;
+    cs[5] = h;
+    aw[7] = ((W.ins_rollcount - 1) * aw[7] + h) / (double)W.ins_rollcount;
+  }
+  const double rc = (double)W.rollcount;
+  aw[0] = ((W.rollcount - 1) * aw[0] + dm) / rc;
+  aw[1] = ((W.rollcount - 1) * aw[1] + e) / rc;
+  aw[2] = ((W.rollcount - 1) * aw[2] + e * dm) / rc;
+  aw[3] = ((W.rollcount - 1) * aw[3] + dm * dm) / rc;
+  aw[4] = ((W.rollcount - 1) * aw[4] + e * e) / rc;
+}
+
+// Closes a window (gcmc.f:1887-1928); cs(i) gives species i's cumulative averages.
+template <class CS>
+FMC_HD void window_close(WindowStats& W, int ng, int nwind, double temp, CS cs) {
+  W.avcount++;
+  const double weight = (double)W.rollcount / (double)nwind;
+  for (int i = 0; i < ng; i++) {
+    const double* c = cs(i);
+    double* aw = W.avg[i];
+    aw[5] = calc_qst(c[4], c[1], c[0], c[3], c[2], temp);
+    aw[6] = calc_cv(c[4], c[1], c[0], c[3], c[2], temp);
+    if (i > 0) {
+      const double an = aw[0];
+      for (int j = 0; j < i; j++) {
+        if (an == 0) continue;
+        const double sel = W.avg[j][0] / an;
+        const double delta = weight * (sel - W.seltot[i][j]);
+        W.seltot[i][j] = W.seltot[i][j] + delta / W.avcount;
+        W.selwin[i][j] = W.selwin[i][j] + weight * (sel * sel - W.selwin[i][j]) / (W.avcount - 1 + weight);
+        W.seltot[j][i] = ((W.avcount - 1 + weight) * W.selwin[i][j] -
+                          ((W.avcount - 1 + weight) * W.seltot[i][j] * W.seltot[i][j])) /
+                         (W.avcount - 1 + weight);
+      }
+    }
+  }
+  for (int i = 0; i < ng; i++)
+    for (int k = 0; k < 8; k++) {
+      const double delta = weight * (W.avg[i][k] - W.sum[i][k]);
+      W.sum[i][k] = W.sum[i][k] + delta / W.avcount;
+      W.var[i][k] = W.var[i][k] + delta * weight * (W.avg[i][k] - W.sum[i][k]);
+      W.avg[i][k] = 0.0;
+    }
+  W.rollcount = 0;
+}
+
 // 3-point interpolation of a tabulated function on r_l = l*dr (ewald.f:670-684,
 // vdw_terms.f:476-489).  tab[0] is defined as tab[1].
 FMC_HD double interp3(const double* tab, double rrr, double rdr) {

@@ -418,6 +418,7 @@ void read_field(const std::string& dir, InputDeck& d, const Scan& s, std::vector
         Record h = f.next();
         h.lower();
         bool guest = h.has("&guest");
+        if (guest) h.take_word(6);  // the species name follows the keyword (readinputs.f:131-141)
         h.strip();
         int nummols = 0, numatoms = 0;
         std::vector<std::string> names;

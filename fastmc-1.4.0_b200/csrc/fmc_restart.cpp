@@ -294,6 +294,119 @@ int write_prob_cube(const std::string& path, const InputDeck& d, const double* g
   return 0;
 }
 
+void final_stats(int ng, double temp, const double* chainstats, const WindowStats& W, const double* gasmol,
+                 const double* gaseng, double* out) {
+  const int windn = 5;  // gcmc.f:119
+  std::vector<double> cs(chainstats, chainstats + 1 + 14 * ng);
+  WindowStats V = W;
+  int avcount = V.avcount;
+  const double weight = cs[0];
+  if (weight > 0) {
+    for (int i = 0; i < ng; i++) {
+      const int is = 1 + 14 * i;
+      if (weight <= kSampleCap) {
+        const long long nw = (long long)weight / windn;
+        avcount = windn;
+        double sum[8] = {0}, var[8] = {0};
+        for (int x = 1; x <= windn; x++) {
+          const size_t y = (size_t)i * kSampleCap + (size_t)(x - 1) * nw;
+          const size_t cap = (size_t)ng * kSampleCap + 1;
+          double an = 0, e = 0, en = 0, n2 = 0, e2 = 0;
+          for (size_t k = y; k <= y + (size_t)nw; k++) {
+            const double m = (gasmol && k < cap) ? gasmol[k] : 0.0, g = (gaseng && k < cap) ? gaseng[k] : 0.0;
+            an += m;
+            e += g;
+            en += m * g;
+            n2 += m * m;
+            e2 += g * g;
+          }
+          double avg[7];
+          avg[0] = an / nw;
+          avg[1] = e / nw;
+          avg[2] = en / nw;
+          avg[3] = n2 / nw;
+          avg[4] = e2 / nw;
+          avg[5] = calc_qst(avg[4], avg[1], avg[0], avg[3], avg[2], temp);
+          avg[6] = calc_cv(avg[4], avg[1], avg[0], avg[3], avg[2], temp);
+          for (int z = 0; z < 7; z++) {
+            const double delta = avg[z] - sum[z];
+            sum[z] = sum[z] + delta / x;
+            var[z] = var[z] + delta * (avg[z] - sum[z]);
+          }
+        }
+        for (int z = 0; z < 6; z++) cs[is + z] = sum[z];
+        for (int z = 0; z < 8; z++) V.var[i][z] = z < 7 ? var[z] : 0.0;
+      }
+      for (int z = 0; z < 8; z++) cs[is + 6 + z] = std::sqrt(V.var[i][z] / avcount);
+    }
+  }
+  std::memcpy(out, cs.data(), sizeof(double) * cs.size());
+}
+
+void window_stats_out(const WindowStats& W, int ng, double* out) {
+  out[0] = W.avcount;
+  out[1] = W.rollcount;
+  double* o = out + 2;
+  for (int i = 0; i < ng; i++)
+    for (int k = 0; k < 8; k++) {
+      o[8 * i + k] = W.sum[i][k];
+      o[8 * ng + 8 * i + k] = W.var[i][k];
+      o[16 * ng + 8 * i + k] = W.avg[i][k];
+    }
+  for (int i = 0; i < ng; i++)
+    for (int j = 0; j < ng; j++) o[24 * ng + i * ng + j] = W.seltot[i][j];
+}
+
+int write_report(const std::string& path, const InputDeck& d, const double* cs, const WindowStats& W, double temp,
+                 std::string& err) {
+  std::ofstream f(path, std::ios::trunc);
+  if (!f) {
+    err = "cannot write " + path;
+    return -1;
+  }
+  char buf[256];
+  const std::string stars(75, '*');
+  f << "\n" << stars << "\n   Data reported from node   0\n" << stars << "\n\n";
+  // one record per value, a blank record after each block (the formats of gcmc.f:2095-2108)
+  auto row = [&](const char* label, double v) {
+    std::snprintf(buf, sizeof(buf), "     %60s%20.9f\n", label, v);
+    f << buf;
+  };
+  const int ng = (int)d.guests.size();
+  for (int i = 0; i < ng; i++) {
+    const double* c = cs + 1 + 14 * i;
+    std::string name = d.guests[i].name.substr(0, 40);
+    name.resize(40, ' ');
+    std::snprintf(buf, sizeof(buf), "     guest %2d: %s\n\n", i + 1, name.c_str());
+    f << buf;
+    row("<N>: ", c[0]);
+    row("<E>: ", c[1]);
+    row("<E*N>: ", c[2]);
+    row("<N*N>: ", c[3]);
+    row("<E*E>: ", c[4]);
+    std::snprintf(buf, sizeof(buf), "     %60s%20lld\n", "Multiplier: ", (long long)cs[0]);
+    f << buf;
+    row("Isosteric heat of adsorption (kcal/mol): ", calc_qst(c[4], c[1], c[0], c[3], c[2], temp));
+    row("Isosteric heat error: ", c[11]);
+    row("Heat capacity, Cv (kcal/mol/K): ", calc_cv(c[4], c[1], c[0], c[3], c[2], temp));
+    row("Heat capacity error: ", c[12]);
+    f << "\n";
+  }
+  if (ng > 1)
+    for (int i = 0; i < ng; i++)
+      for (int j = 0; j < i; j++) {
+        std::snprintf(buf, sizeof(buf), "     guest %2d over guest %2d\n\n", j + 1, i + 1);
+        f << buf;
+        row("<S>: ", W.seltot[i][j]);
+        f << "\n";
+      }
+  if (!f) {
+    err = "write failed: " + path;
+    return -1;
+  }
+  return 0;
+}
+
 std::vector<std::vector<double>> revive_guest_xyz(const InputDeck& d, const Revive& r) {
   std::vector<std::vector<double>> out(d.guests.size());
   for (size_t i = 0; i < d.mols.size(); i++) {

@@ -5,6 +5,7 @@
 #include <string>
 #include <vector>
 
+#include "fmc_common.h"
 #include "fmc_inputs.h"
 
 namespace fmc {
@@ -45,6 +46,24 @@ int atomic_number(double mass);
 // a line and a new line after every c row.  `grid` is na*nb*nc values, c fastest.
 int write_prob_cube(const std::string& path, const InputDeck& d, const double* grid, long long steps,
                     std::string& err);
+
+// The final statistics of the reference's report (gcmc.f:1960-2037), in the chainstats layout:
+// out[0] production moves; per species g at 1 + 14 g: <N>, <E>, <EN>, <N^2>, <E^2>, the sixth
+// average, then the errors of N, E, EN, N^2, E^2, Q_st, Cv and the sixth.  Up to 500,000
+// production moves the averages and errors come from 5 blocks of the stored samples (gasmol,
+// gaseng; each block sums the nwind + 1 samples of an inclusive slice and divides by nwind, as
+// the reference does); beyond, from the averaging windows closed during the run.
+void final_stats(int ng, double temp, const double* chainstats, const WindowStats& W, const double* gasmol,
+                 const double* gaseng, double* out);
+
+// Window state as a flat array: avcount, rollcount, then sum[8 ng], var[8 ng], avg[8 ng] and
+// seltot[ng ng] (species-major).
+void window_stats_out(const WindowStats& W, int ng, double* out);
+
+// The reference's per-node report block (gcmc.f:2052-2117) for one chain: every species'
+// averages, production moves, Q_st and Cv with their errors, then the selectivities.
+int write_report(const std::string& path, const InputDeck& d, const double* final_cs, const WindowStats& W,
+                 double temp, std::string& err);
 
 // Per-species interleaved guest coordinates of a REVIVE.
 std::vector<std::vector<double>> revive_guest_xyz(const InputDeck& d, const Revive& r);

@@ -296,6 +296,7 @@ class Server {
     double b = 1.15 * nv * per_vox * (sizeof(double4) + 1) + 4.0 * (nv + 1) + 36.0 * h.nf;
     b += 12.0 * (h.erc.size() + h.vvv.size()) + 4.0 * h.pair_row.size() + 60.0 * h.K;
     b += 36.0 * h.deck.maxguest * h.deck.guests.size();
+    b += 2.0 * 8.0 * ((double)kSampleCap * h.deck.guests.size() + 1);  // stored production samples
     return (size_t)b + (64u << 10);
   }
 

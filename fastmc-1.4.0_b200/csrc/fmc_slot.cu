@@ -171,7 +171,7 @@ int build_slot(const HostSystem& h, int slot, const int seed[4], SlotMemory& mem
     Y.sk_fw = skfw;
     DevAllocFn alloc = [&mem](void** p, size_t n) { return mem.alloc(p, n); };
     // an empty framework: guest energy 0 (single_point, gcmc.f:2518-2710)
-    return init_chain_state(h.deck, h, skfw, 0.0, slot, seed, C, alloc, st, err);
+    return init_chain_state(h.deck, h, skfw, 0.0, slot, seed, C, alloc, st, err, true);
   }
 fail:
   err = std::string("slot set-up failed on the device: ") + cudaGetErrorString(e);

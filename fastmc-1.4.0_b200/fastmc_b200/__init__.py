@@ -67,6 +67,22 @@ def write_prob_cube(deck_dir, path, grid, steps):
     check(lib().fmc_write_prob_cube(str(deck_dir).encode(), str(path).encode(), dp(g), int(steps)))
 
 
+def write_report(deck_dir, final_stats, path, seltot=None):
+    """The reference's per-node report block (gcmc.f:2052-2117) from final statistics in the
+    chainstats layout ([0] production moves, 14 values a species); host only."""
+    fs = np.ascontiguousarray(final_stats, dtype=np.float64)
+    sel = None if seltot is None else np.ascontiguousarray(seltot, dtype=np.float64)
+    check(lib().fmc_write_report(str(deck_dir).encode(), dp(fs), None if sel is None else dp(sel),
+                                 str(path).encode()))
+
+
+def _window(out, ng):
+    o = out[2:]
+    return {"avcount": int(out[0]), "rollcount": int(out[1]), "sum": o[:8 * ng].reshape(ng, 8),
+            "var": o[8 * ng:16 * ng].reshape(ng, 8), "avg": o[16 * ng:24 * ng].reshape(ng, 8),
+            "seltot": o[24 * ng:24 * ng + ng * ng].reshape(ng, ng)}
+
+
 def _prob(call):
     dims = np.zeros(4, dtype=np.int32)
     check(call(0, ip(dims), None))
@@ -182,6 +198,22 @@ class Chain:
         check(lib().fmc_guest_coords(self.h, int(iguest), dp(buf), ctypes.byref(n), ctypes.byref(ns)))
         return buf[: n.value]
 
+    def window_stats(self):
+        ng = self.info()["nspecies"]
+        out = np.zeros(2 + 24 * ng + ng * ng)
+        check(lib().fmc_chain_window_stats(self.h, dp(out)))
+        return _window(out, ng)
+
+    def final_stats(self):
+        """The report's statistics (averages and errors, chainstats layout)."""
+        ng = self.info()["nspecies"]
+        out = np.zeros(1 + 14 * ng)
+        check(lib().fmc_chain_final_stats(self.h, dp(out)))
+        return out
+
+    def write_report(self, path):
+        check(lib().fmc_chain_write_report(self.h, str(path).encode()))
+
     def prob(self):
         """Probability plots: array [plots, na, nb, nc] of binned weights (storeprob)."""
         return _prob(lambda k, dims, out: lib().fmc_chain_prob(self.h, k, dims, out))
@@ -214,6 +246,7 @@ class Batch:
         s = np.ascontiguousarray(np.asarray(seeds, dtype=np.int32).reshape(n, 4))
         arr = (ctypes.c_char_p * n)(*dirs)
         self.n = n
+        self.dirs = [str(d) for d in directories]
         self.h = ctypes.c_void_p()
         check(lib().fmc_batch_open(n, arr, ip(s), int(device), ctypes.byref(self.h)))
 
@@ -267,6 +300,23 @@ class Batch:
         out = np.zeros(40)
         check(lib().fmc_batch_chain_state(self.h, int(chain), dp(out)))
         return dict(zip(self._STATE, out.tolist()))
+
+    def window_stats(self, chain):
+        ng = self._ng(chain)
+        out = np.zeros(2 + 24 * ng + ng * ng)
+        check(lib().fmc_batch_window_stats(self.h, int(chain), dp(out)))
+        return _window(out, ng)
+
+    def final_stats(self, chain):
+        out = np.zeros(1 + 14 * self._ng(chain))
+        check(lib().fmc_batch_final_stats(self.h, int(chain), dp(out)))
+        return out
+
+    def write_report(self, chain, path):
+        check(lib().fmc_batch_write_report(self.h, int(chain), str(path).encode()))
+
+    def _ng(self, chain):
+        return int(deck_inspect(self.dirs[chain])["nspecies"])
 
     def prob(self, chain):
         return _prob(lambda k, dims, out: lib().fmc_batch_prob(self.h, int(chain), k, dims, out))

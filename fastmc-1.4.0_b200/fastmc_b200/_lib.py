@@ -58,6 +58,13 @@ SIGNATURES = {
     "fmc_batch_write_revive": (_ci, [_vp, _ci, ctypes.c_char_p]),
     "fmc_batch_restart": (_ci, [_vp, _ci, ctypes.c_char_p]),
     "fmc_chain_prob": (_ci, [_vp, _ci, _ip, _dp]),
+    "fmc_chain_window_stats": (_ci, [_vp, _dp]),
+    "fmc_chain_final_stats": (_ci, [_vp, _dp]),
+    "fmc_chain_write_report": (_ci, [_vp, ctypes.c_char_p]),
+    "fmc_write_report": (_ci, [ctypes.c_char_p, _dp, _dp, ctypes.c_char_p]),
+    "fmc_batch_window_stats": (_ci, [_vp, _ci, _dp]),
+    "fmc_batch_final_stats": (_ci, [_vp, _ci, _dp]),
+    "fmc_batch_write_report": (_ci, [_vp, _ci, ctypes.c_char_p]),
     "fmc_write_prob_cube": (_ci, [ctypes.c_char_p, ctypes.c_char_p, _dp, ctypes.c_longlong]),
     "fmc_atomic_number": (_ci, [ctypes.c_double]),
     "fmc_chain_write_prob": (_ci, [_vp, ctypes.c_char_p]),

@@ -118,6 +118,21 @@ int fmc_revive_read(const char* path, const char* deck_dir, int* production, int
 int fmc_chain_write_revive(fmc_chain* c, const char* outdir);  /* replaces revive */
 int fmc_chain_restart(fmc_chain* c, const char* revive_path);   /* replaces revread + restart */
 
+/* ---------------------------------------------------------------- statistics
+ * The reference's averaging windows (gcmc.f:1814-1928) run on every production move; the final
+ * statistics (gcmc.f:1960-2037) use 5 blocks of the first production samples up to 500,000
+ * production moves, the closed windows beyond.  final_stats out[1 + 14 ng]: production moves,
+ * then per species <N>, <E>, <EN>, <N^2>, <E^2>, the sixth average, and the errors of N, E, EN,
+ * N^2, E^2, Q_st, Cv and the sixth.  window_stats out[2 + 24 ng + ng ng]: avcount, rollcount,
+ * the window sums, variances and current means (8 per species), the selectivities.  The report
+ * is the reference's per-node block (gcmc.f:2052-2117). */
+int fmc_chain_window_stats(fmc_chain* c, double* out);
+int fmc_chain_final_stats(fmc_chain* c, double* out);
+int fmc_chain_write_report(fmc_chain* c, const char* path);
+/* The same report from statistics already at hand (pooled over chains, say), on the host
+ * alone: final_stats in the layout above, seltot[ng ng] species-major or NULL. */
+int fmc_write_report(const char* deck_dir, const double* final_stats, const double* seltot, const char* path);
+
 /* ---------------------------------------------------------------- probability plots
  * CONTROL `probability` plots (per guest: sites binned, 0 = centre of mass), `grid spacing`,
  * `grid factors`.  Every production move bins each guest molecule's sites into its species'
@@ -175,6 +190,11 @@ int fmc_batch_restart(fmc_batch* b, int chain, const char* revive_path);
 /* Probability plots of one chain of a batch (as fmc_chain_prob; the device sums weights in
  * fixed point, 2^-32 units, so the grids do not depend on the order of the adds). */
 int fmc_batch_prob(fmc_batch* b, int chain, int plot, int* dims, double* out);
+/* Statistics of one chain of a batch (as the fmc_chain_ functions; the stored samples live on
+ * the device, 16 MB a species a chain). */
+int fmc_batch_window_stats(fmc_batch* b, int chain, double* out);
+int fmc_batch_final_stats(fmc_batch* b, int chain, double* out);
+int fmc_batch_write_report(fmc_batch* b, int chain, const char* path);
 int fmc_batch_write_prob(fmc_batch* b, int chain, const char* outdir);
 
 /* ---------------------------------------------------------------- serving

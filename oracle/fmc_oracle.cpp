@@ -31,6 +31,15 @@ static const double R4PIE0 = 138935.4835;
 static const double KBOLTZ = 1.9872041e-3;
 static const double BOLTZ = 1.3806503e-23;
 static const double RGAS = 8.314472 / 4184.0;
+// calc_Qst, calc_Cv (utility_pack.f:2280-2316)
+static double calc_qst(double E2, double E, double N, double N2, double EN, double temp) {
+  (void)E2;
+  return -1.0 * (EN - E * N) / (N2 - N * N) + RGAS * temp;
+}
+static double calc_cv(double E2, double E, double N, double N2, double EN, double temp) {
+  const double d = EN - E * N;
+  return (3.0 / 2.0 * RGAS) + (E2 - (E * E) - d * d / (N2 - N * N)) / (N * KBOLTZ * temp * temp);
+}
 static const double MINANGLE = PI / 18.0;
 static const double DELRMIN = 0.1;
 static const int LENREC = 150;
@@ -451,6 +460,11 @@ struct Chain {
   long long prodcount = 0;
   bool last_accepted = false;
   int jump_count = 0, accept_jump = 0;
+  // windowed statistics (gcmc.f:1814-1935) and the first 500,000 production samples
+  // (gasmol / gaseng) for the blocked errors of the final report (gcmc.f:1960-2037)
+  int rollcount = 0, ins_rollcount = 0, avcount = 0;
+  std::vector<double> avgwindow, sumwindowav, varwindow, seltot, selwin;  // [8*ng], [ng*ng]
+  std::vector<double> gasmol, gaseng;                                     // [ng*500000 + 1]
   std::vector<double> chainstats;
   bool tick_tock[5] = {false, false, false, false, false};
   bool lgchk = true;
@@ -2115,6 +2129,13 @@ static void setup(Chain& C, const std::string& dir, int si, int sj, int sk, int 
   C.accept_tran.assign(C.ntpguest, 0);
   C.tran_count.assign(C.ntpguest, 0);
   C.chainstats.assign(1 + 14 * C.ntpguest, 0.0);
+  C.avgwindow.assign(8 * C.ntpguest, 0.0);
+  C.sumwindowav.assign(8 * C.ntpguest, 0.0);
+  C.varwindow.assign(8 * C.ntpguest, 0.0);
+  C.seltot.assign(C.ntpguest * C.ntpguest, 0.0);
+  C.selwin.assign(C.ntpguest * C.ntpguest, 0.0);
+  C.gasmol.assign((size_t)C.ntpguest * 500000 + 1, 0.0);
+  C.gaseng.assign((size_t)C.ntpguest * 500000 + 1, 0.0);
   if (!C.plots.empty()) {  // gcmc.f:246-265
     for (int i = 0; i < 3; i++)
       C.ngrid[i] = C.gridfactor[i] * (int)std::ceil(C.celprp[i] / (C.griddim * C.gridfactor[i]));
@@ -2529,10 +2550,15 @@ static void gcmc_step(Chain& C, MoveRec* rec) {
   if (C.production) {
     if ((C.laccsample && accepted) || !C.laccsample) {
       C.prodcount++;
+      C.rollcount++;
       C.chainstats[0] = (double)C.prodcount;
       for (int i = 0; i < C.ntpguest; i++) {
         double dm = (double)(float)C.mols[C.locguest[i]].nummols;
         double m2 = dm * dm, e = C.energy[i], e2 = e * e;
+        if (C.prodcount <= 500001) {
+          C.gasmol[(size_t)i * 500000 + C.prodcount - 1] = dm;
+          C.gaseng[(size_t)i * 500000 + C.prodcount - 1] = e;
+        }
         int is = 14 * i;
         double* cs = C.chainstats.data();
         double pc = (double)C.prodcount;
@@ -2546,7 +2572,54 @@ static void gcmc_step(Chain& C, MoveRec* rec) {
         cs[is + 4] = cs[is + 4] + delta / pc;
         delta = e2 - cs[is + 5];
         cs[is + 5] = cs[is + 5] + delta / pc;
+        double* aw = C.avgwindow.data() + 8 * i;
+        if (insert && iguest == i && accepted) {  // rolling <exp(-dE/kT)> (gcmc.f:1856-1866)
+          double h = std::exp(-1.0 * C.delE[i] / KBOLTZ / C.temp);
+          C.ins_rollcount++;
+          delta = h - cs[is + 6];
+          h = cs[is + 6] + delta / C.accept_ins;
+          cs[is + 6] = h;
+          aw[7] = ((C.ins_rollcount - 1) * aw[7] + h) / (double)C.ins_rollcount;
+        }
+        const double rc = (double)C.rollcount;
+        aw[0] = ((C.rollcount - 1) * aw[0] + dm) / rc;
+        aw[1] = ((C.rollcount - 1) * aw[1] + e) / rc;
+        aw[2] = ((C.rollcount - 1) * aw[2] + e * dm) / rc;
+        aw[3] = ((C.rollcount - 1) * aw[3] + m2) / rc;
+        aw[4] = ((C.rollcount - 1) * aw[4] + e2) / rc;
       }
+    }
+    if (C.prodcount % C.nwind == 0 || !C.lgchk) {  // close a window (gcmc.f:1887-1928)
+      C.avcount++;
+      const double weight = (double)C.rollcount / (double)C.nwind;
+      const int ng = C.ntpguest;
+      for (int i = 0; i < ng; i++) {
+        const double* cs = C.chainstats.data() + 14 * i;
+        double* aw = C.avgwindow.data() + 8 * i;
+        aw[5] = calc_qst(cs[5], cs[2], cs[1], cs[4], cs[3], C.temp);
+        aw[6] = calc_cv(cs[5], cs[2], cs[1], cs[4], cs[3], C.temp);
+        if (i > 0) {
+          const double an = aw[0];
+          for (int j = 0; j < i; j++) {
+            if (an == 0) continue;
+            double sel = C.avgwindow[8 * j] / an;
+            double& st = C.seltot[i * ng + j];
+            double& sw = C.selwin[i * ng + j];
+            double delta = weight * (sel - st);
+            st = st + delta / C.avcount;
+            sw = sw + weight * (sel * sel - sw) / (C.avcount - 1 + weight);
+            C.seltot[j * ng + i] = ((C.avcount - 1 + weight) * sw - ((C.avcount - 1 + weight) * st * st)) /
+                                   (C.avcount - 1 + weight);
+          }
+        }
+      }
+      for (int k = 0; k < 8 * ng; k++) {
+        double delta = weight * (C.avgwindow[k] - C.sumwindowav[k]);
+        C.sumwindowav[k] = C.sumwindowav[k] + delta / C.avcount;
+        C.varwindow[k] = C.varwindow[k] + delta * weight * (C.avgwindow[k] - C.sumwindowav[k]);
+        C.avgwindow[k] = 0.0;
+      }
+      C.rollcount = 0;
     }
     if (!C.plots.empty()) storeprob(C);  // gcmc.f:1929-1931, every production move
   }
@@ -2808,6 +2881,74 @@ void orc_restart_flags(void* p, int production, const double* chainstats) {
   if (C.eqsteps == 0) C.production = true;
   for (size_t i = 0; i < C.chainstats.size(); i++) C.chainstats[i] = chainstats[i];
   C.prodcount = 0;
+}
+// Final statistics of the report (gcmc.f:1960-2037) on a copy of the chain's statistics:
+// out[1 + 14 g + 0..13] = <N>, <E>, <EN>, <N^2>, <E^2>, 6th slot, then the errors of N, E, EN,
+// N^2, E^2, Q_st, Cv and the 6th slot; out[0] = production moves.  Up to 500,000 production
+// moves the averages and errors come from 5 blocks of the stored samples (each block sums
+// the nwind + 1 samples of an inclusive slice and divides by nwind, as the reference does);
+// beyond, from the windows closed during the run.
+void orc_final_stats(void* p, double* out) {
+  Chain& C = ((OrcHandle*)p)->C;
+  const int ng = C.ntpguest, windn = 5;
+  std::vector<double> cs = C.chainstats, var = C.varwindow, sum = C.sumwindowav, avg = C.avgwindow;
+  int avcount = C.avcount;
+  if (C.prodcount > 0) {
+    const double weight = cs[0];
+    for (int i = 0; i < ng; i++) {
+      const int is = 14 * i, vs = 8 * i;
+      if (weight <= 500000) {
+        const long long nw = (long long)weight / windn;
+        avcount = windn;
+        std::fill(var.begin(), var.end(), 0.0);
+        std::fill(sum.begin(), sum.end(), 0.0);
+        std::fill(avg.begin(), avg.end(), 0.0);
+        for (int x = 1; x <= windn; x++) {
+          const size_t y = (size_t)i * 500000 + (size_t)(x - 1) * nw;
+          double an = 0, e = 0, en = 0, n2 = 0, e2 = 0;
+          for (size_t k = y; k <= y + nw; k++) {
+            double m = k < C.gasmol.size() ? C.gasmol[k] : 0.0, g = k < C.gaseng.size() ? C.gaseng[k] : 0.0;
+            an += m;
+            e += g;
+            en += m * g;
+            n2 += m * m;
+            e2 += g * g;
+          }
+          avg[0] = an / nw;
+          avg[1] = e / nw;
+          avg[2] = en / nw;
+          avg[3] = n2 / nw;
+          avg[4] = e2 / nw;
+          avg[5] = calc_qst(avg[4], avg[1], avg[0], avg[3], avg[2], C.temp);
+          avg[6] = calc_cv(avg[4], avg[1], avg[0], avg[3], avg[2], C.temp);
+          for (int z = 0; z < 7; z++) {
+            double delta = avg[z] - sum[z];
+            sum[z] = sum[z] + delta / x;
+            var[vs + z] = var[vs + z] + delta * (avg[z] - sum[z]);
+            avg[z] = 0.0;
+          }
+        }
+        for (int z = 0; z < 6; z++) cs[is + 1 + z] = sum[z];
+      }
+      for (int z = 0; z < 8; z++) cs[is + 7 + z] = std::sqrt(var[vs + z] / avcount);
+    }
+  }
+  std::memcpy(out, cs.data(), sizeof(double) * cs.size());
+}
+// Window state: avcount, rollcount, then sumwindowav[8 ng], varwindow[8 ng], avgwindow[8 ng]
+// and seltot[ng ng].
+void orc_window_stats(void* p, double* out) {
+  Chain& C = ((OrcHandle*)p)->C;
+  const int ng = C.ntpguest;
+  out[0] = C.avcount;
+  out[1] = C.rollcount;
+  double* o = out + 2;
+  for (int k = 0; k < 8 * ng; k++) {
+    o[k] = C.sumwindowav[k];
+    o[8 * ng + k] = C.varwindow[k];
+    o[16 * ng + k] = C.avgwindow[k];
+  }
+  for (int k = 0; k < ng * ng; k++) o[24 * ng + k] = C.seltot[k];
 }
 // Probability plots: dims[0..3] = plots, na, nb, nc; grid of plot ip when out is non-null.
 int orc_prob(void* p, int ip, int* dims, double* out) {

@@ -69,6 +69,8 @@ def lib():
         L.orc_stats.argtypes = [vp, ctypes.c_int, dp]
         L.orc_restart_flags.argtypes = [vp, ctypes.c_int, dp]
         L.orc_prob.argtypes = [vp, ctypes.c_int, ip, dp]
+        L.orc_final_stats.argtypes = [vp, dp]
+        L.orc_window_stats.argtypes = [vp, dp]
         assert L.orc_sizeof_moverec() == MOVE_DTYPE.itemsize
         _lib = L
     return _lib
@@ -214,6 +216,25 @@ class Chain:
 
     def duni(self):
         return lib().orc_duni(self.h)
+
+    def final_stats(self):
+        """The report's statistics (gcmc.f:1960-2037) as chainstats: [0] production moves, then
+        per species 14 values (<N>,<E>,<EN>,<N^2>,<E^2>, 6th, errors of N,E,EN,N^2,E^2,Qst,Cv,6th)."""
+        ng = self.ints()["ntpguest"]
+        out = np.zeros(1 + 14 * ng)
+        lib().orc_final_stats(self.h, _dp(out))
+        return out
+
+    def window_stats(self):
+        """Averaging-window state (gcmc.f:1814-1928): avcount, rollcount, window sums, variances,
+        current means (8 per species) and selectivities."""
+        ng = self.ints()["ntpguest"]
+        out = np.zeros(2 + 24 * ng + ng * ng)
+        lib().orc_window_stats(self.h, _dp(out))
+        o = out[2:]
+        return {"avcount": int(out[0]), "rollcount": int(out[1]), "sum": o[:8 * ng].reshape(ng, 8),
+                "var": o[8 * ng:16 * ng].reshape(ng, 8), "avg": o[16 * ng:24 * ng].reshape(ng, 8),
+                "seltot": o[24 * ng:24 * ng + ng * ng].reshape(ng, ng)}
 
     def prob(self):
         """Probability grids (storeprob): array [plots, na, nb, nc] of binned weights."""

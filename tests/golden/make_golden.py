@@ -17,6 +17,7 @@ expected.json come from that example's OUTPUT and REVIVE:
 * REVIVE      its production flag, chainstats and natms, and the SHA-256 of REVIVE and REVCON,
               so that a writer restating revive (utility_pack.f:1772-1817) can be checked
               byte for byte without the files themselves
+* OUTPUT      the per-node report block (report_node0.txt), to check the report writer's layout
 """
 import hashlib
 import json
@@ -88,13 +89,21 @@ def main(ref):
     # the mass windows of atmnumber (utility_pack.f:1992-2237) as data, to check the writer's
     # atomic numbers against them
     import re
-    src = open(os.path.join(ref, "fastmc", "utility_pack.f")).read()
-    body = src[src.index("integer function atmnumber"):src.index("end function atmnumber")]
+    upack = open(os.path.join(ref, "fastmc", "utility_pack.f")).read()
+    body = upack[upack.index("integer function atmnumber"):upack.index("end function atmnumber")]
     wins = [[float(lo), float(hi), int(z)] for lo, hi, z in
             re.findall(r"\(i\.ge\.([0-9.]+)\)\.and\.\(i\.le\.([0-9.]+)\)\)then\s*\n\s*atmnumber=(\d+)", body)]
     with open(os.path.join(HERE, "atmnumber_windows.json"), "w") as f:
         json.dump(wins, f)
     print("wrote", len(wins), "atmnumber windows")
+    # the per-node report block of the example's OUTPUT (gcmc.f:2052-2108): from the blank line
+    # before the banner through the blank line after the species block
+    lines = open(os.path.join(src, "OUTPUT")).read().split("\n")
+    i0 = next(i for i, s in enumerate(lines) if "Data reported from node" in s) - 2
+    i1 = next(i for i in range(i0, len(lines)) if "Heat capacity error" in lines[i]) + 1
+    with open(os.path.join(out, "report_node0.txt"), "w") as f:
+        f.write("\n".join(lines[i0:i1 + 1]) + "\n")
+    print("wrote report block, OUTPUT lines", i0 + 1, "-", i1 + 1)
 
 
 if __name__ == "__main__":

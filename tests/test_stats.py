@@ -20,3 +20,28 @@ def test_pooled_jackknife_of_identical_chains_is_exact():
     p = stats.pooled(st, 300.0)
     assert p["chains"] == 8 and abs(p["N"] - 10.5) < 1e-12
     assert p["N_err"] > 0 and np.isfinite(p["Qst_err"])
+
+
+def test_report_block_matches_reference_output(tmp_path):
+    """The report writer against the per-node block of the CALF-20 example's OUTPUT
+    (gcmc.f:2052-2108), fed the moments, multiplier and errors that block prints."""
+    import os
+
+    import fastmc_b200
+
+    gold = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "calf20")
+    ref = open(os.path.join(gold, "report_node0.txt")).read().split("\n")
+    fs = np.zeros(15)
+    fs[0] = 100000001
+    fs[1:6] = [91.811777992, -756.809149592, -69669.494245516, 8449.961248488, 574495.827703705]
+    fs[12], fs[13] = 0.058306353, 0.000088536
+    out = tmp_path / "report"
+    fastmc_b200.write_report(gold, fs, out)
+    got = out.read_text().split("\n")
+    assert len(got) == len(ref)
+    for g, r in zip(got, ref):
+        if "Isosteric heat of adsorption" in r or "Heat capacity, Cv" in r:
+            # computed from the 9-decimal moments above rather than the run's own
+            assert g[:65] == r[:65] and abs(float(g[65:]) - float(r[65:])) < 2e-8, (g, r)
+        else:
+            assert g == r
