@@ -110,6 +110,15 @@ class ClockSampler:
             self.proc = None
         return self
 
+    def ready(self, timeout=5.0):
+        """Waits for the first sample, so that nvidia-smi's start-up stays outside a timed region."""
+        t0 = time.perf_counter()
+        while self.proc and time.perf_counter() - t0 < timeout:
+            self.f.flush()
+            if os.path.getsize(self.path) > 0 or self.proc.poll() is not None:
+                return
+            time.sleep(0.02)
+
     def __exit__(self, *a):
         if self.proc:
             self.proc.terminate()
@@ -232,14 +241,15 @@ def run_plain(args, dist):
     guests_at_start = chain.guest_coords(0)
     dist.barrier()
     ms_total = 0.0
-    wall0 = time.perf_counter()
     traces = []
     with ClockSampler(dist.local) as clk:
+        clk.ready()
+        wall0 = time.perf_counter()
         for _ in range(args.steps):
             tr, ms = chain.run_timed(args.moves, trace=True)
             traces.append(tr)
             ms_total += ms
-    wall = time.perf_counter() - wall0
+        wall = time.perf_counter() - wall0
     dist.barrier()
     prof = chain.profile(0)
     t_dev = dist.max(ms_total / 1000.0)
@@ -331,12 +341,13 @@ def run_batched(args, dist):
         b.run(args.moves)
     dist.barrier()
     kernel_ms = 0.0
-    wall0 = time.perf_counter()
     with ClockSampler(dist.local) as clk:
+        clk.ready()
+        wall0 = time.perf_counter()
         for _ in range(args.steps):
             _, ms = b.run(args.moves)
             kernel_ms += ms
-    wall = time.perf_counter() - wall0
+        wall = time.perf_counter() - wall0
     dist.barrier()
     t_dev = dist.max(kernel_ms / 1000.0)
     t_wall = dist.max(wall)
@@ -357,8 +368,8 @@ def run_batched(args, dist):
     tpm = profiled_traffic("batch_kernel_batched", "traffic_bytes_per_chain_move")
     traffic = tpm * n * args.moves if tpm else None
     peak, peak_kind = peaks()
-    from fastmc_b200._lib import lib as _l  # noqa: F401
-    cb = 1512  # bytes of one chain control block moved each way per step (sizeof(ChainDev))
+    from fastmc_b200._lib import lib as _l
+    cb = int(_l().fmc_batch_control_block_bytes())  # one chain's control block, moved each way per step
     result = {
         "metric": BATCHED_METRIC,
         "value": total_moves / t_dev,
@@ -496,8 +507,9 @@ def run_serve(args, dist):
     nxt = 0
     dev_ms, steps, occ = 0.0, 0, 0.0
     log = []  # per step: wall start, wall end, device ms, moves run, active slots
-    wall0 = time.perf_counter()
     with ClockSampler(dist.local) as clk:
+        clk.ready()
+        wall0 = time.perf_counter()
         while len(done_t) < n_req:
             now = time.perf_counter() - wall0
             while nxt < n_req and arrivals[nxt] <= now:
@@ -518,7 +530,7 @@ def run_serve(args, dist):
                 if res["state"] in (srv.DONE, srv.REJECTED, srv.CANCELLED):
                     done_t[live[rid]] = (end - arrivals[live[rid]], res)
                     del live[rid]
-    wall = time.perf_counter() - wall0
+        wall = time.perf_counter() - wall0
     dist.barrier()
     lat = np.array([v[0] for v in done_t.values()])
     rejected = sum(1 for v in done_t.values() if v[1]["state"] != srv.DONE)
@@ -537,7 +549,9 @@ def run_serve(args, dist):
     used, budget = srv.memory()
     sstats = srv.stats()
     srv.close()
-    # host<->device bytes per step: slot control blocks (SysConst + ChainDev) each way
+    # host<->device bytes per step: every slot's system block and control block in, control blocks out
+    from fastmc_b200._lib import lib as _l
+    cb, sb = int(_l().fmc_batch_control_block_bytes()), int(_l().fmc_system_block_bytes())
     return {
         "metric": "MC trial moves/s on 1 B200 (continuous-batching serving); p50/p99 time-to-completion",
         "value": total / t_dev, "unit": "moves/s", "n_gpus": dist.world, "steps": len(win), "warmup": 1,
@@ -563,7 +577,7 @@ def run_serve(args, dist):
                       "slot_occupancy": occ / max(dev_ms, 1e-9) / args.serve_slots},
         "gpu_launches": len(win),
         "e2e": {"value": total / t_wall, "unit": "moves/s",
-                "h2d_bytes_per_step": args.serve_slots * 2 * 1512, "d2h_bytes_per_step": args.serve_slots * 1512},
+                "h2d_bytes_per_step": args.serve_slots * (sb + cb), "d2h_bytes_per_step": args.serve_slots * cb},
         "clocks": clk.summary(),
         "memory": {"slots_bytes_at_end": used, "budget_bytes": budget},
         "server": sstats,

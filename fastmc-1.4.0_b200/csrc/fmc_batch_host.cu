@@ -459,6 +459,9 @@ struct fmc_batch {
 
 extern "C" {
 
+int fmc_batch_control_block_bytes(void) { return (int)sizeof(fmc::ChainDev); }
+int fmc_system_block_bytes(void) { return (int)sizeof(fmc::SysConst); }
+
 int fmc_batch_open(int nchains, const char* const* dirs, const int* seeds, int device, fmc_batch** out) {
   if (!dirs || !seeds || !out || nchains < 1) {
     fmc::set_last_error("null argument or empty batch");

@@ -63,6 +63,8 @@ SIGNATURES = {
     "fmc_chain_write_report": (_ci, [_vp, ctypes.c_char_p]),
     "fmc_write_report": (_ci, [ctypes.c_char_p, _dp, _dp, ctypes.c_char_p]),
     "fmc_batch_window_stats": (_ci, [_vp, _ci, _dp]),
+    "fmc_batch_control_block_bytes": (_ci, []),
+    "fmc_system_block_bytes": (_ci, []),
     "fmc_batch_final_stats": (_ci, [_vp, _ci, _dp]),
     "fmc_batch_write_report": (_ci, [_vp, _ci, ctypes.c_char_p]),
     "fmc_write_prob_cube": (_ci, [ctypes.c_char_p, ctypes.c_char_p, _dp, ctypes.c_longlong]),

@@ -193,6 +193,10 @@ int fmc_batch_prob(fmc_batch* b, int chain, int plot, int* dims, double* out);
 /* Statistics of one chain of a batch (as the fmc_chain_ functions; the stored samples live on
  * the device, 16 MB a species a chain). */
 int fmc_batch_window_stats(fmc_batch* b, int chain, double* out);
+/* Bytes of one chain's control block (copied host->device and back around every run). */
+int fmc_batch_control_block_bytes(void);
+/* Bytes of one system's constant block (a serving slot copies it host->device every step). */
+int fmc_system_block_bytes(void);
 int fmc_batch_final_stats(fmc_batch* b, int chain, double* out);
 int fmc_batch_write_report(fmc_batch* b, int chain, const char* path);
 int fmc_batch_write_prob(fmc_batch* b, int chain, const char* outdir);
