@@ -28,6 +28,13 @@ struct MoveSmem {
   int vb[2 * kBatchMaxSites], vl[2 * kBatchMaxSites], pre[2 * kBatchMaxSites + 1];
   int gpre[kMaxGuestTypes + 1];
   double lrc_term[kBatchMaxTab];
+  // multi-jump (gcmc.f:1557-1785) across the two loop trips of one move: stage 1 while the
+  // first jump is evaluated and committed, 2 for the second jump; the first molecule's choice
+  // and old sites, its energy change, the energy before the move and the commit action
+  // (1: park S(k) in the chain's global copy, then commit; 2: restore S(k) and the first molecule)
+  int mj_stage, mj_first, mj_lo, mj_action;
+  double mj_estep, mj_energy0;
+  double mj_old[3 * kBatchMaxSites];
 };
 
 __device__ double lrc_device(const SysConst& Y, const int* numtyp) {
@@ -80,6 +87,12 @@ template <bool kProf>
 __device__ __noinline__ void move_begin(ChainDev& C, const SysConst& Y, const DevSystem& S, MoveSmem& M) {
   if (kProf) C.prof[7] -= clock64();
   DuniLocal R(C.rng);  // written back before every return
+  M.mj_action = 0;
+  int g = M.g, mtype = kMultiJump;
+  if (M.mj_stage == 1) {
+    M.mj_stage = 2;  // the second jump of a multi-jump: no count, selection or adaptation
+  } else {
+  M.mj_first = 0;  // a new move: no molecule to avoid
   C.gcmccount++;
   if (C.gcmccount % 400 == 0) {
     int totalguests = 0;
@@ -108,11 +121,10 @@ __device__ __noinline__ void move_begin(ChainDev& C, const SysConst& Y, const De
     }
   }
   const int ng = Y.nspecies;
-  int g = 0;
+  g = 0;
   if (ng > 1) g = (int)floor(R.next() * ng);
   double randmov = R.next();
   const double* c = C.mvcum[g];
-  int mtype;
   if (randmov < c[0]) mtype = kInsert;
   else if (randmov < c[1]) mtype = kDelete;
   else if (randmov < c[2]) mtype = kDisplace;
@@ -120,10 +132,9 @@ __device__ __noinline__ void move_begin(ChainDev& C, const SysConst& Y, const De
   else if (randmov < c[5]) mtype = kNoop;  // flex, swap (gcmc.f:1789-1795)
   else if (randmov < c[6]) mtype = kTranslate;
   else if (randmov < c[7]) mtype = kRotate;
-  else if (randmov < c[8]) mtype = -1;
+  else if (randmov < c[8]) mtype = kMultiJump;
   else mtype = kDisplace;
-  const SpeciesConst& P = Y.sp[g];
-  const int ns = P.nsite, nmols = C.nmol[g];
+  const int nmols = C.nmol[g];
   // step-size adaptation (gcmc.f:794-834)
   if (nmols >= 1 && C.disp_count[g] >= 1) {
     if (C.disp_count[g] % 100 == 0) {
@@ -142,7 +153,16 @@ __device__ __noinline__ void move_begin(ChainDev& C, const SysConst& Y, const De
     if ((C.accept_rota / (double)C.rota_count) > C.rota_ratio) C.rota_rotangle = C.rota_rotangle * 1.05;
     else if (C.rota_rotangle > kMinAngle) C.rota_rotangle = C.rota_rotangle * 0.95;
   }
-  if (nmols == 0) mtype = kInsert;
+  if (nmols == 0 || (nmols == 1 && mtype == kMultiJump)) mtype = kInsert;  // gcmc.f:837-847
+  if (mtype == kMultiJump) {
+    C.jump_count++;
+    M.mj_stage = 1;
+    M.mj_first = 0;
+    M.mj_energy0 = C.energy[g];
+  }
+  }
+  const SpeciesConst& P = Y.sp[g];
+  const int ns = P.nsite, nmols = C.nmol[g];
   if (kProf) C.prof[7] += clock64();  // minus the stamp taken at entry: selection + adaptation
   M.mtype = mtype;
   M.g = g;
@@ -156,11 +176,6 @@ __device__ __noinline__ void move_begin(ChainDev& C, const SysConst& Y, const De
   M.need_lrc = 0;
   M.rande_drawn = 0;
   M.recheck = 0;
-  if (mtype < 0) {
-    C.status = 3;
-    R.store(C.rng);
-    return;
-  }
   double* x = M.x;
   double* y = M.y;
   double* z = M.z;
@@ -194,10 +209,15 @@ __device__ __noinline__ void move_begin(ChainDev& C, const SysConst& Y, const De
     M.nold = ns;
     for (int i = 0; i < ns; i++) C.numtyp[P.type[i]]--;
     M.need_lrc = 1;
-  } else if (mtype == kJump) {
-    // long jump (gcmc.f:1389-1547): the choice first, then the seven draws of random_jump
-    C.jump_count++;
-    int randchoice = (int)floor(R.next() * nmols) + 1;
+  } else if (mtype == kJump || mtype == kMultiJump) {
+    // long jump (gcmc.f:1389-1547): the choice first, then the seven draws of random_jump; the
+    // second jump of a multi-jump draws until it hits a molecule other than the first
+    if (mtype == kJump) C.jump_count++;
+    int randchoice;
+    do {
+      randchoice = (int)floor(R.next() * nmols) + 1;
+    } while (randchoice == M.mj_first);
+    if (mtype == kMultiJump && M.mj_stage == 1) M.mj_first = randchoice;
     M.randchoice = randchoice;
     M.mol = randchoice - 1;
     M.ex_lo = C.seg_off[g] + M.mol * ns;
@@ -294,10 +314,17 @@ __device__ __forceinline__ void assemble(const SysConst& Y, MoveSmem& M, const d
 // instead (returns 1).  Random numbers are drawn exactly where the reference draws them.
 __device__ __forceinline__ int decide(ChainDev& C, const SysConst& Y, MoveSmem& M, double band) {
   const int g = M.g, mtype = M.mtype, nmols = C.nmol[g];
-  const double e = M.estep;
+  double e = M.estep;
   if (mtype == kNoop) {  // nothing to accept or reject; no draw
     M.accepted = 0;
     return 0;
+  }
+  if (mtype == kMultiJump) {
+    if (M.mj_stage == 1) {  // the first jump is kept for now; its dE must be the FP64 one
+      M.accepted = 1;
+      return band > 0.0 ? 1 : 0;
+    }
+    e = M.mj_estep + e;  // one test on the summed change (gcmc.f:1730-1739)
   }
   if (mtype == kInsert || mtype == kDelete) {
     if (!M.rande_drawn) {
@@ -364,8 +391,34 @@ __device__ __noinline__ void bookkeep(ChainDev& C, const SysConst& Y, MoveSmem& 
   const SpeciesConst& P = Y.sp[g];
   const int nmols = C.nmol[g];
   const bool accepted = M.accepted;
-  const double estep = M.estep;
+  double estep = M.estep;
   M.seg_end = C.seg_off[g] + nmols * ns;
+  if (mtype == kMultiJump) {
+    M.commit_lo = M.ex_lo;
+    if (M.mj_stage == 1) {
+      // the first jump stands while the second is tried (gcmc.f:1697-1715): remember where it
+      // came from; the move is counted once, when the second jump is decided
+      M.mj_estep = estep;
+      M.mj_lo = M.ex_lo;
+      for (int i = 0; i < ns; i++) {
+        M.mj_old[3 * i] = M.x[i];
+        M.mj_old[3 * i + 1] = M.y[i];
+        M.mj_old[3 * i + 2] = M.z[i];
+      }
+      M.mj_action = 1;
+      C.energy[g] = M.mj_energy0 + estep;
+      return;
+    }
+    estep = M.mj_estep + estep;
+    M.mj_stage = 0;
+    if (accepted) {
+      C.accept_jump++;
+      C.energy[g] = M.mj_energy0 + estep;
+    } else {
+      M.mj_action = 2;
+      C.energy[g] = M.mj_energy0;
+    }
+  }
   if (mtype == kInsert) {
     M.commit_lo = M.seg_end;
     if (accepted) {
@@ -388,7 +441,7 @@ __device__ __noinline__ void bookkeep(ChainDev& C, const SysConst& Y, MoveSmem& 
     } else {
       for (int i = 0; i < ns; i++) C.numtyp[P.type[i]]++;
     }
-  } else if (mtype != kNoop) {
+  } else if (mtype != kNoop && mtype != kMultiJump) {
     M.commit_lo = M.ex_lo;
     if (accepted) {
       if (mtype == kTranslate) C.accept_tran[g]++;
@@ -782,8 +835,10 @@ __global__ void __launch_bounds__(kBatchThreads, 2) fmc_batch_kernel(BatchLaunch
   // out (the reference's do-while(lgchk) loop, gcmc.f:589-736), or at its move budget
   long long nmoves = C.lgchk ? L.moves : 0;
   if (C.budget > 0) nmoves = min(nmoves, C.budget - C.moves_done);
-  for (int mv = 0; mv < nmoves; mv++) {
-    if (mixed && L.recompute_every > 0 && C.since_recompute >= L.recompute_every) {
+  if (tid == 0) M.mj_stage = 0;
+  bool pending = false;  // the first half of a multi-jump ended the last trip; the move goes on
+  for (int mv = 0; mv < nmoves;) {
+    if (mixed && L.recompute_every > 0 && C.since_recompute >= L.recompute_every && !pending) {
       recompute_sk(S, Y, C, nseg, kp, Sk);
       __syncthreads();
       if (tid == 0) {
@@ -896,6 +951,14 @@ __global__ void __launch_bounds__(kBatchThreads, 2) fmc_batch_kernel(BatchLaunch
       C.prof[3] += t1 - t0;
       t0 = t1;
     }
+    if (M.mj_action == 1)  // park S(k) before the first jump of a multi-jump is committed
+      for (int k = tid; k < K; k += blockDim.x) C.sk[k] = Sk[k];
+    if (M.mj_action == 2) {  // rejected multi-jump: S(k) and the first molecule as they were
+      for (int k = tid; k < K; k += blockDim.x) Sk[k] = C.sk[k];
+      if (tid < M.ns)
+        C.gsite[M.mj_lo + tid] =
+            make_double4(M.mj_old[3 * tid], M.mj_old[3 * tid + 1], M.mj_old[3 * tid + 2], Y.sp[M.g].q[tid]);
+    }
     if (M.accepted) {
       for (int k = tid; k < K; k += blockDim.x) Sk[k] = Sn[k];
       const int ns = M.ns, mtype = M.mtype;
@@ -923,12 +986,15 @@ __global__ void __launch_bounds__(kBatchThreads, 2) fmc_batch_kernel(BatchLaunch
         C.gtype[M.commit_lo + tid] = M.type[st];
       }
     }
-    // read before the barrier: thread 0 may change the production flag in the next move_begin
-    const bool store = Y.nplots && C.production;
+    // read before the barrier: thread 0 may change these in the next move_begin
+    pending = M.mj_stage == 1;
+    const bool store = Y.nplots && C.production && !pending;
     __syncthreads();
     if (prof && tid == 0) C.prof[4] += clock64() - t0;
     if (store) prob_store(Y, C);  // every production move (gcmc.f:1929-1931)
+    if (pending) continue;
     if (last) break;
+    mv++;
   }
   for (int k = tid; k < K; k += blockDim.x) C.sk[k] = Sk[k];
   __syncthreads();

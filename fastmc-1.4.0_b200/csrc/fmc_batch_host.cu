@@ -126,10 +126,6 @@ int init_chain_state(const InputDeck& d, const HostSystem& H, const double2* sk_
       nrm = 1;
       f = {1.0 / 3.0, 1.0 / 3.0, 1.0 / 3.0, 0, 0, 0, 0, 0, 0};
     }
-    if (f[8] != 0) {
-      err = "multi-jump moves are outside the GCMC trial-move path";
-      return -3;
-    }
     C.mvcum[g][0] = f[0] / nrm;
     for (int k = 1; k < 9; k++) C.mvcum[g][k] = C.mvcum[g][k - 1] + (f[k] / nrm);
     C.disp_ratio[g] = d.disp_ratio[g];

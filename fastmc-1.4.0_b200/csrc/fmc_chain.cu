@@ -118,7 +118,7 @@ Chain::~Chain() {
   if (st) {
     cudaSetDevice(device);
     cudaStreamSynchronize(st);
-    for (void* p : {(void*)sk, (void*)sk_new, (void*)gsite, (void*)gtype, (void*)W.recip_part, (void*)W.site_e,
+    for (void* p : {(void*)sk, (void*)sk_new, (void*)sk_save, (void*)gsite, (void*)gtype, (void*)W.recip_part, (void*)W.site_e,
                     (void*)W.counter, (void*)W.result, (void*)recip_scratch, (void*)recip_parts, (void*)all_atoms})
       if (p) cudaFree(p);
     if (h_result) cudaFreeHost(h_result);
@@ -194,6 +194,7 @@ int Chain::open_prepared(HostSystem&& prepared, const int seed[4], int dev, std:
   gcap = off;
   FMC_CUDA(cudaMalloc(&sk, sizeof(double2) * std::max(K, 1)));
   FMC_CUDA(cudaMalloc(&sk_new, sizeof(double2) * std::max(K, 1)));
+  FMC_CUDA(cudaMalloc(&sk_save, sizeof(double2) * std::max(K, 1)));
   FMC_CUDA(cudaMalloc(&gsite, sizeof(double4) * std::max(gcap, 1)));
   FMC_CUDA(cudaMalloc(&gtype, sizeof(int) * std::max(gcap, 1)));
   FMC_CUDA(cudaMalloc(&W.recip_part, sizeof(double) * (pass_recip_blocks(dsys.view) + 1)));
@@ -590,7 +591,7 @@ int Chain::step(MoveRecord* rec) {
   else if (randmov < c[5]) mtype = kNoop;  // flex, swap (gcmc.f:1789-1795)
   else if (randmov < c[6]) mtype = kTranslate;
   else if (randmov < c[7]) mtype = kRotate;
-  else if (randmov < c[8]) return -3;
+  else if (randmov < c[8]) mtype = kMultiJump;
   else mtype = kDisplace;
   Species& s = sp[g];
   const GuestSpecies& G = d.guests[g];
@@ -614,7 +615,7 @@ int Chain::step(MoveRecord* rec) {
     if ((accept_rota / (double)rota_count) > d.rota_ratio) rota_rotangle = rota_rotangle * 1.05;
     else if (rota_rotangle > kMinAngle) rota_rotangle = rota_rotangle * 0.95;
   }
-  if (nmols == 0) mtype = kInsert;
+  if (nmols == 0 || (nmols == 1 && mtype == kMultiJump)) mtype = kInsert;  // gcmc.f:837-847
   MoveRecord R;
   std::memset(&R, 0, sizeof(R));
   R.step = gcmccount;
@@ -710,6 +711,67 @@ int Chain::step(MoveRecord* rec) {
       accept_jump++;
       if ((rc = commit(kDisplace, g, mol, newx))) return rc;
       energy[g] += delE[g];
+    }
+  } else if (mtype == kMultiJump) {
+    // two distinct molecules jump one after the other (gcmc.f:1557-1785); the first jump is
+    // committed before the second is evaluated, one test decides on the summed change and a
+    // rejection puts the first molecule and S(k) back
+    jump_count++;
+    const double origenergy = energy[g];
+    cudaError_t ce = cudaMemcpyAsync(sk_save, sk, sizeof(double2) * std::max(sys.K, 1), cudaMemcpyDeviceToDevice, st);
+    if (ce != cudaSuccess) return sync_error(ce);
+    int first = 0, mol = -1;
+    double first_old[3 * kMaxGuestSites];
+    for (int mv = 1; mv <= 2; mv++) {
+      int randchoice;
+      do {  // a molecule that has not jumped in this move
+        randchoice = (int)std::floor(duni_next(rng) * nmols) + 1;
+      } while (randchoice == first);
+      if (mv == 1) first = randchoice;
+      R.randchoice = randchoice;
+      mol = randchoice - 1;
+      std::copy(s.xyz.begin() + (size_t)mol * 3 * natms, s.xyz.begin() + (size_t)(mol + 1) * 3 * natms, oldx);
+      double r[7];
+      for (int i = 0; i < 7; i++) r[i] = duni_next(rng);
+      double x[kMaxGuestSites], y[kMaxGuestSites], z[kMaxGuestSites];
+      for (int i = 0; i < natms; i++) {
+        x[i] = oldx[3 * i];
+        y[i] = oldx[3 * i + 1];
+        z[i] = oldx[3 * i + 2];
+      }
+      trial_jump(sys.cell, G.mass.data(), natms, r, x, y, z);
+      for (int i = 0; i < natms; i++) {
+        newx[3 * i] = x[i];
+        newx[3 * i + 1] = y[i];
+        newx[3 * i + 2] = z[i];
+      }
+      if ((rc = pass(kDisplace, g, mol, oldx, newx, e))) return rc;
+      estep = estep + (e[0] + e[1] + e[2]) / sys.engunit;
+      if (mv == 1) {
+        std::copy(oldx, oldx + 3 * natms, first_old);
+        if ((rc = commit(kDisplace, g, mol, newx))) return rc;
+        delE[g] = estep;
+        energy[g] = origenergy + delE[g];
+      }
+    }
+    if (estep < 0.0) {
+      accepted = true;
+    } else {
+      rande = duni_next(rng);
+      accepted = accept_move(estep, rande, sys.statvolm, d.press[g], nmols, d.temp, sys.beta, kDisplace);
+    }
+    if (accepted) {
+      delE[g] = estep;
+      accept_jump++;
+      if ((rc = commit(kDisplace, g, mol, newx))) return rc;
+      energy[g] = origenergy + delE[g];
+    } else {
+      delE[g] = 0.0;
+      // S(k) back to its state before the move; the first molecule back to its old sites
+      ce = cudaMemcpyAsync(sk_new, sk_save, sizeof(double2) * std::max(sys.K, 1), cudaMemcpyDeviceToDevice, st);
+      if (ce != cudaSuccess) return sync_error(ce);
+      if ((rc = commit(kDisplace, g, first - 1, first_old))) return rc;
+      energy[g] = origenergy;
     }
   } else if (mtype == kNoop) {
     accepted = last_accepted;  // the reference leaves `accepted` as the last move set it

@@ -46,6 +46,7 @@ class Chain {
   // device chain state
   double2* sk = nullptr;
   double2* sk_new = nullptr;
+  double2* sk_save = nullptr;  // S(k) before a multi-jump, restored if it is rejected
   double4* gsite = nullptr;
   int* gtype = nullptr;
   int gcap = 0;

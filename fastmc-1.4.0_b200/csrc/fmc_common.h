@@ -26,8 +26,18 @@ constexpr int kMaxGuestSites = 50;           // mxguestsite, utility_pack.f:76
 constexpr int kMaxGuestTypes = 4;
 
 // kJump: long jump (gcmc.f:1389-1547); kNoop: flex and swap, which the reference selects but
-// does not implement (gcmc.f:1789-1795)
-enum MoveType : int { kInsert = 1, kDelete = 2, kDisplace = 3, kTranslate = 4, kRotate = 5, kJump = 6, kNoop = 7 };
+// does not implement (gcmc.f:1789-1795); kMultiJump: two long jumps under one acceptance test
+// (gcmc.f:1557-1785)
+enum MoveType : int {
+  kInsert = 1,
+  kDelete = 2,
+  kDisplace = 3,
+  kTranslate = 4,
+  kRotate = 5,
+  kJump = 6,
+  kNoop = 7,
+  kMultiJump = 8
+};
 
 // ------------------------------------------------------------------ duni
 // Marsaglia-Zaman-Tsang universal generator in IEEE single precision, as duni in

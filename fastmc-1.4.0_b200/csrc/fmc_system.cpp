@@ -320,10 +320,6 @@ int build_host_system(const InputDeck& d, HostSystem& s, std::string& err, doubl
       nrm = 1;
       f = {1.0 / 3.0, 1.0 / 3.0, 1.0 / 3.0, 0, 0, 0, 0, 0, 0};
     }
-    if (f[8] != 0) {
-      err = "multi-jump moves are outside the GCMC trial-move path";
-      return -3;
-    }
     std::array<double, 9> c;
     c[0] = f[0] / nrm;
     for (int k = 1; k < 9; k++) c[k] = c[k - 1] + (f[k] / nrm);

@@ -11,7 +11,8 @@ import os
 import numpy as np
 
 from . import _lib
-from ._lib import DELETE, DISPLACE, INSERT, JUMP, MOVE_DTYPE, NOOP, ROTATE, TRANSLATE, FastMCError, check, dp, ip, lib
+from ._lib import (DELETE, DISPLACE, INSERT, JUMP, MOVE_DTYPE, MULTIJUMP, NOOP, ROTATE, TRANSLATE, FastMCError, check,
+                   dp, ip, lib)
 
 __all__ = ["Chain", "Batch", "Server", "deck_inspect", "FastMCError", "INSERT", "DELETE", "DISPLACE", "TRANSLATE", "ROTATE",
            "MOVE_DTYPE"]

@@ -18,7 +18,7 @@ MOVE_DTYPE = np.dtype([
     ("delrc", np.float64), ("estep", np.float64), ("rande", np.float64), ("energy_after", np.float64),
 ])
 
-INSERT, DELETE, DISPLACE, TRANSLATE, ROTATE, JUMP, NOOP = 1, 2, 3, 4, 5, 6, 7  # NOOP: flex / swap
+INSERT, DELETE, DISPLACE, TRANSLATE, ROTATE, JUMP, NOOP, MULTIJUMP = 1, 2, 3, 4, 5, 6, 7, 8  # NOOP: flex / swap
 
 # Every function the C ABI exports: name -> (restype, argtypes)
 _vp, _ip, _dp, _ci, _cd = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double), \

@@ -2072,7 +2072,6 @@ static void setup(Chain& C, const std::string& dir, int si, int sj, int sk, int 
       C.mcdisf[i] = 1.0 / 3.0;
       C.mcjmpf[i] = C.mcflxf[i] = C.mcswpf[i] = C.mctraf[i] = C.mcrotf[i] = C.mcmjpf[i] = 0.0;
     }
-    if (C.mcmjpf[i] != 0) fail(-3, "multi-jump moves are not part of this restatement");
     C.mcinsf[i] = C.mcinsf[i] / nrm;
     C.mcdelf[i] = C.mcinsf[i] + (C.mcdelf[i] / nrm);
     C.mcdisf[i] = C.mcdelf[i] + (C.mcdisf[i] / nrm);
@@ -2195,7 +2194,8 @@ static void gcmc_step(Chain& C, MoveRec* rec) {
   int iguest = 0;
   if (C.ntpguest > 1) iguest = (int)std::floor(C.rng.next() * C.ntpguest);
   double randmov = C.rng.next();
-  bool insert = false, del = false, displace = false, tran = false, rota = false, jump = false, noop = false;
+  bool insert = false, del = false, displace = false, tran = false, rota = false, jump = false, noop = false,
+       mjump = false;
   if (randmov < C.mcinsf[iguest])
     insert = true;
   else if (randmov < C.mcdelf[iguest])
@@ -2213,7 +2213,7 @@ static void gcmc_step(Chain& C, MoveRec* rec) {
     displace = true;
     rota = true;
   } else if (randmov < C.mcmjpf[iguest])
-    fail(-3, "multi-jump selected");
+    mjump = true;
   else
     displace = true;
   MolType& M = C.mols[C.locguest[iguest]];
@@ -2245,9 +2245,9 @@ static void gcmc_step(Chain& C, MoveRec* rec) {
     else if (C.rota_rotangle > MINANGLE)
       C.rota_rotangle = C.rota_rotangle * 0.95;
   }
-  if (nmols == 0) {
+  if (nmols == 0 || (nmols == 1 && mjump)) {  // gcmc.f:837-847
     insert = true;
-    del = displace = tran = rota = jump = noop = false;
+    del = displace = tran = rota = jump = noop = mjump = false;
   }
   MoveRec R;
   std::memset(&R, 0, sizeof(R));
@@ -2540,6 +2540,116 @@ static void gcmc_step(Chain& C, MoveRec* rec) {
       }
       condense(C);
       C.energy[iguest] += C.delE[iguest];
+    }
+  } else if (mjump) {
+    // multiple long jumps (gcmc.f:1557-1785): two distinct molecules jump one after the other,
+    // the first one committed before the second is evaluated; one acceptance test on the summed
+    // energy change, after which both stay or both return (framework and S(k) restored).
+    R.mtype = 8;
+    C.jump_count++;
+    C.delE[iguest] = 0.0;
+    estep = 0.0;
+    const std::vector<double> ox = M.fx, oy = M.fy, oz = M.fz;
+    const std::vector<double> ockc = C.ckcsum, ocks = C.ckssum;
+    const double origenergy = C.energy[iguest];
+    const int nummove = 2;
+    std::vector<int> prev(nmols, 0);
+    int at = 0;
+    for (int mv = 1; mv <= nummove; mv++) {
+      ewld1eng = ewld2sum = vdwsum = 0.0;
+      int randchoice = 0;
+      for (;;) {  // a molecule that has not jumped in this move
+        randchoice = (int)std::floor(C.rng.next() * nmols) + 1;
+        bool fresh = true;
+        for (int p : prev) fresh = fresh && p != randchoice;
+        if (fresh) {
+          prev[mv - 1] = randchoice;
+          break;
+        }
+      }
+      R.randchoice = randchoice;
+      int atmadd = guest_offset(C, iguest);
+      at = (randchoice - 1) * natms;
+      for (int k = 0; k < natms; k++) {
+        C.ind[k] = atmadd + at + k;
+        C.newx[k] = M.fx[at + k];
+        C.newy[k] = M.fy[at + k];
+        C.newz[k] = M.fz[at + k];
+      }
+      ewald1_guest(C, iguest, natms, C.newx.data(), C.newy.data(), C.newz.data(), MV_DISPLACE, 1);
+      for (int i = 0; i < natms; i++) {
+        chg[i] = C.atmcharge[C.ind[i]];
+        styp[i] = C.ltype[C.ind[i]];
+      }
+      {
+        std::vector<double> se(natms), sv(natms);
+        double a, b;
+        guest_realspace(C, natms, C.newx.data(), C.newy.data(), C.newz.data(), C.ind.data(), chg.data(),
+                        styp.data(), &a, &b, se.data(), sv.data());
+        for (int i = 0; i < natms; i++) {
+          ewld2sum = ewld2sum - se[i];
+          vdwsum = vdwsum - sv[i];
+        }
+      }
+      double ra = C.rng.next(), rb = C.rng.next(), rc_ = C.rng.next();
+      double r1 = C.rng.next(), r2 = C.rng.next(), r3 = C.rng.next(), r4 = C.rng.next();
+      random_jump(C, M, natms, ra, rb, rc_, r1, r2, r3, r4);
+      ewld1eng = ewald1_guest(C, iguest, natms, C.newx.data(), C.newy.data(), C.newz.data(), MV_DISPLACE, 2);
+      {
+        std::vector<double> se(natms), sv(natms);
+        double a, b;
+        guest_realspace(C, natms, C.newx.data(), C.newy.data(), C.newz.data(), C.ind.data(), chg.data(),
+                        styp.data(), &a, &b, se.data(), sv.data());
+        for (int i = 0; i < natms; i++) {
+          ewld2sum = ewld2sum + se[i];
+          vdwsum = vdwsum + sv[i];
+        }
+      }
+      estep = estep + (ewld1eng + ewld2sum + vdwsum) / C.engunit;
+      if (mv < nummove) {  // the state after this jump is the next jump's starting point
+        C.delE[iguest] = estep;
+        for (int j = 0; j < natms; j++) {
+          M.fx[at + j] = C.newx[j];
+          M.fy[at + j] = C.newy[j];
+          M.fz[at + j] = C.newz[j];
+        }
+        for (int i = 0; i < C.newld; i++) {
+          C.ckcsum[i] = C.ckcsnew[i];
+          C.ckssum[i] = C.ckssnew[i];
+        }
+        condense(C);
+        C.energy[iguest] = origenergy + C.delE[iguest];
+      }
+    }
+    if (estep < 0.0) {
+      accepted = true;
+    } else {
+      rande = C.rng.next();
+      accepted = energy_eval(estep, rande, C.statvolm, C.gstpress[iguest], M.nummols, C.temp, C.beta, MV_DISPLACE);
+    }
+    if (accepted) {
+      C.delE[iguest] = estep;
+      C.accept_jump++;
+      for (int j = 0; j < natms; j++) {
+        M.fx[at + j] = C.newx[j];
+        M.fy[at + j] = C.newy[j];
+        M.fz[at + j] = C.newz[j];
+      }
+      for (int i = 0; i < C.newld; i++) {
+        C.ckcsum[i] = C.ckcsnew[i];
+        C.ckssum[i] = C.ckssnew[i];
+      }
+      condense(C);
+      C.energy[iguest] = origenergy + C.delE[iguest];
+    } else {
+      C.delE[iguest] = 0.0;
+      M.fx = ox;
+      M.fy = oy;
+      M.fz = oz;
+      C.ckcsum = ockc;
+      C.ckssum = ocks;
+      condense(C);
+      C.energy[iguest] = origenergy;
     }
   } else if (noop) {
     R.mtype = 7;

@@ -59,6 +59,12 @@ def decks(tmp_path_factory):
                                       tuple(synth.kmax_for(x) for x in L),
                                       moves={"insert": 0.3, "delete": 0.25, "displace": 0.15, "jump": 0.15,
                                              "flex": 0.05, "swap": 0.05, "rotate": 0.05})
+    # hot and dense enough that some multi-jumps are accepted: most random jumps overlap
+    # framework atoms by tens of kcal/mol
+    out["multijump"] = synth.write_inputs(str(root / "multijump"), fws[2], ["CO2"], [50000.0], 30000.0,
+                                          tuple(synth.kmax_for(x) for x in L),
+                                          moves={"insert": 0.3, "delete": 0.2, "multi": 0.3, "jump": 0.1,
+                                                 "displace": 0.1})
     fw = fws[0]
     out["mixture"] = synth.write_inputs(str(root / "mixture"), fw, ["CO2", "N2"], [0.15, 0.85], 298.0,
                                         tuple(synth.kmax_for(fw.cell[j, j]) for j in range(3)))

@@ -68,3 +68,26 @@ def test_batch_jump_flex_swap_replay_oracle(fmc, oracle_mod, decks):
         assert np.any(ref["mtype"] == fmc.JUMP) and np.any(ref["mtype"] == fmc.NOOP)
         accepted_jumps += int(np.sum((ref["mtype"] == fmc.JUMP) & (ref["accepted"] == 1)))
     assert accepted_jumps > 0
+
+
+def test_batch_multi_jump_replays_oracle(fmc, oracle_mod, decks):
+    """Multiple long jumps (gcmc.f:1557-1785): the first jump is committed inside the launch while
+    the second is evaluated, and a rejection restores S(k) and the first molecule; the trace,
+    energies and final coordinates follow the oracle over launches that end mid-run."""
+    seeds = [(4, 8, 15, 16), (23, 42, 4, 8), (1, 2, 3, 4)]
+    b = fmc.Batch([decks["multijump"]] * 3, seeds)
+    tr1, _ = b.run(1300, trace=True)
+    tr2, _ = b.run(1200, trace=True)
+    tr = np.concatenate([tr1, tr2], axis=1)
+    acc_mj = rej_mj = 0
+    for i, s in enumerate(seeds):
+        orc = oracle_mod.Chain(decks["multijump"], seed=s)
+        ref = orc.run(2500)
+        _compare_traces(tr[i], ref)
+        mj = ref["mtype"] == fmc.MULTIJUMP
+        acc_mj += int(np.sum(mj & (ref["accepted"] == 1)))
+        rej_mj += int(np.sum(mj & (ref["accepted"] == 0)))
+        st = b.state(i)
+        assert st["nmol0"] == ref["nmols_after"][-1]
+        assert abs(st["energy0"] - ref["energy_after"][-1]) <= 1e-9 * max(1.0, abs(ref["energy_after"][-1]))
+    assert acc_mj > 0 and rej_mj > 0

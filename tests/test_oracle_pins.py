@@ -72,3 +72,27 @@ def test_rng_draw_order_displacement_skips_rande_when_downhill(oracle_mod, decks
     down = disp & (tr["estep"] < 0)
     assert np.all(tr["rande"][down] == -1.0)
     assert np.all(tr["accepted"][down] == 1)
+
+
+def test_multi_jump_commits_or_restores_both_molecules(oracle_mod, decks):
+    """Multiple long jumps (gcmc.f:1557-1785): two distinct molecules jump, one acceptance test
+    on the summed energy change; on rejection both molecules and S(k) return to where they
+    were.  The running energy must stay equal to a fresh single point of the state."""
+    c = oracle_mod.Chain(decks["multijump"], seed=(12, 34, 56, 78))
+    tr = c.run(2500)
+    mj = tr["mtype"] == 8
+    acc = tr["accepted"] == 1
+    assert mj.sum() > 500 and 0 < (mj & acc).sum() < mj.sum()
+    e = np.concatenate([[0.0], tr["energy_after"]])
+    de = np.diff(e)
+    # a rejected multi-jump leaves the energy where it was; an accepted one adds the summed dE
+    assert np.all(de[mj & ~acc] == 0.0)
+    assert np.allclose(de[mj & acc], tr["estep"][mj & acc], rtol=1e-12, atol=1e-9)
+    # the molecule count never changes on a multi-jump
+    n = np.concatenate([[0], tr["nmols_after"]])
+    assert np.all(np.diff(n)[mj] == 0)
+    coords = c.guest_coords(0)
+    e_run = c.scalars()["energy"]
+    c2 = oracle_mod.Chain(decks["multijump"], seed=(12, 34, 56, 78))
+    c2.load_guests(0, coords.reshape(-1, 3))
+    assert abs(c2.scalars()["spenergy"] - e_run) <= 1e-8 * max(1.0, abs(e_run))
