@@ -382,6 +382,13 @@ int fmc_chain_write_prob(fmc_chain* c, const char* outdir) {
   return 0;
 }
 
+int fmc_chain_open_outputs(fmc_chain* c, const char* outdir) {
+  CHECK_CHAIN(c);
+  std::string err;
+  int rc = c->impl.open_outputs(outdir ? outdir : "", err);
+  return rc ? fail(rc, err) : 0;
+}
+
 int fmc_chain_window_stats(fmc_chain* c, double* out) {
   CHECK_CHAIN(c);
   fmc::window_stats_out(c->impl.win, (int)c->impl.sp.size(), out);

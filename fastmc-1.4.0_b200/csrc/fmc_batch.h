@@ -178,7 +178,13 @@ class Batch {
   // One step: control blocks host->device, `moves` moves of every chain, control blocks (and
   // the optional per-move trace) device->host.  *ms: CUDA-event time of the kernel alone.
   int run(int moves, MoveRecord* trace_host, float* ms, std::string& err, double* shadow_host = nullptr);
+  // numguests.out lines (gcmc.f:1937-1951) of chain c's last run, rebuilt from its move trace
+  // and the per-species counts and energies the run started from
+  int write_numguests(int c, const MoveRecord* trace, int nmoves, const std::string& outdir, bool append,
+                      std::string& err) const;
   int profile = 0;
+  std::vector<int> run_nmol;        // [chain][species] at the start of the last run
+  std::vector<double> run_energy;   // [chain][species]
 };
 
 }  // namespace fmc

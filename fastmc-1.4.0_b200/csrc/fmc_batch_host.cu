@@ -187,7 +187,36 @@ int init_chain(const InputDeck& d, const Chain& ch, int sys, const int* seed, Ch
     if (e == cudaSuccess) allocations.push_back(*p);
     return e;
   };
-  return init_chain_state(d, ch.sys, ch.sk, ch.spenergy, sys, seed, C, alloc, st, err, true);
+  int rc = init_chain_state(d, ch.sys, ch.sk, ch.spenergy, sys, seed, C, alloc, st, err, true);
+  if (rc) return rc;
+  // guests preloaded by the deck (FIELD NUMMOLS > 0 with their sites in CONFIG): the system's
+  // chain already holds them in S(k) and in the single-point energy; copy their sites
+  for (size_t g = 0; g < ch.sp.size(); g++) {
+    const GuestSpecies& G = ch.sys.deck.guests[g];
+    const int n = ch.sp[g].nmol * G.nsite;
+    if (n == 0) continue;
+    if (n > C.seg_cap[g]) {
+      err = "preloaded guests exceed the chain's capacity (max guest atoms)";
+      return -75;
+    }
+    std::vector<double4> a(n);
+    std::vector<int> t(n);
+    for (int i = 0; i < n; i++) {
+      a[i] = make_double4(ch.sp[g].xyz[3 * i], ch.sp[g].xyz[3 * i + 1], ch.sp[g].xyz[3 * i + 2],
+                          G.charge[i % G.nsite]);
+      t[i] = G.type[i % G.nsite];
+      C.numtyp[t[i]]++;
+    }
+    cudaError_t e = cudaMemcpy(C.gsite + C.seg_off[g], a.data(), sizeof(double4) * n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(C.gtype + C.seg_off[g], t.data(), sizeof(int) * n, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      err = std::string("preloaded guest upload failed: ") + cudaGetErrorString(e);
+      return -100 - (int)e;
+    }
+    C.nmol[g] = ch.sp[g].nmol;
+    C.totatm += n;
+  }
+  return 0;
 }
 
 Batch::~Batch() {
@@ -218,11 +247,6 @@ int Batch::open(const std::vector<std::string>& dirs, const std::vector<int>& se
       err = dirs[c] + ": " + err;
       return rc;
     }
-    for (auto& g : decks[c].guests)
-      if (g.nmols) {
-        err = dirs[c] + ": the batched path starts chains from an empty framework (NUMMOLS 0 for guests)";
-        return -8;
-      }
     std::string key = system_key(dirs[c], decks[c]);
     auto it = sys_of_key.find(key);
     if (it == sys_of_key.end()) {
@@ -378,8 +402,68 @@ int Batch::restart(int c, const std::string& path, std::string& err) {
   return 0;
 }
 
+int Batch::write_numguests(int c, const MoveRecord* trace, int nmoves, const std::string& outdir, bool append,
+                           std::string& err) const {
+  const InputDeck& d = sys_chains[chain_sys[c]]->sys.deck;
+  const int ng = (int)d.guests.size();
+  if ((int)run_nmol.size() < kMaxGuestTypes * nchains) {
+    err = "the batch has not run yet";
+    return -1;
+  }
+  int nmol[kMaxGuestTypes];
+  double eng[kMaxGuestTypes];
+  for (int i = 0; i < ng; i++) {
+    nmol[i] = run_nmol[(size_t)c * kMaxGuestTypes + i];
+    eng[i] = run_energy[(size_t)c * kMaxGuestTypes + i];
+  }
+  std::vector<std::FILE*> f(ng, nullptr);
+  for (int i = 0; i < ng; i++) {
+    char a[64];
+    if (ng > 1) std::snprintf(a, sizeof(a), "/numguests%02d.out", i + 1);
+    else std::snprintf(a, sizeof(a), "/numguests.out");
+    f[i] = std::fopen((outdir + a).c_str(), append ? "a" : "w");
+    if (!f[i]) {
+      err = "cannot write numguests.out under " + outdir;
+      for (std::FILE* h : f)
+        if (h) std::fclose(h);
+      return -1;
+    }
+  }
+  for (int m = 0; m < nmoves; m++) {
+    const MoveRecord& r = trace[m];
+    if (r.step == 0) break;  // the chain finished before this record
+    const int g = r.iguest;
+    nmol[g] = r.nmols_after;
+    eng[g] = r.energy_after;
+    if (r.step % d.nnumg != 0) continue;
+    int fl[6] = {0, 0, 0, 0, 0, 0};
+    if (r.mtype == kInsert) fl[0] = 1;
+    else if (r.mtype == kDelete) fl[1] = 1;
+    else if (r.mtype == kDisplace) fl[2] = 1;
+    else if (r.mtype == kTranslate) fl[2] = 2;
+    else if (r.mtype == kRotate) fl[2] = 3;
+    else if (r.mtype == kJump) fl[3] = 1;
+    else if (r.mtype == kMultiJump) fl[3] = 2;
+    const double de = (r.mtype != kNoop && r.accepted) ? r.estep : 0.0;
+    for (int i = 0; i < ng; i++) {
+      const bool me = i == g;
+      std::fprintf(f[i], "%9d%7d%20.6f%20.6f%4d%4d%4d%4d%4d%4d\n", r.step, nmol[i], eng[i], me ? de : 0.0,
+                   me ? fl[0] : 0, me ? fl[1] : 0, me ? fl[2] : 0, me ? fl[3] : 0, me ? fl[4] : 0, me ? fl[5] : 0);
+    }
+  }
+  for (std::FILE* h : f) std::fclose(h);
+  return 0;
+}
+
 int Batch::run(int moves, MoveRecord* trace_host, float* ms, std::string& err, double* shadow_host) {
   cudaSetDevice(device);
+  run_nmol.resize((size_t)kMaxGuestTypes * nchains);
+  run_energy.resize((size_t)kMaxGuestTypes * nchains);
+  for (int c = 0; c < nchains; c++)
+    for (int i = 0; i < kMaxGuestTypes; i++) {
+      run_nmol[(size_t)c * kMaxGuestTypes + i] = h_chains[c].nmol[i];
+      run_energy[(size_t)c * kMaxGuestTypes + i] = h_chains[c].energy[i];
+    }
   BatchLaunch L;
   L.chains = d_chains;
   L.systems = d_sys;
@@ -662,6 +746,19 @@ int batch_chain_stats(fmc_batch* b, int chain, std::vector<double>& cs, std::vec
   return 0;
 }
 }  // namespace
+
+int fmc_batch_write_numguests(fmc_batch* b, int chain, const void* trace, int nmoves, const char* outdir,
+                              int append) {
+  if (!b || chain < 0 || chain >= b->impl.nchains || !trace || nmoves < 0 || !outdir) {
+    fmc::set_last_error("bad batch handle, chain index, trace or directory");
+    return -1;
+  }
+  std::string err;
+  int rc = b->impl.write_numguests(chain, static_cast<const fmc::MoveRecord*>(trace), nmoves, outdir, append != 0,
+                                   err);
+  if (rc) fmc::set_last_error(err);
+  return rc;
+}
 
 int fmc_batch_window_stats(fmc_batch* b, int chain, double* out) {
   if (!b || chain < 0 || chain >= b->impl.nchains || !out) {

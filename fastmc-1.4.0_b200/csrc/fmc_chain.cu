@@ -112,7 +112,44 @@ fail:
   return -1;
 }
 
+void Chain::close_outputs() {
+  for (std::FILE* f : numg_f)
+    if (f) std::fclose(f);
+  for (std::FILE* f : his_f)
+    if (f) std::fclose(f);
+  numg_f.clear();
+  his_f.clear();
+}
+
+int Chain::open_outputs(const std::string& dir, std::string& err) {
+  close_outputs();
+  if (dir.empty()) return 0;
+  const int ng = (int)sp.size();
+  for (int i = 0; i < ng; i++) {
+    char a[64], b[64];
+    if (ng > 1) {
+      std::snprintf(a, sizeof(a), "/numguests%02d.out", i + 1);
+      std::snprintf(b, sizeof(b), "/his%02d.xyz", i + 1);
+    } else {
+      std::snprintf(a, sizeof(a), "/numguests.out");
+      std::snprintf(b, sizeof(b), "/his.xyz");
+    }
+    numg_f.push_back(std::fopen((dir + a).c_str(), "w"));
+    if (sys.deck.nhis != 0) his_f.push_back(std::fopen((dir + b).c_str(), "w"));
+  }
+  for (std::FILE* f : numg_f)
+    if (!f) err = "cannot write numguests.out under " + dir;
+  for (std::FILE* f : his_f)
+    if (!f) err = "cannot write his.xyz under " + dir;
+  if (!err.empty()) {
+    close_outputs();
+    return -1;
+  }
+  return 0;
+}
+
 Chain::~Chain() {
+  close_outputs();
   if (ev0) cudaEventDestroy(ev0);
   if (ev1) cudaEventDestroy(ev1);
   if (st) {
@@ -596,6 +633,16 @@ int Chain::step(MoveRecord* rec) {
   Species& s = sp[g];
   const GuestSpecies& G = d.guests[g];
   const int natms = s.nsite, nmols = s.nmol;
+  // guest geometries before the move (gcmc.f:785-792, hisarchive 2491-2517)
+  if (d.nhis != 0 && gcmccount % std::abs(d.nhis) == 0 && !his_f.empty() && (d.nhis < 0 || prodcount > 0))
+    for (int k = 0; k < ng; k++) {
+      const GuestSpecies& H = d.guests[k];
+      std::fprintf(his_f[k], "%6d\nstep %7d\n", sp[k].nmol * sp[k].nsite, gcmccount);
+      for (int i = 0, a = 0; i < sp[k].nmol; i++)
+        for (int j = 0; j < sp[k].nsite; j++, a++)
+          std::fprintf(his_f[k], "  %c%16.6f%16.6f%16.6f\n", H.site_name[j].empty() ? ' ' : H.site_name[j][0],
+                       sp[k].xyz[3 * a], sp[k].xyz[3 * a + 1], sp[k].xyz[3 * a + 2]);
+    }
   // step-size adaptation (gcmc.f:794-834), applied on every iteration whose counter sits on
   // a multiple of 50/100
   if (nmols >= 1 && disp_count[g] >= 1) {
@@ -854,6 +901,23 @@ int Chain::step(MoveRecord* rec) {
   if (production && (prodcount % d.nwind == 0 || !lgchk))
     window_close(win, ng, d.nwind, d.temp, [this](int i) { return (const double*)chainstats.data() + 14 * i + 1; });
   if (production && !prob.empty()) store_prob();  // gcmc.f:1929-1931, every production move
+  // numguests.out (gcmc.f:1937-1951): only the moved species carries its dE and move flags
+  if (!numg_f.empty() && gcmccount % d.nnumg == 0) {
+    int fl[6] = {0, 0, 0, 0, 0, 0};
+    if (mtype == kInsert) fl[0] = 1;
+    else if (mtype == kDelete) fl[1] = 1;
+    else if (mtype == kDisplace) fl[2] = 1;
+    else if (mtype == kTranslate) fl[2] = 2;
+    else if (mtype == kRotate) fl[2] = 3;
+    else if (mtype == kJump) fl[3] = 1;
+    else if (mtype == kMultiJump) fl[3] = 2;
+    for (int i = 0; i < ng; i++) {
+      const bool me = i == g;
+      std::fprintf(numg_f[i], "%9d%7d%20.6f%20.6f%4d%4d%4d%4d%4d%4d\n", gcmccount, sp[i].nmol, energy[i],
+                   me ? delE[i] : 0.0, me ? fl[0] : 0, me ? fl[1] : 0, me ? fl[2] : 0, me ? fl[3] : 0,
+                   me ? fl[4] : 0, me ? fl[5] : 0);
+    }
+  }
   R.accepted = accepted;
   R.nmols_after = s.nmol;
   R.ewld1 = e[0];

@@ -1,6 +1,7 @@
 // One GCMC chain on one GPU: device-resident system + S(k) + guest sites, and the host move
 // loop of the plain path (gcmc.f:589-1380 restated, energies from fmc_kernels.cu).
 #pragma once
+#include <cstdio>
 #include <cuda_runtime.h>
 
 #include <string>
@@ -82,8 +83,14 @@ class Chain {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double pass_ms = 0.0;
   long long pass_timed = 0;
+  // numguests.out and his.xyz (gcmc.f:418-450), open while a caller asked for them
+  std::vector<std::FILE*> numg_f, his_f;
 
   ~Chain();
+  // Opens the trajectory files in `dir` (numguestsNN.out / hisNN.xyz per species for
+  // mixtures); an empty dir closes them.
+  int open_outputs(const std::string& dir, std::string& err);
+  void close_outputs();
   int open(const std::string& dir, const int seed[4], int device, std::string& err);
   // open from a system already built on the host by prepare_system (the device part only)
   int open_prepared(HostSystem&& prepared, const int seed[4], int device, std::string& err);

@@ -612,7 +612,7 @@ void read_control(const std::string& dir, InputDeck& d) {
   d.disp_ratio.assign(ng, 0.5);
   d.tran_ratio.assign(ng, 0.5);
   std::vector<char> own_moves(ng, 0), own_disp(ng, 0), own_tran(ng, 0);
-  bool ltemp = false, lsteps = false, leq = false, lwind = false;
+  bool ltemp = false, lsteps = false, leq = false, lwind = false, lnumg = false;
   int nblocks = 0;
   // move keyword -> slot, tested in the reference's order (readinputs.f:649-667, 785-834)
   static const char* mv_keys[] = {"ins", "del", "dis", "jum", "fle", "swa", "tra", "rot", "mul"};
@@ -684,7 +684,13 @@ void read_control(const std::string& dir, InputDeck& d) {
       d.mcsteps = r.take_int();
       lsteps = true;
     } else if (r.has("pressure") || r.has("total press")) {
-    } else if (r.has("numg") || r.has("fuga") || r.has("hist")) {
+    } else if (r.has("numg")) {
+      d.nnumg = r.take_int();
+      if (d.nnumg <= 0) d.nnumg = 1000;
+      lnumg = true;
+    } else if (r.has("fuga")) {
+    } else if (r.has("hist")) {
+      d.nhis = r.take_int();
     } else if (r.has("equilibr")) {
       d.eqsteps = r.take_int();
       leq = d.eqsteps != 0;
@@ -733,6 +739,7 @@ void read_control(const std::string& dir, InputDeck& d) {
     }
   }
   if (!leq) d.eqsteps = 0;
+  if (!lnumg) d.nnumg = d.eqsteps > 1000 ? d.eqsteps / 1000 : 1;
   if (!lsteps) {
     d.mcsteps = 1;
     d.lspe = true;

@@ -60,6 +60,10 @@ struct InputDeck {
   // readcontrol
   double temp = 0;
   int mcsteps = 1, eqsteps = 0, nwind = 100000;
+  // numguests.out every nnumg moves (CONTROL `numguests`, else max(1, eqsteps / 1000)) and the
+  // guest geometries to his.xyz every |nhis| moves, during production only when nhis > 0
+  // (readinputs.f:708-717, 860-866)
+  int nnumg = 1, nhis = 0;
   bool laccsample = false, lspe = false;
   std::vector<double> press;  // Pa, per guest
   std::vector<std::array<double, 9>> movefreq;  // ins,del,dis,jmp,flx,swp,tra,rot,mjp (raw)

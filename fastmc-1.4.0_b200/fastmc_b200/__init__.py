@@ -199,6 +199,10 @@ class Chain:
         check(lib().fmc_guest_coords(self.h, int(iguest), dp(buf), ctypes.byref(n), ctypes.byref(ns)))
         return buf[: n.value]
 
+    def open_outputs(self, directory):
+        """Write numguests.out and his.xyz into `directory` as the chain runs; None closes them."""
+        check(lib().fmc_chain_open_outputs(self.h, None if directory is None else str(directory).encode()))
+
     def window_stats(self):
         ng = self.info()["nspecies"]
         out = np.zeros(2 + 24 * ng + ng * ng)
@@ -301,6 +305,12 @@ class Batch:
         out = np.zeros(40)
         check(lib().fmc_batch_chain_state(self.h, int(chain), dp(out)))
         return dict(zip(self._STATE, out.tolist()))
+
+    def write_numguests(self, chain, trace, directory, append=False):
+        """numguests.out of one chain from the trace of the last run(trace=True)."""
+        rec = np.ascontiguousarray(trace[chain] if trace.ndim == 2 else trace)
+        check(lib().fmc_batch_write_numguests(self.h, int(chain), rec.ctypes.data, int(rec.shape[0]),
+                                              str(directory).encode(), int(bool(append))))
 
     def window_stats(self, chain):
         ng = self._ng(chain)

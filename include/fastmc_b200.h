@@ -118,6 +118,16 @@ int fmc_revive_read(const char* path, const char* deck_dir, int* production, int
 int fmc_chain_write_revive(fmc_chain* c, const char* outdir);  /* replaces revive */
 int fmc_chain_restart(fmc_chain* c, const char* revive_path);   /* replaces revread + restart */
 
+/* ---------------------------------------------------------------- trajectory files
+ * numguests.out (gcmc.f:1937-1951): every nnumg moves (CONTROL `numguests`, else
+ * max(1, equilibration / 1000)) one line per species: move, molecules, energy, the move's dE
+ * and its insert/delete/displace/jump/flex/swap flags.  his.xyz (hisarchive, gcmc.f:2491-2517):
+ * every |nhis| moves (CONTROL `history`; positive: production only) the guest sites before the
+ * move.  Mixtures get numguestsNN.out / hisNN.xyz per species.  The plain chain writes both
+ * while they are open (NULL closes them); a batched chain's numguests.out is rebuilt from the
+ * move trace of its last run (`append` adds to the file). */
+int fmc_chain_open_outputs(fmc_chain* c, const char* outdir);
+
 /* ---------------------------------------------------------------- statistics
  * The reference's averaging windows (gcmc.f:1814-1928) run on every production move; the final
  * statistics (gcmc.f:1960-2037) use 5 blocks of the first production samples up to 500,000
@@ -193,6 +203,9 @@ int fmc_batch_prob(fmc_batch* b, int chain, int plot, int* dims, double* out);
 /* Statistics of one chain of a batch (as the fmc_chain_ functions; the stored samples live on
  * the device, 16 MB a species a chain). */
 int fmc_batch_window_stats(fmc_batch* b, int chain, double* out);
+/* numguests.out of one chain of a batch (see the trajectory files above). */
+int fmc_batch_write_numguests(fmc_batch* b, int chain, const void* trace, int nmoves, const char* outdir,
+                              int append);
 /* Bytes of one chain's control block (copied host->device and back around every run). */
 int fmc_batch_control_block_bytes(void);
 /* Bytes of one system's constant block (a serving slot copies it host->device every step). */

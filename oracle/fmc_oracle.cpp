@@ -430,6 +430,9 @@ struct Chain {
   double temp = 0;
   bool ltemp = false, lspe = false, laccsample = false;
   int mcsteps = 1, eqsteps = 0, nwind = 100000;
+  // numguests.out / his.xyz (readinputs.f:708-717, 860-866; gcmc.f:418-450, 785-792, 1937-1951)
+  int nnumg = 1, nhis = 0;
+  std::vector<FILE*> numg_f, his_f;
   std::vector<double> gstpress, mcinsf, mcdelf, mcdisf, mcjmpf, mcflxf, mcswpf, mctraf, mcrotf, mcmjpf;
   std::vector<double> disp_ratio, tran_ratio;
   double rota_ratio = 0.5;
@@ -1012,7 +1015,7 @@ static void readcontrol(Chain& C, const std::string& dir) {
   C.tran_ratio.assign(ng, 0.5);
   C.rota_ratio = 0.5;
   std::vector<char> mvspefid(ng, 0), disp_spefid(ng, 0), tran_spefid(ng, 0);
-  bool lmcsteps = false, leqsteps = false, lwind = false;
+  bool lmcsteps = false, leqsteps = false, lwind = false, lnumg = false;
   int ngst = 0;
   if (!f.getrec(r)) fail(53, "end of CONTROL file encountered");
   bool loop = true;
@@ -1090,8 +1093,12 @@ static void readcontrol(Chain& C, const std::string& dir) {
     } else if (findstring("pressure", d) || findstring("total press", d)) {
       dblstr(d, LENREC);
     } else if (findstring("numg", d)) {
+      lnumg = true;
+      C.nnumg = intstr(d, LENREC, nullptr);
+      if (C.nnumg <= 0) C.nnumg = 1000;
     } else if (findstring("fuga", d)) {
     } else if (findstring("hist", d)) {
+      C.nhis = intstr(d, LENREC, nullptr);
     } else if (findstring("equilibr", d)) {
       C.eqsteps = intstr(d, LENREC, nullptr);
       if (C.eqsteps != 0) leqsteps = true;
@@ -1158,6 +1165,7 @@ static void readcontrol(Chain& C, const std::string& dir) {
     C.lspe = true;
   }
   if (!lwind) C.nwind = 100000;
+  if (!lnumg) C.nnumg = C.eqsteps > 1000 ? C.eqsteps / 1000 : 1;
   if (ngst != ng) fail(2312, "number of &guest blocks differs from the FIELD guests");
   if (!C.ltemp) fail(380, "simulation temperature not specified");
 }
@@ -2218,6 +2226,16 @@ static void gcmc_step(Chain& C, MoveRec* rec) {
     displace = true;
   MolType& M = C.mols[C.locguest[iguest]];
   int natms = M.numatoms, nmols = M.nummols;
+  // guest geometries before the move (gcmc.f:785-792, hisarchive 2491-2517)
+  if (C.nhis != 0 && C.gcmccount % std::abs(C.nhis) == 0 && !C.his_f.empty() && (C.nhis < 0 || C.prodcount > 0))
+    for (int k = 0; k < C.ntpguest; k++) {
+      const MolType& G = C.mols[C.locguest[k]];
+      std::fprintf(C.his_f[k], "%6d\nstep %7d\n", G.nummols * G.numatoms, C.gcmccount);
+      for (int i = 0, iatm = 0; i < G.nummols; i++)
+        for (int j = 0; j < G.numatoms; j++, iatm++)
+          std::fprintf(C.his_f[k], "  %c%16.6f%16.6f%16.6f\n", G.atmname[j].empty() ? ' ' : G.atmname[j][0],
+                       G.fx[iatm], G.fy[iatm], G.fz[iatm]);
+    }
   // step-size adaptation gcmc.f:794-834 (applied on every pass while the counters sit on a
   // multiple of 50/100, as the reference does)
   if (nmols >= 1 && C.disp_count[iguest] >= 1) {
@@ -2733,6 +2751,18 @@ static void gcmc_step(Chain& C, MoveRec* rec) {
     }
     if (!C.plots.empty()) storeprob(C);  // gcmc.f:1929-1931, every production move
   }
+  // numguests.out (gcmc.f:1937-1951): only the moved species carries its dE and move flags,
+  // the others' were cleared when their last move ended
+  if (!C.numg_f.empty() && C.gcmccount % C.nnumg == 0) {
+    const int fl[6] = {insert ? 1 : 0, del ? 1 : 0, displace ? (tran ? 2 : rota ? 3 : 1) : 0,
+                       jump ? 1 : mjump ? 2 : 0, 0, 0};
+    for (int i = 0; i < C.ntpguest; i++) {
+      const bool me = i == iguest;
+      std::fprintf(C.numg_f[i], "%9d%7d%20.6f%20.6f%4d%4d%4d%4d%4d%4d\n", C.gcmccount,
+                   C.mols[C.locguest[i]].nummols, C.energy[i], me ? C.delE[i] : 0.0, me ? fl[0] : 0,
+                   me ? fl[1] : 0, me ? fl[2] : 0, me ? fl[3] : 0, me ? fl[4] : 0, me ? fl[5] : 0);
+    }
+  }
   R.accepted = accepted ? 1 : 0;
   R.nmols_after = M.nummols;
   R.ewld1 = ewld1eng;
@@ -2754,6 +2784,15 @@ using namespace orc;
 struct OrcHandle {
   Chain C;
   std::string err;
+  void close_outputs() {
+    for (FILE* f : C.numg_f)
+      if (f) std::fclose(f);
+    for (FILE* f : C.his_f)
+      if (f) std::fclose(f);
+    C.numg_f.clear();
+    C.his_f.clear();
+  }
+  ~OrcHandle() { close_outputs(); }
 };
 
 static thread_local std::string g_last_error;
@@ -2782,6 +2821,32 @@ void* orc_open(const char* dir, int si, int sj, int sk, int sl, int* code) {
 }
 
 void orc_close(void* p) { delete (OrcHandle*)p; }
+// Opens numguests.out and, when the deck asks for a history, his.xyz in `dir` (numguestsNN.out
+// and hisNN.xyz per species for mixtures, gcmc.f:418-450); a null dir closes them.
+int orc_open_outputs(void* p, const char* dir) {
+  OrcHandle* h = (OrcHandle*)p;
+  Chain& C = h->C;
+  h->close_outputs();
+  if (!dir) return 0;
+  const int ng = C.ntpguest;
+  for (int i = 0; i < ng; i++) {
+    char a[64], b[64];
+    if (ng > 1) {
+      std::snprintf(a, sizeof(a), "/numguests%02d.out", i + 1);
+      std::snprintf(b, sizeof(b), "/his%02d.xyz", i + 1);
+    } else {
+      std::snprintf(a, sizeof(a), "/numguests.out");
+      std::snprintf(b, sizeof(b), "/his.xyz");
+    }
+    C.numg_f.push_back(std::fopen((std::string(dir) + a).c_str(), "w"));
+    if (C.nhis != 0) C.his_f.push_back(std::fopen((std::string(dir) + b).c_str(), "w"));
+  }
+  for (FILE* f : C.numg_f)
+    if (!f) return -1;
+  for (FILE* f : C.his_f)
+    if (!f) return -1;
+  return 0;
+}
 
 // Scalars: [0] alpha [1] rcut [2] delr [3] volm [4] engunit [5] temp [6] beta [7] drewd
 // [8] dlrpot [9] spenergy [10] dlpeng [11] ewald1sum [12] elrc [13] energy(1) [14] statvolm

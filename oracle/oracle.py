@@ -71,6 +71,7 @@ def lib():
         L.orc_prob.argtypes = [vp, ctypes.c_int, ip, dp]
         L.orc_final_stats.argtypes = [vp, dp]
         L.orc_window_stats.argtypes = [vp, dp]
+        L.orc_open_outputs.argtypes = [vp, ctypes.c_char_p]
         assert L.orc_sizeof_moverec() == MOVE_DTYPE.itemsize
         _lib = L
     return _lib
@@ -224,6 +225,13 @@ class Chain:
         out = np.zeros(1 + 14 * ng)
         lib().orc_final_stats(self.h, _dp(out))
         return out
+
+    def open_outputs(self, directory):
+        """numguests.out (every nnumg moves) and his.xyz (CONTROL `history`) into `directory`;
+        None closes them."""
+        r = lib().orc_open_outputs(self.h, None if directory is None else str(directory).encode())
+        if r:
+            raise OracleError(-r, "cannot open the output files")
 
     def window_stats(self):
         """Averaging-window state (gcmc.f:1814-1928): avcount, rollcount, window sums, variances,

@@ -1,4 +1,5 @@
 import os
+import shutil
 import subprocess
 import sys
 
@@ -65,6 +66,16 @@ def decks(tmp_path_factory):
                                           tuple(synth.kmax_for(x) for x in L),
                                           moves={"insert": 0.3, "delete": 0.2, "multi": 0.3, "jump": 0.1,
                                                  "displace": 0.1})
+    # the reference's restart example 2: a binary CO2 + TIP4P-Ew deck on the unary run's REVCON,
+    # with the CO2 count set to the REVCON's 90 molecules as its README instructs
+    binary = root / "binary_preloaded"
+    shutil.copytree(os.path.join(GOLDEN, "binary_preloaded"), binary)
+    fld = (binary / "FIELD").read_text().split("\n")
+    fld[next(i for i, ln in enumerate(fld) if ln.startswith("NUMMOLS"))] = "NUMMOLS 90"
+    (binary / "FIELD").write_text("\n".join(fld))
+    out["binary_preloaded"] = str(binary)
+    out["calf20_co2_n2"] = os.path.join(GOLDEN, "calf20_co2_n2")
+    out["guest_moves"] = os.path.join(GOLDEN, "guest_moves")
     fw = fws[0]
     out["mixture"] = synth.write_inputs(str(root / "mixture"), fw, ["CO2", "N2"], [0.15, 0.85], 298.0,
                                         tuple(synth.kmax_for(fw.cell[j, j]) for j in range(3)))

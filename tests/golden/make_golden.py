@@ -18,6 +18,7 @@ expected.json come from that example's OUTPUT and REVIVE:
               so that a writer restating revive (utility_pack.f:1772-1817) can be checked
               byte for byte without the files themselves
 * OUTPUT      the per-node report block (report_node0.txt), to check the report writer's layout
+* examples/advance/2 and 3, examples/restart/2 inputs as further parity decks
 """
 import hashlib
 import json
@@ -96,6 +97,23 @@ def main(ref):
     with open(os.path.join(HERE, "atmnumber_windows.json"), "w") as f:
         json.dump(wins, f)
     print("wrote", len(wins), "atmnumber windows")
+    # the other shipped examples as parity decks: a CO2/N2 mixture with probability plots, guest-
+    # specific move and acceptance directives, and a binary CO2 + TIP4P-Ew deck whose CONFIG is the
+    # unary run's REVCON (its README's recipe; the test sets the CO2 NUMMOLS)
+    for name, sub in (("calf20_co2_n2", "examples/advance/2_absorbtion_of_co2_n2_in_calf-20"),
+                      ("guest_moves", "examples/advance/3_guest_specific_move")):
+        dst = os.path.join(HERE, name)
+        os.makedirs(dst, exist_ok=True)
+        for f in ("CONTROL", "FIELD", "CONFIG"):
+            shutil.copyfile(os.path.join(ref, sub, f), os.path.join(dst, f))
+        print("wrote", dst)
+    ex2 = os.path.join(ref, "examples/restart/2_start_binary_from_pre-loaded_unary_outputs")
+    dst = os.path.join(HERE, "binary_preloaded")
+    os.makedirs(dst, exist_ok=True)
+    for f in ("CONTROL", "FIELD"):
+        shutil.copyfile(os.path.join(ex2, "binary_from_pre-loaded_configuration", f), os.path.join(dst, f))
+    shutil.copyfile(os.path.join(ex2, "pre-loaded_configuration", "branch01", "REVCON"), os.path.join(dst, "CONFIG"))
+    print("wrote", dst)
     # the per-node report block of the example's OUTPUT (gcmc.f:2052-2108): from the blank line
     # before the banner through the blank line after the species block
     lines = open(os.path.join(src, "OUTPUT")).read().split("\n")

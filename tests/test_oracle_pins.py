@@ -96,3 +96,13 @@ def test_multi_jump_commits_or_restores_both_molecules(oracle_mod, decks):
     c2 = oracle_mod.Chain(decks["multijump"], seed=(12, 34, 56, 78))
     c2.load_guests(0, coords.reshape(-1, 3))
     assert abs(c2.scalars()["spenergy"] - e_run) <= 1e-8 * max(1.0, abs(e_run))
+
+
+def test_binary_deck_on_unary_revcon_single_point_pin(oracle_mod, decks):
+    """The reference's restart example 2 (a binary CO2 + TIP4P-Ew run started from the unary
+    run's REVCON): the single point of the 90 CO2 it holds must equal the energy the unary run
+    stored in its REVIVE for the same state, up to REVCON's 10 significant digits."""
+    c = oracle_mod.Chain(decks["binary_preloaded"], seed=(12, 34, 56, 78))
+    ref = expected()["revive_energy_kcal"]
+    assert c.ints()["ntpguest"] == 2
+    assert abs(c.scalars()["spenergy"] - ref) <= 1e-8 * abs(ref)
