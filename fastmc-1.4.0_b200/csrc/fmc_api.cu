@@ -382,6 +382,15 @@ int fmc_chain_write_prob(fmc_chain* c, const char* outdir) {
   return 0;
 }
 
+int fmc_chain_pressures(fmc_chain* c, double* out) {
+  CHECK_CHAIN(c);
+  if (!out) return fail(-1, "bad arguments");
+  const fmc::Chain& C = c->impl;
+  for (size_t i = 0; i < C.gstpress.size(); i++) out[i] = C.gstpress[i];
+  out[C.gstpress.size()] = C.despre;
+  return 0;
+}
+
 int fmc_chain_open_outputs(fmc_chain* c, const char* outdir) {
   CHECK_CHAIN(c);
   std::string err;

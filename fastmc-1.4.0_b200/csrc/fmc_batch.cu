@@ -83,35 +83,35 @@ struct DuniLocal {
 
 // Thread 0: bookkeeping of gcmc.f:594-736 (production / termination every 400 moves),
 // random choices and the trial sites.
-template <bool kProf>
-__device__ __noinline__ void move_begin(ChainDev& C, const SysConst& Y, const DevSystem& S, MoveSmem& M) {
-  if (kProf) C.prof[7] -= clock64();
-  DuniLocal R(C.rng);  // written back before every return
-  M.mj_action = 0;
-  int g = M.g, mtype = kMultiJump;
-  if (M.mj_stage == 1) {
-    M.mj_stage = 2;  // the second jump of a multi-jump: no count, selection or adaptation
+// Thread 0, every 400 moves (gcmc.f:594-736): the end of production, the switch to production
+// and the pressure equilibration; a rare path, kept out of line.
+__device__ __noinline__ void check400(ChainDev& C, const SysConst& Y) {
+  int totalguests = 0;
+  for (int g = 0; g < Y.nspecies; g++) totalguests += C.nmol[g];
+  if (C.production) {
+    if (C.mcsteps < 0) {
+      for (int t = 4; t > 0; t--) C.tick[t] = C.tick[t - 1];
+      C.tick[0] = !(C.prodcount < (long long)(-C.mcsteps) * (totalguests + 1));
+      bool all = true;
+      for (int t = 0; t < 5; t++) all = all && C.tick[t];
+      if (all) C.lgchk = 0;
+    } else if (C.prodcount >= C.mcsteps) {
+      C.lgchk = 0;
+    }
   } else {
-  M.mj_first = 0;  // a new move: no molecule to avoid
-  C.gcmccount++;
-  if (C.gcmccount % 400 == 0) {
-    int totalguests = 0;
-    for (int g = 0; g < Y.nspecies; g++) totalguests += C.nmol[g];
-    if (C.production) {
-      if (C.mcsteps < 0) {
-        for (int t = 4; t > 0; t--) C.tick[t] = C.tick[t - 1];
-        C.tick[0] = !(C.prodcount < (long long)(-C.mcsteps) * (totalguests + 1));
-        bool all = true;
-        for (int t = 0; t < 5; t++) all = all && C.tick[t];
-        if (all) C.lgchk = 0;
-      } else if (C.prodcount >= C.mcsteps) {
-        C.lgchk = 0;
-      }
-    } else if (C.eqsteps > 0) {
-      if (C.gcmccount >= C.eqsteps) C.production = 1;
+    if (C.despre > 0) {  // pressure equilibration (gcmc.f:637-696)
+      for (int t = 4; t > 0; t--) C.tick[t] = C.tick[t - 1];
+      C.tick[0] = !(C.prodcount < (long long)(-C.eqsteps) * (totalguests + 1) / 4);
+      if (C.tick[0])
+        pressure_adjust(Y.nspecies, C.press, &C.stats[0][0], 6, C.adspres, C.adsguen, C.packf, Y.volm, C.temp,
+                        C.presrate, C.despre, C.gcmccount, C.prodcount, C.eqsteps);
+    }
+    if (C.eqsteps > 0) {
+      if (C.gcmccount >= C.eqsteps && C.despre == 0) C.production = 1;
     } else if (C.eqsteps < 0) {
       for (int t = 4; t > 0; t--) C.tick[t] = C.tick[t - 1];
       C.tick[0] = !((long long)C.gcmccount < (long long)(-C.eqsteps) * (totalguests + 1));
+      if (C.despre > 0) C.tick[0] = 0;
       bool all = true;
       for (int t = 0; t < 5; t++) all = all && C.tick[t];
       if (all) {
@@ -120,6 +120,23 @@ __device__ __noinline__ void move_begin(ChainDev& C, const SysConst& Y, const De
       }
     }
   }
+}
+
+template <bool kProf>
+__device__ __noinline__ void move_begin(ChainDev& C, const SysConst& Y, const DevSystem& S, MoveSmem& M) {
+  if (kProf) C.prof[7] -= clock64();
+  M.mj_action = 0;
+  const bool second = M.mj_stage == 1;  // the second jump of a multi-jump: no count or selection
+  if (!second) {
+    M.mj_first = 0;  // a new move: no molecule to avoid
+    C.gcmccount++;
+    if (C.gcmccount % 400 == 0) check400(C, Y);
+  }
+  DuniLocal R(C.rng);  // written back before every return
+  int g = M.g, mtype = kMultiJump;
+  if (second) {
+    M.mj_stage = 2;
+  } else {
   const int ng = Y.nspecies;
   g = 0;
   if (ng > 1) g = (int)floor(R.next() * ng);
@@ -455,6 +472,12 @@ __device__ __noinline__ void bookkeep(ChainDev& C, const SysConst& Y, MoveSmem& 
   const bool counted = mtype == kNoop ? (C.last_accepted != 0) : accepted;
   if (mtype != kNoop) C.last_accepted = accepted;
   if (C.production) production_sample(C, Y, mtype == kInsert && accepted ? g : -1, counted, estep);
+  else if (C.despre > 0 && ((C.laccsample && counted) || !C.laccsample)) {
+    // running loading while the pressures equilibrate (gcmc.f:1796-1808)
+    C.prodcount++;
+    for (int i = 0; i < Y.nspecies; i++)
+      C.stats[i][0] = C.stats[i][0] + ((double)(float)C.nmol[i] - C.stats[i][0]) / (double)C.prodcount;
+  }
   C.last_dE = accepted ? estep : 0.0;
   C.moves_done++;
   C.since_recompute++;

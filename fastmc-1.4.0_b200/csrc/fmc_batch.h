@@ -66,6 +66,8 @@ struct ChainDev {
   double last_dE;  // energy change of the last move if accepted, else 0 (the reference's delE)
   int production, lgchk, tick[5];
   long long prodcount;
+  // pressure equilibration (gcmc.f:637-696, 1796-1808), on while despre > 0; press[] changes
+  double despre, packf, presrate, adspres[kMaxGuestTypes], adsguen[kMaxGuestTypes];
   double stats[kMaxGuestTypes][6];  // rolling <N>, <E>, <EN>, <N^2>, <E^2>, <exp(-dE/kT)> of insertions
   WindowStats win;                  // the reference's averaging windows
   int nwind;                        // production samples per window (CONTROL `averaging window`)

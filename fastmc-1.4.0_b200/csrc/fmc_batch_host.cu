@@ -135,6 +135,12 @@ int init_chain_state(const InputDeck& d, const HostSystem& H, const double2* sk_
     C.energy[g] = energy0;
   }
   C.rota_ratio = d.rota_ratio;
+  C.despre = d.despre;
+  C.packf = d.packf;
+  for (int g = 0; g < ng; g++) {
+    C.adspres[g] = d.adspres[g];
+    C.adsguen[g] = d.adsguen[g];
+  }
   C.maxguest = d.maxguest;
   C.mcsteps = d.mcsteps;
   C.eqsteps = d.eqsteps;
@@ -431,7 +437,7 @@ int Batch::write_numguests(int c, const MoveRecord* trace, int nmoves, const std
   }
   for (int m = 0; m < nmoves; m++) {
     const MoveRecord& r = trace[m];
-    if (r.step == 0) break;  // the chain finished before this record
+    if (r.mtype == 0) break;  // the chain finished before this record
     const int g = r.iguest;
     nmol[g] = r.nmols_after;
     eng[g] = r.energy_after;
@@ -758,6 +764,18 @@ int fmc_batch_write_numguests(fmc_batch* b, int chain, const void* trace, int nm
                                    err);
   if (rc) fmc::set_last_error(err);
   return rc;
+}
+
+int fmc_batch_pressures(fmc_batch* b, int chain, double* out) {
+  if (!b || chain < 0 || chain >= b->impl.nchains || !out) {
+    fmc::set_last_error("bad batch handle or chain index");
+    return -1;
+  }
+  const fmc::Batch& B = b->impl;
+  const int ng = (int)B.sys_chains[B.chain_sys[chain]]->sys.deck.guests.size();
+  for (int i = 0; i < ng; i++) out[i] = B.h_chains[chain].press[i];
+  out[ng] = B.h_chains[chain].despre;
+  return 0;
 }
 
 int fmc_batch_window_stats(fmc_batch* b, int chain, double* out) {

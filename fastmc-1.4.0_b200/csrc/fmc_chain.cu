@@ -276,6 +276,9 @@ int Chain::open_prepared(HostSystem&& prepared, const int seed[4], int dev, std:
   rotangle = kPi / 3.0;
   rota_rotangle = rotangle;
   chainstats.assign(1 + 14 * ng, 0.0);
+  gstpress = deck.press;
+  despre = deck.despre;
+  presrate = 0.0;
   std::memset(&win, 0, sizeof(win));
   gasmol.assign((size_t)ng * kSampleCap + 1, 0.0);
   gaseng.assign((size_t)ng * kSampleCap + 1, 0.0);
@@ -603,16 +606,26 @@ int Chain::step(MoveRecord* rec) {
       } else if (prodcount >= d.mcsteps) {
         lgchk = false;
       }
-    } else if (d.eqsteps > 0) {
-      if (gcmccount >= d.eqsteps) production = true;
-    } else if (d.eqsteps < 0) {
-      for (int t = 4; t > 0; t--) tick_tock[t] = tick_tock[t - 1];
-      tick_tock[0] = !((long long)gcmccount < (long long)(-d.eqsteps) * (totalguests + 1));
-      bool all = true;
-      for (bool b : tick_tock) all = all && b;
-      if (all) {
-        production = true;
-        for (bool& b : tick_tock) b = false;
+    } else {
+      if (despre > 0) {  // pressure equilibration (gcmc.f:637-696)
+        for (int t = 4; t > 0; t--) tick_tock[t] = tick_tock[t - 1];
+        tick_tock[0] = !(prodcount < (long long)(-d.eqsteps) * (totalguests + 1) / 4);
+        if (tick_tock[0])
+          pressure_adjust(ng, gstpress.data(), chainstats.data() + 1, 14, d.adspres.data(), d.adsguen.data(), d.packf,
+                          sys.cell.volm, d.temp, presrate, despre, gcmccount, prodcount, d.eqsteps);
+      }
+      if (d.eqsteps > 0) {
+        if (gcmccount >= d.eqsteps && despre == 0) production = true;
+      } else if (d.eqsteps < 0) {
+        for (int t = 4; t > 0; t--) tick_tock[t] = tick_tock[t - 1];
+        tick_tock[0] = !((long long)gcmccount < (long long)(-d.eqsteps) * (totalguests + 1));
+        if (despre > 0) tick_tock[0] = false;
+        bool all = true;
+        for (bool b : tick_tock) all = all && b;
+        if (all) {
+          production = true;
+          for (bool& b : tick_tock) b = false;
+        }
       }
     }
   }
@@ -692,7 +705,7 @@ int Chain::step(MoveRecord* rec) {
     ewld3 = sys.ewald3en[g];
     estep = (e[0] + e[1] + ewld3 + e[2] + delrc) / sys.engunit;
     rande = duni_next(rng);
-    accepted = accept_move(estep, rande, sys.statvolm, d.press[g], nmols, d.temp, sys.beta, kInsert);
+    accepted = accept_move(estep, rande, sys.statvolm, gstpress[g], nmols, d.temp, sys.beta, kInsert);
     if (accepted) {
       delE[g] = estep;
       accept_ins++;
@@ -714,7 +727,7 @@ int Chain::step(MoveRecord* rec) {
     ewld3 = sys.ewald3en[g];
     estep = (e[0] - e[1] - ewld3 - e[2] + delrc) / sys.engunit;
     rande = duni_next(rng);
-    accepted = accept_move(estep, rande, sys.statvolm, d.press[g], nmols, d.temp, sys.beta, kDelete);
+    accepted = accept_move(estep, rande, sys.statvolm, gstpress[g], nmols, d.temp, sys.beta, kDelete);
     if (accepted) {
       delE[g] = estep;
       accept_del++;
@@ -751,7 +764,7 @@ int Chain::step(MoveRecord* rec) {
       accepted = true;
     } else {
       rande = duni_next(rng);
-      accepted = accept_move(estep, rande, sys.statvolm, d.press[g], nmols, d.temp, sys.beta, kDisplace);
+      accepted = accept_move(estep, rande, sys.statvolm, gstpress[g], nmols, d.temp, sys.beta, kDisplace);
     }
     if (accepted) {
       delE[g] = estep;
@@ -805,7 +818,7 @@ int Chain::step(MoveRecord* rec) {
       accepted = true;
     } else {
       rande = duni_next(rng);
-      accepted = accept_move(estep, rande, sys.statvolm, d.press[g], nmols, d.temp, sys.beta, kDisplace);
+      accepted = accept_move(estep, rande, sys.statvolm, gstpress[g], nmols, d.temp, sys.beta, kDisplace);
     }
     if (accepted) {
       delE[g] = estep;
@@ -866,7 +879,7 @@ int Chain::step(MoveRecord* rec) {
       accepted = true;
     } else {
       rande = duni_next(rng);
-      accepted = accept_move(estep, rande, sys.statvolm, d.press[g], nmols, d.temp, sys.beta, kDisplace);
+      accepted = accept_move(estep, rande, sys.statvolm, gstpress[g], nmols, d.temp, sys.beta, kDisplace);
     }
     if (accepted) {
       delE[g] = estep;
@@ -878,6 +891,14 @@ int Chain::step(MoveRecord* rec) {
     }
   }
   last_accepted = accepted;
+  // running loading while the pressures equilibrate (gcmc.f:1796-1808)
+  if (!production && despre > 0 && ((d.laccsample && accepted) || !d.laccsample)) {
+    prodcount++;
+    for (int i = 0; i < ng; i++) {
+      double* a = chainstats.data() + 14 * i + 1;
+      *a = *a + ((double)(float)sp[i].nmol - *a) / (double)prodcount;
+    }
+  }
   if (production && ((d.laccsample && accepted) || !d.laccsample)) {
     prodcount++;
     win.rollcount++;

@@ -77,6 +77,10 @@ class Chain {
   long long prodcount = 0;
   bool tick_tock[5] = {false, false, false, false, false};
   std::vector<double> chainstats;  // 1 + 14*ntpguest, <N>,<E>,<EN>,<N^2>,<E^2> rolling
+  // partial pressures (Pa) the acceptance uses; the pressure equilibration changes them while
+  // despre > 0 (gcmc.f:637-696)
+  std::vector<double> gstpress;
+  double despre = 0, presrate = 0;
   // launch accounting and optional CUDA-event timing of the pass kernel
   long long passes = 0, commits = 0;
   bool profile = false;

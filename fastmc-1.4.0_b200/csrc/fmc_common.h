@@ -368,6 +368,45 @@ FMC_HD double calc_cv(double E2, double E, double N, double N2, double EN, doubl
 // The reference's averaging windows (gcmc.f:1814-1928): rolling window means of N, E, EN, N^2,
 // E^2 (and <exp(-dE/kT)> of insertions), closed every `nwind` production samples into weighted
 // running means and variances, with the selectivities between species.
+// Pressure equilibration (gcmc.f:649-693), at a 400-move check: the partial pressures are
+// redistributed from the target loadings (adsguen), the running loading since the last
+// adjustment (read and cleared through nmean, `stride` doubles apart) and the ideal-gas term of
+// the free volume, then rescaled to the same total; the tolerance and the move count are cleared
+// once the last species' rate falls under it or the move count passes -50 * eqsteps.  The
+// reference indexes these arrays by FIELD molecule index, so guests come first in FIELD.
+FMC_HD void pressure_adjust(int ng, double* press, double* nmean, int stride, const double* adspres,
+                            const double* adsguen, double packf, double volm, double temp, double& presrate,
+                            double& despre, int& gcmccount, long long& prodcount, int eqsteps) {
+  double totpres = 0.0;
+  for (int i = 0; i < ng; i++) totpres += press[i];
+  double dqp[kMaxGuestTypes];
+  for (int i = 0; i < ng; i++) {
+    const double temppres = (press[i] * (1 - packf) * volm / packf) / (temp * 13806874.7924278);
+    dqp[i] = adsguen[i] - nmean[i * stride] + (adspres[i] - temppres);
+    nmean[i * stride] = 0;
+  }
+  double presleft = 0.0;
+  for (int i = 0; i < ng - 1; i++) {
+    double sd = 0.0;
+    for (int k = 0; k < ng; k++) sd += dqp[k];
+    presrate = dqp[i] - sd * press[i] / totpres;
+    press[i] = dqp[i] * totpres / sd;
+    if (press[i] < 0) press[i] = 0;
+    presleft = presleft + press[i];
+  }
+  press[ng - 1] = totpres - presleft;
+  if (press[ng - 1] < 0) press[ng - 1] = 0;
+  double sp = 0.0;
+  for (int i = 0; i < ng; i++) sp += press[i];
+  const double changerate = totpres / sp;
+  for (int i = 0; i < ng; i++) press[i] = press[i] * changerate;
+  prodcount = 0;
+  if (fabs(presrate) < despre || (long long)gcmccount > -50LL * eqsteps) {
+    gcmccount = 0;
+    despre = 0;
+  }
+}
+
 struct WindowStats {
   int rollcount, ins_rollcount, avcount;
   double avg[kMaxGuestTypes][8], sum[kMaxGuestTypes][8], var[kMaxGuestTypes][8];

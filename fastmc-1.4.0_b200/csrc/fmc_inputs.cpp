@@ -608,6 +608,8 @@ void read_control(const std::string& dir, InputDeck& d) {
   Deck f(dir + "/CONTROL", 53, "end of CONTROL file encountered");
   const int ng = (int)d.guests.size();
   d.press.assign(ng, 0.0);
+  d.adspres.assign(ng, 0.0);
+  d.adsguen.assign(ng, 0.0);
   d.movefreq.assign(ng, {0, 0, 0, 0, 0, 0, 0, 0, 0});
   d.disp_ratio.assign(ng, 0.5);
   d.tran_ratio.assign(ng, 0.5);
@@ -707,10 +709,17 @@ void read_control(const std::string& dir, InputDeck& d) {
       lwind = true;
     } else if (r.has("max guest atoms")) {
       d.maxguest = r.take_int();
-    } else if (r.has("max framework atoms") || r.has("desorb") || r.has("adsorb press") ||
-               r.has("adsorb guests") || r.has("packing fraction")) {
+    } else if (r.has("max framework atoms")) {
+    } else if (r.has("desorb")) {
+      d.desorb = r.take_int();
+    } else if (r.has("adsorb press")) {
+      for (int i = 0; i < ng; i++) d.adspres[i] = r.take_double();
+    } else if (r.has("adsorb guests")) {
+      for (int i = 0; i < ng; i++) d.adsguen[i] = r.take_double();
+    } else if (r.has("packing fraction")) {
+      d.packf = r.take_double();
     } else if (r.has("finishment")) {
-      raise(-2, "pressure-equilibration mode is outside the GCMC trial-move path");
+      d.despre = r.take_double();
     } else if (r.has("move")) {
       for (int k = 0; k < 9; k++)
         if (r.has(mv_keys[k])) {
@@ -740,6 +749,11 @@ void read_control(const std::string& dir, InputDeck& d) {
   }
   if (!leq) d.eqsteps = 0;
   if (!lnumg) d.nnumg = d.eqsteps > 1000 ? d.eqsteps / 1000 : 1;
+  if (d.despre > 0) {
+    // the reference allocates its work array only for desorb 1 and indexes the per-guest arrays
+    // by FIELD molecule index (gcmc.f:275-281, 655-679)
+    if (d.desorb != 1) raise(-2, "finishment needs desorb 1");
+  }
   if (!lsteps) {
     d.mcsteps = 1;
     d.lspe = true;
@@ -762,6 +776,11 @@ int read_input_deck(const std::string& dir, InputDeck& d, std::string& err) {
     read_control(dir, d);
     for (const MolBlock& b : blocks)
       d.mols.push_back({b.guest ? b.index : -1, b.guest ? 0 : b.index, b.nummols, b.numatoms});
+    // pressure equilibration indexes the per-guest arrays by FIELD molecule index (gcmc.f:655-679)
+    if (d.despre > 0)
+      for (size_t i = 0; i < d.guests.size(); i++)
+        if (i >= d.mols.size() || d.mols[i].guest != (int)i)
+          raise(-2, "pressure equilibration needs the guests first in FIELD");
     if (!d.plots.empty()) {  // gcmc.f:246-256
       double cp[10];
       cell_props(d.cell, cp);

@@ -64,6 +64,11 @@ struct InputDeck {
   // guest geometries to his.xyz every |nhis| moves, during production only when nhis > 0
   // (readinputs.f:708-717, 860-866)
   int nnumg = 1, nhis = 0;
+  // pressure equilibration during equilibration (CONTROL desorb, adsorb press, adsorb guests,
+  // packing fraction, finishment; readinputs.f:749-762): on while despre > 0
+  int desorb = 0;
+  double despre = 0, packf = 0;
+  std::vector<double> adspres, adsguen;
   bool laccsample = false, lspe = false;
   std::vector<double> press;  // Pa, per guest
   std::vector<std::array<double, 9>> movefreq;  // ins,del,dis,jmp,flx,swp,tra,rot,mjp (raw)
@@ -72,8 +77,8 @@ struct InputDeck {
 };
 
 // Reads dir/{CONTROL,FIELD,CONFIG}.  Returns 0, or the reference's error code (>0); `err`
-// receives a message.  Directives outside this path (restart, pressure equilibration) are
-// rejected with a negative code.
+// receives a message.  Directives outside this path (the restart scan) are rejected with a
+// negative code.
 int read_input_deck(const std::string& dir, InputDeck& deck, std::string& err);
 
 }  // namespace fmc

@@ -199,6 +199,13 @@ class Chain:
         check(lib().fmc_guest_coords(self.h, int(iguest), dp(buf), ctypes.byref(n), ctypes.byref(ns)))
         return buf[: n.value]
 
+    def pressures(self):
+        """(partial pressures in Pa, pressure-equilibration tolerance still in force)."""
+        ng = self.info()["nspecies"]
+        out = np.zeros(ng + 1)
+        check(lib().fmc_chain_pressures(self.h, dp(out)))
+        return out[:ng], float(out[ng])
+
     def open_outputs(self, directory):
         """Write numguests.out and his.xyz into `directory` as the chain runs; None closes them."""
         check(lib().fmc_chain_open_outputs(self.h, None if directory is None else str(directory).encode()))
@@ -305,6 +312,12 @@ class Batch:
         out = np.zeros(40)
         check(lib().fmc_batch_chain_state(self.h, int(chain), dp(out)))
         return dict(zip(self._STATE, out.tolist()))
+
+    def pressures(self, chain):
+        ng = self._ng(chain)
+        out = np.zeros(ng + 1)
+        check(lib().fmc_batch_pressures(self.h, int(chain), dp(out)))
+        return out[:ng], float(out[ng])
 
     def write_numguests(self, chain, trace, directory, append=False):
         """numguests.out of one chain from the trace of the last run(trace=True)."""

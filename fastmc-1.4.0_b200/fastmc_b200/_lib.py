@@ -59,6 +59,8 @@ SIGNATURES = {
     "fmc_batch_restart": (_ci, [_vp, _ci, ctypes.c_char_p]),
     "fmc_chain_prob": (_ci, [_vp, _ci, _ip, _dp]),
     "fmc_chain_open_outputs": (_ci, [_vp, ctypes.c_char_p]),
+    "fmc_chain_pressures": (_ci, [_vp, _dp]),
+    "fmc_batch_pressures": (_ci, [_vp, _ci, _dp]),
     "fmc_batch_write_numguests": (_ci, [_vp, _ci, _vp, _ci, ctypes.c_char_p, _ci]),
     "fmc_chain_window_stats": (_ci, [_vp, _dp]),
     "fmc_chain_final_stats": (_ci, [_vp, _dp]),

@@ -118,6 +118,13 @@ int fmc_revive_read(const char* path, const char* deck_dir, int* production, int
 int fmc_chain_write_revive(fmc_chain* c, const char* outdir);  /* replaces revive */
 int fmc_chain_restart(fmc_chain* c, const char* revive_path);   /* replaces revread + restart */
 
+/* ---------------------------------------------------------------- pressure equilibration
+ * CONTROL `desorb 1`, `adsorb press`, `adsorb guests`, `packing fraction` and `finishment d`
+ * make the equilibration adjust the partial pressures every 400 moves (gcmc.f:637-696) until the
+ * rate falls under d.  out[ng + 1]: the partial pressures (Pa) the acceptance uses now, then the
+ * tolerance still in force (0 once equilibrated). */
+int fmc_chain_pressures(fmc_chain* c, double* out);
+
 /* ---------------------------------------------------------------- trajectory files
  * numguests.out (gcmc.f:1937-1951): every nnumg moves (CONTROL `numguests`, else
  * max(1, equilibration / 1000)) one line per species: move, molecules, energy, the move's dE
@@ -203,6 +210,8 @@ int fmc_batch_prob(fmc_batch* b, int chain, int plot, int* dims, double* out);
 /* Statistics of one chain of a batch (as the fmc_chain_ functions; the stored samples live on
  * the device, 16 MB a species a chain). */
 int fmc_batch_window_stats(fmc_batch* b, int chain, double* out);
+/* Partial pressures of one chain of a batch (as fmc_chain_pressures). */
+int fmc_batch_pressures(fmc_batch* b, int chain, double* out);
 /* numguests.out of one chain of a batch (see the trajectory files above). */
 int fmc_batch_write_numguests(fmc_batch* b, int chain, const void* trace, int nmoves, const char* outdir,
                               int append);

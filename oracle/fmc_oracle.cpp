@@ -433,6 +433,11 @@ struct Chain {
   // numguests.out / his.xyz (readinputs.f:708-717, 860-866; gcmc.f:418-450, 785-792, 1937-1951)
   int nnumg = 1, nhis = 0;
   std::vector<FILE*> numg_f, his_f;
+  // pressure equilibration (CONTROL desorb / adsorb press / adsorb guests / packing fraction /
+  // finishment; readinputs.f:749-762, gcmc.f:275-281, 637-696, 1796-1808)
+  int desorb = 0;
+  double despre = 0, packf = 0, presleft = 0, presrate = 0;
+  std::vector<double> adspres, adsguen, dqp;
   std::vector<double> gstpress, mcinsf, mcdelf, mcdisf, mcjmpf, mcflxf, mcswpf, mctraf, mcrotf, mcmjpf;
   std::vector<double> disp_ratio, tran_ratio;
   double rota_ratio = 0.5;
@@ -1009,6 +1014,8 @@ static void readcontrol(Chain& C, const std::string& dir) {
   Rec r;
   int ng = C.ntpguest;
   C.gstpress.assign(ng, 0.0);
+  C.adspres.assign(ng, 0.0);
+  C.adsguen.assign(ng, 0.0);
   for (auto* v : {&C.mcinsf, &C.mcdelf, &C.mcdisf, &C.mcjmpf, &C.mcflxf, &C.mcswpf, &C.mctraf, &C.mcrotf, &C.mcmjpf})
     v->assign(ng, 0.0);
   C.disp_ratio.assign(ng, 0.5);
@@ -1119,11 +1126,15 @@ static void readcontrol(Chain& C, const std::string& dir) {
     } else if (findstring("max framework atoms", d)) {
       C.maxatm = intstr(d, LENREC, nullptr);
     } else if (findstring("desorb", d)) {
+      C.desorb = intstr(d, LENREC, nullptr);
     } else if (findstring("adsorb press", d)) {
+      for (int i = 0; i < ng; i++) C.adspres[i] = dblstr(d, LENREC);
     } else if (findstring("adsorb guests", d)) {
+      for (int i = 0; i < ng; i++) C.adsguen[i] = dblstr(d, LENREC);
     } else if (findstring("packing fraction", d)) {
+      C.packf = dblstr(d, LENREC);
     } else if (findstring("finishment", d)) {
-      fail(-2, "pressure-equilibration mode is not part of this restatement");
+      C.despre = dblstr(d, LENREC);
     } else if (findstring("move", d)) {
       std::vector<double>* tgt = nullptr;
       if (findstring("ins", d)) tgt = &C.mcinsf;
@@ -1166,6 +1177,15 @@ static void readcontrol(Chain& C, const std::string& dir) {
   }
   if (!lwind) C.nwind = 100000;
   if (!lnumg) C.nnumg = C.eqsteps > 1000 ? C.eqsteps / 1000 : 1;
+  if (C.despre > 0) {
+    // the reference allocates its work array only for desorb 1, and indexes the per-guest
+    // arrays by FIELD molecule index (gcmc.f:655-679), which is the guest index only when the
+    // guests come first in FIELD
+    if (C.desorb != 1) fail(-2, "finishment needs desorb 1");
+    for (int i = 0; i < ng; i++)
+      if (C.locguest[i] != i) fail(-2, "pressure equilibration needs the guests first in FIELD");
+  }
+  if (C.desorb == 1) C.dqp.assign(ng, 0.0);
   if (ngst != ng) fail(2312, "number of &guest blocks differs from the FIELD guests");
   if (!C.ltemp) fail(380, "simulation temperature not specified");
 }
@@ -2184,12 +2204,53 @@ static void gcmc_step(Chain& C, MoveRec* rec) {
         C.lgchk = false;
       }
     } else {
+      if (C.despre > 0) {  // pressure equilibration (gcmc.f:637-696)
+        for (int t = 4; t > 0; t--) C.tick_tock[t] = C.tick_tock[t - 1];
+        C.tick_tock[0] = true;
+        if (C.prodcount < (long long)(-C.eqsteps) * (totalguests + 1) / 4) C.tick_tock[0] = false;
+        if (C.tick_tock[0]) {
+          const int ng = C.ntpguest;
+          double totpres = 0.0;
+          for (int i = 0; i < ng; i++) totpres += C.gstpress[i];
+          for (int i = 0; i < ng; i++) {
+            const int is = 14 * i, mol = C.locguest[i];
+            double temppres = (C.gstpress[mol] * (1 - C.packf) * C.volm / C.packf) / (C.temp * 13806874.7924278);
+            C.dqp[mol] = C.adsguen[mol] - C.chainstats[is + 1] + (C.adspres[mol] - temppres);
+            C.chainstats[is + 1] = 0;
+          }
+          auto sum_dqp = [&C]() {
+            double t = 0.0;
+            for (double v : C.dqp) t += v;
+            return t;
+          };
+          for (int i = 0; i < ng - 1; i++) {
+            const int mol = C.locguest[i];
+            C.presrate = C.dqp[mol] - sum_dqp() * C.gstpress[mol] / totpres;
+            C.gstpress[mol] = C.dqp[mol] * totpres / sum_dqp();
+            if (C.gstpress[mol] < 0) C.gstpress[mol] = 0;
+            C.presleft = C.presleft + C.gstpress[mol];
+          }
+          C.gstpress[C.locguest[ng - 1]] = totpres - C.presleft;
+          if (C.gstpress[C.locguest[ng - 1]] < 0) C.gstpress[C.locguest[ng - 1]] = 0;
+          double sp = 0.0;
+          for (int i = 0; i < ng; i++) sp += C.gstpress[i];
+          const double changerate = totpres / sp;
+          for (int i = 0; i < ng; i++) C.gstpress[C.locguest[i]] = C.gstpress[C.locguest[i]] * changerate;
+          C.presleft = 0.0;
+          C.prodcount = 0;
+          if (std::fabs(C.presrate) < C.despre || (long long)C.gcmccount > -50LL * C.eqsteps) {
+            C.gcmccount = 0;
+            C.despre = 0;
+          }
+        }
+      }
       if (C.eqsteps > 0) {
-        if (C.gcmccount >= C.eqsteps) C.production = true;
+        if (C.gcmccount >= C.eqsteps && C.despre == 0) C.production = true;
       } else if (C.eqsteps < 0) {
         for (int t = 4; t > 0; t--) C.tick_tock[t] = C.tick_tock[t - 1];
         C.tick_tock[0] = true;
         if ((long long)C.gcmccount < (long long)(-C.eqsteps) * (totalguests + 1)) C.tick_tock[0] = false;
+        if (C.despre > 0) C.tick_tock[0] = false;
         bool all = true;
         for (bool b : C.tick_tock) all = all && b;
         if (all) {
@@ -2674,6 +2735,15 @@ static void gcmc_step(Chain& C, MoveRec* rec) {
     accepted = C.last_accepted;  // the reference leaves `accepted` as the last move set it
   }
   C.last_accepted = accepted;
+  // running loading while the pressures equilibrate (gcmc.f:1796-1808)
+  if (!C.production && C.despre > 0 && ((C.laccsample && accepted) || !C.laccsample)) {
+    C.prodcount++;
+    for (int i = 0; i < C.ntpguest; i++) {
+      const double dm = (double)(float)C.mols[C.locguest[i]].nummols;
+      double* a = &C.chainstats[14 * i + 1];
+      *a = *a + (dm - *a) / (double)C.prodcount;
+    }
+  }
   // production statistics gcmc.f:1814-1860 (rolling <N>,<E>,<EN>,<N^2>,<E^2>)
   if (C.production) {
     if ((C.laccsample && accepted) || !C.laccsample) {
@@ -2856,6 +2926,12 @@ void orc_scalars(void* p, double* out) {
                   C.dlrpot, C.spenergy, C.dlpeng, C.ewald1sum, C.elrc, C.energy.empty() ? 0 : C.energy[0],
                   C.statvolm};
   std::memcpy(out, v, sizeof(v));
+}
+// Partial pressures (Pa) per guest, then the remaining pressure-equilibration tolerance.
+void orc_pressures(void* p, double* out) {
+  Chain& C = ((OrcHandle*)p)->C;
+  for (int i = 0; i < C.ntpguest; i++) out[i] = C.gstpress[i];
+  out[C.ntpguest] = C.despre;
 }
 // Integers: [0] imcon [1] kmax1 [2] kmax2 [3] kmax3 [4] newld [5] totatm [6] ntpguest
 // [7] ntpatm [8] mxgrid [9] framatm-equivalent (framework atoms) [10] gcmccount [11] maxvdw

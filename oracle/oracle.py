@@ -72,6 +72,7 @@ def lib():
         L.orc_final_stats.argtypes = [vp, dp]
         L.orc_window_stats.argtypes = [vp, dp]
         L.orc_open_outputs.argtypes = [vp, ctypes.c_char_p]
+        L.orc_pressures.argtypes = [vp, dp]
         assert L.orc_sizeof_moverec() == MOVE_DTYPE.itemsize
         _lib = L
     return _lib
@@ -225,6 +226,14 @@ class Chain:
         out = np.zeros(1 + 14 * ng)
         lib().orc_final_stats(self.h, _dp(out))
         return out
+
+    def pressures(self):
+        """Partial pressures (Pa) per guest and the pressure-equilibration tolerance still in
+        force (0 once the pressures have equilibrated)."""
+        ng = self.ints()["ntpguest"]
+        out = np.zeros(ng + 1)
+        lib().orc_pressures(self.h, _dp(out))
+        return out[:ng], float(out[ng])
 
     def open_outputs(self, directory):
         """numguests.out (every nnumg moves) and his.xyz (CONTROL `history`) into `directory`;

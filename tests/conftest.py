@@ -76,6 +76,16 @@ def decks(tmp_path_factory):
     out["binary_preloaded"] = str(binary)
     out["calf20_co2_n2"] = os.path.join(GOLDEN, "calf20_co2_n2")
     out["guest_moves"] = os.path.join(GOLDEN, "guest_moves")
+    # CO2 + N2 with the reference's pressure equilibration: the partial pressures move every 400
+    # moves until the forced stop at 50 x 100 cycles, then equilibration and production follow
+    peq = synth.write_inputs(str(root / "pressure_eq"), fws[0], ["CO2", "N2"], [0.5, 0.5], 298.0,
+                             tuple(synth.kmax_for(fws[0].cell[j, j]) for j in range(3)), eq_cycles=-100,
+                             prod_cycles=-5)
+    ctl = open(os.path.join(peq, "CONTROL")).read().replace(
+        "finish", "desorb 1\nadsorb press 0.3 0.7\nadsorb guests 6.0 2.0\npacking fraction 0.5\n"
+                  "finishment 1e-9\nfinish")
+    open(os.path.join(peq, "CONTROL"), "w").write(ctl)
+    out["pressure_eq"] = peq
     fw = fws[0]
     out["mixture"] = synth.write_inputs(str(root / "mixture"), fw, ["CO2", "N2"], [0.15, 0.85], 298.0,
                                         tuple(synth.kmax_for(fw.cell[j, j]) for j in range(3)))
