@@ -735,6 +735,9 @@ __device__ __noinline__ void sums(const DevSystem& S, const ChainDev& C, const M
   if (S.cell.imcon == 1) real_space<kMixed, 1>(S, C, M, nseg, prow_s, nt1, fp32_mask, v);
   else if (S.cell.imcon == 2) real_space<kMixed, 2>(S, C, M, nseg, prow_s, nt1, fp32_mask, v);
   else if (S.cell.imcon == 3) real_space<kMixed, 3>(S, C, M, nseg, prow_s, nt1, fp32_mask, v);
+  else if (S.cell.imcon == 4) real_space<kMixed, 4>(S, C, M, nseg, prow_s, nt1, fp32_mask, v);
+  else if (S.cell.imcon == 5) real_space<kMixed, 5>(S, C, M, nseg, prow_s, nt1, fp32_mask, v);
+  else if (S.cell.imcon == 7) real_space<kMixed, 7>(S, C, M, nseg, prow_s, nt1, fp32_mask, v);
   else real_space<kMixed, 0>(S, C, M, nseg, prow_s, nt1, fp32_mask, v);
 }
 

@@ -88,21 +88,29 @@ struct CellGeom {
   double h[9];    // cell vectors a,b,c (cell(1..9) of the reference, a = h[0..2])
   double rh[9];   // inverse (invert, utility_pack.f:1417)
   double inv[3];  // 1/h[0], 1/h[4], 1/h[8]: the reciprocals images() forms once per call
+  double hex[3];  // hexagonal prism (imcon 7): a/(2 rt3), a/rt3, rt3/a as images() forms them
   double volm;    // volume used by Ewald and acceptance
   int imcon;
 };
+
+// The reference's own truncated constants of images (utility_pack.f:1149-1150).
+constexpr double kImgRt2 = 1.41421356623, kImgRt3 = 1.7320508075;
 
 inline void cell_reciprocals(CellGeom& c) {
   c.inv[0] = 1.0 / c.h[0];
   c.inv[1] = 1.0 / c.h[4];
   c.inv[2] = 1.0 / c.h[8];
+  c.hex[0] = c.h[0] / (kImgRt3 * 2.0);
+  c.hex[1] = c.h[0] / kImgRt3;
+  c.hex[2] = kImgRt3 / c.h[0];
 }
 
 // Fortran nint: nearest integer, halves away from zero.
 FMC_HD double fnint(double x) { return round(x); }
 
-// Minimum image of one separation vector for imcon 1, 2, 3 (images, utility_pack.f:1138-1202),
-// for a boundary condition known at compile time (other values: no image).
+// Minimum image of one separation vector (images, utility_pack.f:1138-1349) for imcon 1, 2, 3
+// and the half-shift cells 4 (truncated octahedron), 5 (rhombic dodecahedron) and 7 (hexagonal
+// prism), for a boundary condition known at compile time (other values: no image).
 template <int kImcon>
 FMC_HD void min_image_t(const CellGeom& c, double& x, double& y, double& z) {
   if (kImcon == 1) {
@@ -125,6 +133,34 @@ FMC_HD void min_image_t(const CellGeom& c, double& x, double& y, double& z) {
     x = c.h[0] * sx + c.h[3] * sy + c.h[6] * sz;
     y = c.h[1] * sx + c.h[4] * sy + c.h[7] * sz;
     z = c.h[2] * sx + c.h[5] * sy + c.h[8] * sz;
+  } else if (kImcon == 4) {
+    const double a = c.h[0], ra = c.inv[0];
+    x = x - a * fnint(ra * x);
+    y = y - a * fnint(ra * y);
+    z = z - a * fnint(ra * z);
+    if ((fabs(x) + fabs(y) + fabs(z)) >= (0.75 * a)) {
+      x = x - 0.5 * copysign(fabs(a), x);
+      y = y - 0.5 * copysign(fabs(a), y);
+      z = z - 0.5 * copysign(fabs(a), z);
+    }
+  } else if (kImcon == 5) {
+    const double a = c.h[0], cz = c.h[8];
+    x = x - a * fnint(c.inv[0] * x);
+    y = y - a * fnint(c.inv[0] * y);
+    z = z - cz * fnint(c.inv[2] * z);
+    if ((fabs(x) + fabs(y) + fabs(kImgRt2 * z)) >= a) {
+      x = x - 0.5 * copysign(fabs(a), x);
+      y = y - 0.5 * copysign(fabs(a), y);
+      z = z - 0.5 * copysign(fabs(cz), z);
+    }
+  } else if (kImcon == 7) {
+    const double aaa = c.hex[0], bbb = c.hex[1];
+    y = y - bbb * fnint(c.hex[2] * y);
+    z = z - c.h[8] * fnint(c.inv[2] * z);
+    if ((fabs(y) + fabs(kImgRt3 * x)) >= bbb) {
+      x = x - kImgRt3 * copysign(fabs(aaa), x);
+      y = y - copysign(fabs(aaa), y);
+    }
   }
 }
 
@@ -133,6 +169,26 @@ FMC_HD void min_image(const CellGeom& c, double& x, double& y, double& z) {
   if (c.imcon == 1) min_image_t<1>(c, x, y, z);
   else if (c.imcon == 2) min_image_t<2>(c, x, y, z);
   else if (c.imcon == 3) min_image_t<3>(c, x, y, z);
+  else if (c.imcon == 4) min_image_t<4>(c, x, y, z);
+  else if (c.imcon == 5) min_image_t<5>(c, x, y, z);
+  else if (c.imcon == 7) min_image_t<7>(c, x, y, z);
+}
+
+// Squared distance to the nearest lattice image of a separation: for imcon 4, 5 and 7 the
+// lattice is the box's plus the box's shifted by half its a and b (and c for 4 and 5), so the
+// nearest image is the nearer of the box-nearest images of the separation and of its shift.
+// Builders of neighbour lists use it as a lower bound of the distance images() returns.
+FMC_HD double shifted_lattice_dist2(const CellGeom& c, double x, double y, double z) {
+  double best = 1e300;
+  for (int k = 0; k < 2; k++) {
+    double u = x + (k ? 0.5 * c.h[0] : 0.0), v = y + (k ? 0.5 * c.h[4] : 0.0);
+    double w = z + (k && c.imcon != 7 ? 0.5 * c.h[8] : 0.0);
+    u = u - c.h[0] * fnint(c.inv[0] * u);
+    v = v - c.h[4] * fnint(c.inv[1] * v);
+    w = w - c.h[8] * fnint(c.inv[2] * w);
+    best = fmin(best, u * u + v * v + w * w);
+  }
+  return best;
 }
 
 // ------------------------------------------------------------------ trial generators

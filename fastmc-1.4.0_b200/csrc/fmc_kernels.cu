@@ -310,6 +310,7 @@ cudaError_t launch_single_point_rs(const DevSystem& S, const GuestView& G, int n
 // Every framework atom whose true minimum-image distance to a voxel's centre is below
 // sqrt(lim2) (rcut + the voxel's circumradius), in ascending atom order.
 __device__ __forceinline__ double true_dist2_dev(const CellGeom& c, double dx, double dy, double dz) {
+  if (c.imcon == 4 || c.imcon == 5 || c.imcon == 7) return shifted_lattice_dist2(c, dx, dy, dz);
   min_image(c, dx, dy, dz);
   double best = dx * dx + dy * dy + dz * dz;
   if (c.imcon == 3) {

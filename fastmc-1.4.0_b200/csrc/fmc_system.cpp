@@ -129,6 +129,7 @@ double nint_image_dist2(const CellGeom& c, double dx, double dy, double dz) {
 
 // True minimum-image distance^2 (the nint image and its 26 neighbours).
 double true_dist2(const CellGeom& c, double dx, double dy, double dz) {
+  if (c.imcon == 4 || c.imcon == 5 || c.imcon == 7) return shifted_lattice_dist2(c, dx, dy, dz);
   min_image(c, dx, dy, dz);
   if (c.imcon == 1 || c.imcon == 2) return dx * dx + dy * dy + dz * dz;
   double best = dx * dx + dy * dy + dz * dz;
@@ -175,8 +176,8 @@ double lrc_energy(const HostSystem& s, const std::vector<int>& numtyp, const std
 int build_host_system(const InputDeck& d, HostSystem& s, std::string& err, double voxel_edge) {
   s = HostSystem();
   s.deck = d;
-  if (d.imcon < 1 || d.imcon > 3) {
-    err = "only cubic, orthorhombic and parallelepiped cells (imcon 1-3) are supported on the device";
+  if (d.imcon < 1 || d.imcon > 7 || d.imcon == 6) {
+    err = "the slab (imcon 6) and non-periodic (imcon 0) cells are not supported on the device";
     return -4;
   }
   if (d.lspe) {

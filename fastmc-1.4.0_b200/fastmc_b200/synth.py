@@ -65,9 +65,11 @@ class Framework:
         return Framework(cell, names, xyz, q, self.lj)
 
 
-def _place_atoms(rng, lengths, n, dmin=1.8):
-    """Uniform random positions in an orthorhombic box with a periodic minimum separation."""
+def _place_atoms(rng, lengths, n, dmin=1.8, shift=None):
+    """Uniform random positions in an orthorhombic box with a periodic minimum separation; with
+    `shift`, the lattice also holds the box shifted by that vector (the half-shift cells)."""
     L = np.asarray(lengths, dtype=np.float64)
+    shifts = [np.zeros(3)] + ([np.asarray(shift, dtype=np.float64)] if shift is not None else [])
     pts = np.zeros((n, 3))
     count = 0
     tries = 0
@@ -77,16 +79,19 @@ def _place_atoms(rng, lengths, n, dmin=1.8):
             raise RuntimeError("could not place atoms at the requested density")
         p = rng.uniform(0.0, 1.0, 3) * L
         if count:
-            d = pts[:count] - p
-            d -= L * np.round(d / L)
-            if np.min(np.einsum("ij,ij->i", d, d)) < dmin * dmin:
+            close = False
+            for sv in shifts:
+                d = pts[:count] - p + sv
+                d -= L * np.round(d / L)
+                close = close or np.min(np.einsum("ij,ij->i", d, d)) < dmin * dmin
+            if close:
                 continue
         pts[count] = p
         count += 1
     return pts
 
 
-def make_framework(lengths, natoms, seed):
+def make_framework(lengths, natoms, seed, shift=None):
     """Synthetic framework: type mix Zn 8% / O 24% / C 45% / H 23%, q ~ N(0, 0.4) shifted to
     sum to zero, LJ eps ~ U(0.02, 0.3) kcal/mol and sigma ~ U(2.5, 3.8) A per type."""
     rng = np.random.default_rng(seed)
@@ -95,7 +100,7 @@ def make_framework(lengths, natoms, seed):
     names = []
     for (name, _, _), c in zip(FRAMEWORK_TYPES, counts):
         names += [name] * c
-    xyz = _place_atoms(rng, lengths, natoms)
+    xyz = _place_atoms(rng, lengths, natoms, shift=shift)
     q = rng.normal(0.0, 0.4, natoms)
     q -= q.mean()
     q = np.round(q, 10)
@@ -106,6 +111,26 @@ def make_framework(lengths, natoms, seed):
         lj[name] = (float(rng.uniform(0.02, 0.3)), float(rng.uniform(2.5, 3.8)))
     cell = np.diag(np.asarray(lengths, dtype=np.float64))
     return Framework(cell, names, xyz, q, lj)
+
+
+def half_shift_framework(imcon, edge, seed, rho=0.025):
+    """A framework in the box of a half-shift cell: imcon 4 (truncated octahedron in an a x a x a
+    box), 5 (rhombic dodecahedron, a x a x sqrt(2) a) or 7 (hexagonal prism, sqrt(3) b x b x c with
+    c = b = edge).  The cell's lattice holds the box shifted by half its a, b (and c for 4, 5), so
+    the periodic cell is half the box and holds rho x box volume / 2 atoms."""
+    if imcon == 4:
+        L = (edge, edge, edge)
+        shift = (edge / 2, edge / 2, edge / 2)
+    elif imcon == 5:
+        L = (edge, edge, math.sqrt(2.0) * edge)
+        shift = (edge / 2, edge / 2, L[2] / 2)
+    elif imcon == 7:
+        L = (math.sqrt(3.0) * edge, edge, edge)
+        shift = (L[0] / 2, edge / 2, 0.0)
+    else:
+        raise ValueError("imcon must be 4, 5 or 7")
+    n = int(round(rho * L[0] * L[1] * L[2] / 2))
+    return make_framework(L, n, seed, shift=shift)
 
 
 def _fmt(x):

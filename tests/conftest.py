@@ -86,6 +86,12 @@ def decks(tmp_path_factory):
                   "finishment 1e-9\nfinish")
     open(os.path.join(peq, "CONTROL"), "w").write(ctl)
     out["pressure_eq"] = peq
+    # the half-shift cells: truncated octahedron, rhombic dodecahedron, hexagonal prism
+    for imcon, edge in ((4, 30.0), (5, 26.0), (7, 26.0)):
+        hf = synth.half_shift_framework(imcon, edge, seed=40 + imcon)
+        out[f"imcon{imcon}"] = synth.write_inputs(str(root / f"imcon{imcon}"), hf, ["CO2"], [2.0], 298.0,
+                                                  tuple(synth.kmax_for(hf.cell[j, j]) for j in range(3)),
+                                                  imcon=imcon)
     fw = fws[0]
     out["mixture"] = synth.write_inputs(str(root / "mixture"), fw, ["CO2", "N2"], [0.15, 0.85], 298.0,
                                         tuple(synth.kmax_for(fw.cell[j, j]) for j in range(3)))

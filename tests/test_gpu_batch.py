@@ -91,3 +91,15 @@ def test_batch_multi_jump_replays_oracle(fmc, oracle_mod, decks):
         assert st["nmol0"] == ref["nmols_after"][-1]
         assert abs(st["energy0"] - ref["energy_after"][-1]) <= 1e-9 * max(1.0, abs(ref["energy_after"][-1]))
     assert acc_mj > 0 and rej_mj > 0
+
+
+@pytest.mark.parametrize("name", ["imcon4", "imcon5", "imcon7"])
+def test_batch_half_shift_cells_replay_oracle(fmc, oracle_mod, decks, name):
+    """Truncated octahedron, rhombic dodecahedron and hexagonal prism cells: the images of
+    utility_pack.f:1203-1346 in the real-space loop, voxel lists built over the box with the
+    half-shift lattice's nearest images."""
+    seeds = [(31, 41, 59, 26), (2, 7, 1, 8)]
+    b = fmc.Batch([decks[name]] * 2, seeds)
+    tr, _ = b.run(2000, trace=True)
+    for i, s in enumerate(seeds):
+        _compare_traces(tr[i], oracle_mod.Chain(decks[name], seed=s).run(2000))

@@ -99,7 +99,11 @@ def _compare_traces(tr_d, tr_o):
         bad = np.nonzero(tr_d[key] != tr_o[key])[0]
         assert bad.size == 0, f"{key} differs first at move {bad[:1]}"
     assert np.array_equal(tr_d["rande"], tr_o["rande"])
-    scale = np.maximum(np.abs(tr_o["estep"]), 1e-3)
+    # dE relative to the move's energy scale: a dE that nearly cancels its components carries
+    # their rounding, so the scale is the larger of |dE|, the summed |components| (internal
+    # units of 10 J/mol, 418.4 to a kcal/mol) and 1e-3 kcal/mol
+    comp = (np.abs(tr_o["ewld1"]) + np.abs(tr_o["ewld2"]) + np.abs(tr_o["ewld3"]) + np.abs(tr_o["vdw"])) / 418.4
+    scale = np.maximum(np.maximum(np.abs(tr_o["estep"]), comp), 1e-3)
     err = np.abs(tr_d["estep"] - tr_o["estep"]) / scale
     assert err.max() < REL, f"max rel dE error {err.max():.3e} at move {int(err.argmax())}"
     # components are in internal units (10 J/mol); the floor is the same 1e-3 kcal/mol as dE's
@@ -111,7 +115,8 @@ def _compare_traces(tr_d, tr_o):
 
 
 @pytest.mark.parametrize("deck,n", [("small", 4000), ("mixture", 3000), ("ortho1", 2000), ("forms", 2000),
-                                    ("jumps", 2500), ("multijump", 2500)])
+                                    ("jumps", 2500), ("multijump", 2500), ("imcon4", 2000), ("imcon5", 2000),
+                                    ("imcon7", 2000)])
 def test_move_loop_matches_oracle_sequence(fmc, oracle_mod, decks, deck, n):
     seed = (31, 41, 59, 26)
     c = fmc.Chain(decks[deck], seed=seed)

@@ -30,7 +30,8 @@ def test_library_exports_every_declared_symbol(fmc):
     assert L.fmc_version() == 10400
 
 
-@pytest.mark.parametrize("name", ["calf20", "small", "large", "ortho0", "ortho1", "mixture"])
+@pytest.mark.parametrize("name", ["calf20", "small", "large", "ortho0", "ortho1", "mixture", "imcon4", "imcon5",
+                                  "imcon7"])
 def test_deck_tables_match_oracle_bit_exact(fmc, oracle_mod, decks, name):
     info = fmc.deck_inspect(decks[name])
     orc = oracle_mod.Chain(decks[name])
