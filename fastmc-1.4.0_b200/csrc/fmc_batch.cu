@@ -629,7 +629,8 @@ __device__ __noinline__ void real_space(const DevSystem& S, const ChainDev& C, c
         // FP32 for the components selected by fp32_mask (bit 1 Coulomb, bit 2 vdW); the
         // separation and minimum image stay FP64
         double dx = M.x[st] - c[u].a.x, dy = M.y[st] - c[u].a.y, dz = M.z[st] - c[u].a.z;
-        min_image_t<kImcon>(S.cell, dx, dy, dz);
+        if (kImcon < 0) min_image(S.cell, dx, dy, dz);
+        else min_image_t<kImcon>(S.cell, dx, dy, dz);
         double rsq = dx * dx + dy * dy + dz * dz;
         if (rsq < S.rcut2) {
           const bool need64 = (fp32_mask & 6) != 6;
@@ -735,10 +736,9 @@ __device__ __noinline__ void sums(const DevSystem& S, const ChainDev& C, const M
   if (S.cell.imcon == 1) real_space<kMixed, 1>(S, C, M, nseg, prow_s, nt1, fp32_mask, v);
   else if (S.cell.imcon == 2) real_space<kMixed, 2>(S, C, M, nseg, prow_s, nt1, fp32_mask, v);
   else if (S.cell.imcon == 3) real_space<kMixed, 3>(S, C, M, nseg, prow_s, nt1, fp32_mask, v);
-  else if (S.cell.imcon == 4) real_space<kMixed, 4>(S, C, M, nseg, prow_s, nt1, fp32_mask, v);
-  else if (S.cell.imcon == 5) real_space<kMixed, 5>(S, C, M, nseg, prow_s, nt1, fp32_mask, v);
-  else if (S.cell.imcon == 7) real_space<kMixed, 7>(S, C, M, nseg, prow_s, nt1, fp32_mask, v);
-  else real_space<kMixed, 0>(S, C, M, nseg, prow_s, nt1, fp32_mask, v);
+  // the half-shift cells share one instantiation that reads the boundary condition from the
+  // cell: each compiled copy of this loop costs instruction cache (one per cell kind cost 8%)
+  else real_space<kMixed, -1>(S, C, M, nseg, prow_s, nt1, fp32_mask, v);
 }
 
 // All threads, in production: storeprob (utility_pack.f:496-561) for the chain's state after the
