@@ -736,8 +736,9 @@ __device__ __noinline__ void sums(const DevSystem& S, const ChainDev& C, const M
   if (S.cell.imcon == 1) real_space<kMixed, 1>(S, C, M, nseg, prow_s, nt1, fp32_mask, v);
   else if (S.cell.imcon == 2) real_space<kMixed, 2>(S, C, M, nseg, prow_s, nt1, fp32_mask, v);
   else if (S.cell.imcon == 3) real_space<kMixed, 3>(S, C, M, nseg, prow_s, nt1, fp32_mask, v);
-  // the half-shift cells share one instantiation that reads the boundary condition from the
-  // cell: each compiled copy of this loop costs instruction cache (one per cell kind cost 8%)
+  // the half-shift cells and the slab share one instantiation that reads the boundary condition
+  // from the cell: each compiled copy of this loop costs instruction cache (one per cell kind
+  // cost 8%)
   else real_space<kMixed, -1>(S, C, M, nseg, prow_s, nt1, fp32_mask, v);
 }
 

@@ -89,6 +89,9 @@ struct CellGeom {
   double rh[9];   // inverse (invert, utility_pack.f:1417)
   double inv[3];  // 1/h[0], 1/h[4], 1/h[8]: the reciprocals images() forms once per call
   double hex[3];  // hexagonal prism (imcon 7): a/(2 rt3), a/rt3, rt3/a as images() forms them
+  double slab[4];  // slab (imcon 6): the in-plane inverse r1, r2, r4, r5 as images() forms it
+  // slab voxel layers along z: the lowest layer's bottom, the layer height and its inverse
+  double zlo, dz, rdz;
   double volm;    // volume used by Ewald and acceptance
   int imcon;
 };
@@ -103,14 +106,21 @@ inline void cell_reciprocals(CellGeom& c) {
   c.hex[0] = c.h[0] / (kImgRt3 * 2.0);
   c.hex[1] = c.h[0] / kImgRt3;
   c.hex[2] = kImgRt3 / c.h[0];
+  double det = c.h[0] * c.h[4] - c.h[1] * c.h[3];
+  det = 1.0 / det;
+  c.slab[0] = det * c.h[4];
+  c.slab[1] = -det * c.h[1];
+  c.slab[2] = -det * c.h[3];
+  c.slab[3] = det * c.h[0];
 }
 
 // Fortran nint: nearest integer, halves away from zero.
 FMC_HD double fnint(double x) { return round(x); }
 
-// Minimum image of one separation vector (images, utility_pack.f:1138-1349) for imcon 1, 2, 3
-// and the half-shift cells 4 (truncated octahedron), 5 (rhombic dodecahedron) and 7 (hexagonal
-// prism), for a boundary condition known at compile time (other values: no image).
+// Minimum image of one separation vector (images, utility_pack.f:1138-1349) for imcon 1, 2, 3,
+// the half-shift cells 4 (truncated octahedron), 5 (rhombic dodecahedron) and 7 (hexagonal
+// prism) and the slab 6, for a boundary condition known at compile time (other values: no
+// image).
 template <int kImcon>
 FMC_HD void min_image_t(const CellGeom& c, double& x, double& y, double& z) {
   if (kImcon == 1) {
@@ -153,6 +163,11 @@ FMC_HD void min_image_t(const CellGeom& c, double& x, double& y, double& z) {
       y = y - 0.5 * copysign(fabs(a), y);
       z = z - 0.5 * copysign(fabs(cz), z);
     }
+  } else if (kImcon == 6) {  // periodic in the a-b plane only
+    const double sx = c.slab[0] * x + c.slab[2] * y, sy = c.slab[1] * x + c.slab[3] * y;
+    const double xss = sx - fnint(sx), yss = sy - fnint(sy);
+    x = c.h[0] * xss + c.h[3] * yss;
+    y = c.h[1] * xss + c.h[4] * yss;
   } else if (kImcon == 7) {
     const double aaa = c.hex[0], bbb = c.hex[1];
     y = y - bbb * fnint(c.hex[2] * y);
@@ -171,7 +186,21 @@ FMC_HD void min_image(const CellGeom& c, double& x, double& y, double& z) {
   else if (c.imcon == 3) min_image_t<3>(c, x, y, z);
   else if (c.imcon == 4) min_image_t<4>(c, x, y, z);
   else if (c.imcon == 5) min_image_t<5>(c, x, y, z);
+  else if (c.imcon == 6) min_image_t<6>(c, x, y, z);
   else if (c.imcon == 7) min_image_t<7>(c, x, y, z);
+}
+
+// Nearest in-plane image of a separation in a slab: the nint image and its eight neighbours in
+// the a-b plane, z as it is.  A lower bound of the distance images() returns.
+FMC_HD double slab_dist2(const CellGeom& c, double x, double y, double z) {
+  min_image_t<6>(c, x, y, z);
+  double best = 1e300;
+  for (int i = -1; i <= 1; i++)
+    for (int j = -1; j <= 1; j++) {
+      const double u = x + i * c.h[0] + j * c.h[3], v = y + i * c.h[1] + j * c.h[4];
+      best = fmin(best, u * u + v * v + z * z);
+    }
+  return best;
 }
 
 // Squared distance to the nearest lattice image of a separation: for imcon 4, 5 and 7 the

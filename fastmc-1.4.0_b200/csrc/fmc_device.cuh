@@ -103,9 +103,22 @@ __device__ __forceinline__ void pair_energy(const DevSystem& S, double dx, doubl
   }
 }
 
-// Voxel of a position (wrapped into the cell).
+// Voxel of a position (wrapped into the cell; a slab's z clamped to its layers, whose lowest and
+// highest hold no atom).
 __device__ __forceinline__ int voxel_of(const DevSystem& S, double x, double y, double z) {
   double s[3];
+  if (S.cell.imcon == 6) {
+    const CellGeom& c = S.cell;
+    s[0] = c.slab[0] * x + c.slab[2] * y;
+    s[1] = c.slab[1] * x + c.slab[3] * y;
+    s[2] = 0.0;
+    double t = (z - c.zlo) * c.rdz;
+    int k = t < 0.0 ? 0 : (t >= (double)S.nvox[2] ? S.nvox[2] - 1 : (int)t);
+    int v0 = (int)((s[0] - floor(s[0])) * S.nvox[0]), v1 = (int)((s[1] - floor(s[1])) * S.nvox[1]);
+    v0 = v0 < 0 ? 0 : (v0 >= S.nvox[0] ? S.nvox[0] - 1 : v0);
+    v1 = v1 < 0 ? 0 : (v1 >= S.nvox[1] ? S.nvox[1] - 1 : v1);
+    return (v0 * S.nvox[1] + v1) * S.nvox[2] + k;
+  }
   frac_coords(S.cell, x, y, z, s);
   int v[3];
   for (int a = 0; a < 3; a++) {

@@ -311,6 +311,7 @@ cudaError_t launch_single_point_rs(const DevSystem& S, const GuestView& G, int n
 // sqrt(lim2) (rcut + the voxel's circumradius), in ascending atom order.
 __device__ __forceinline__ double true_dist2_dev(const CellGeom& c, double dx, double dy, double dz) {
   if (c.imcon == 4 || c.imcon == 5 || c.imcon == 7) return shifted_lattice_dist2(c, dx, dy, dz);
+  if (c.imcon == 6) return slab_dist2(c, dx, dy, dz);
   min_image(c, dx, dy, dz);
   double best = dx * dx + dy * dy + dz * dz;
   if (c.imcon == 3) {
@@ -329,6 +330,12 @@ __device__ __forceinline__ double true_dist2_dev(const CellGeom& c, double dx, d
 __device__ __forceinline__ void voxel_centre(const CellGeom& c, int v, int n0, int n1, int n2, double* p) {
   int a = v / (n1 * n2), b = (v / n2) % n1, cc = v % n2;
   double fa = (a + 0.5) / n0, fb = (b + 0.5) / n1, fc = (cc + 0.5) / n2;
+  if (c.imcon == 6) {  // slab: in-plane cell, z layers from zlo
+    p[0] = fa * c.h[0] + fb * c.h[3];
+    p[1] = fa * c.h[1] + fb * c.h[4];
+    p[2] = c.zlo + (cc + 0.5) * c.dz;
+    return;
+  }
   p[0] = fa * c.h[0] + fb * c.h[3] + fc * c.h[6];
   p[1] = fa * c.h[1] + fb * c.h[4] + fc * c.h[7];
   p[2] = fa * c.h[2] + fb * c.h[5] + fc * c.h[8];

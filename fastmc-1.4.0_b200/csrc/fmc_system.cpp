@@ -130,6 +130,7 @@ double nint_image_dist2(const CellGeom& c, double dx, double dy, double dz) {
 // True minimum-image distance^2 (the nint image and its 26 neighbours).
 double true_dist2(const CellGeom& c, double dx, double dy, double dz) {
   if (c.imcon == 4 || c.imcon == 5 || c.imcon == 7) return shifted_lattice_dist2(c, dx, dy, dz);
+  if (c.imcon == 6) return slab_dist2(c, dx, dy, dz);
   min_image(c, dx, dy, dz);
   if (c.imcon == 1 || c.imcon == 2) return dx * dx + dy * dy + dz * dz;
   double best = dx * dx + dy * dy + dz * dz;
@@ -176,8 +177,8 @@ double lrc_energy(const HostSystem& s, const std::vector<int>& numtyp, const std
 int build_host_system(const InputDeck& d, HostSystem& s, std::string& err, double voxel_edge) {
   s = HostSystem();
   s.deck = d;
-  if (d.imcon < 1 || d.imcon > 7 || d.imcon == 6) {
-    err = "the slab (imcon 6) and non-periodic (imcon 0) cells are not supported on the device";
+  if (d.imcon < 1 || d.imcon > 7) {
+    err = "cells without periodic boundaries (imcon 0) are not supported on the device";
     return -4;
   }
   if (d.lspe) {
@@ -342,6 +343,30 @@ int build_host_system(const InputDeck& d, HostSystem& s, std::string& err, doubl
     double e[3][3];
     for (int a = 0; a < 3; a++)
       for (int k = 0; k < 3; k++) e[a][k] = s.cell.h[3 * a + k] / s.nvox[a];
+    if (d.imcon == 6) {
+      // slab: layers of height voxel_edge along z over the framework's z range, widened by one
+      // layer beyond the list radius at each end so that the end layers hold no atom and a
+      // position beyond them can be clamped into them
+      double zmin = 0.0, zmax = 0.0;
+      for (int j = 0; j < (int)d.fz.size(); j++) {
+        zmin = j ? std::min(zmin, d.fz[j]) : d.fz[j];
+        zmax = j ? std::max(zmax, d.fz[j]) : d.fz[j];
+      }
+      e[2][0] = e[2][1] = 0.0;
+      e[2][2] = voxel_edge;
+      double circ6 = 0.0;
+      for (int sa = -1; sa <= 1; sa += 2)
+        for (int sb = -1; sb <= 1; sb += 2) {
+          double v[3];
+          for (int k = 0; k < 3; k++) v[k] = e[0][k] + sa * e[1][k] + sb * e[2][k];
+          circ6 = std::max(circ6, 0.5 * std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]));
+        }
+      const double reach = s.rcut + circ6 + 1.0;  // the list radius, with room for the guest extent
+      s.cell.dz = voxel_edge;
+      s.cell.rdz = 1.0 / voxel_edge;
+      s.cell.zlo = zmin - reach - voxel_edge;
+      s.nvox[2] = (int)std::ceil((zmax - zmin + 2.0 * (reach + voxel_edge)) / voxel_edge);
+    }
     double circ = 0.0;
     for (int sa = -1; sa <= 1; sa += 2)
       for (int sb = -1; sb <= 1; sb += 2) {

@@ -133,6 +133,15 @@ def half_shift_framework(imcon, edge, seed, rho=0.025):
     return make_framework(L, n, seed, shift=shift)
 
 
+def slab_framework(edge, thickness, height, seed, rho=0.025):
+    """A slab (imcon 6): atoms in an edge x edge x thickness layer at the bottom of an
+    edge x edge x height cell, periodic in the plane only; rho atoms per A^3 of the layer."""
+    n = int(round(rho * edge * edge * thickness))
+    fw = make_framework((edge, edge, thickness), n, seed)
+    fw.cell = np.diag([edge, edge, float(height)])
+    return fw
+
+
 def _fmt(x):
     return f"{x:.10f}"
 

@@ -92,6 +92,9 @@ def decks(tmp_path_factory):
         out[f"imcon{imcon}"] = synth.write_inputs(str(root / f"imcon{imcon}"), hf, ["CO2"], [2.0], 298.0,
                                                   tuple(synth.kmax_for(hf.cell[j, j]) for j in range(3)),
                                                   imcon=imcon)
+    slab = synth.slab_framework(26.0, 20.0, 60.0, seed=46)
+    out["imcon6"] = synth.write_inputs(str(root / "imcon6"), slab, ["CO2"], [2.0], 298.0,
+                                       tuple(synth.kmax_for(slab.cell[j, j]) for j in range(3)), imcon=6)
     fw = fws[0]
     out["mixture"] = synth.write_inputs(str(root / "mixture"), fw, ["CO2", "N2"], [0.15, 0.85], 298.0,
                                         tuple(synth.kmax_for(fw.cell[j, j]) for j in range(3)))

@@ -93,7 +93,7 @@ def test_batch_multi_jump_replays_oracle(fmc, oracle_mod, decks):
     assert acc_mj > 0 and rej_mj > 0
 
 
-@pytest.mark.parametrize("name", ["imcon4", "imcon5", "imcon7"])
+@pytest.mark.parametrize("name", ["imcon4", "imcon5", "imcon6", "imcon7"])
 def test_batch_half_shift_cells_replay_oracle(fmc, oracle_mod, decks, name):
     """Truncated octahedron, rhombic dodecahedron and hexagonal prism cells: the images of
     utility_pack.f:1203-1346 in the real-space loop, voxel lists built over the box with the

@@ -116,7 +116,7 @@ def _compare_traces(tr_d, tr_o):
 
 @pytest.mark.parametrize("deck,n", [("small", 4000), ("mixture", 3000), ("ortho1", 2000), ("forms", 2000),
                                     ("jumps", 2500), ("multijump", 2500), ("imcon4", 2000), ("imcon5", 2000),
-                                    ("imcon7", 2000)])
+                                    ("imcon6", 2000), ("imcon7", 2000)])
 def test_move_loop_matches_oracle_sequence(fmc, oracle_mod, decks, deck, n):
     seed = (31, 41, 59, 26)
     c = fmc.Chain(decks[deck], seed=seed)

@@ -31,7 +31,7 @@ def test_library_exports_every_declared_symbol(fmc):
 
 
 @pytest.mark.parametrize("name", ["calf20", "small", "large", "ortho0", "ortho1", "mixture", "imcon4", "imcon5",
-                                  "imcon7"])
+                                  "imcon6", "imcon7"])
 def test_deck_tables_match_oracle_bit_exact(fmc, oracle_mod, decks, name):
     info = fmc.deck_inspect(decks[name])
     orc = oracle_mod.Chain(decks[name])
