@@ -49,17 +49,24 @@ def parse():
 
 # ------------------------------------------------------------------ distributed plumbing
 class Dist:
+    """One process per GPU (NCCL); on a host without GPUs the same steps run over gloo, which is
+    how the multi-rank logic is tested on CPU."""
+
     def __init__(self, n):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
         self.pg = None
+        self.device = "cpu"
         if self.world > 1:
             import torch
             import torch.distributed as dist
 
-            torch.cuda.set_device(self.local)
-            dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+            backend = "gloo"
+            if torch.cuda.is_available():
+                torch.cuda.set_device(self.local)
+                backend, self.device = "nccl", f"cuda:{self.local}"
+            dist.init_process_group(backend, timeout=__import__("datetime").timedelta(seconds=120))
             self.pg = dist
 
     def barrier(self):
@@ -71,7 +78,7 @@ class Dist:
             return x
         import torch
 
-        t = torch.tensor([float(x)], device=f"cuda:{self.local}")
+        t = torch.tensor([float(x)], device=self.device)
         self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
         return float(t.item())
 
@@ -80,7 +87,7 @@ class Dist:
             return x
         import torch
 
-        t = torch.tensor([float(x)], device=f"cuda:{self.local}")
+        t = torch.tensor([float(x)], device=self.device)
         self.pg.all_reduce(t, op=self.pg.ReduceOp.SUM)
         return float(t.item())
 
