@@ -37,21 +37,6 @@ struct MoveSmem {
   double mj_old[3 * kBatchMaxSites];
 };
 
-__device__ double lrc_device(const SysConst& Y, const int* numtyp) {
-  if (!Y.lrc_on) return 0.0;
-  const double twopi = 2.0 * kPi, v = Y.volm;
-  double e = 0.0;
-  int ivdw = 0;
-  for (int i = 1; i <= Y.ntypes; i++)
-    for (int j = 1; j <= i; j++) {
-      ivdw++;
-      double den =
-          twopi * ((double)numtyp[i] * (double)numtyp[j] - (double)Y.numfrz[i] * (double)Y.numfrz[j]) / (v * v);
-      e = e + v * den * Y.steadd[ivdw];
-    }
-  return e;
-}
-
 // duni (gcmc.f:2712-2805) with ir, jr and c held in registers across a run of draws; the
 // arithmetic is duni_next's, draw for draw.
 struct DuniLocal {

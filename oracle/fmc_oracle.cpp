@@ -206,11 +206,6 @@ static std::string getword(char* s, int len1, int len2) {
   }
   return std::string(seq, 8);
 }
-static std::string word8(const std::string& s) {
-  std::string w = s.substr(0, std::min<size_t>(8, s.size()));
-  w.resize(8, ' ');
-  return w;
-}
 
 // ---------------------------------------------------------------- geometry (utility_pack.f)
 // invert utility_pack.f:1417-1467
