@@ -41,6 +41,8 @@ def parse():
     ap.add_argument("--serve-cycle-scale", type=float, default=0.1,
                     help="scale of the U(2k,20k) cycle budgets so that requests finish within the run")
     ap.add_argument("--moves", type=int, default=2000, help="trial moves per chain per step")
+    ap.add_argument("--voxel-edge", type=float, default=0.0,
+                    help="batched: neighbour-list voxel edge in A (0: picked by the autotuner)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="bounded CPU baseline sample")
     ap.add_argument("--skip-baselines", action="store_true",
                     help="omit the plain-path and CPU samples (profiling runs of the batched kernel)")
@@ -337,7 +339,12 @@ def run_batched(args, dist):
     dirs = make_batched_decks(tmp)
     n = len(dirs)
     seeds = [(12, 34, 56, (78 + 7 * i + 13 * dist.rank) % 169) for i in range(n)]
-    b = fm.Batch(dirs, seeds, device=dist.local)
+    # neighbour-list voxel edge: the autotuner times throwaway batches of the same chains
+    tune = None
+    edge = args.voxel_edge
+    if edge <= 0:
+        edge, tune = fm.autotune_voxel_edge(dirs, seeds, device=dist.local)
+    b = fm.Batch(dirs, seeds, device=dist.local, voxel_edge=edge)
     setup_s = time.perf_counter() - t0
     infos = {}
     for d in dirs:
@@ -393,7 +400,8 @@ def run_batched(args, dist):
         "config": {"workload": BATCHED_WORKLOAD, "chains": n, "moves_per_chain_per_step": args.moves,
                    "guests_mean": float(np.mean([s["nmol0"] for s in states])),
                    "K_range": [int(min(i["K"] for i in infos.values())), int(max(i["K"] for i in infos.values()))],
-                   "setup_s": setup_s,
+                   "setup_s": setup_s, "voxel_edge_A": edge,
+                   "voxel_autotune_ms": tune,
                    "l2": "per-chain S(k) is shared-memory resident; frameworks + voxel lists exceed L2 (no flush)",
                    "parallelism": f"replicas{dist.world}"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,

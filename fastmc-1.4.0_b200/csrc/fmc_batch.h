@@ -172,7 +172,8 @@ class Batch {
   size_t shadow_cap = 0;
   int nchains = 0;
   ~Batch();
-  int open(const std::vector<std::string>& dirs, const std::vector<int>& seeds, int device, std::string& err);
+  int open(const std::vector<std::string>& dirs, const std::vector<int>& seeds, int device, std::string& err,
+           double voxel_edge = 2.0);
   // REVIVE + REVCON of chain c into outdir; restart of chain c from a REVIVE (call before
   // the chain's first run to match the reference's restart, which re-seeds duni).
   int write_revive(int c, const std::string& outdir, std::string& err);

@@ -237,7 +237,8 @@ Batch::~Batch() {
   }
 }
 
-int Batch::open(const std::vector<std::string>& dirs, const std::vector<int>& seeds, int dev, std::string& err) {
+int Batch::open(const std::vector<std::string>& dirs, const std::vector<int>& seeds, int dev, std::string& err,
+                double voxel_edge) {
   device = dev;
   nchains = (int)dirs.size();
   if (cudaSetDevice(dev) != cudaSuccess || cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
@@ -258,7 +259,7 @@ int Batch::open(const std::vector<std::string>& dirs, const std::vector<int>& se
     if (it == sys_of_key.end()) {
       auto ch = std::make_unique<Chain>();
       int s4[4] = {12, 34, 56, 78};
-      rc = ch->open(dirs[c], s4, dev, err);
+      rc = ch->open(dirs[c], s4, dev, err, voxel_edge);
       if (rc) {
         err = dirs[c] + ": " + err;
         return rc;
@@ -565,6 +566,54 @@ int fmc_batch_open(int nchains, const char* const* dirs, const int* seeds, int d
     return rc;
   }
   *out = b;
+  return 0;
+}
+
+int fmc_batch_open_edge(int nchains, const char* const* dirs, const int* seeds, int device, double voxel_edge,
+                        fmc_batch** out) {
+  if (!dirs || !seeds || !out || nchains < 1 || !(voxel_edge >= 0.5 && voxel_edge <= 8.0)) {
+    fmc::set_last_error("null argument, empty batch or voxel edge outside 0.5-8 A");
+    return -1;
+  }
+  fmc_batch* b = new fmc_batch();
+  std::vector<std::string> d(dirs, dirs + nchains);
+  std::vector<int> s(seeds, seeds + 4 * nchains);
+  std::string err;
+  int rc = b->impl.open(d, s, device, err, voxel_edge);
+  if (rc) {
+    delete b;
+    *out = nullptr;
+    fmc::set_last_error(err);
+    return rc;
+  }
+  *out = b;
+  return 0;
+}
+
+int fmc_batch_autotune(int nchains, const char* const* dirs, const int* seeds, int device, const double* edges,
+                       int nedges, int moves, double* best_edge, float* ms) {
+  if (!dirs || !seeds || !edges || nedges < 1 || moves < 1 || !best_edge) {
+    fmc::set_last_error("bad autotune arguments");
+    return -1;
+  }
+  // every candidate on a throwaway batch of the same chains: one warm-up launch, one timed
+  double best = 0.0;
+  float best_ms = 0.0f;
+  for (int i = 0; i < nedges; i++) {
+    fmc_batch* b = nullptr;
+    int rc = fmc_batch_open_edge(nchains, dirs, seeds, device, edges[i], &b);
+    float t = 0.0f;
+    if (!rc) rc = fmc_batch_run(b, moves, nullptr, &t);
+    if (!rc) rc = fmc_batch_run(b, moves, nullptr, &t);
+    if (b) fmc_batch_close(b);
+    if (rc) return rc;
+    if (ms) ms[i] = t;
+    if (i == 0 || t < best_ms) {
+      best = edges[i];
+      best_ms = t;
+    }
+  }
+  *best_edge = best;
   return 0;
 }
 

@@ -180,7 +180,7 @@ GuestView Chain::guest_view() const {
   return G;
 }
 
-int prepare_system(const std::string& dir, HostSystem& sys, std::string& err) {
+int prepare_system(const std::string& dir, HostSystem& sys, std::string& err, double voxel_edge) {
   InputDeck deck;
   int rc = read_input_deck(dir, deck, err);
   if (rc) return rc;
@@ -193,12 +193,12 @@ int prepare_system(const std::string& dir, HostSystem& sys, std::string& err) {
       err = "framework atoms must be frozen (rigid framework)";
       return -6;
     }
-  return build_host_system(deck, sys, err);
+  return build_host_system(deck, sys, err, voxel_edge);
 }
 
-int Chain::open(const std::string& dir, const int seed[4], int dev, std::string& err) {
+int Chain::open(const std::string& dir, const int seed[4], int dev, std::string& err, double voxel_edge) {
   HostSystem h;
-  int rc = prepare_system(dir, h, err);
+  int rc = prepare_system(dir, h, err, voxel_edge);
   if (rc) return rc;
   return open_prepared(std::move(h), seed, dev, err);
 }

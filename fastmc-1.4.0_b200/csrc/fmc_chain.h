@@ -36,7 +36,8 @@ struct Species {
 
 // Host part of opening a chain: reads the deck, checks what the GPU path supports and
 // builds the host tables.  Thread-safe (no device calls).
-int prepare_system(const std::string& dir, HostSystem& sys, std::string& err);
+// voxel_edge: target edge (A) of the voxels whose neighbour lists the kernels read.
+int prepare_system(const std::string& dir, HostSystem& sys, std::string& err, double voxel_edge = 2.0);
 
 class Chain {
  public:
@@ -95,7 +96,7 @@ class Chain {
   // mixtures); an empty dir closes them.
   int open_outputs(const std::string& dir, std::string& err);
   void close_outputs();
-  int open(const std::string& dir, const int seed[4], int device, std::string& err);
+  int open(const std::string& dir, const int seed[4], int device, std::string& err, double voxel_edge = 2.0);
   // open from a system already built on the host by prepare_system (the device part only)
   int open_prepared(HostSystem&& prepared, const int seed[4], int device, std::string& err);
   GuestView guest_view() const;

@@ -247,20 +247,40 @@ class Chain:
         return dict(zip(["N", "E", "EN", "N2", "E2", "prodcount"], out.tolist()))
 
 
+def _chain_args(directories, seeds):
+    dirs = [str(d).encode() for d in directories]
+    n = len(dirs)
+    if seeds is None:
+        seeds = [(12, 34, 56, (78 + i) % 169) for i in range(n)]
+    s = np.ascontiguousarray(np.asarray(seeds, dtype=np.int32).reshape(n, 4))
+    return (ctypes.c_char_p * n)(*dirs), s, n
+
+
+def autotune_voxel_edge(directories, seeds=None, device=0, edges=(2.0, 1.5, 1.2, 1.0), moves=500):
+    """The voxel edge (A) under which these chains run fastest, timed on throwaway batches;
+    returns (best edge, {edge: device ms of one `moves`-move launch})."""
+    arr, s, n = _chain_args(directories, seeds)
+    e = np.ascontiguousarray(np.asarray(edges, dtype=np.float64))
+    ms = (ctypes.c_float * len(e))()
+    best = ctypes.c_double(0.0)
+    check(lib().fmc_batch_autotune(n, arr, ip(s), int(device), dp(e), len(e), int(moves), ctypes.byref(best), ms))
+    return best.value, {float(k): float(v) for k, v in zip(e, ms)}
+
+
 class Batch:
     """Many independent chains advanced by one persistent kernel (the batched path)."""
 
-    def __init__(self, directories, seeds=None, device=0):
-        dirs = [str(d).encode() for d in directories]
-        n = len(dirs)
-        if seeds is None:
-            seeds = [(12, 34, 56, (78 + i) % 169) for i in range(n)]
-        s = np.ascontiguousarray(np.asarray(seeds, dtype=np.int32).reshape(n, 4))
-        arr = (ctypes.c_char_p * n)(*dirs)
+    def __init__(self, directories, seeds=None, device=0, voxel_edge=None):
+        """voxel_edge: edge (A) of the neighbour-list voxels (None: the library's 2 A; see
+        autotune_voxel_edge)."""
+        arr, s, n = _chain_args(directories, seeds)
         self.n = n
         self.dirs = [str(d) for d in directories]
         self.h = ctypes.c_void_p()
-        check(lib().fmc_batch_open(n, arr, ip(s), int(device), ctypes.byref(self.h)))
+        if voxel_edge is None:
+            check(lib().fmc_batch_open(n, arr, ip(s), int(device), ctypes.byref(self.h)))
+        else:
+            check(lib().fmc_batch_open_edge(n, arr, ip(s), int(device), float(voxel_edge), ctypes.byref(self.h)))
 
     def close(self):
         if self.h:

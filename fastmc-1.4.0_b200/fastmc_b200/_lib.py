@@ -44,6 +44,10 @@ SIGNATURES = {
     "fmc_run_timed": (_ci, [_vp, _ci, _vp, ctypes.POINTER(ctypes.c_float)]),
     "fmc_ewald1_guest_noalloc": (_ci, [_ci, _ip, _dp, _vp, _vp, _vp, _ci, _ci, _ci, _dp, _cd, _cd, _vp, _vp, _vp]),
     "fmc_batch_open": (_ci, [_ci, ctypes.POINTER(ctypes.c_char_p), _ip, _ci, ctypes.POINTER(_vp)]),
+    "fmc_batch_open_edge": (_ci, [_ci, ctypes.POINTER(ctypes.c_char_p), _ip, _ci, ctypes.c_double,
+                                  ctypes.POINTER(_vp)]),
+    "fmc_batch_autotune": (_ci, [_ci, ctypes.POINTER(ctypes.c_char_p), _ip, _ci, _dp, _ci, _ci, _dp,
+                                 ctypes.POINTER(ctypes.c_float)]),
     "fmc_batch_close": (None, [_vp]),
     "fmc_batch_run": (_ci, [_vp, _ci, _vp, ctypes.POINTER(ctypes.c_float)]),
     "fmc_batch_profile": (_ci, [_vp, _ci]),

@@ -168,10 +168,19 @@ int fmc_chain_write_prob(fmc_chain* c, const char* outdir);
  * Many independent chains (isotherm points) advanced by one persistent kernel, one CTA per
  * chain, the whole move loop of gcmc.f:589-1380 on the device (no counterpart in the
  * reference, which runs one chain per MPI rank, gcmc.f:334-417).  Chains are opened from
- * their own CONTROL/FIELD/CONFIG directories, must start from an empty framework, and chains
+ * their own CONTROL/FIELD/CONFIG directories (guests the deck preloads included), and chains
  * whose FIELD, CONFIG, cut-offs and Ewald parameters coincide share one device system. */
 typedef struct fmc_batch fmc_batch;
 int fmc_batch_open(int nchains, const char* const* dirs, const int* seeds, int device, fmc_batch** out);
+/* The same with the edge (A, 0.5-8) of the voxels whose neighbour lists the kernel reads
+ * (fmc_batch_open uses 2 A): finer voxels mean shorter lists per trial site and more memory. */
+int fmc_batch_open_edge(int nchains, const char* const* dirs, const int* seeds, int device, double voxel_edge,
+                        fmc_batch** out);
+/* Autotuner of the voxel edge: opens a throwaway batch of the same chains for every candidate
+ * edge, runs `moves` moves twice and keeps the edge whose second launch was fastest (device ms of
+ * each candidate in ms[nedges] when given).  The chains the caller opens afterwards start afresh. */
+int fmc_batch_autotune(int nchains, const char* const* dirs, const int* seeds, int device, const double* edges,
+                       int nedges, int moves, double* best_edge, float* ms);
 void fmc_batch_close(fmc_batch* b);
 /* Advances every chain by `moves` trial moves in one launch; trace (nullable) receives
  * nchains*moves records, chain-major; *device_ms is the launch's CUDA-event time.  A chain

@@ -103,3 +103,20 @@ def test_batch_half_shift_cells_replay_oracle(fmc, oracle_mod, decks, name):
     tr, _ = b.run(2000, trace=True)
     for i, s in enumerate(seeds):
         _compare_traces(tr[i], oracle_mod.Chain(decks[name], seed=s).run(2000))
+
+
+def test_batch_finer_voxels_replay_oracle(fmc, oracle_mod, decks):
+    """Neighbour lists over 1 A voxels (the autotuner's finest candidate) give the same moves."""
+    seeds = [(9, 9, 9, 9), (10, 20, 30, 40)]
+    names = ["ortho0", "mixture"]
+    b = fmc.Batch([decks[n] for n in names], seeds, voxel_edge=1.0)
+    tr, _ = b.run(1500, trace=True)
+    for i, (n, s) in enumerate(zip(names, seeds)):
+        _compare_traces(tr[i], oracle_mod.Chain(decks[n], seed=s).run(1500))
+
+
+def test_voxel_autotune_returns_a_candidate(fmc, decks):
+    dirs = [decks["ortho0"], decks["ortho1"]]
+    edge, ms = fmc.autotune_voxel_edge(dirs, edges=(2.0, 1.25), moves=200)
+    assert edge in (2.0, 1.25) and set(ms) == {2.0, 1.25} and all(v > 0 for v in ms.values())
+    assert ms[edge] == min(ms.values())
