@@ -173,6 +173,11 @@ int fmc_commit(fmc_chain* c, int move, int iguest, int mol, const double* xyz) {
   return 0;
 }
 
+int fmc_reject(fmc_chain* c) {
+  CHECK_CHAIN(c);
+  return 0;
+}
+
 int fmc_set_guests(fmc_chain* c, int iguest, int nmol, const double* xyz) {
   CHECK_CHAIN(c);
   fmc::Chain& C = c->impl;

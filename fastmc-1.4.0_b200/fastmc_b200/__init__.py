@@ -147,6 +147,9 @@ class Chain:
         x = None if xyz is None else np.ascontiguousarray(xyz, dtype=np.float64)
         check(lib().fmc_commit(self.h, int(move), int(iguest), int(mol), None if x is None else dp(x)))
 
+    def reject(self):
+        check(lib().fmc_reject(self.h))
+
     def set_guests(self, iguest, xyz):
         xyz = np.ascontiguousarray(xyz, dtype=np.float64)
         nsite = xyz.shape[1] if xyz.ndim == 3 else None

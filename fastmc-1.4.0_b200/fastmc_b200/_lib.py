@@ -33,6 +33,7 @@ SIGNATURES = {
     "fmc_ewald1_guest": (_ci, [_vp, _ci, _ci, _dp, _ci, _ci, _dp]),
     "fmc_guest_realspace": (_ci, [_vp, _ci, _ci, _dp, _ci, _dp, _dp]),
     "fmc_commit": (_ci, [_vp, _ci, _ci, _ci, _dp]),
+    "fmc_reject": (_ci, [_vp]),
     "fmc_set_guests": (_ci, [_vp, _ci, _ci, _dp]),
     "fmc_single_point": (_ci, [_vp, _dp, _dp]),
     "fmc_get_sk": (_ci, [_vp, _ci, _dp, _dp]),

@@ -76,6 +76,11 @@ int fmc_guest_realspace(fmc_chain* c, int iguest, int natms, const double* xyz, 
  * displace overwrites molecule `mol`; gcmc.f:966-970, 1134-1138, 1352-1357). */
 int fmc_commit(fmc_chain* c, int move, int iguest, int mol, const double* xyz);
 
+/* Reject the last evaluated move: S(k) and the sites stay as they were (the reference skips the
+ * commit, gcmc.f:954-1002) and the pending S_new is dropped; the next pass overwrites it.  It
+ * touches no device memory and is there so that a caller states either outcome. */
+int fmc_reject(fmc_chain* c);
+
 /* Replaces all molecules of species `iguest` (the condense of utility_pack.f:3325), then
  * recomputes S(k).  xyz holds nmol*nsite sites, molecule-major. */
 int fmc_set_guests(fmc_chain* c, int iguest, int nmol, const double* xyz);
