@@ -129,3 +129,26 @@ def test_move_loop_matches_oracle_sequence(fmc, oracle_mod, decks, deck, n):
         assert gd.shape == go.shape
         if gd.size:
             assert np.max(np.abs(gd - go)) < 1e-9
+
+
+def test_dropin_reject_keeps_and_commit_takes_s_new(fmc, oracle_mod, decks):
+    """The call surface a Fortran move loop uses: ewald1_guest + guest_realspace for a trial,
+    then reject (S(k) and the sites untouched) or commit (S(k) <- S_new, the molecule added)."""
+    d = decks["small"]
+    c = fmc.Chain(d)
+    tmpl, _, _, _ = oracle_mod.Chain(d).guest_template(0)
+    lines = open(os.path.join(d, "CONFIG")).read().split("\n")
+    cell = np.array([[float(v) for v in lines[k].split()] for k in (2, 3, 4)])
+    xyz = _random_guest(np.random.default_rng(11), tmpl, cell)
+    s0 = c.sk()
+    c.ewald1_guest(0, xyz, fmc.INSERT)
+    c.guest_realspace(0, xyz, -1)
+    pending = c.sk(pending=True)
+    assert not np.array_equal(pending, s0)
+    c.reject()
+    assert np.array_equal(c.sk(), s0) and c.guest_coords(0).shape[0] == 0
+    c.ewald1_guest(0, xyz, fmc.INSERT)
+    c.commit(fmc.INSERT, 0, -1, xyz)
+    assert np.array_equal(c.sk(), pending)
+    g = c.guest_coords(0)
+    assert g.shape[0] == 1 and np.allclose(g[0], xyz)
