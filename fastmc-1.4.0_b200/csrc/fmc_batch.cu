@@ -732,7 +732,6 @@ __device__ __noinline__ void sums(const DevSystem& S, const ChainDev& C, const M
 __device__ __noinline__ void prob_store(const SysConst& Y, const ChainDev& C) {
   const int na = Y.ngrid[0], nb = Y.ngrid[1], nc = Y.ngrid[2];
   const long long cells = (long long)na * nb * nc;
-  int base = 0;
   for (int g = 0; g < Y.nspecies; g++) {
     const SpeciesConst& P = Y.sp[g];
     const int ns = P.nsite, nmol = C.nmol[g];
@@ -766,9 +765,7 @@ __device__ __noinline__ void prob_store(const SysConst& Y, const ChainDev& C) {
         }
       }
     }
-    base += nmol;
   }
-  (void)base;
 }
 
 // All threads: FP64 recompute of S(k) = S_framework(k) + sum over guest sites (bounds the drift

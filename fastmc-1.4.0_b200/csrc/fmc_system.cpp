@@ -122,11 +122,6 @@ double lrc_eadd(int key, const std::array<double, 5>& p, double rcut) {
   }
 }
 
-double nint_image_dist2(const CellGeom& c, double dx, double dy, double dz) {
-  min_image(c, dx, dy, dz);
-  return dx * dx + dy * dy + dz * dz;
-}
-
 // True minimum-image distance^2 (the nint image and its 26 neighbours).
 double true_dist2(const CellGeom& c, double dx, double dy, double dz) {
   if (c.imcon == 4 || c.imcon == 5 || c.imcon == 7) return shifted_lattice_dist2(c, dx, dy, dz);
@@ -377,7 +372,6 @@ int build_host_system(const InputDeck& d, HostSystem& s, std::string& err, doubl
     double lim = s.rcut + circ + 1e-6;
     s.vox_lim2 = lim * lim;
   }
-  (void)nint_image_dist2;
   return 0;
 }
 
