@@ -115,10 +115,9 @@ int fmc_ewald1_guest(fmc_chain* c, int iguest, int natms, const double* xyz, int
     A.type[w] = (unsigned char)G.type[i];
   }
   cudaError_t e = fmc::launch_pass(C.dsys.view, C.guest_view(), A, C.sk, C.sk_new, C.W, C.st);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(C.h_result, C.W.result, sizeof(double) * 3, cudaMemcpyDeviceToHost, C.st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(C.st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(C.st);  // the kernel wrote the result to pinned memory
   if (e != cudaSuccess) return fail(-100 - (int)e, cudaGetErrorString(e));
-  out[0] = C.h_result[0];
+  out[0] = C.W.result[0];
   if (A.move == fmc::kDisplace) c->pending_g = -1;
   if (engcpe) *engcpe = out[0];
   return 0;
@@ -151,11 +150,10 @@ int fmc_guest_realspace(fmc_chain* c, int iguest, int natms, const double* xyz, 
     A.type[i] = (unsigned char)G.type[i];
   }
   cudaError_t e = fmc::launch_pass(C.dsys.view, C.guest_view(), A, C.sk, C.sk_new, C.W, C.st);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(C.h_result, C.W.result, sizeof(double) * 3, cudaMemcpyDeviceToHost, C.st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(C.st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(C.st);  // the kernel wrote the result to pinned memory
   if (e != cudaSuccess) return fail(-100 - (int)e, cudaGetErrorString(e));
-  if (ewld2) *ewld2 = C.h_result[1];
-  if (vdw) *vdw = C.h_result[2];
+  if (ewld2) *ewld2 = C.W.result[1];
+  if (vdw) *vdw = C.W.result[2];
   return 0;
 }
 

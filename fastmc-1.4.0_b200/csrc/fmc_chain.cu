@@ -156,9 +156,9 @@ Chain::~Chain() {
     cudaSetDevice(device);
     cudaStreamSynchronize(st);
     for (void* p : {(void*)sk, (void*)sk_new, (void*)sk_save, (void*)gsite, (void*)gtype, (void*)W.recip_part, (void*)W.site_e,
-                    (void*)W.counter, (void*)W.result, (void*)recip_scratch, (void*)recip_parts, (void*)all_atoms})
+                    (void*)W.counter, (void*)recip_scratch, (void*)recip_parts, (void*)all_atoms})
       if (p) cudaFree(p);
-    if (h_result) cudaFreeHost(h_result);
+    if (W.result) cudaFreeHost(W.result);
     cudaStreamDestroy(st);
   }
 }
@@ -238,8 +238,9 @@ int Chain::open_prepared(HostSystem&& prepared, const int seed[4], int dev, std:
   FMC_CUDA(cudaMalloc(&W.site_e, sizeof(double) * 2 * kMaxPassSites));
   FMC_CUDA(cudaMalloc(&W.counter, sizeof(unsigned)));
   FMC_CUDA(cudaMemset(W.counter, 0, sizeof(unsigned)));
-  FMC_CUDA(cudaMalloc(&W.result, sizeof(double) * 4));
-  FMC_CUDA(cudaMallocHost(&h_result, sizeof(double) * 64));
+  // the pass result goes straight to pinned host memory, which the kernel addresses through unified
+  // addressing: a copy back per pass cost as much as a third of the plain path's time
+  FMC_CUDA(cudaMallocHost(&W.result, sizeof(double) * 4));
   all_cap = sys.nf + gcap;
   FMC_CUDA(cudaMalloc(&all_atoms, sizeof(double4) * std::max(all_cap, 1)));
   recip_scratch_n = recip_scratch_doubles(dsys.view, all_cap);
@@ -531,8 +532,7 @@ int Chain::pass(int move, int g, int mol, const double* old_xyz, const double* n
   if (profile) cudaEventRecord(ev0, st);
   cudaError_t e = launch_pass(dsys.view, guest_view(), A, sk, sk_new, W, st);
   if (profile) cudaEventRecord(ev1, st);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(h_result, W.result, sizeof(double) * 3, cudaMemcpyDeviceToHost, st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // the kernel wrote the result to pinned memory
   if (e != cudaSuccess) return sync_error(e);
   if (profile) {
     float ms = 0.f;
@@ -540,9 +540,9 @@ int Chain::pass(int move, int g, int mol, const double* old_xyz, const double* n
     pass_ms += ms;
     pass_timed++;
   }
-  out[0] = h_result[0];
-  out[1] = h_result[1];
-  out[2] = h_result[2];
+  out[0] = W.result[0];
+  out[1] = W.result[1];
+  out[2] = W.result[2];
   passes++;
   return 0;
 }

@@ -53,7 +53,6 @@ class Chain {
   int* gtype = nullptr;
   int gcap = 0;
   PassScratch W{};
-  double* h_result = nullptr;  // pinned
   double* recip_scratch = nullptr;
   double* recip_parts = nullptr;
   size_t recip_scratch_n = 0;

@@ -25,7 +25,7 @@ struct PassScratch {
   double* recip_part;  // [ceil(K/256)]
   double* site_e;      // [2*kMaxPassSites]
   unsigned* counter;   // last-block ticket, left at zero by the kernel
-  double* result;      // {ewld1, ewld2, vdw}
+  double* result;      // {ewld1, ewld2, vdw} in pinned host memory, written by the kernel directly
 };
 
 struct CommitArgs {
