@@ -530,9 +530,22 @@ int Chain::pass(int move, int g, int mol, const double* old_xyz, const double* n
     cudaEventCreate(&ev1);
   }
   if (profile) cudaEventRecord(ev0, st);
+  pass_seq += 1.0;
+  A.seq = pass_seq;
   cudaError_t e = launch_pass(dsys.view, guest_view(), A, sk, sk_new, W, st);
   if (profile) cudaEventRecord(ev1, st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // the kernel wrote the result to pinned memory
+  if (e == cudaSuccess && !profile) {
+    // the kernel writes its energies and then this pass's sequence number into pinned host memory;
+    // waiting for the number is quicker than synchronising the stream.  The wait is bounded (well
+    // over a second), after which the stream is synchronised, which also reports a failed kernel.
+    volatile double* flag = W.result + 3;
+    long long spins = 0;
+    while (*flag != pass_seq && ++spins < 400000000LL) {
+    }
+    if (*flag != pass_seq) e = cudaStreamSynchronize(st);
+  } else if (e == cudaSuccess) {
+    e = cudaStreamSynchronize(st);  // profiled passes: the events need the stream
+  }
   if (e != cudaSuccess) return sync_error(e);
   if (profile) {
     float ms = 0.f;

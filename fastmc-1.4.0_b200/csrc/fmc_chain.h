@@ -83,6 +83,7 @@ class Chain {
   double despre = 0, presrate = 0;
   // launch accounting and optional CUDA-event timing of the pass kernel
   long long passes = 0, commits = 0;
+  double pass_seq = 0.0;  // sequence number the pass kernel echoes next to its energies
   bool profile = false;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double pass_ms = 0.0;

@@ -116,6 +116,8 @@ __global__ void __launch_bounds__(kPassThreads) fmc_pass_kernel(DevSystem S, Gue
     W.result[0] = ewld1;
     W.result[1] = e2;
     W.result[2] = ev;
+    __threadfence_system();  // the energies reach the host before the sequence number does
+    ((volatile double*)W.result)[3] = A.seq;
     *W.counter = 0u;
   }
 }

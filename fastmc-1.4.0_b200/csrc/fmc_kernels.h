@@ -16,6 +16,7 @@ struct PassArgs {
   int nold, nnew;
   int ex_lo, ex_hi;   // guest-site range of the moving molecule (excluded from real space)
   double engsic;      // self-interaction term of the species (ewald.f:87-93)
+  double seq;         // copied to result[3] after the energies, for a host that polls (0: none)
   double x[kMaxPassSites], y[kMaxPassSites], z[kMaxPassSites], q[kMaxPassSites];
   unsigned char type[kMaxPassSites];
 };
@@ -25,7 +26,7 @@ struct PassScratch {
   double* recip_part;  // [ceil(K/256)]
   double* site_e;      // [2*kMaxPassSites]
   unsigned* counter;   // last-block ticket, left at zero by the kernel
-  double* result;      // {ewld1, ewld2, vdw} in pinned host memory, written by the kernel directly
+  double* result;      // {ewld1, ewld2, vdw, seq} in pinned host memory, written by the kernel directly
 };
 
 struct CommitArgs {
