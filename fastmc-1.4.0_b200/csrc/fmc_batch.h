@@ -45,7 +45,7 @@ struct SysConst {
 // Per-chain parameters and mutable state (device memory).
 struct ChainDev {
   int sys;
-  int status;  // 0 ok; 75 guest capacity exhausted; 3 unsupported move drawn
+  int status;  // 0 ok; 75 guest capacity exhausted (the reference's error 75)
   int active;  // 0: an empty serving slot (the launch skips it)
   long long budget;  // total moves this chain is to run (0: unlimited)
   // parameters (CONTROL)

@@ -156,7 +156,8 @@ int init_chain_state(const InputDeck& d, const HostSystem& H, const double2* sk_
   C.lgchk = 1;
   C.active = 1;
   C.budget = 0;
-  // buffers: S(k) starts as the framework's (empty framework), guest segments per species
+  // buffers: S(k) starts as the system's (framework plus any guests the deck preloads), guest
+  // segments per species
   cudaError_t e = alloc((void**)&C.sk, sizeof(double2) * std::max(H.K, 1));
   if (e == cudaSuccess) e = cudaMemcpyAsync(C.sk, sk_src, sizeof(double2) * H.K, cudaMemcpyDeviceToDevice, st);
   int off = 0;
@@ -404,7 +405,7 @@ int Batch::restart(int c, const std::string& path, std::string& err) {
   C.production = r.production;
   if (C.production && C.eqsteps > 0) C.production = 0;  // gcmc.f:396-409
   if (C.eqsteps == 0) C.production = 1;                 // gcmc.f:553-554
-  // the system chain goes back to the empty framework for the next restart or inspection
+  // the system chain is left without guests: the batch's chains no longer read its state
   for (int g = 0; g < ng; g++) S.set_guests(g, 0, nullptr);
   return 0;
 }
@@ -652,7 +653,7 @@ int fmc_batch_run_shadow(fmc_batch* b, int moves, fmc_move_record* trace, double
   for (int i = 0; i < b->impl.nchains; i++) {
     const fmc::ChainDev& c = b->impl.h_chains[i];
     if (c.status) {
-      fmc::set_last_error(c.status == 75 ? "too many atoms in specified system" : "unsupported move drawn");
+      fmc::set_last_error(c.status == 75 ? "too many atoms in specified system" : "chain stopped with an unknown status");
       return c.status;
     }
   }
@@ -673,7 +674,7 @@ int fmc_batch_run(fmc_batch* b, int moves, fmc_move_record* trace, float* device
   for (int i = 0; i < b->impl.nchains; i++) {
     const fmc::ChainDev& c = b->impl.h_chains[i];
     if (c.status) {
-      fmc::set_last_error(c.status == 75 ? "too many atoms in specified system" : "unsupported move drawn");
+      fmc::set_last_error(c.status == 75 ? "too many atoms in specified system" : "chain stopped with an unknown status");
       return c.status;
     }
   }

@@ -508,7 +508,7 @@ class Server {
         Request& r = req(id);
         snapshot(i, r);
         r.state = C.status ? kRejected : kDone;
-        if (C.status) r.err = C.status == 75 ? "too many atoms in specified system" : "unsupported move drawn";
+        if (C.status) r.err = C.status == 75 ? "too many atoms in specified system" : "chain stopped with an unknown status";
         release(i);
         retired++;
       }

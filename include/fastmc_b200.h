@@ -3,8 +3,8 @@
  * Drop-in boundary for FastMC 1.4.0's energy routines.  Plain C types only: pointers, sizes,
  * int status codes.  Status: 0 = ok; > 0 = the reference's own error code (error.f: 3, 4, 25,
  * 52-55, 75, 95, 380, 410, 2311, 2312); < 0 = this library (-2 directive outside the path,
- * -3 move type outside the path, -4 cell convention outside imcon 1-3, -5 too many species,
- * -6 non-rigid framework, -100-e = CUDA error e).  fmc_last_error() gives the message of the
+ * -4 a cell without periodic boundaries (imcon 0), -5 too many species, -6 non-rigid
+ * framework, -100-e = CUDA error e).  fmc_last_error() gives the message of the
  * calling thread's last failure.
  *
  * Coordinates are Angstrom, interleaved x,y,z per site; energies follow the reference's
