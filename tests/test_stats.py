@@ -45,3 +45,22 @@ def test_report_block_matches_reference_output(tmp_path):
             assert g[:65] == r[:65] and abs(float(g[65:]) - float(r[65:])) < 2e-8, (g, r)
         else:
             assert g == r
+
+
+def test_report_for_a_mixture_has_each_species_and_the_selectivity(decks, tmp_path):
+    """Two guest species: a block per species, then one selectivity block for the pair
+    (gcmc.f:2052-2117 writes `guest j over guest i` for j < i)."""
+    import fastmc_b200
+
+    fs = np.zeros(1 + 14 * 2)
+    fs[0] = 5000
+    fs[1:6] = [3.0, -20.0, -65.0, 10.0, 420.0]
+    fs[15:20] = [1.5, -6.0, -10.0, 2.5, 40.0]
+    sel = np.array([[0.0, 0.0], [2.25, 0.0]])
+    out = tmp_path / "report"
+    fastmc_b200.write_report(decks["mixture"], fs, out, seltot=sel)
+    text = out.read_text()
+    assert text.count("Multiplier:") == 2 and text.count("Isosteric heat of adsorption") == 2
+    assert "guest  1 over guest  2" in text and "guest  2 over guest  1" not in text
+    line = next(ln for ln in text.split("\n") if "<S>:" in ln)
+    assert abs(float(line.split()[-1]) - 2.25) < 1e-9
