@@ -343,7 +343,9 @@ def run_batched(args, dist):
     t0 = time.perf_counter()
     dirs = make_batched_decks(tmp)
     n = len(dirs)
-    seeds = [(12, 34, 56, (78 + 7 * i + 13 * dist.rank) % 169) for i in range(n)]
+    from fastmc_b200 import synth
+
+    seeds = [synth.batched_seed(i, dist.rank) for i in range(n)]
     # neighbour-list voxel edge: the autotuner times throwaway batches of the same chains
     tune = None
     edge = args.voxel_edge
@@ -372,6 +374,13 @@ def run_batched(args, dist):
     t_wall = dist.max(wall)
     moves = n * args.moves * args.steps
     total_moves = dist.sum(moves)
+    # load balance of the last timed launch: every CTA's own time on the device clock
+    tm = b.timing()
+    cta_ms = (tm[:, 1] - tm[:, 0]) / 1e6
+    balance = {"cta_ms_max": float(cta_ms.max()), "cta_ms_mean": float(cta_ms.mean()),
+               "cta_ms_min": float(cta_ms.min()), "max_over_mean": float(cta_ms.max() / cta_ms.mean()),
+               "launch_span_ms": float((tm[:, 1].max() - tm[:, 0].min()) / 1e6),
+               "sms_used": int(len(set(tm[:, 2].tolist())))}
     # algorithmic bytes of one launch: every move of every chain reads S(k), akk and writes
     # S_new (40 B per k-vector) and reads its sites' neighbours within rcut (36 B each)
     per_launch = 0.0
@@ -405,7 +414,7 @@ def run_batched(args, dist):
         "config": {"workload": BATCHED_WORKLOAD, "chains": n, "moves_per_chain_per_step": args.moves,
                    "guests_mean": float(np.mean([s["nmol0"] for s in states])),
                    "K_range": [int(min(i["K"] for i in infos.values())), int(max(i["K"] for i in infos.values()))],
-                   "setup_s": setup_s, "voxel_edge_A": edge,
+                   "setup_s": setup_s, "voxel_edge_A": edge, "load_balance": balance,
                    "voxel_autotune_ms": tune,
                    "l2": "per-chain S(k) is shared-memory resident; frameworks + voxel lists exceed L2 (no flush)",
                    "parallelism": f"replicas{dist.world}"},
@@ -415,7 +424,7 @@ def run_batched(args, dist):
                      "peak_kind": f"{peak_kind} (hbm_gbs)"},
         "gpu_launches": args.steps,
         "e2e": {"value": total_moves / t_wall, "unit": "moves/s", "h2d_bytes_per_step": n * cb,
-                "d2h_bytes_per_step": n * cb},
+                "d2h_bytes_per_step": n * (cb + 24)},
         "clocks": clk.summary(),
     }
     if dist.rank == 0 and dist.world == 1 and not args.skip_baselines:

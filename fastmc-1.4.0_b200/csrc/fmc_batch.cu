@@ -508,6 +508,13 @@ __device__ __forceinline__ void lrc_warp(const ChainDev& C, const SysConst& Y, M
   }
 }
 
+// Device clock in nanoseconds (%globaltimer: one time base for every SM, unlike clock64).
+__device__ __forceinline__ long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return (long long)t;
+}
+
 // One real-space candidate: a framework atom from a site's voxel list or a guest site.
 struct Cand {
   double4 a;
@@ -808,6 +815,7 @@ __global__ void __launch_bounds__(kBatchThreads, 2) fmc_batch_kernel(BatchLaunch
   const int tid = threadIdx.x, cidx = blockIdx.x, warp = tid >> 5, lane = tid & 31;
   if (cidx >= L.nchains) return;
   if (!L.chains[cidx].active) return;
+  const long long t_start = L.timing && tid == 0 ? global_ns() : 0;
   {
     const int* src = reinterpret_cast<const int*>(&L.chains[cidx]);
     int* dst = reinterpret_cast<int*>(&C);
@@ -1011,6 +1019,13 @@ __global__ void __launch_bounds__(kBatchThreads, 2) fmc_batch_kernel(BatchLaunch
     const int* src = reinterpret_cast<const int*>(&C);
     int* dst = reinterpret_cast<int*>(&L.chains[cidx]);
     for (int i = tid; i < (int)(sizeof(ChainDev) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
+  }
+  if (L.timing && tid == 0) {
+    unsigned sm;
+    asm volatile("mov.u32 %0, %%smid;" : "=r"(sm));
+    L.timing[3 * cidx] = t_start;
+    L.timing[3 * cidx + 1] = global_ns();
+    L.timing[3 * cidx + 2] = sm;
   }
 }
 

@@ -102,6 +102,7 @@ struct BatchLaunch {
   long long recompute_every;  // mixed: moves between FP64 recomputes of S(k) (0: never)
   double* shadow;     // mixed, optional [nchains][moves][4]: FP64 {ewld1, ewld2, vdw, dE} of every
                       // move on the same state
+  long long* timing;  // optional [nchains][3]: the CTA's start and end (%globaltimer, ns) and its SM
 };
 
 cudaError_t launch_batch(const BatchLaunch& L, int smem_bytes, int tab_stride, cudaStream_t st);
@@ -170,6 +171,8 @@ class Batch {
   long long recompute_every = 0;
   double* d_shadow = nullptr;
   size_t shadow_cap = 0;
+  long long* d_timing = nullptr;  // per chain {start ns, end ns, SM} of the last launch
+  long long* h_timing = nullptr;  // pinned host copy
   int nchains = 0;
   ~Batch();
   int open(const std::vector<std::string>& dirs, const std::vector<int>& seeds, int device, std::string& err,

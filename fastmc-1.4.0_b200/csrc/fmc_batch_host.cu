@@ -234,6 +234,7 @@ Batch::~Batch() {
     if (d_trace) cudaFree(d_trace);
     if (d_shadow) cudaFree(d_shadow);
     if (h_chains) cudaFreeHost(h_chains);
+    if (h_timing) cudaFreeHost(h_timing);
     cudaStreamDestroy(st);
   }
 }
@@ -308,6 +309,11 @@ int Batch::open(const std::vector<std::string>& dirs, const std::vector<int>& se
   if (e == cudaSuccess) e = cudaMalloc(&d_chains, sizeof(ChainDev) * nchains);
   if (e == cudaSuccess) allocations.push_back(d_chains);
   if (e == cudaSuccess) e = cudaMemcpy(d_chains, h_chains, sizeof(ChainDev) * nchains, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMalloc(&d_timing, sizeof(long long) * 3 * nchains);
+  if (e == cudaSuccess) allocations.push_back(d_timing);
+  if (e == cudaSuccess) e = cudaMemset(d_timing, 0, sizeof(long long) * 3 * nchains);
+  if (e == cudaSuccess) e = cudaMallocHost(&h_timing, sizeof(long long) * 3 * nchains);
+  if (e == cudaSuccess) std::memset(h_timing, 0, sizeof(long long) * 3 * nchains);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) {
     err = std::string("batch upload failed: ") + cudaGetErrorString(e);
@@ -483,6 +489,7 @@ int Batch::run(int moves, MoveRecord* trace_host, float* ms, std::string& err, d
   L.recompute_every = recompute_every;
   L.trace = nullptr;
   L.shadow = nullptr;
+  L.timing = d_timing;
   cudaError_t e = cudaSuccess;
   if (shadow_host && mixed) {
     size_t need = (size_t)nchains * moves;
@@ -519,6 +526,8 @@ int Batch::run(int moves, MoveRecord* trace_host, float* ms, std::string& err, d
     e = cudaMemcpyAsync(shadow_host, d_shadow, sizeof(double) * 4 * (size_t)nchains * moves, cudaMemcpyDeviceToHost,
                         st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(h_chains, d_chains, cb, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(h_timing, d_timing, sizeof(long long) * 3 * nchains, cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   float t = 0.f;
   if (e == cudaSuccess) cudaEventElapsedTime(&t, a, b);
@@ -713,6 +722,15 @@ int fmc_batch_chain_state(fmc_batch* b, int chain, double* out) {
   v[37] = (double)C.recomputes;
   v[38] = C.lgchk ? 0.0 : 1.0;
   std::memcpy(out, v, sizeof(v));
+  return 0;
+}
+
+int fmc_batch_chain_timing(fmc_batch* b, int chain, long long* out) {
+  if (!b || chain < 0 || chain >= b->impl.nchains || !out) {
+    fmc::set_last_error("bad batch handle or chain index");
+    return -1;
+  }
+  for (int k = 0; k < 3; k++) out[k] = b->impl.h_timing ? b->impl.h_timing[3 * chain + k] : 0;
   return 0;
 }
 

@@ -1,4 +1,5 @@
 // Chain: device upload, single-point set-up and the plain-path host move loop.
+#include <atomic>
 #include "fmc_chain.h"
 #include "fmc_restart.h"
 
@@ -542,6 +543,8 @@ int Chain::pass(int move, int g, int mol, const double* old_xyz, const double* n
     long long spins = 0;
     while (*flag != pass_seq && ++spins < 400000000LL) {
     }
+    // the energies were written before the number: read them only after the number (acquire)
+    std::atomic_thread_fence(std::memory_order_acquire);
     if (*flag != pass_seq) e = cudaStreamSynchronize(st);
   } else if (e == cudaSuccess) {
     e = cudaStreamSynchronize(st);  // profiled passes: the events need the stream

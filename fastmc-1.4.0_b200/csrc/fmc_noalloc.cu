@@ -77,10 +77,12 @@ __global__ void __launch_bounds__(kNoAllocThreads)
     n = lmn[3 * k + 2];
   }
   int am = m < 0 ? -m : m, an = n < 0 ? -n : n;
-  // a k-vector outside the kmax the caller declared would index past the phase tables
+  // a k-vector outside the kmax the caller declared would index past the phase tables: its
+  // S_new is S and its energy term NaN, so the pass energy comes back NaN
   if (k < P.K && (l < 0 || l > k1 || am > k2 || an > k3)) {
     sk_new[2 * k] = sk[2 * k];
     sk_new[2 * k + 1] = sk[2 * k + 1];
+    v[0] = __longlong_as_double(0x7ff8000000000000LL);
   } else if (k < P.K) {
     double2 aold = make_double2(0.0, 0.0), anew = make_double2(0.0, 0.0);
     for (int s = 0; s < nsite; s++) {
@@ -208,15 +210,17 @@ int fmc_ewald1_guest_noalloc(int K, const int* kmax, const double* cell, const i
     P.q[s] = sites[4 * s + 3];
   }
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  // the ticket must start at zero: clear it in stream order before the launch
-  cudaError_t e = cudaMemsetAsync(scratch + kNoAllocMaxBlocks, 0, sizeof(double), st);
-  if (e != cudaSuccess) return reject(-100 - (int)e, std::string("clearing scratch: ") + cudaGetErrorString(e));
+  // every check before the first device-side effect: a rejected call leaves the scratch alone
   int smem = (nold + nnew) * ((kmax[0] + 1) + (kmax[1] + 1) + (kmax[2] + 1)) * (int)sizeof(double2);
   if (smem > 200 * 1024) return reject(-7, "sites x (kmax1+kmax2+kmax3+3) phase table exceeds 200 KB of shared memory");
+  cudaError_t e = cudaSuccess;
   if (smem > 48 * 1024) {
     e = cudaFuncSetAttribute(fmc_recip_pass_noalloc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return reject(-100 - (int)e, cudaGetErrorString(e));
   }
+  // the ticket must start at zero: clear it in stream order before the launch
+  e = cudaMemsetAsync(scratch + kNoAllocMaxBlocks, 0, sizeof(double), st);
+  if (e != cudaSuccess) return reject(-100 - (int)e, std::string("clearing scratch: ") + cudaGetErrorString(e));
   fmc_recip_pass_noalloc_kernel<<<P.nbk, kNoAllocThreads, smem, st>>>(P, d_lmn, d_akk, d_sk, d_sk_new, d_engcpe,
                                                                       scratch);
   e = cudaGetLastError();

@@ -336,6 +336,14 @@ class Batch:
         check(lib().fmc_batch_chain_state(self.h, int(chain), dp(out)))
         return dict(zip(self._STATE, out.tolist()))
 
+    def timing(self):
+        """Per chain of the last run: CTA start and end on the device clock (ns) and the SM it
+        ran on, as an (n, 3) int64 array."""
+        out = np.zeros((self.n, 3), dtype=np.int64)
+        for c in range(self.n):
+            check(lib().fmc_batch_chain_timing(self.h, c, out[c].ctypes.data_as(ctypes.POINTER(ctypes.c_longlong))))
+        return out
+
     def pressures(self, chain):
         ng = self._ng(chain)
         out = np.zeros(ng + 1)

@@ -55,6 +55,7 @@ SIGNATURES = {
     "fmc_batch_set_precision": (_ci, [_vp, _ci, ctypes.c_longlong]),
     "fmc_batch_run_shadow": (_ci, [_vp, _ci, _vp, _vp, ctypes.POINTER(ctypes.c_float)]),
     "fmc_batch_chain_state": (_ci, [_vp, _ci, _dp]),
+    "fmc_batch_chain_timing": (_ci, [_vp, _ci, ctypes.POINTER(ctypes.c_longlong)]),
     "fmc_batch_guest_coords": (_ci, [_vp, _ci, _ci, _dp, _ip, _ip]),
     "fmc_revive_write_state": (_ci, [ctypes.c_char_p, ctypes.c_char_p, _ci, _ip, _dp, _dp, _dp, ctypes.c_double]),
     "fmc_revive_read": (_ci, [ctypes.c_char_p, ctypes.c_char_p, _ip, _ip, _dp, _dp, _dp, _ip]),

@@ -293,8 +293,9 @@ def batched_frameworks(n=16, seed=2024, rho=0.025, lo=18.0, hi=52.0, rcut=RCUT):
 
 
 def write_batched(root, n_frameworks=16, n_pressures=16, gases=("CO2",), fractions=(1.0,), total_bar=None,
-                  cycles=5000, temp=298.0, seed=2024):
-    """Write one input directory per chain: root/chain_FFF_PP.  Returns the list of dirs."""
+                  cycles=5000, temp=298.0, seed=2024, select=None):
+    """Write one input directory per chain: root/chain_FFF_PP (chain index F * n_pressures + P).
+    Returns the list of dirs; with `select` (chain indices) only those chains, in that order."""
     fws = batched_frameworks(n_frameworks, seed=seed)
     dirs = []
     pressures = np.logspace(-2, 1, n_pressures)
@@ -302,13 +303,23 @@ def write_batched(root, n_frameworks=16, n_pressures=16, gases=("CO2",), fractio
         L = np.diag(fw.cell)
         kmax = tuple(kmax_for(l) for l in L)
         for p_i, p in enumerate(pressures):
+            if select is not None and f * n_pressures + p_i not in select:
+                continue
             tot = p if total_bar is None else total_bar
             parts = [tot * fr for fr in fractions]
             d = os.path.join(root, f"chain_{f:03d}_{p_i:02d}")
             write_inputs(d, fw, list(gases), parts, temp, kmax, eq_cycles=-cycles, prod_cycles=-cycles,
                          title=f"synthetic orthorhombic framework {f} ({fw.natoms} atoms)")
             dirs.append(d)
+    if select is not None:
+        order = {int(os.path.basename(d)[6:9]) * n_pressures + int(d[-2:]): d for d in dirs}
+        return [order[i] for i in select]
     return dirs
+
+
+def batched_seed(i, rank=0):
+    """duni seed of chain i of the 256-chain batched workload on a rank."""
+    return (12, 34, 56, (78 + 7 * i + 13 * rank) % 169)
 
 
 def serving_requests(n, seed=7, rate_hz=50.0):

@@ -213,6 +213,10 @@ int fmc_batch_profile(fmc_batch* b, int enable);
  * (thread 0's share) k-space, + real space, move selection, trial generation, then FP64
  * re-evaluations and S(k) recomputes (mixed precision), then 1 once the chain has finished. */
 int fmc_batch_chain_state(fmc_batch* b, int chain, double* out);
+/* Load balance of the last run (no counterpart in the reference): out[0..2] = the chain's CTA
+ * start and end on the device clock (%globaltimer, ns) and the SM it ran on.  Recorded on every
+ * run (two clock reads per CTA); 0 for a chain that has not run. */
+int fmc_batch_chain_timing(fmc_batch* b, int chain, long long* out);
 int fmc_batch_guest_coords(fmc_batch* b, int chain, int iguest, double* xyz, int* nmol, int* nsite);
 /* Checkpoint / restart of one chain of a batch (formats as fmc_chain_write_revive).  A restart
  * before the chain's first run matches the reference's restart, which re-seeds duni. */
@@ -287,6 +291,8 @@ int fmc_run_timed(fmc_chain* c, int nmoves, fmc_move_record* trace, float* devic
  *   host arrays kmax[3], cell[9] (cell vectors a,b,c), sites[4*(nold+nnew)] (x,y,z,q; the nold
  *   old sites first); recip_pref = 2*(2 pi/V)*r4pie0, engsic the species' self term.
  * move: FMC_INSERT (nold = 0), FMC_DELETE (nnew = 0) or FMC_DISPLACE (both, one fused pass).
+ * Every k-vector of d_lmn must lie inside kmax (|l|,|m|,|n| <= kmax[0..2]); one outside makes the
+ * pass energy NaN (the call itself cannot see the device-side table and returns 0).
  * Scratch is a fixed array in the library image sized for K <= 32768 and 1..100 sites; larger
  * requests are rejected (status -7, message in fmc_last_error()).  The first call on a device
  * looks up that array's address and should come before any stream capture.  All calls share
