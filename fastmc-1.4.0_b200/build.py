@@ -25,9 +25,9 @@ NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--ex
 CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-Wall", "-Wno-unused-function", f"-I{INCLUDE}", f"-I{CSRC}",
             "-I/usr/local/cuda/include"]
 
-SOURCES = ["fmc_inputs.cpp", "fmc_restart.cpp", "fmc_system.cpp", "fmc_kernels.cu", "fmc_chain.cu", "fmc_api.cu", "fmc_noalloc.cu", "fmc_batch.cu",
+SOURCES = ["fmc_inputs.cpp", "fmc_desc.cpp", "fmc_restart.cpp", "fmc_system.cpp", "fmc_kernels.cu", "fmc_chain.cu", "fmc_api.cu", "fmc_noalloc.cu", "fmc_batch.cu",
            "fmc_batch_host.cu", "fmc_slot.cu", "fmc_serve.cu"]
-HEADERS = ["fmc_common.h", "fmc_inputs.h", "fmc_system.h", "fmc_device.cuh", "fmc_kernels.h", "fmc_chain.h", "fmc_batch.h", "fmc_restart.h"]
+HEADERS = ["fmc_common.h", "fmc_inputs.h", "fmc_desc.h", "fmc_system.h", "fmc_device.cuh", "fmc_kernels.h", "fmc_chain.h", "fmc_batch.h", "fmc_restart.h"]
 
 
 def _newest_header():

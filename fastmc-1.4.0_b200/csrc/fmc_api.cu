@@ -5,6 +5,7 @@
 
 #include "../../include/fastmc_b200.h"
 #include "fmc_chain.h"
+#include "fmc_desc.h"
 #include "fmc_restart.h"
 
 struct fmc_chain {
@@ -49,6 +50,46 @@ int fmc_chain_open(const char* dir, const int* seed, int device, fmc_chain** out
 }
 
 void fmc_chain_close(fmc_chain* c) { delete c; }
+
+int fmc_chain_create(const fmc_system_desc* desc, const int* seed, int device, fmc_chain** out) {
+  if (!desc || !seed || !out) return fail(-1, "null argument");
+  *out = nullptr;
+  fmc::InputDeck deck;
+  std::string err;
+  int rc = fmc::deck_from_desc(*desc, deck, err);
+  if (rc) return fail(rc, err);
+  fmc::HostSystem h;
+  rc = fmc::build_host_system(deck, h, err);
+  if (rc) return fail(rc, err);
+  fmc_chain* c = new fmc_chain();
+  rc = c->impl.open_prepared(std::move(h), seed, device, err);
+  if (rc) {
+    delete c;
+    return fail(rc, err);
+  }
+  *out = c;
+  return 0;
+}
+
+int fmc_deck_describe(const char* dir, fmc_system_desc* out) {
+  if (!dir || !out) return fail(-1, "null argument");
+  std::string err;
+  int rc = fmc::describe_deck(dir, *out, err);
+  if (rc) return fail(rc, err);
+  return 0;
+}
+
+void fmc_desc_free(fmc_system_desc* desc) {
+  if (desc && desc->owner) fmc::free_desc(*desc);
+}
+
+int fmc_desc_sizes(int* out) {
+  if (!out) return fail(-1, "null argument");
+  out[0] = (int)sizeof(fmc_system_desc);
+  out[1] = (int)sizeof(fmc_guest_desc);
+  out[2] = (int)sizeof(fmc_vdw_desc);
+  return 0;
+}
 
 int fmc_chain_info(fmc_chain* c, int* ints, double* dbls) {
   CHECK_CHAIN(c);
@@ -174,6 +215,43 @@ int fmc_commit(fmc_chain* c, int move, int iguest, int mol, const double* xyz) {
 int fmc_reject(fmc_chain* c) {
   CHECK_CHAIN(c);
   return 0;
+}
+
+namespace {
+// x[n], y[n], z[n] -> interleaved x,y,z (the layout of the calls above)
+bool interleave(int n, const double* x, const double* y, const double* z, double* out) {
+  if (n < 0 || n > fmc::kMaxGuestSites || !x || !y || !z) return false;
+  for (int i = 0; i < n; i++) {
+    out[3 * i] = x[i];
+    out[3 * i + 1] = y[i];
+    out[3 * i + 2] = z[i];
+  }
+  return true;
+}
+}  // namespace
+
+int fmc_ewald1_guest_xyz(fmc_chain* c, int iguest, int natms, const double* x, const double* y, const double* z,
+                         int move, int pass, double* engcpe) {
+  double xyz[3 * fmc::kMaxGuestSites];
+  if (!interleave(natms, x, y, z, xyz)) return fail(-1, "null coordinate array or site count out of range");
+  return fmc_ewald1_guest(c, iguest, natms, xyz, move, pass, engcpe);
+}
+
+int fmc_guest_realspace_xyz(fmc_chain* c, int iguest, int natms, const double* x, const double* y, const double* z,
+                            int mol, double* ewld2, double* vdw) {
+  double xyz[3 * fmc::kMaxGuestSites];
+  if (!interleave(natms, x, y, z, xyz)) return fail(-1, "null coordinate array or site count out of range");
+  return fmc_guest_realspace(c, iguest, natms, xyz, mol, ewld2, vdw);
+}
+
+int fmc_commit_xyz(fmc_chain* c, int move, int iguest, int mol, const double* x, const double* y, const double* z) {
+  CHECK_CHAIN(c);
+  if (move == FMC_DELETE) return fmc_commit(c, move, iguest, mol, nullptr);
+  if (iguest < 0 || iguest >= (int)c->impl.sp.size()) return fail(-1, "species index out of range");
+  double xyz[3 * fmc::kMaxGuestSites];
+  if (!interleave(c->impl.sp[iguest].nsite, x, y, z, xyz))
+    return fail(-1, "null coordinate array or site count out of range");
+  return fmc_commit(c, move, iguest, mol, xyz);
 }
 
 int fmc_set_guests(fmc_chain* c, int iguest, int nmol, const double* xyz) {
@@ -492,15 +570,13 @@ int fmc_deck_vdw(const char* dir, int k, double* out, int* ntables) {
   return 0;
 }
 
-int fmc_deck_inspect(const char* dir, int* ints, double* dbls, int* lmn, double* akk, double* erc, double* charges,
-                     int* K, int* nerc) {
-  if (!dir) return fail(-1, "null argument");
-  fmc::InputDeck deck;
-  std::string err;
-  int rc = fmc::read_input_deck(dir, deck, err);
-  if (rc) return fail(rc, err);
+namespace {
+// Host tables of a deck: what fmc_deck_inspect and fmc_desc_inspect report.
+int inspect_deck(const fmc::InputDeck& deck, int* ints, double* dbls, int* lmn, double* akk, double* erc,
+                 double* charges, int* K, int* nerc, double* vvv, int* ntables) {
   fmc::HostSystem S;
-  rc = fmc::build_host_system(deck, S, err);
+  std::string err;
+  int rc = fmc::build_host_system(deck, S, err);
   if (rc) return fail(rc, err);
   int nv = S.nvox[0] * S.nvox[1] * S.nvox[2];
   int natoms = S.nf;
@@ -523,9 +599,33 @@ int fmc_deck_inspect(const char* dir, int* ints, double* dbls, int* lmn, double*
     for (int i = 0; i <= S.mxgrid; i++) erc[i] = S.erc[i];
   if (charges)
     for (int i = 0; i < S.nf; i++) charges[i] = S.fq[i];
+  if (vvv)  // rows 1..ntables, mxgrid+1 values each
+    std::memcpy(vvv, S.vvv.data() + (S.mxgrid + 1), sizeof(double) * (size_t)S.ntables * (S.mxgrid + 1));
   if (K) *K = S.K;
   if (nerc) *nerc = S.mxgrid + 1;
+  if (ntables) *ntables = S.ntables;
   return 0;
+}
+}  // namespace
+
+int fmc_deck_inspect(const char* dir, int* ints, double* dbls, int* lmn, double* akk, double* erc, double* charges,
+                     int* K, int* nerc) {
+  if (!dir) return fail(-1, "null argument");
+  fmc::InputDeck deck;
+  std::string err;
+  int rc = fmc::read_input_deck(dir, deck, err);
+  if (rc) return fail(rc, err);
+  return inspect_deck(deck, ints, dbls, lmn, akk, erc, charges, K, nerc, nullptr, nullptr);
+}
+
+int fmc_desc_inspect(const fmc_system_desc* desc, int* ints, double* dbls, int* lmn, double* akk, double* erc,
+                     double* charges, int* K, int* nerc, double* vvv, int* ntables) {
+  if (!desc) return fail(-1, "null argument");
+  fmc::InputDeck deck;
+  std::string err;
+  int rc = fmc::deck_from_desc(*desc, deck, err);
+  if (rc) return fail(rc, err);
+  return inspect_deck(deck, ints, dbls, lmn, akk, erc, charges, K, nerc, vvv, ntables);
 }
 
 }  // extern "C"

@@ -765,6 +765,64 @@ void read_control(const std::string& dir, InputDeck& d) {
 
 }  // namespace
 
+int finish_deck_from_arrays(InputDeck& d, std::string& err) {
+  try {
+    const int nt = (int)d.types.size();
+    if (d.imcon < 1 || d.imcon > 7) raise(-4, "the device path needs periodic boundaries (imcon 1-7)");
+    if (!(d.rcut > 0.0)) raise(-1, "cut-off must be positive");
+    if (!(d.alpha > 0.0) || d.kmax[0] < 1 || d.kmax[1] < 1 || d.kmax[2] < 1)
+      raise(2311, "GCMC sim needs ewald (alpha and kmax) specified");
+    if (nt < 1) raise(4, "no atom types");
+    const double* c = d.cell;
+    auto bad = [] { raise(410, "cell not consistent with image convention"); };
+    if (d.imcon == 1 || d.imcon == 4 || d.imcon == 5) {
+      double axx = (std::fabs(c[0]) + std::fabs(c[4])) / 2.0, test = 1e-8 * axx;
+      if (std::fabs(c[0] - axx) > test || std::fabs(c[4] - axx) > test) bad();
+      double want = d.imcon == 5 ? axx * std::sqrt(2.0) : axx;
+      if (std::fabs(c[8] - want) > test) bad();
+    }
+    if (d.imcon == 7 && std::fabs(c[0] - std::sqrt(3.0) * c[4]) >= 1e-6) bad();
+    if (d.imcon == 6 && (std::fabs(c[2]) > 1e-10 || std::fabs(c[5]) > 1e-10 || std::fabs(c[6]) > 1e-10 ||
+                         std::fabs(c[7]) > 1e-10))
+      bad();
+    if (d.imcon == 1 || d.imcon == 2 || d.imcon == 4 || d.imcon == 5 || d.imcon == 7)
+      for (int i : {1, 2, 3, 5, 6, 7})
+        if (std::fabs(c[i]) > 1e-10) bad();
+    double cp[10];
+    cell_props(d.cell, cp);
+    d.volm = volume_of(d.imcon, cp);
+    if (d.rcut > half_width(d, cp)) raise(95, "potential cutoff exceeds half-cell width");
+    if (!(d.rvdw > 0.0)) d.rvdw = d.rcut;
+    d.keyfce = 2;
+    d.maxvdw = std::max(d.ntpvdw, (nt * (nt + 1)) / 2);
+    d.mxgrid = std::max(1000, (int)(d.rvdw / 0.01 + 0.5) + 4);  // utility_pack.f:725
+    // pair tables: every pair without a line of its own gets the zero table (vdw_terms.f:160-182)
+    if ((int)d.ltpvdw.size() != d.ntpvdw + 1 || (int)d.prmvdw.size() != d.ntpvdw + 1 ||
+        (int)d.lstvdw.size() != (nt * (nt + 1)) / 2 + 1)
+      raise(-1, "vdW tables sized inconsistently with the pair count");
+    d.ltpvdw.resize(d.maxvdw + 2, -1);
+    d.prmvdw.resize(d.maxvdw + 2, {0, 0, 0, 0, 0});
+    d.lstvdw.resize(d.maxvdw + 2, 0);
+    const int ntab = nt * (nt + 1) / 2;
+    if (d.ntpvdw < ntab)
+      for (int i = 1; i <= ntab; i++)
+        if (d.lstvdw[i] == 0) d.lstvdw[i] = d.ntpvdw + 1;
+    for (int t : d.ftype)
+      if (t < 1 || t > nt) raise(4, "framework atom of an unknown type");
+    for (const GuestSpecies& g : d.guests) {
+      if (g.nsite < 1 || g.nsite > 50) raise(75, "guest site count outside 1-50");
+      for (int t : g.type)
+        if (t < 1 || t > nt) raise(4, "guest site of an unknown type");
+    }
+    if (d.temp <= 0.0) raise(380, "simulation temperature not specified");
+    d.nnumg = d.eqsteps > 1000 ? d.eqsteps / 1000 : 1;
+    return 0;
+  } catch (const InputError& e) {
+    err = e.msg;
+    return e.code;
+  }
+}
+
 int read_input_deck(const std::string& dir, InputDeck& d, std::string& err) {
   try {
     d = InputDeck();

@@ -81,4 +81,12 @@ struct InputDeck {
 // negative code.
 int read_input_deck(const std::string& dir, InputDeck& deck, std::string& err);
 
+// A deck whose arrays a caller filled in memory (the state the reference's module arrays hold
+// after readfield / readconfig / readcontrol): checks the cell against its image convention and
+// the cut-off against the half-cell width as readconfig does, then derives the volume, mxgrid,
+// the vdW pair-table map (undefined pairs -> the zero table) and the numguests interval.
+// Expects types, framework and guest arrays, ntpvdw with ltpvdw / prmvdw [ntpvdw+1] and lstvdw
+// [ntypes*(ntypes+1)/2+1] (0 = no line), cell, imcon, alpha, kmax, rcut and the control fields.
+int finish_deck_from_arrays(InputDeck& d, std::string& err);
+
 }  // namespace fmc

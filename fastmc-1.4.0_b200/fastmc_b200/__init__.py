@@ -14,7 +14,7 @@ from . import _lib
 from ._lib import (DELETE, DISPLACE, INSERT, JUMP, MOVE_DTYPE, MULTIJUMP, NOOP, ROTATE, TRANSLATE, FastMCError, check,
                    dp, ip, lib)
 
-__all__ = ["Chain", "Batch", "Server", "deck_inspect", "FastMCError", "INSERT", "DELETE", "DISPLACE", "TRANSLATE", "ROTATE",
+__all__ = ["Chain", "SystemDesc", "Batch", "Server", "deck_inspect", "FastMCError", "INSERT", "DELETE", "DISPLACE", "TRANSLATE", "ROTATE",
            "MOVE_DTYPE"]
 
 _INFO_INTS = ["imcon", "kmax1", "kmax2", "kmax3", "K", "natoms", "nspecies", "ntypes", "mxgrid", "nframework",
@@ -96,13 +96,105 @@ def _prob(call):
     return out
 
 
+class SystemDesc:
+    """A system handed over as arrays (fmc_system_desc): what the reference's module arrays hold
+    once its readers have run.  `from_deck` reads a deck directory into one (arrays owned by the
+    library); `from_arrays` builds one from the caller's own arrays (kept alive here)."""
+
+    def __init__(self):
+        self.s = _lib.SystemDescStruct()
+        self._keep = []
+        self._owned = False
+
+    @classmethod
+    def from_deck(cls, directory):
+        d = cls()
+        check(lib().fmc_deck_describe(str(directory).encode(), ctypes.byref(d.s)))
+        d._owned = True
+        return d
+
+    @classmethod
+    def from_arrays(cls, imcon, cell, alpha, kmax, rcut, types, fw_xyz, fw_charge, fw_type, guests, vdw, temperature,
+                    eq_steps, prod_steps, delr=1.0, engunit=418.4, fw_mass=None, max_guest_atoms=0,
+                    averaging_window=0, rota_ratio=0.5):
+        """types: names; fw_type and guest types 1-based.  guests: dicts with name, mass, charge,
+        template (nsite, 3, centred on the mass centre), type, pressure_pa, move_freq (9), and
+        optionally xyz (nmol, nsite, 3), disp_ratio, tran_ratio.  vdw: (type_i, type_j, form,
+        prm[5]) with energies in internal units (10 J/mol)."""
+        d = cls()
+        s = d.s
+        s.imcon = int(imcon)
+        s.cell[:] = [float(v) for v in np.asarray(cell, dtype=np.float64).reshape(-1)]
+        s.alpha = float(alpha)
+        s.kmax[:] = [int(k) for k in kmax]
+        s.rcut, s.rvdw, s.delr, s.engunit = float(rcut), 0.0, float(delr), float(engunit)
+        names = (ctypes.c_char_p * len(types))(*[t.encode() for t in types])
+        s.ntypes, s.type_names = len(types), names
+        arr = lambda a, t=np.float64: d.keep(np.ascontiguousarray(a, dtype=t))  # noqa: E731
+        fx, fq, ft = arr(np.asarray(fw_xyz).reshape(-1)), arr(fw_charge), arr(fw_type, np.int32)
+        s.nframework = len(fq)
+        s.fw_xyz, s.fw_charge, s.fw_type = dp(fx), dp(fq), ip(ft)
+        if fw_mass is not None:
+            s.fw_mass = dp(arr(fw_mass))
+        gd = (_lib.GuestDesc * len(guests))()
+        for g, G in zip(gd, guests):
+            t = np.asarray(G["template"], dtype=np.float64).reshape(-1, 3)
+            g.name = d.keep(G.get("name", "guest").encode())
+            g.nsite = len(t)
+            g.mass, g.charge = dp(arr(G["mass"])), dp(arr(G["charge"]))
+            g.tx, g.ty, g.tz = dp(arr(t[:, 0])), dp(arr(t[:, 1])), dp(arr(t[:, 2]))
+            g.type = ip(arr(G["type"], np.int32))
+            xyz = G.get("xyz")
+            g.nmols = 0 if xyz is None else int(np.asarray(xyz).shape[0])
+            if g.nmols:
+                g.xyz = dp(arr(np.asarray(xyz).reshape(-1)))
+            g.pressure_pa = float(G["pressure_pa"])
+            g.move_freq[:] = [float(v) for v in G["move_freq"]]
+            g.disp_ratio, g.tran_ratio = float(G.get("disp_ratio", 0.5)), float(G.get("tran_ratio", 0.5))
+        s.nguest, s.guests = len(guests), gd
+        vd = (_lib.VdwDesc * max(len(vdw), 1))()
+        for v, (i, j, form, prm) in zip(vd, vdw):
+            v.type_i, v.type_j, v.form = int(i), int(j), int(form)
+            v.prm[:] = [float(x) for x in prm]
+        s.nvdw, s.vdw = len(vdw), vd
+        s.temperature, s.eq_steps, s.prod_steps = float(temperature), int(eq_steps), int(prod_steps)
+        s.max_guest_atoms, s.averaging_window, s.rota_ratio = int(max_guest_atoms), int(averaging_window), rota_ratio
+        d._keep += [names, gd, vd]
+        return d
+
+    def keep(self, obj):
+        self._keep.append(obj)
+        return obj
+
+    def set_guests(self, g, xyz):
+        """Replace the molecules of species g present at creation: xyz (nmol, nsite, 3)."""
+        a = self.keep(np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1))
+        self.s.guests[g].nmols = int(np.asarray(xyz).shape[0])
+        self.s.guests[g].xyz = dp(a) if len(a) else ctypes.POINTER(ctypes.c_double)()
+
+    def free(self):
+        if self._owned:
+            lib().fmc_desc_free(ctypes.byref(self.s))
+            self._owned = False
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
 class Chain:
-    """One GCMC chain on one GPU (the plain FP64 path)."""
+    """One GCMC chain on one GPU (the plain FP64 path), opened from a deck directory or created
+    from a SystemDesc."""
 
     def __init__(self, directory, seed=(12, 34, 56, 78), device=0):
         self.h = ctypes.c_void_p()
         s = np.asarray(seed, dtype=np.int32)
-        check(lib().fmc_chain_open(str(directory).encode(), ip(s), int(device), ctypes.byref(self.h)))
+        if isinstance(directory, SystemDesc):
+            check(lib().fmc_chain_create(ctypes.byref(directory.s), ip(s), int(device), ctypes.byref(self.h)))
+        else:
+            check(lib().fmc_chain_open(str(directory).encode(), ip(s), int(device), ctypes.byref(self.h)))
 
     def close(self):
         if self.h:
@@ -142,6 +234,25 @@ class Chain:
         check(lib().fmc_guest_realspace(self.h, int(iguest), xyz.shape[0], dp(xyz), int(mol), ctypes.byref(e2),
                                         ctypes.byref(ev)))
         return e2.value, ev.value
+
+    def ewald1_guest_xyz(self, iguest, x, y, z, move, pass_=1):
+        """ewald1_guest on separate coordinate arrays (the reference's newx/newy/newz)."""
+        x, y, z = (np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z))
+        e = ctypes.c_double(0)
+        check(lib().fmc_ewald1_guest_xyz(self.h, int(iguest), len(x), dp(x), dp(y), dp(z), int(move), int(pass_),
+                                         ctypes.byref(e)))
+        return e.value
+
+    def guest_realspace_xyz(self, iguest, x, y, z, mol=-1):
+        x, y, z = (np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z))
+        e2, ev = ctypes.c_double(0), ctypes.c_double(0)
+        check(lib().fmc_guest_realspace_xyz(self.h, int(iguest), len(x), dp(x), dp(y), dp(z), int(mol),
+                                            ctypes.byref(e2), ctypes.byref(ev)))
+        return e2.value, ev.value
+
+    def commit_xyz(self, move, iguest, mol, x=None, y=None, z=None):
+        a = [None if v is None else np.ascontiguousarray(v, dtype=np.float64) for v in (x, y, z)]
+        check(lib().fmc_commit_xyz(self.h, int(move), int(iguest), int(mol), *[None if v is None else dp(v) for v in a]))
 
     def commit(self, move, iguest, mol, xyz=None):
         x = None if xyz is None else np.ascontiguousarray(xyz, dtype=np.float64)

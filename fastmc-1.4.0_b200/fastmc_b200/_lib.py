@@ -20,6 +20,37 @@ MOVE_DTYPE = np.dtype([
 
 INSERT, DELETE, DISPLACE, TRANSLATE, ROTATE, JUMP, NOOP, MULTIJUMP = 1, 2, 3, 4, 5, 6, 7, 8  # NOOP: flex / swap
 
+class GuestDesc(ctypes.Structure):
+    """fmc_guest_desc of the C ABI."""
+    _fields_ = [("name", ctypes.c_char_p), ("nsite", ctypes.c_int), ("site_name", ctypes.POINTER(ctypes.c_char_p)),
+                ("mass", ctypes.POINTER(ctypes.c_double)), ("charge", ctypes.POINTER(ctypes.c_double)),
+                ("tx", ctypes.POINTER(ctypes.c_double)), ("ty", ctypes.POINTER(ctypes.c_double)),
+                ("tz", ctypes.POINTER(ctypes.c_double)), ("type", ctypes.POINTER(ctypes.c_int)),
+                ("nmols", ctypes.c_int), ("xyz", ctypes.POINTER(ctypes.c_double)), ("pressure_pa", ctypes.c_double),
+                ("move_freq", ctypes.c_double * 9), ("disp_ratio", ctypes.c_double), ("tran_ratio", ctypes.c_double)]
+
+
+class VdwDesc(ctypes.Structure):
+    """fmc_vdw_desc of the C ABI."""
+    _fields_ = [("type_i", ctypes.c_int), ("type_j", ctypes.c_int), ("form", ctypes.c_int),
+                ("prm", ctypes.c_double * 5)]
+
+
+class SystemDescStruct(ctypes.Structure):
+    """fmc_system_desc of the C ABI."""
+    _fields_ = [("imcon", ctypes.c_int), ("cell", ctypes.c_double * 9), ("alpha", ctypes.c_double),
+                ("kmax", ctypes.c_int * 3), ("rcut", ctypes.c_double), ("rvdw", ctypes.c_double),
+                ("delr", ctypes.c_double), ("engunit", ctypes.c_double), ("ntypes", ctypes.c_int),
+                ("type_names", ctypes.POINTER(ctypes.c_char_p)), ("nframework", ctypes.c_int),
+                ("fw_xyz", ctypes.POINTER(ctypes.c_double)), ("fw_charge", ctypes.POINTER(ctypes.c_double)),
+                ("fw_type", ctypes.POINTER(ctypes.c_int)), ("fw_mass", ctypes.POINTER(ctypes.c_double)),
+                ("nguest", ctypes.c_int), ("guests", ctypes.POINTER(GuestDesc)), ("nvdw", ctypes.c_int),
+                ("vdw", ctypes.POINTER(VdwDesc)), ("temperature", ctypes.c_double), ("eq_steps", ctypes.c_int),
+                ("prod_steps", ctypes.c_int), ("max_guest_atoms", ctypes.c_int),
+                ("averaging_window", ctypes.c_int), ("acceptance_sampling", ctypes.c_int),
+                ("rota_ratio", ctypes.c_double), ("owner", ctypes.c_void_p)]
+
+
 # Every function the C ABI exports: name -> (restype, argtypes)
 _vp, _ip, _dp, _ci, _cd = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double), \
     ctypes.c_int, ctypes.c_double
@@ -28,6 +59,14 @@ SIGNATURES = {
     "fmc_last_error": (ctypes.c_char_p, []),
     "fmc_chain_open": (_ci, [ctypes.c_char_p, _ip, _ci, ctypes.POINTER(_vp)]),
     "fmc_chain_close": (None, [_vp]),
+    "fmc_chain_create": (_ci, [ctypes.POINTER(SystemDescStruct), _ip, _ci, ctypes.POINTER(_vp)]),
+    "fmc_deck_describe": (_ci, [ctypes.c_char_p, ctypes.POINTER(SystemDescStruct)]),
+    "fmc_desc_free": (None, [ctypes.POINTER(SystemDescStruct)]),
+    "fmc_desc_sizes": (_ci, [_ip]),
+    "fmc_desc_inspect": (_ci, [ctypes.POINTER(SystemDescStruct), _ip, _dp, _ip, _dp, _dp, _dp, _ip, _ip, _dp, _ip]),
+    "fmc_ewald1_guest_xyz": (_ci, [_vp, _ci, _ci, _dp, _dp, _dp, _ci, _ci, _dp]),
+    "fmc_guest_realspace_xyz": (_ci, [_vp, _ci, _ci, _dp, _dp, _dp, _ci, _dp, _dp]),
+    "fmc_commit_xyz": (_ci, [_vp, _ci, _ci, _ci, _dp, _dp, _dp]),
     "fmc_chain_info": (_ci, [_vp, _ip, _dp]),
     "fmc_ewald1": (_ci, [_vp, _dp, _ip]),
     "fmc_ewald1_guest": (_ci, [_vp, _ci, _ci, _dp, _ci, _ci, _dp]),

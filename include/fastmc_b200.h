@@ -49,6 +49,82 @@ const char* fmc_last_error(void);
 int fmc_chain_open(const char* dir, const int* seed, int device, fmc_chain** out);
 void fmc_chain_close(fmc_chain* c);
 
+/* ---------------------------------------------------------------- system from caller arrays
+ * The state the reference keeps in its module arrays once readfield / readconfig / readcontrol
+ * have run (utility_pack.f:8-68, vdw_module.f:19-24), handed over by pointer instead of files:
+ * a Fortran caller whose in-memory state differs from the decks on disk (a restart remap,
+ * gcmc.f:353-418, or a framework it generated) passes c_loc of its own arrays.  Types are
+ * 1-based as the reference's ltype; energies of vdW parameters in internal units (10 J/mol, the
+ * reference's prmvdw after the FIELD `units` scaling). */
+typedef struct fmc_guest_desc {
+  const char* name;              /* species name (NUL-terminated; NULL: "guest") */
+  int nsite;                     /* sites per molecule (1-50; 16 on the batched path) */
+  const char* const* site_name;  /* [nsite] site names, or NULL (the type names) */
+  const double* mass;            /* [nsite] */
+  const double* charge;          /* [nsite] e */
+  const double* tx;              /* [nsite] template, centred on the mass centre (readinputs.f:246-268) */
+  const double* ty;
+  const double* tz;
+  const int* type;               /* [nsite] atom types, 1-based */
+  int nmols;                     /* molecules present (framwkxxx rows) */
+  const double* xyz;             /* [3*nmols*nsite] x,y,z per site, molecule-major; NULL if nmols = 0 */
+  double pressure_pa;            /* partial pressure, Pa (the reference's gstpress) */
+  double move_freq[9];           /* move weights: insert, delete, displace, jump, flex, swap, translate,
+                                    rotate, multi-jump (gcmc.f:282-331 normalises them) */
+  double disp_ratio, tran_ratio; /* target acceptance of displacements / translations (0.5 in CONTROL) */
+} fmc_guest_desc;
+
+/* One vdW pair line (define_van_der_waals, vdw_terms.f:1-187): the two atom types, the form
+ * (keypot: 1 12-6, 2 lj, 3 n-m, 4 buck, 5 bhm, 6 hbnd, 7 shifted n-m, 8 morse, 9 wca) and its
+ * five parameters with energies in internal units.  Pairs without a line get the zero table. */
+typedef struct fmc_vdw_desc {
+  int type_i, type_j, form;
+  double prm[5];
+} fmc_vdw_desc;
+
+typedef struct fmc_system_desc {
+  int imcon;                       /* 1-7 (imcon 0 has no device path) */
+  double cell[9];                  /* cell vectors a, b, c (Angstrom) */
+  double alpha;                    /* Ewald alpha (1/Angstrom) */
+  int kmax[3];
+  double rcut, rvdw, delr;         /* rvdw 0: rcut */
+  double engunit;                  /* internal units per FIELD energy unit (kcal/mol: 418.4) */
+  int ntypes;                      /* unique atom types */
+  const char* const* type_names;   /* [ntypes] names (8 characters), or NULL ("T1", "T2", ...) */
+  int nframework;                  /* rigid framework atoms, condensed order */
+  const double* fw_xyz;            /* [3*nframework] */
+  const double* fw_charge;         /* [nframework] */
+  const int* fw_type;              /* [nframework] 1-based */
+  const double* fw_mass;           /* [nframework] or NULL (only the probability-cube writer reads it) */
+  int nguest;                      /* guest species (1-4) */
+  const fmc_guest_desc* guests;    /* [nguest] */
+  int nvdw;                        /* vdW pair lines */
+  const fmc_vdw_desc* vdw;         /* [nvdw] */
+  double temperature;              /* K */
+  int eq_steps, prod_steps;        /* CONTROL equilibration / steps (negative: cycles of N+1 moves) */
+  int max_guest_atoms;             /* CONTROL `max guest atoms` (0: 3000) */
+  int averaging_window;            /* CONTROL `averaging window` (0: 100000) */
+  int acceptance_sampling;         /* CONTROL `sampling` (statistics only on accepted moves) */
+  double rota_ratio;               /* target acceptance of rotations (0: 0.5) */
+  void* owner;                     /* set by fmc_deck_describe for fmc_desc_free; callers leave NULL */
+} fmc_system_desc;
+
+/* fmc_chain_open from a descriptor instead of a deck directory (no counterpart in the reference,
+ * whose state lives in module arrays): the same tables, single point and S(k).  The arrays are
+ * read during the call only. */
+int fmc_chain_create(const fmc_system_desc* desc, const int* seed, int device, fmc_chain** out);
+/* Host only: read a deck directory into a descriptor whose arrays the library owns (release
+ * them with fmc_desc_free).  A caller may change the arrays it points to -- the guests present,
+ * say -- before fmc_chain_create. */
+int fmc_deck_describe(const char* dir, fmc_system_desc* out);
+void fmc_desc_free(fmc_system_desc* desc);
+/* sizeof of fmc_system_desc, fmc_guest_desc and fmc_vdw_desc in out[0..2] (binding checks). */
+int fmc_desc_sizes(int* out);
+/* Host only: the tables a descriptor builds, as fmc_deck_inspect reports them for a deck, plus
+ * the vdW tables (vvv[ntables*(mxgrid+1)], table 1 first; NULL to skip, *ntables their count). */
+int fmc_desc_inspect(const fmc_system_desc* desc, int* ints, double* dbls, int* lmn, double* akk, double* erc,
+                     double* charges, int* K, int* nerc, double* vvv, int* ntables);
+
 /* ints[0..15]: imcon, kmax1, kmax2, kmax3, K (newld), total atoms, guest species, atom types,
  * mxgrid, framework atoms, moves done, voxel count, guest-site capacity, 0, 0, 0.
  * dbls[0..15]: alpha, rcut, delr, volume, engunit, temperature, beta, drewd, dlrpot,
@@ -80,6 +156,15 @@ int fmc_commit(fmc_chain* c, int move, int iguest, int mol, const double* xyz);
  * commit, gcmc.f:954-1002) and the pending S_new is dropped; the next pass overwrites it.  It
  * touches no device memory and is there so that a caller states either outcome. */
 int fmc_reject(fmc_chain* c);
+
+/* The same three calls on separate coordinate arrays, as the reference's module arrays
+ * newx/newy/newz hold a trial molecule (ewald1_guest ewald.f:32-365, guestlistgen
+ * utility_pack.f:3113-3177, the commit gcmc.f:966-982): x[natms], y[natms], z[natms]. */
+int fmc_ewald1_guest_xyz(fmc_chain* c, int iguest, int natms, const double* x, const double* y, const double* z,
+                         int move, int pass, double* engcpe);
+int fmc_guest_realspace_xyz(fmc_chain* c, int iguest, int natms, const double* x, const double* y, const double* z,
+                            int mol, double* ewld2, double* vdw);
+int fmc_commit_xyz(fmc_chain* c, int move, int iguest, int mol, const double* x, const double* y, const double* z);
 
 /* Replaces all molecules of species `iguest` (the condense of utility_pack.f:3325), then
  * recomputes S(k).  xyz holds nmol*nsite sites, molecule-major. */
