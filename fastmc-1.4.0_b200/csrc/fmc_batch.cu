@@ -20,6 +20,7 @@ struct MoveSmem {
   int mtype, g, mol, nold, nnew, accepted, ex_lo, ex_hi;
   int commit_lo, seg_end, ns, randchoice, need_lrc, rande_drawn, recheck;
   double delrc, rande;
+  double r[7], dis_delr, dis_rot;  // the trial's random numbers and step sizes (select_move)
   double ewld1, ewld2, vdw, ewld3, estep;
   double x[2 * kBatchMaxSites], y[2 * kBatchMaxSites], z[2 * kBatchMaxSites], q[2 * kBatchMaxSites];
   int type[2 * kBatchMaxSites];
@@ -105,188 +106,6 @@ __device__ __noinline__ void check400(ChainDev& C, const SysConst& Y) {
       }
     }
   }
-}
-
-template <bool kProf>
-__device__ __noinline__ void move_begin(ChainDev& C, const SysConst& Y, const DevSystem& S, MoveSmem& M) {
-  if (kProf) C.prof[7] -= clock64();
-  M.mj_action = 0;
-  const bool second = M.mj_stage == 1;  // the second jump of a multi-jump: no count or selection
-  if (!second) {
-    M.mj_first = 0;  // a new move: no molecule to avoid
-    C.gcmccount++;
-    if (C.gcmccount % 400 == 0) check400(C, Y);
-  }
-  DuniLocal R(C.rng);  // written back before every return
-  int g = M.g, mtype = kMultiJump;
-  if (second) {
-    M.mj_stage = 2;
-  } else {
-  const int ng = Y.nspecies;
-  g = 0;
-  if (ng > 1) g = (int)floor(R.next() * ng);
-  double randmov = R.next();
-  const double* c = C.mvcum[g];
-  if (randmov < c[0]) mtype = kInsert;
-  else if (randmov < c[1]) mtype = kDelete;
-  else if (randmov < c[2]) mtype = kDisplace;
-  else if (randmov < c[3]) mtype = kJump;
-  else if (randmov < c[5]) mtype = kNoop;  // flex, swap (gcmc.f:1789-1795)
-  else if (randmov < c[6]) mtype = kTranslate;
-  else if (randmov < c[7]) mtype = kRotate;
-  else if (randmov < c[8]) mtype = kMultiJump;
-  else mtype = kDisplace;
-  const int nmols = C.nmol[g];
-  // step-size adaptation (gcmc.f:794-834)
-  if (nmols >= 1 && C.disp_count[g] >= 1) {
-    if (C.disp_count[g] % 100 == 0) {
-      if ((C.accept_disp[g] / (double)C.disp_count[g]) > C.disp_ratio[g]) C.delrdisp[g] = C.delrdisp[g] * 1.05;
-      else if (C.delrdisp[g] > kDelrMin) C.delrdisp[g] = C.delrdisp[g] * 0.95;
-    } else if (C.disp_count[g] % 50 == 0) {
-      if ((C.accept_disp[g] / (double)C.disp_count[g]) > C.disp_ratio[g]) C.rotangle = C.rotangle * 1.05;
-      else if (C.rotangle > kMinAngle) C.rotangle = C.rotangle * 0.95;
-    }
-  }
-  if (nmols >= 1 && C.tran_count[g] >= 1 && C.tran_count[g] % 100 == 0) {
-    if ((C.accept_tran[g] / (double)C.tran_count[g]) > C.tran_ratio[g]) C.tran_delr[g] = C.tran_delr[g] * 1.05;
-    else if (C.tran_delr[g] > kDelrMin) C.tran_delr[g] = C.tran_delr[g] * 0.95;
-  }
-  if (nmols >= 1 && C.rota_count >= 1 && C.rota_count % 100 == 0) {
-    if ((C.accept_rota / (double)C.rota_count) > C.rota_ratio) C.rota_rotangle = C.rota_rotangle * 1.05;
-    else if (C.rota_rotangle > kMinAngle) C.rota_rotangle = C.rota_rotangle * 0.95;
-  }
-  if (nmols == 0 || (nmols == 1 && mtype == kMultiJump)) mtype = kInsert;  // gcmc.f:837-847
-  if (mtype == kMultiJump) {
-    C.jump_count++;
-    M.mj_stage = 1;
-    M.mj_first = 0;
-    M.mj_energy0 = C.energy[g];
-  }
-  }
-  const SpeciesConst& P = Y.sp[g];
-  const int ns = P.nsite, nmols = C.nmol[g];
-  if (kProf) C.prof[7] += clock64();  // minus the stamp taken at entry: selection + adaptation
-  M.mtype = mtype;
-  M.g = g;
-  M.ns = ns;
-  M.mol = -1;
-  M.randchoice = 0;
-  M.ex_lo = M.ex_hi = -1;
-  M.nold = M.nnew = 0;
-  M.delrc = 0.0;
-  M.rande = -1.0;
-  M.need_lrc = 0;
-  M.rande_drawn = 0;
-  M.recheck = 0;
-  double* x = M.x;
-  double* y = M.y;
-  double* z = M.z;
-  if (kProf) C.prof[8] -= clock64();  // trial generation and site loads
-  if (mtype == kInsert) {
-    C.ins_count++;
-    if ((C.totatm - C.framatm) + ns >= C.maxguest || (nmols + 1) * ns > C.seg_cap[g]) {
-      C.status = 75;
-      R.store(C.rng);
-      return;
-    }
-    double r[7];
-    for (int i = 0; i < 7; i++) r[i] = R.next();
-    trial_insert(S.cell, P.tx, P.ty, P.tz, ns, r, x, y, z);
-    M.nnew = ns;
-    for (int i = 0; i < ns; i++) C.numtyp[P.type[i]]++;
-    M.need_lrc = 1;
-  } else if (mtype == kDelete) {
-    C.del_count++;
-    int randchoice = (int)floor(R.next() * nmols) + 1;
-    M.randchoice = randchoice;
-    M.mol = randchoice - 1;
-    M.ex_lo = C.seg_off[g] + M.mol * ns;
-    M.ex_hi = M.ex_lo + ns;
-    for (int i = 0; i < ns; i++) {
-      double4 a = C.gsite[M.ex_lo + i];
-      x[i] = a.x;
-      y[i] = a.y;
-      z[i] = a.z;
-    }
-    M.nold = ns;
-    for (int i = 0; i < ns; i++) C.numtyp[P.type[i]]--;
-    M.need_lrc = 1;
-  } else if (mtype == kJump || mtype == kMultiJump) {
-    // long jump (gcmc.f:1389-1547): the choice first, then the seven draws of random_jump; the
-    // second jump of a multi-jump draws until it hits a molecule other than the first
-    if (mtype == kJump) C.jump_count++;
-    int randchoice;
-    do {
-      randchoice = (int)floor(R.next() * nmols) + 1;
-    } while (randchoice == M.mj_first);
-    if (mtype == kMultiJump && M.mj_stage == 1) M.mj_first = randchoice;
-    M.randchoice = randchoice;
-    M.mol = randchoice - 1;
-    M.ex_lo = C.seg_off[g] + M.mol * ns;
-    M.ex_hi = M.ex_lo + ns;
-    double r[7];
-    for (int i = 0; i < 7; i++) r[i] = R.next();
-    for (int i = 0; i < ns; i++) {
-      double4 a = C.gsite[M.ex_lo + i];
-      x[i] = a.x;
-      y[i] = a.y;
-      z[i] = a.z;
-      x[ns + i] = a.x;
-      y[ns + i] = a.y;
-      z[ns + i] = a.z;
-    }
-    trial_jump(S.cell, P.mass, ns, r, x + ns, y + ns, z + ns);
-    M.nold = ns;
-    M.nnew = ns;
-  } else if (mtype == kNoop) {
-    // nothing moves; no sites, no draws beyond the move choice
-  } else {
-    double r[7], dis_delr, dis_rot;
-    if (mtype == kTranslate) {
-      C.tran_count[g]++;
-      r[0] = R.next();
-      r[1] = R.next();
-      r[2] = R.next();
-      r[3] = r[4] = r[5] = r[6] = 0.0;
-      dis_delr = C.tran_delr[g];
-      dis_rot = 0.0;
-    } else if (mtype == kRotate) {
-      C.rota_count++;
-      r[0] = r[1] = r[2] = 0.5;
-      for (int i = 3; i < 7; i++) r[i] = R.next();
-      dis_delr = 0.0;
-      dis_rot = C.rota_rotangle;
-    } else {
-      C.disp_count[g]++;
-      for (int i = 0; i < 7; i++) r[i] = R.next();
-      dis_delr = C.delrdisp[g];
-      dis_rot = C.rotangle;
-    }
-    int randchoice = (int)floor(R.next() * nmols) + 1;
-    M.randchoice = randchoice;
-    M.mol = randchoice - 1;
-    M.ex_lo = C.seg_off[g] + M.mol * ns;
-    M.ex_hi = M.ex_lo + ns;
-    for (int i = 0; i < ns; i++) {
-      double4 a = C.gsite[M.ex_lo + i];
-      x[i] = a.x;
-      y[i] = a.y;
-      z[i] = a.z;
-      x[ns + i] = a.x;
-      y[ns + i] = a.y;
-      z[ns + i] = a.z;
-    }
-    trial_displace(S.cell, P.mass, ns, dis_delr, dis_rot, r, x + ns, y + ns, z + ns);
-    M.nold = ns;
-    M.nnew = ns;
-  }
-  for (int i = 0; i < M.nold + M.nnew; i++) {
-    int s = i < M.nold ? i : i - M.nold;
-    M.q[i] = P.q[s];
-    M.type[i] = P.type[s];
-  }
-  R.store(C.rng);
-  if (kProf) C.prof[8] += clock64();
 }
 
 // Thread 0: energy assembly of the move (gcmc.f:946, 1112, 1328).  v = {sum akk*d|S|^2,
@@ -589,6 +408,317 @@ __device__ __forceinline__ void build_phases(const DevSystem& S, const MoveSmem&
   }
 }
 
+// Lane 0 of warp 0: the serial part of a move's set-up (gcmc.f:594-847): the move count and
+// the 400-move checks, species and move choice, step-size adaptation, the counters, and every
+// random number of the trial in the reference's order (utility_pack.f:2545-3000), which
+// select_move leaves in M.r for the warp to build the trial sites from.
+template <bool kProf>
+__device__ __noinline__ void select_move(ChainDev& C, const SysConst& Y, MoveSmem& M) {
+  if (kProf) C.prof[7] -= clock64();
+  M.mj_action = 0;
+  const bool second = M.mj_stage == 1;  // the second jump of a multi-jump: no count or selection
+  if (!second) {
+    M.mj_first = 0;  // a new move: no molecule to avoid
+    C.gcmccount++;
+    if (C.gcmccount % 400 == 0) check400(C, Y);
+  }
+  DuniLocal R(C.rng);  // written back before every return
+  int g = M.g, mtype = kMultiJump;
+  if (second) {
+    M.mj_stage = 2;
+  } else {
+  const int ng = Y.nspecies;
+  g = 0;
+  if (ng > 1) g = (int)floor(R.next() * ng);
+  double randmov = R.next();
+  const double* c = C.mvcum[g];
+  if (randmov < c[0]) mtype = kInsert;
+  else if (randmov < c[1]) mtype = kDelete;
+  else if (randmov < c[2]) mtype = kDisplace;
+  else if (randmov < c[3]) mtype = kJump;
+  else if (randmov < c[5]) mtype = kNoop;  // flex, swap (gcmc.f:1789-1795)
+  else if (randmov < c[6]) mtype = kTranslate;
+  else if (randmov < c[7]) mtype = kRotate;
+  else if (randmov < c[8]) mtype = kMultiJump;
+  else mtype = kDisplace;
+  const int nmols = C.nmol[g];
+  // step-size adaptation (gcmc.f:794-834)
+  if (nmols >= 1 && C.disp_count[g] >= 1) {
+    if (C.disp_count[g] % 100 == 0) {
+      if ((C.accept_disp[g] / (double)C.disp_count[g]) > C.disp_ratio[g]) C.delrdisp[g] = C.delrdisp[g] * 1.05;
+      else if (C.delrdisp[g] > kDelrMin) C.delrdisp[g] = C.delrdisp[g] * 0.95;
+    } else if (C.disp_count[g] % 50 == 0) {
+      if ((C.accept_disp[g] / (double)C.disp_count[g]) > C.disp_ratio[g]) C.rotangle = C.rotangle * 1.05;
+      else if (C.rotangle > kMinAngle) C.rotangle = C.rotangle * 0.95;
+    }
+  }
+  if (nmols >= 1 && C.tran_count[g] >= 1 && C.tran_count[g] % 100 == 0) {
+    if ((C.accept_tran[g] / (double)C.tran_count[g]) > C.tran_ratio[g]) C.tran_delr[g] = C.tran_delr[g] * 1.05;
+    else if (C.tran_delr[g] > kDelrMin) C.tran_delr[g] = C.tran_delr[g] * 0.95;
+  }
+  if (nmols >= 1 && C.rota_count >= 1 && C.rota_count % 100 == 0) {
+    if ((C.accept_rota / (double)C.rota_count) > C.rota_ratio) C.rota_rotangle = C.rota_rotangle * 1.05;
+    else if (C.rota_rotangle > kMinAngle) C.rota_rotangle = C.rota_rotangle * 0.95;
+  }
+  if (nmols == 0 || (nmols == 1 && mtype == kMultiJump)) mtype = kInsert;  // gcmc.f:837-847
+  if (mtype == kMultiJump) {
+    C.jump_count++;
+    M.mj_stage = 1;
+    M.mj_first = 0;
+    M.mj_energy0 = C.energy[g];
+  }
+  }
+  const SpeciesConst& P = Y.sp[g];
+  const int ns = P.nsite, nmols = C.nmol[g];
+  if (kProf) C.prof[7] += clock64();  // minus the stamp taken at entry: selection + adaptation
+  M.mtype = mtype;
+  M.g = g;
+  M.ns = ns;
+  M.mol = -1;
+  M.randchoice = 0;
+  M.ex_lo = M.ex_hi = -1;
+  M.nold = M.nnew = 0;
+  M.delrc = 0.0;
+  M.rande = -1.0;
+  M.need_lrc = 0;
+  M.rande_drawn = 0;
+  M.recheck = 0;
+  double* r = M.r;
+  if (mtype == kInsert) {
+    C.ins_count++;
+    if ((C.totatm - C.framatm) + ns >= C.maxguest || (nmols + 1) * ns > C.seg_cap[g]) {
+      C.status = 75;
+      R.store(C.rng);
+      return;
+    }
+    for (int i = 0; i < 7; i++) r[i] = R.next();
+    M.nnew = ns;
+    for (int i = 0; i < ns; i++) C.numtyp[P.type[i]]++;
+    M.need_lrc = 1;
+  } else if (mtype == kDelete) {
+    C.del_count++;
+    int randchoice = (int)floor(R.next() * nmols) + 1;
+    M.randchoice = randchoice;
+    M.mol = randchoice - 1;
+    M.ex_lo = C.seg_off[g] + M.mol * ns;
+    M.ex_hi = M.ex_lo + ns;
+    M.nold = ns;
+    for (int i = 0; i < ns; i++) C.numtyp[P.type[i]]--;
+    M.need_lrc = 1;
+  } else if (mtype == kJump || mtype == kMultiJump) {
+    // long jump (gcmc.f:1389-1547): the choice first, then the seven draws of random_jump; the
+    // second jump of a multi-jump draws until it hits a molecule other than the first
+    if (mtype == kJump) C.jump_count++;
+    int randchoice;
+    do {
+      randchoice = (int)floor(R.next() * nmols) + 1;
+    } while (randchoice == M.mj_first);
+    if (mtype == kMultiJump && M.mj_stage == 1) M.mj_first = randchoice;
+    M.randchoice = randchoice;
+    M.mol = randchoice - 1;
+    M.ex_lo = C.seg_off[g] + M.mol * ns;
+    M.ex_hi = M.ex_lo + ns;
+    for (int i = 0; i < 7; i++) r[i] = R.next();
+    M.nold = ns;
+    M.nnew = ns;
+  } else if (mtype == kNoop) {
+    // nothing moves; no sites, no draws beyond the move choice
+  } else {
+    if (mtype == kTranslate) {
+      C.tran_count[g]++;
+      r[0] = R.next();
+      r[1] = R.next();
+      r[2] = R.next();
+      r[3] = r[4] = r[5] = r[6] = 0.0;
+      M.dis_delr = C.tran_delr[g];
+      M.dis_rot = 0.0;
+    } else if (mtype == kRotate) {
+      C.rota_count++;
+      r[0] = r[1] = r[2] = 0.5;
+      for (int i = 3; i < 7; i++) r[i] = R.next();
+      M.dis_delr = 0.0;
+      M.dis_rot = C.rota_rotangle;
+    } else {
+      C.disp_count[g]++;
+      for (int i = 0; i < 7; i++) r[i] = R.next();
+      M.dis_delr = C.delrdisp[g];
+      M.dis_rot = C.rotangle;
+    }
+    int randchoice = (int)floor(R.next() * nmols) + 1;
+    M.randchoice = randchoice;
+    M.mol = randchoice - 1;
+    M.ex_lo = C.seg_off[g] + M.mol * ns;
+    M.ex_hi = M.ex_lo + ns;
+    M.nold = ns;
+    M.nnew = ns;
+  }
+  R.store(C.rng);
+}
+
+// ------------------------------------------------------------------ the trial sites, one lane each
+// The trial generators of fmc_common.h restated for a warp: lane i holds site i, so the moved
+// molecule's sites load at once and each site takes the same arithmetic as there; the mass centre
+// sums run over the sites in order in every lane (gathered by shuffles), so every lane holds the
+// same centre.
+__device__ __forceinline__ void com_lanes(const double* mass, int n, double x, double y, double z, double* c) {
+  double w = 0.0, sx = 0.0, sy = 0.0, sz = 0.0;
+  for (int j = 0; j < n; j++) {
+    const double xj = __shfl_sync(0xffffffffu, x, j), yj = __shfl_sync(0xffffffffu, y, j),
+                 zj = __shfl_sync(0xffffffffu, z, j);
+    w = w + mass[j];
+    sx = sx + xj * mass[j];
+    sy = sy + yj * mass[j];
+    sz = sz + zj * mass[j];
+  }
+  c[0] = sx / w;
+  c[1] = sy / w;
+  c[2] = sz / w;
+}
+
+// One site rotated by quaternion q (rotate_sites' matrix).
+__device__ __forceinline__ void rotate_site(const double q[4], double& x, double& y, double& z) {
+  const double q1 = q[0], q2 = q[1], q3 = q[2], q4 = q[3];
+  const double Q0 = 2.0 * q2 * q2 + 2.0 * q1 * q1 - 1.0, Q1 = 2.0 * q2 * q3 - 2.0 * q1 * q4;
+  const double Q2 = 2.0 * q2 * q4 + 2.0 * q1 * q3, Q3 = 2.0 * q2 * q3 + 2.0 * q1 * q4;
+  const double Q4 = 2.0 * q1 * q1 + 2.0 * q3 * q3 - 1.0, Q5 = 2.0 * q3 * q4 - 2.0 * q1 * q2;
+  const double Q6 = 2.0 * q2 * q4 - 2.0 * q1 * q3, Q7 = 2.0 * q3 * q4 + 2.0 * q1 * q2;
+  const double Q8 = 2.0 * q4 * q4 + 2.0 * q1 * q1 - 1.0;
+  const double tx = Q0 * x + Q1 * y + Q2 * z;
+  const double ty = Q3 * x + Q4 * y + Q5 * z;
+  const double tz = Q6 * x + Q7 * y + Q8 * z;
+  x = tx;
+  y = ty;
+  z = tz;
+}
+
+// Warp 0, after select_move: the trial sites (old sites read from the chain, new ones built by
+// random_ins / random_disp + random_rot / random_jump), their charges and types, their voxel lists
+// and the real-space work list, then their phase tables (ewald.f:95-137).
+template <bool kProf>
+__device__ __noinline__ void build_trial(ChainDev& C, const SysConst& Y, const DevSystem& S, MoveSmem& M, void* tab,
+                                         int stride, bool fp32_phases, int lane) {
+  if (kProf && lane == 0) C.prof[8] -= clock64();
+  const int mtype = M.mtype, ns = M.ns, nold = M.nold, nnew = M.nnew, nseg = Y.nspecies;
+  const SpeciesConst& P = Y.sp[M.g];
+  const bool mine = lane < ns;
+  double ox = 0.0, oy = 0.0, oz = 0.0, nx = 0.0, ny = 0.0, nz = 0.0;
+  if (nold && mine) {
+    const double4 a = C.gsite[M.ex_lo + lane];
+    ox = a.x;
+    oy = a.y;
+    oz = a.z;
+  }
+  const double* r = M.r;
+  const double* h = S.cell.h;
+  if (mtype == kInsert) {
+    // random_ins (utility_pack.f:2545-2650): template rotated, centred at fractional (r0, r1, r2)
+    const double xc = r[0] * h[0] + r[1] * h[3] + r[2] * h[6];
+    const double yc = r[0] * h[1] + r[1] * h[4] + r[2] * h[7];
+    const double zc = r[0] * h[2] + r[1] * h[5] + r[2] * h[8];
+    double q[4];
+    axis_angle_quat(r[3] * 2.0 * kPi, r[4], r[5], r[6], q);
+    if (mine) {
+      nx = P.tx[lane];
+      ny = P.ty[lane];
+      nz = P.tz[lane];
+      rotate_site(q, nx, ny, nz);
+      nx = nx + xc;
+      ny = ny + yc;
+      nz = nz + zc;
+    }
+  } else if (mtype == kJump || mtype == kMultiJump) {
+    // random_jump: the mass centre moved to fractional (r0, r1, r2), a new orientation about it
+    double xd = r[0] * h[0] + r[1] * h[3] + r[2] * h[6];
+    double yd = r[0] * h[1] + r[1] * h[4] + r[2] * h[7];
+    double zd = r[0] * h[2] + r[1] * h[5] + r[2] * h[8];
+    double cm[3];
+    com_lanes(P.mass, ns, ox, oy, oz, cm);
+    xd = xd - cm[0];
+    yd = yd - cm[1];
+    zd = zd - cm[2];
+    nx = xd + ox;
+    ny = yd + oy;
+    nz = zd + oz;
+    com_lanes(P.mass, ns, nx, ny, nz, cm);
+    nx = nx - cm[0];
+    ny = ny - cm[1];
+    nz = nz - cm[2];
+    double q[4];
+    axis_angle_quat(r[3] * (8.0 * atan(1.0)), r[4], r[5], r[6], q);
+    rotate_site(q, nx, ny, nz);
+    nx = nx + cm[0];
+    ny = ny + cm[1];
+    nz = nz + cm[2];
+  } else if (mtype == kDisplace || mtype == kTranslate || mtype == kRotate) {
+    // random_disp + random_rot (utility_pack.f:2679-2763, 2929-3000)
+    const double half = M.dis_delr * 0.5;
+    const double dx = (2.0 * r[0] - 1.0) * half, dy = (2.0 * r[1] - 1.0) * half, dz = (2.0 * r[2] - 1.0) * half;
+    nx = dx + ox;
+    ny = dy + oy;
+    nz = dz + oz;
+    double cm[3];
+    com_lanes(P.mass, ns, nx, ny, nz, cm);
+    const double* rh = S.cell.rh;
+    double fx = rh[0] * cm[0] + rh[3] * cm[1] + rh[6] * cm[2];
+    double fy = rh[1] * cm[0] + rh[4] * cm[1] + rh[7] * cm[2];
+    double fz = rh[2] * cm[0] + rh[5] * cm[1] + rh[8] * cm[2];
+    fx = fx - floor(fx);
+    fy = fy - floor(fy);
+    fz = fz - floor(fz);
+    const double wx = h[0] * fx + h[3] * fy + h[6] * fz;
+    const double wy = h[1] * fx + h[4] * fy + h[7] * fz;
+    const double wz = h[2] * fx + h[5] * fy + h[8] * fz;
+    const double shx = wx - cm[0], shy = wy - cm[1], shz = wz - cm[2];
+    nx = nx + shx - wx;
+    ny = ny + shy - wy;
+    nz = nz + shz - wz;
+    double q[4];
+    axis_angle_quat(r[3] * M.dis_rot, r[4], r[5], r[6], q);
+    rotate_site(q, nx, ny, nz);
+    nx = nx + wx;
+    ny = ny + wy;
+    nz = nz + wz;
+  }
+  // the work list: each trial site's voxel list, then every guest site
+  if (mine && nold) {
+    M.x[lane] = ox;
+    M.y[lane] = oy;
+    M.z[lane] = oz;
+    M.q[lane] = P.q[lane];
+    M.type[lane] = P.type[lane];
+    const int v = voxel_of(S, ox, oy, oz);
+    M.vb[lane] = S.vox_off[v];
+    M.vl[lane] = S.vox_off[v + 1] - S.vox_off[v];
+  }
+  if (mine && nnew) {
+    const int st = nold + lane;
+    M.x[st] = nx;
+    M.y[st] = ny;
+    M.z[st] = nz;
+    M.q[st] = P.q[lane];
+    M.type[st] = P.type[lane];
+    const int v = voxel_of(S, nx, ny, nz);
+    M.vb[st] = S.vox_off[v];
+    M.vl[st] = S.vox_off[v + 1] - S.vox_off[v];
+  }
+  __syncwarp();
+  if (fp32_phases)
+    build_phases<true>(S, M, tab, stride, lane);
+  else
+    build_phases<false>(S, M, tab, stride, lane);
+  if (lane == 0) {
+    int gt = 0;
+    M.gpre[0] = 0;
+    for (int g = 0; g < nseg; g++) {
+      gt += C.nmol[g] * Y.sp[g].nsite;
+      M.gpre[g + 1] = gt;
+    }
+    M.pre[0] = 0;
+    for (int st = 0; st < nold + nnew; st++) M.pre[st + 1] = M.pre[st] + M.vl[st] + gt;
+    if (kProf) C.prof[8] += clock64();
+  }
+}
+
 // All threads: this thread's share of the reciprocal sum and of the real-space pairs.
 // v[0] sum akk*d|S|^2, v[1] ewld2, v[2] vdw, v[3] and v[4] the absolute sums that bound the
 // rounding error of v[0] and v[1]+v[2] (mixed precision).  S_new goes to Sn when write_sn.
@@ -864,7 +994,16 @@ __global__ void __launch_bounds__(kBatchThreads, 2) fmc_batch_kernel(BatchLaunch
       }
     }
     if (prof && tid == 0) t0 = clock64();
-    if (tid == 0) move_begin<kProf>(C, Y, S, M);
+    if (warp == 0) {
+      if (lane == 0) select_move<kProf>(C, Y, M);
+      __syncwarp();
+      // warp 1 may read select_move's results now (named barrier 1: warps 0 and 1)
+      asm volatile("bar.arrive 1, 64;" ::: "memory");
+      if (!C.status) build_trial<kProf>(C, Y, S, M, tab, stride, mixed && (L.mixed & 1), lane);
+    } else if (warp == 1) {
+      asm volatile("bar.sync 1, 64;" ::: "memory");
+      if (M.need_lrc && !C.status) lrc_warp(C, Y, M, lane);
+    }
     __syncthreads();
     if (prof && tid == 0) {
       t1 = clock64();
@@ -872,40 +1011,7 @@ __global__ void __launch_bounds__(kBatchThreads, 2) fmc_batch_kernel(BatchLaunch
       t0 = t1;
     }
     if (C.status) break;
-    const bool last = !C.lgchk;  // thread 0 writes lgchk only in move_begin
-    const int nsite = M.nold + M.nnew;
-    if (warp == 0) {
-      if (mixed && (L.mixed & 1))
-        build_phases<true>(S, M, tab, stride, lane);
-      else
-        build_phases<false>(S, M, tab, stride, lane);
-    } else if (warp == 1) {
-      if (M.need_lrc) lrc_warp(C, Y, M, lane);
-    } else if (warp == 2) {
-      // real-space work list: voxel list of every trial site, then every guest site
-      if (lane < nsite) {
-        int v = voxel_of(S, M.x[lane], M.y[lane], M.z[lane]);
-        M.vb[lane] = S.vox_off[v];
-        M.vl[lane] = S.vox_off[v + 1] - S.vox_off[v];
-      }
-      __syncwarp();
-      if (lane == 0) {
-        int gt = 0;
-        M.gpre[0] = 0;
-        for (int g = 0; g < nseg; g++) {
-          gt += C.nmol[g] * Y.sp[g].nsite;
-          M.gpre[g + 1] = gt;
-        }
-        M.pre[0] = 0;
-        for (int st = 0; st < nsite; st++) M.pre[st + 1] = M.pre[st] + M.vl[st] + gt;
-      }
-    }
-    __syncthreads();
-    if (prof && tid == 0) {
-      t1 = clock64();
-      C.prof[1] += t1 - t0;
-      t0 = t1;
-    }
+    const bool last = !C.lgchk;  // lane 0 of warp 0 writes lgchk only in select_move
     double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     if (mixed)
       sums<true>(S, C, M, nseg, prow_s, nt1, kp, ak, Sk, Sn, tab, stride, true, L.mixed, v);
@@ -1003,7 +1109,7 @@ __global__ void __launch_bounds__(kBatchThreads, 2) fmc_batch_kernel(BatchLaunch
         C.gtype[M.commit_lo + tid] = M.type[st];
       }
     }
-    // read before the barrier: thread 0 may change these in the next move_begin
+    // read before the barrier: thread 0 may change these in the next select_move
     pending = M.mj_stage == 1;
     const bool store = Y.nplots && C.production && !pending;
     __syncthreads();
