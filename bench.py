@@ -32,7 +32,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="batched", choices=["plain", "batched", "serve"])
+    ap.add_argument("--workload", default="batched", choices=["plain", "batched", "serve", "mixture"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--serve-requests", type=int, default=1500)
     ap.add_argument("--serve-slots", type=int, default=296)
@@ -40,6 +40,10 @@ def parse():
     ap.add_argument("--serve-kcap", type=int, default=0, help="0: the largest request's K")
     ap.add_argument("--serve-cycle-scale", type=float, default=0.1,
                     help="scale of the U(2k,20k) cycle budgets so that requests finish within the run")
+    ap.add_argument("--serve-sub-requests", type=int, default=1200,
+                    help="batched workload: requests of the serving sub-record on the same line (0: none)")
+    ap.add_argument("--serve-sub-scale", type=float, default=0.05,
+                    help="cycle-budget scale of the serving sub-record's U(2k,20k) budgets")
     ap.add_argument("--moves", type=int, default=2000, help="trial moves per chain per step")
     ap.add_argument("--voxel-edge", type=float, default=0.0,
                     help="batched: neighbour-list voxel edge in A (0: picked by the autotuner)")
@@ -468,7 +472,91 @@ def run_batched(args, dist):
                                             f"{max(1, n // 8)}th), each from its GPU chain's state, oracle "
                                             f"FP64 restatement, 1 thread, {ct:.1f} s"}
     b.close()
+    if args.serve_sub_requests > 0:
+        # the serving half of the metric on the same line: p50/p99 time-to-completion beside the
+        # aggregate moves/s of continuous batching (bounded run; its own timing and clocks)
+        srv, log, done_t, arrivals, wall, clk, meta = serve_record(args, dist, args.serve_sub_requests,
+                                                                  args.serve_sub_scale, "serve_sub")
+        rec = summarize_serve(args, dist, srv, log, done_t, arrivals, wall, meta, args.serve_sub_scale,
+                              args.serve_sub_requests)
+        srv.close()
+        rec["clocks"] = clk.summary()
+        result["serve"] = rec
     return result
+
+
+MIXTURE_WORKLOAD = ("batched binary mixture: 256 chains = the 16 batched frameworks x 16 seeds, CO2/N2 at 15:85 "
+                    "mole fraction and 1 bar total, 298 K, one persistent launch per step")
+
+
+def run_mixture(args, dist):
+    """The binary-mixture batched workload, timed at FP64 and with the mixed-precision build on the
+    same chains; the mixed run's dE, total energy and loading are reported against FP64."""
+    import numpy as np
+
+    import fastmc_b200 as fm
+    from fastmc_b200 import synth
+
+    tmp = tempfile.mkdtemp(prefix="fmcmix")
+    dirs = synth.write_batched(os.path.join(tmp, "mix"), gases=("CO2", "N2"), fractions=(0.15, 0.85), total_bar=1.0)
+    n = len(dirs)
+    seeds = [synth.batched_seed(i, dist.rank) for i in range(n)]
+    edge = args.voxel_edge if args.voxel_edge > 0 else 1.0
+    arms = {}
+    for prec in ("fp64", "mixed"):
+        b = fm.Batch(dirs, seeds, device=dist.local, voxel_edge=edge)
+        if prec == "mixed":
+            b.set_precision(7, recompute_every=25000)
+        for _ in range(args.warmup):
+            b.run(args.moves)
+        dist.barrier()
+        ms_tot = 0.0
+        traces = []
+        for _ in range(args.steps):
+            tr, ms = b.run(args.moves, trace=True)
+            traces.append(tr)
+            ms_tot += ms
+        t_dev = dist.max(ms_tot / 1000.0)
+        arms[prec] = {"b": b, "t": t_dev, "trace": np.concatenate(traces, axis=1),
+                      "states": [b.state(i) for i in range(n)]}
+    moves = dist.sum(n * args.moves * args.steps)
+    t64, tmx = arms["fp64"]["trace"], arms["mixed"]["trace"]
+    same_seq = all(np.array_equal(t64[i][k], tmx[i][k]) for i in range(n)
+                   for k in ("mtype", "iguest", "randchoice", "accepted", "nmols_after"))
+    de_err = np.abs(tmx["estep"] - t64["estep"]) / np.maximum(np.abs(t64["estep"]), 1.0)
+    e_err = max(abs(a[f"energy{g}"] - b[f"energy{g}"]) / max(abs(b[f"energy{g}"]), 1.0)
+                for a, b in zip(arms["mixed"]["states"], arms["fp64"]["states"]) for g in (0, 1))
+    load_diff = max(abs(a["nmol0"] - b["nmol0"]) + abs(a["nmol1"] - b["nmol1"])
+                    for a, b in zip(arms["mixed"]["states"], arms["fp64"]["states"]))
+    # dE on the same state: a shadow FP64 evaluation of every mixed move
+    bm = arms["mixed"]["b"]
+    rec, sh, _ = bm.run_shadow(args.moves)
+    m = rec["pad0"] == 0
+    sh_err = np.abs(rec["estep"][m] - sh[..., 3][m]) / np.maximum(np.abs(sh[..., 3][m]), 1.0)
+    for a in arms.values():
+        a["b"].close()
+    v64, vmx = moves / arms["fp64"]["t"], moves / arms["mixed"]["t"]
+    use = "mixed" if args.precision == "mixed" else "fp64"
+    return {
+        "metric": "MC trial moves/s on 1 B200 (batched binary mixture)", "value": vmx if use == "mixed" else v64,
+        "unit": "moves/s", "n_gpus": dist.world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": arms[use]["t"] * 1000.0 / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64" if use == "fp64" else "f32+f64",
+        "data": "synthetic (seeded framework generator, FastMC input formats)",
+        "config": {"workload": MIXTURE_WORKLOAD, "chains": n, "moves_per_chain_per_step": args.moves,
+                   "voxel_edge_A": edge, "precision": use, "parallelism": f"replicas{dist.world}"},
+        "precision_comparison": {
+            "fp64_moves_per_s": v64, "mixed_moves_per_s": vmx, "mixed_over_fp64": vmx / v64,
+            "mixed_mask": "FP32 reciprocal phases + Coulomb + vdW pair terms; FP64 S(k), totals, dE assembly",
+            "same_move_sequence": bool(same_seq),
+            "dE_rel_err_max_same_state": float(sh_err.max()) if sh_err.size else 0.0,
+            "dE_rel_err_p99_same_state": float(np.percentile(sh_err, 99)) if sh_err.size else 0.0,
+            "dE_rel_err_max_trajectory": float(de_err.max()),
+            "total_energy_rel_err_max": float(e_err), "loading_diff_max_molecules": int(load_diff),
+            "fp64_rechecks": int(sum(s["rechecks"] for s in arms["mixed"]["states"])),
+            "err_scale": "relative to max(|dE_fp64|, 1 kcal/mol)"},
+        "gpu_launches": args.steps,
+    }
 
 
 def _write_request(job):
@@ -492,50 +580,47 @@ SERVE_WORKLOAD = ("serving: Poisson stream of isotherm-point requests, each a fr
                   "U(2k,20k) x {scale} per phase (a cycle = N_guests+1 moves), continuous batching over {slots} slots")
 
 
-def run_serve(args, dist):
-    """Continuous-batching server on a Poisson request stream; time-to-completion p50/p99."""
+def serve_record(args, dist, n_req, cycle_scale, tag):
+    """Continuous-batching server on a Poisson request stream: time-to-completion p50/p99, device
+    and end-to-end moves/s over the loaded window (the steps started while requests still
+    arrived), slot occupancy.  A saturating pilot first measures the server's capacity; arrivals
+    are then offered at 90% of it."""
     import numpy as np
 
     from fastmc_b200 import synth
 
     tmp = tempfile.mkdtemp(prefix="fmcserve")
-    n_pilot, n_req = args.serve_slots + 64, args.serve_requests
+    n_pilot = args.serve_slots + 64
     reqs = synth.serving_requests(n_pilot + n_req, seed=7 + 1000 * dist.rank)
     for r in reqs:
-        r["cycles"] = max(1, int(round(r["cycles"] * args.serve_cycle_scale)))
+        r["cycles"] = max(1, int(round(r["cycles"] * cycle_scale)))
     t0 = time.perf_counter()
-    dirs = write_requests(tmp, reqs)  # before the first CUDA call (spawned pool)
+    dirs = write_requests(os.path.join(tmp, tag), reqs)  # spawned pool
     gen_s = time.perf_counter() - t0
     import fastmc_b200 as fm
 
     # k capacity: the largest request's K (cubic cells: K grows with the edge)
     kcap = args.serve_kcap or int(fm.deck_inspect(dirs[int(np.argmax([r["edge"] for r in reqs]))])["K"])
     srv = fm.Server(slots=args.serve_slots, device=dist.local, k_capacity=kcap)
-    if args.precision == "mixed":
-        srv.set_precision(7, recompute_every=1000)
-    # pilot (warm-up): more requests than slots at once; the launches that ran with every
-    # slot busy give the server's capacity in moves/s
+    # pilot (warm-up): more requests than slots at once; the launches that ran with every slot busy
+    # give the server's capacity in moves/s
     ids = [srv.submit(d, (12, 34, 56, 1 + r["id"] % 168)) for d, r in zip(dirs[:n_pilot], reqs[:n_pilot])]
     full_ms = []
-    while True:
+    while srv.busy():
         a, q, ms = srv.step(args.serve_moves)
         if a == args.serve_slots:
             full_ms.append(ms)
-        if not a and not q:
-            break
+    srv.poll_done()
     pil = [srv.poll(i) for i in ids]
     moves_per_req = float(np.mean([r["moves"] for r in pil]))
     capacity = args.serve_slots * args.serve_moves / (float(np.median(full_ms)) / 1000.0) if full_ms else None
-    # offered load: 90% of that capacity
     rate = 0.9 * capacity / moves_per_req if capacity else 50.0
     rng = np.random.default_rng(99 + dist.rank)
     arrivals = np.cumsum(rng.exponential(1.0 / rate, n_req))
     dist.barrier()
-    live = {}
-    done_t = {}
+    live, done_t = {}, {}
     nxt = 0
-    dev_ms, steps, occ = 0.0, 0, 0.0
-    log = []  # per step: wall start, wall end, device ms, moves run, active slots
+    log = []  # per step: wall start, wall end, device ms and moves of the launch it completed, slots in it
     with ClockSampler(dist.local) as clk:
         clk.ready()
         wall0 = time.perf_counter()
@@ -545,26 +630,27 @@ def run_serve(args, dist):
                 rid = srv.submit(dirs[n_pilot + nxt], (12, 34, 56, 1 + reqs[n_pilot + nxt]["id"] % 168))
                 live[rid] = nxt
                 nxt += 1
-            if not live:
-                time.sleep(max(0.0, min(arrivals[nxt] - now, 0.05)))
+            if not srv.busy():
+                time.sleep(max(0.0, min(arrivals[nxt] - now, 0.05)) if nxt < n_req else 0.0)
                 continue
             a, q, ms = srv.step(args.serve_moves)
             end = time.perf_counter() - wall0
-            log.append((now, end, ms, int(srv.stats()["last_moves"]), a))
-            dev_ms += ms
-            occ += a * ms
-            steps += 1
-            for rid in list(live):
-                res = srv.poll(rid)
-                if res["state"] in (srv.DONE, srv.REJECTED, srv.CANCELLED):
-                    done_t[live[rid]] = (end - arrivals[live[rid]], res)
-                    del live[rid]
+            log.append((now, end, ms, int(srv.stats()["last_moves"]) if ms > 0 else 0, a))
+            for rid, state, _ in srv.poll_done():
+                if rid in live:
+                    k = live.pop(rid)
+                    done_t[k] = (end - arrivals[k], state)
         wall = time.perf_counter() - wall0
     dist.barrier()
+    return srv, log, done_t, arrivals, wall, clk, {"capacity": capacity, "rate": rate, "n_pilot": n_pilot,
+                                                   "moves_per_req": moves_per_req, "gen_s": gen_s, "kcap": kcap}
+
+
+def summarize_serve(args, dist, srv, log, done_t, arrivals, wall, meta, cycle_scale, n_req):
+    import numpy as np
+
     lat = np.array([v[0] for v in done_t.values()])
-    rejected = sum(1 for v in done_t.values() if v[1]["state"] != srv.DONE)
-    # loaded window: the steps that started while requests were still arriving; the drain of
-    # the last (longest) requests afterwards is reported separately
+    rejected = sum(1 for v in done_t.values() if v[1] != srv.DONE)
     t_last = float(arrivals[-1])
     win = [x for x in log if x[0] <= t_last]
     w_moves = sum(x[3] for x in win)
@@ -572,44 +658,61 @@ def run_serve(args, dist):
     w_wall = win[-1][1] if win else 0.0
     w_occ = sum(x[4] * x[2] for x in win) / max(sum(x[2] for x in win), 1e-9) / args.serve_slots
     all_moves = sum(x[3] for x in log)
+    dev_ms = sum(x[2] for x in log)
+    occ = sum(x[4] * x[2] for x in log)
     t_dev = dist.max(w_dev)
     t_wall = dist.max(w_wall)
     total = dist.sum(w_moves)
     used, budget = srv.memory()
     sstats = srv.stats()
-    srv.close()
-    # host<->device bytes per step: every slot's system block and control block in, control blocks out
     from fastmc_b200._lib import lib as _l
     cb, sb = int(_l().fmc_batch_control_block_bytes()), int(_l().fmc_system_block_bytes())
     return {
-        "metric": "MC trial moves/s on 1 B200 (continuous-batching serving); p50/p99 time-to-completion",
-        "value": total / t_dev, "unit": "moves/s", "n_gpus": dist.world, "steps": len(win), "warmup": 1,
-        "ms_per_step": t_dev * 1000.0 / max(len(win), 1), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "f32+f64",
-        "data": "synthetic (seeded request generator, FastMC input formats)",
-        "config": {"workload": SERVE_WORKLOAD.format(scale=args.serve_cycle_scale, slots=args.serve_slots),
-                   "requests": n_req, "pilot_requests": n_pilot, "arrival_rate_hz": rate,
-                   "capacity_moves_per_s": capacity, "offered_load": 0.9,
-                   "moves_per_request_mean": moves_per_req, "moves_per_step": args.serve_moves,
-                   "precision": args.precision, "deck_generation_s": gen_s, "k_capacity": kcap,
-                   "l2": "per-chain S(k) shared-memory resident; frameworks + voxel lists exceed L2 (no flush)",
-                   "parallelism": f"replicas{dist.world}"},
+        "value": total / t_dev, "e2e_value": total / t_wall, "unit": "moves/s",
+        "e2e_over_device": (total / t_wall) / (total / t_dev),
         "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                       "mean": float(lat.mean()), "max": float(lat.max())},
-        "rejected": rejected,
-        "window": {"what": "value/e2e cover the steps started before the last arrival",
+        "requests": n_req, "rejected": rejected, "cycle_scale": cycle_scale,
+        "workload": SERVE_WORKLOAD.format(scale=cycle_scale, slots=args.serve_slots),
+        "pilot_requests": meta["n_pilot"], "arrival_rate_hz": meta["rate"],
+        "capacity_moves_per_s": meta["capacity"], "offered_load": 0.9, "moves_per_request_mean": meta["moves_per_req"],
+        "moves_per_step": args.serve_moves, "k_capacity": meta["kcap"], "deck_generation_s": meta["gen_s"],
+        "window": {"what": "device and end-to-end figures cover the steps started before the last arrival",
                    "steps": len(win), "moves": w_moves, "device_s": w_dev, "wall_s": w_wall,
                    "slot_occupancy": w_occ},
-        "whole_run": {"steps": steps, "moves": all_moves, "device_s": dev_ms / 1000.0, "wall_s": wall,
+        "whole_run": {"steps": len(log), "moves": all_moves, "device_s": dev_ms / 1000.0, "wall_s": wall,
                       "moves_per_device_s": all_moves / max(dev_ms / 1000.0, 1e-9),
                       "moves_per_wall_s": all_moves / max(wall, 1e-9),
                       "slot_occupancy": occ / max(dev_ms, 1e-9) / args.serve_slots},
-        "gpu_launches": len(win),
-        "e2e": {"value": total / t_wall, "unit": "moves/s",
-                "h2d_bytes_per_step": args.serve_slots * (sb + cb), "d2h_bytes_per_step": args.serve_slots * cb},
-        "clocks": clk.summary(),
-        "memory": {"slots_bytes_at_end": used, "budget_bytes": budget},
-        "server": sstats,
+        "h2d_bytes_per_step": args.serve_slots * (sb + cb), "d2h_bytes_per_step": args.serve_slots * cb,
+        "memory": {"slots_bytes_at_end": used, "budget_bytes": budget}, "server": sstats,
+    }
+
+
+def run_serve(args, dist):
+    """The serving workload on its own line (metric: moves/s with p50/p99 time-to-completion)."""
+    srv, log, done_t, arrivals, wall, clk, meta = serve_record(args, dist, args.serve_requests,
+                                                              args.serve_cycle_scale, "serve")
+    rec = summarize_serve(args, dist, srv, log, done_t, arrivals, wall, meta, args.serve_cycle_scale,
+                          args.serve_requests)
+    srv.close()
+    w = rec["window"]
+    return {
+        "metric": "MC trial moves/s on 1 B200 (continuous-batching serving); p50/p99 time-to-completion",
+        "value": rec["value"], "unit": "moves/s", "n_gpus": dist.world, "steps": w["steps"], "warmup": 1,
+        "ms_per_step": w["device_s"] * 1000.0 / max(w["steps"], 1), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded request generator, FastMC input formats)",
+        "config": {"workload": rec["workload"], "requests": rec["requests"], "pilot_requests": rec["pilot_requests"],
+                   "arrival_rate_hz": rec["arrival_rate_hz"], "capacity_moves_per_s": rec["capacity_moves_per_s"],
+                   "offered_load": 0.9, "moves_per_request_mean": rec["moves_per_request_mean"],
+                   "moves_per_step": args.serve_moves, "k_capacity": rec["k_capacity"],
+                   "l2": "per-chain S(k) shared-memory resident; frameworks + voxel lists exceed L2 (no flush)",
+                   "parallelism": f"replicas{dist.world}"},
+        "latency_s": rec["latency_s"], "rejected": rec["rejected"], "window": rec["window"],
+        "whole_run": rec["whole_run"], "gpu_launches": w["steps"],
+        "e2e": {"value": rec["e2e_value"], "unit": "moves/s", "h2d_bytes_per_step": rec["h2d_bytes_per_step"],
+                "d2h_bytes_per_step": rec["d2h_bytes_per_step"]},
+        "clocks": clk.summary(), "memory": rec["memory"], "server": rec["server"],
     }
 
 
@@ -683,6 +786,8 @@ def main():
             res = run_plain(args, dist)
         elif args.workload == "serve":
             res = run_serve(args, dist)
+        elif args.workload == "mixture":
+            res = run_mixture(args, dist)
         else:
             res = run_batched(args, dist)
         if dist.rank == 0 and res is not None:

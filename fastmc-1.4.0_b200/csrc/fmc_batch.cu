@@ -1120,6 +1120,8 @@ __global__ void __launch_bounds__(kBatchThreads, 2) fmc_batch_kernel(BatchLaunch
     mv++;
   }
   for (int k = tid; k < K; k += blockDim.x) C.sk[k] = Sk[k];
+  if (tid == 0 && L.retire_finished && ((C.budget > 0 && C.moves_done >= C.budget) || !C.lgchk || C.status))
+    C.active = 0;
   __syncthreads();
   {
     const int* src = reinterpret_cast<const int*>(&C);

@@ -103,6 +103,8 @@ struct BatchLaunch {
   double* shadow;     // mixed, optional [nchains][moves][4]: FP64 {ewld1, ewld2, vdw, dE} of every
                       // move on the same state
   long long* timing;  // optional [nchains][3]: the CTA's start and end (%globaltimer, ns) and its SM
+  int retire_finished;  // a chain that ends its budget, its deck's cycles or on an error marks itself
+                        // inactive, so that a launch queued behind this one skips it (serving)
 };
 
 cudaError_t launch_batch(const BatchLaunch& L, int smem_bytes, int tab_stride, cudaStream_t st);

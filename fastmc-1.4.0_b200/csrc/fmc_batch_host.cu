@@ -490,6 +490,7 @@ int Batch::run(int moves, MoveRecord* trace_host, float* ms, std::string& err, d
   L.trace = nullptr;
   L.shadow = nullptr;
   L.timing = d_timing;
+  L.retire_finished = 0;
   cudaError_t e = cudaSuccess;
   if (shadow_host && mixed) {
     size_t need = (size_t)nchains * moves;

@@ -1,12 +1,14 @@
 // Serving: isotherm-point requests (a FastMC input deck + seed + budget) run as chains of
 // the persistent batched kernel with continuous batching.  Host worker threads parse each
-// queued request's deck and build its host tables ahead of time; each step admits prepared
-// requests from the front of the queue into free slots while the device-memory budget allows
-// (every slot holds its own framework system and chain state), advances every active slot by
-// up to `moves` moves in one launch, and retires the chains that have used their budget (a
-// move count, or with 0 the deck's own equilibration + production cycles), freeing their
-// slots and memory for the next step.  The reference runs one such isotherm point per MPI
-// rank (gcmc.f:334-417).
+// queued request's deck and build its host tables ahead of time.  Launches are pipelined: a
+// step queues the next launch of every running slot (the device keeps each chain's control
+// block between launches) and only then completes the previous launch: it retires the chains
+// that used their budget (a move count, or with 0 the deck's own equilibration + production
+// cycles; a finished chain marks itself inactive, so the launch already queued skips it) and
+// admits prepared requests from the front of the queue into free slots while the device-memory
+// budget allows, building them on a second stream beside the running launch for the launch after
+// it.  So launches follow one another without waiting for the host.  The reference runs one
+// such isotherm point per MPI rank (gcmc.f:334-417).
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -32,6 +34,13 @@ double now_ms() {
 }
 }  // namespace
 
+struct Prebuilt {
+  SlotMemory mem;
+  SysConst Y;
+  ChainDev C;
+  long long vox_cap = 0;
+};
+
 class Server {
  public:
   enum State { kQueued = 0, kRunning = 1, kDone = 2, kRejected = -1, kCancelled = -2 };
@@ -48,6 +57,14 @@ class Server {
     std::string prep_err;
     std::unique_ptr<HostSystem> host;
     size_t bytes_estimate = 0;
+    // the device slot a worker built ahead of admission (null: built at admission instead)
+    std::unique_ptr<struct Prebuilt> pre;
+  };
+  // A worker's own stream, pinned staging and voxel-count word for building slots ahead.
+  struct WorkerRes {
+    cudaStream_t st = nullptr;
+    Staging stage;
+    int* vox_total = nullptr;
   };
   struct Slot {
     int request = -1;
@@ -62,7 +79,12 @@ class Server {
   int device = 0;
   cudaStream_t st = nullptr;
   int nslots = 0, kcap = 0, tab_sites = 2 * kServeMaxSites, tab_stride = 0, smem = 0;
-  size_t budget = 0, used = 0;
+  size_t budget = 0;
+  std::atomic<size_t> used{0};      // device bytes of admitted slots
+  size_t prebuilt_bytes = 0;        // device bytes of slots built ahead (guarded by mu)
+  int prebuilt_count = 0;
+  static constexpr int kMaxPrebuilt = 64;  // slots built ahead at most
+  std::vector<WorkerRes> wres;
   cudaMemPool_t pool = nullptr;
   int mixed = 0;
   long long recompute_every = 0;
@@ -71,14 +93,22 @@ class Server {
   std::deque<int> queue;                       // admission order (caller's thread only)
   SysConst* h_sys = nullptr;
   SysConst* d_sys = nullptr;
-  ChainDev* h_chains = nullptr;
-  ChainDev* d_chains = nullptr;
-  ChainDev* h_out = nullptr;      // pinned: control blocks as the last launch left them
+  ChainDev* h_chains = nullptr;   // pinned: each slot's control block as of the last completed launch
+  ChainDev* d_chains = nullptr;   // the device copy the launches read and write
+  ChainDev* h_out[2] = {nullptr, nullptr};  // pinned: control blocks after launch buffer b
   int* h_vox_total = nullptr;     // pinned: exact voxel-list size of each slot's last build
-  std::vector<char> launched;     // slots in the current launch
+  std::vector<int> launched[2];   // per slot, the request launch buffer b ran (-1: none)
+  int* h_zero = nullptr;          // pinned 0: the `active` flag of a cancelled slot
+  int inflight = -1;              // buffer of the launch queued and not yet completed (-1: none)
+  int next_buf = 0;
+  std::vector<int> fresh;         // slots admitted since the last launch (uploaded before the next)
+  std::vector<int> deactivate;    // cancelled slots to switch off on the device before the next launch
+  std::vector<std::pair<int, int>> deferred;  // (slot, buffer): memory freed once that launch completed
+  std::vector<int> done_log;      // requests that reached a final state, for poll_done
   cudaStream_t st2 = nullptr;     // admission stream (slot set-up beside the running launch)
   Staging stage;                  // pinned staging of slot uploads
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_h2d = nullptr;
+  cudaEvent_t ev_start[2] = {nullptr, nullptr}, ev_end[2] = {nullptr, nullptr}, ev_done[2] = {nullptr, nullptr};
+  cudaEvent_t ev_admit = nullptr;  // recorded on the admission stream after the last admission
   // worker pool
   std::mutex mu;
   std::condition_variable cv;
@@ -99,16 +129,31 @@ class Server {
     for (auto& t : workers) t.join();
     if (!st) return;
     cudaSetDevice(device);
+    for (auto& r : reqs)
+      if (r->pre) {
+        r->pre->mem.release();
+        r->pre.reset();
+      }
     cudaStreamSynchronize(st);
     if (st2) cudaStreamSynchronize(st2);
-    for (int i = 0; i < nslots; i++) release(i);
+    for (int i = 0; i < nslots; i++) release(i);  // frees on the slot's stream (st2 or a worker's)
     if (st2) cudaStreamSynchronize(st2);
+    for (WorkerRes& w : wres) {
+      if (w.st) cudaStreamSynchronize(w.st);
+      if (w.stage.base) cudaFreeHost(w.stage.base);
+      if (w.vox_total) cudaFreeHost(w.vox_total);
+      if (w.st) cudaStreamDestroy(w.st);
+    }
     if (pool) cudaMemPoolDestroy(pool);
-    if (ev0) cudaEventDestroy(ev0);
-    if (ev1) cudaEventDestroy(ev1);
-    if (ev_h2d) cudaEventDestroy(ev_h2d);
-    if (h_out) cudaFreeHost(h_out);
+    for (int b = 0; b < 2; b++) {
+      if (ev_start[b]) cudaEventDestroy(ev_start[b]);
+      if (ev_end[b]) cudaEventDestroy(ev_end[b]);
+      if (ev_done[b]) cudaEventDestroy(ev_done[b]);
+      if (h_out[b]) cudaFreeHost(h_out[b]);
+    }
+    if (ev_admit) cudaEventDestroy(ev_admit);
     if (h_vox_total) cudaFreeHost(h_vox_total);
+    if (h_zero) cudaFreeHost(h_zero);
     if (stage.base) cudaFreeHost(stage.base);
     if (st2) cudaStreamDestroy(st2);
     if (d_sys) cudaFree(d_sys);
@@ -157,34 +202,55 @@ class Server {
       return -100;
     }
     slots.resize(n);
-    launched.assign(n, 0);
+    launched[0].assign(n, -1);
+    launched[1].assign(n, -1);
     for (auto& sl : slots) {
       sl.mem.st = st2;
       sl.mem.pool = pool;
     }
     stage.cap = 64u << 20;
     cudaError_t e = cudaMallocHost(&stage.base, stage.cap);
-    if (e == cudaSuccess) e = cudaMallocHost(&h_out, sizeof(ChainDev) * n);
+    for (int b = 0; b < 2 && e == cudaSuccess; b++) {
+      e = cudaMallocHost(&h_out[b], sizeof(ChainDev) * n);
+      if (e == cudaSuccess) e = cudaEventCreate(&ev_start[b]);
+      if (e == cudaSuccess) e = cudaEventCreate(&ev_end[b]);
+      if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_done[b], cudaEventDisableTiming);
+    }
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_admit, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaMallocHost(&h_vox_total, sizeof(int) * n);
-    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_h2d, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaMallocHost(&h_zero, sizeof(int));
+    if (e == cudaSuccess) *h_zero = 0;
     if (e == cudaSuccess) e = cudaMallocHost(&h_sys, sizeof(SysConst) * n);
     if (e == cudaSuccess) e = cudaMallocHost(&h_chains, sizeof(ChainDev) * n);
     if (e == cudaSuccess) e = cudaMalloc(&d_sys, sizeof(SysConst) * n);
     if (e == cudaSuccess) e = cudaMalloc(&d_chains, sizeof(ChainDev) * n);
-    if (e == cudaSuccess) e = cudaEventCreate(&ev0);
-    if (e == cudaSuccess) e = cudaEventCreate(&ev1);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_chains, 0, sizeof(ChainDev) * n, st);  // every slot inactive
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) {
       err = std::string("server allocation failed: ") + cudaGetErrorString(e);
       return -100 - (int)e;
     }
     std::memset(h_sys, 0, sizeof(SysConst) * n);
     std::memset(h_chains, 0, sizeof(ChainDev) * n);
-    for (int w = 0; w < nworkers; w++) workers.emplace_back([this] { worker(); });
+    wres.resize(nworkers);
+    for (WorkerRes& w : wres) {
+      if (cudaStreamCreateWithFlags(&w.st, cudaStreamNonBlocking) != cudaSuccess ||
+          cudaMallocHost(&w.vox_total, sizeof(int)) != cudaSuccess) {
+        err = "cannot create a worker's stream";
+        return -100;
+      }
+      w.stage.cap = 8u << 20;
+      if (cudaMallocHost(&w.stage.base, w.stage.cap) != cudaSuccess) {
+        err = "cannot allocate a worker's staging buffer";
+        return -100;
+      }
+    }
+    for (int w = 0; w < nworkers; w++) workers.emplace_back([this, w] { worker(w); });
     return 0;
   }
 
   // Host preparation of one request: deck, host tables and the serving capacity checks.
-  void prepare(Request& r) {
+  void prepare(Request& r, WorkerRes* w = nullptr) {
     const double t0 = now_ms();
     auto h = std::make_unique<HostSystem>();
     std::string err;
@@ -214,13 +280,66 @@ class Server {
     if (!rc) {
       r.bytes_estimate = slot_bytes_estimate(*h);
       r.host = std::move(h);
+      if (w) prebuild(r, *w);
     }
     prep_us += (long long)((now_ms() - t0) * 1000.0);
     r.prepared.store(1, std::memory_order_release);
   }
 
-  // Worker threads: host preparation of queued requests, in submission order.
-  void worker() {
+  // A worker builds the request's device slot on its own stream, while the memory budget allows,
+  // and checks its voxel lists, so that admission only installs it.  On any failure the slot is
+  // left to be built at admission.
+  void prebuild(Request& r, WorkerRes& w) {
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      if (prebuilt_count >= kMaxPrebuilt || used.load() + prebuilt_bytes + r.bytes_estimate > budget) return;
+      prebuilt_bytes += r.bytes_estimate;
+      prebuilt_count++;
+    }
+    auto P = std::make_unique<Prebuilt>();
+    P->mem.st = w.st;
+    P->mem.pool = pool;
+    const size_t need = slot_staging_bytes(*r.host);
+    bool ok = true;
+    if (need > w.stage.cap) {
+      cudaFreeHost(w.stage.base);
+      w.stage.cap = need;
+      if (cudaMallocHost(&w.stage.base, w.stage.cap) != cudaSuccess) {
+        w.stage.base = nullptr;
+        w.stage.cap = 0;
+        ok = false;
+      }
+    }
+    std::string err;
+    for (int attempt = 0; ok && attempt < 2; attempt++) {
+      w.stage.used = 0;
+      if (attempt == 0) P->vox_cap = slot_voxel_capacity(*r.host);
+      ok = build_slot(*r.host, 0, r.seed, P->mem, w.stage, P->vox_cap, w.vox_total, P->Y, P->C, err) == 0 &&
+           cudaStreamSynchronize(w.st) == cudaSuccess;
+      if (ok && (long long)*w.vox_total <= P->vox_cap) break;
+      P->mem.release();  // the lists outgrew the estimate: once more at their exact size
+      P->vox_cap = *w.vox_total;
+      ok = ok && attempt == 0;
+    }
+    std::lock_guard<std::mutex> lk(mu);
+    prebuilt_bytes -= r.bytes_estimate;
+    if (ok) {
+      P->C.budget = r.moves;
+      prebuilt_bytes += P->mem.bytes;
+      r.pre = std::move(P);
+    } else {
+      prebuilt_count--;
+      if (P->mem.bytes) {
+        P->mem.release();
+        cudaStreamSynchronize(w.st);
+      }
+    }
+  }
+
+  // Worker threads: host preparation of queued requests, in submission order, and their device
+  // slots built ahead on the worker's stream.
+  void worker(int wi) {
+    cudaSetDevice(device);
     for (;;) {
       Request* r = nullptr;
       {
@@ -230,7 +349,7 @@ class Server {
         r = reqs[prep_queue.front()].get();
         prep_queue.pop_front();
       }
-      prepare(*r);
+      prepare(*r, &wres[wi]);
     }
   }
 
@@ -271,17 +390,45 @@ class Server {
           break;
         }
       r.state = kCancelled;
+      done_log.push_back(id);
+      if (r.prepared.load(std::memory_order_acquire)) drop_prebuilt(r);
     } else if (r.state == kRunning) {
-      snapshot(r.slot, r);
-      release(r.slot);
+      const int i = r.slot;
+      snapshot(i, r);  // the state as of the last completed launch
       r.state = kCancelled;
+      done_log.push_back(id);
+      auto f = std::find(fresh.begin(), fresh.end(), i);
+      if (f != fresh.end()) {  // built but never launched: nothing on the device reads it
+        fresh.erase(f);
+        release(i);
+      } else {
+        // switched off on the device before the next launch; its memory is freed once the launch
+        // in flight (which may still run it) has completed, or now if none is
+        deactivate.push_back(i);
+        if (inflight >= 0) {
+          slots[i].request = -2;  // held until then
+          deferred.push_back({i, inflight});
+        } else {
+          release(i);
+        }
+      }
     }
     return 0;
   }
 
+  // Frees a request's slot built ahead (its preparation has finished).
+  void drop_prebuilt(Request& r) {
+    if (!r.pre) return;
+    std::lock_guard<std::mutex> lk(mu);
+    prebuilt_bytes -= std::min(prebuilt_bytes, r.pre->mem.bytes);
+    prebuilt_count--;
+    r.pre->mem.release();
+    r.pre.reset();
+  }
+
   void release(int i) {
     Slot& s = slots[i];
-    used -= std::min(used, s.mem.bytes);
+    used -= std::min(used.load(), s.mem.bytes);
     s.mem.release();
     s.request = -1;
     h_chains[i].active = 0;
@@ -329,6 +476,11 @@ class Server {
     r.err = err;
     r.result[1] = rc;
     r.host.reset();
+    for (int id = (int)reqs.size() - 1; id >= 0; id--)
+      if (reqs[id].get() == &r) {
+        done_log.push_back(id);
+        break;
+      }
   }
 
   // Enqueues the slot set-up of prepared request `id` into free slot `i` on the admission
@@ -339,6 +491,27 @@ class Server {
     if (r.prep_rc) {
       reject(r, r.prep_rc, r.prep_err);
       return 0;
+    }
+    if (r.pre) {  // built ahead by a worker: install it
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        prebuilt_bytes -= std::min(prebuilt_bytes, r.pre->mem.bytes);
+        prebuilt_count--;
+      }
+      s.mem = std::move(r.pre->mem);
+      s.vox_cap = r.pre->vox_cap;
+      h_sys[i] = r.pre->Y;
+      h_chains[i] = r.pre->C;
+      h_chains[i].sys = i;
+      r.pre.reset();
+      r.host.reset();
+      s.request = id;
+      s.fresh = false;  // checked by its worker
+      fresh.push_back(i);
+      r.state = kRunning;
+      r.slot = i;
+      admitted++;
+      return s.mem.bytes;
     }
     const size_t need = slot_staging_bytes(*r.host);
     if (stage.used + need > stage.cap) {  // the staged bytes of earlier admissions are read by now
@@ -365,6 +538,7 @@ class Server {
     h_chains[i].budget = r.moves;
     s.request = id;
     s.fresh = true;
+    fresh.push_back(i);
     r.state = kRunning;
     r.slot = i;
     admitted++;
@@ -376,7 +550,7 @@ class Server {
   void admit_queued(int running) {
     const double t0 = now_ms();
     for (int i = 0; i < nslots && !queue.empty(); i++) {
-      if (slots[i].request >= 0) continue;
+      if (slots[i].request != -1) continue;  // running, or cancelled with its memory still held
       const int id = queue.front();
       Request& r = req(id);
       if (workers.empty()) {
@@ -387,7 +561,12 @@ class Server {
         while (!r.prepared.load(std::memory_order_acquire)) std::this_thread::sleep_for(std::chrono::microseconds(200));
         wait_ms += now_ms() - w0;
       }
-      if (!r.prep_rc && used + r.bytes_estimate > budget) {
+      size_t ahead;
+      {
+        std::lock_guard<std::mutex> lk(mu);
+        ahead = prebuilt_bytes;
+      }
+      if (!r.prep_rc && !r.pre && used.load() + ahead + r.bytes_estimate > budget) {
         if (r.bytes_estimate > budget) {
           queue.pop_front();
           reject(r, -10, "the request's device footprint exceeds the server's memory budget");
@@ -418,7 +597,7 @@ class Server {
       s.fresh = false;
       Request& r = req(s.request);
       if ((long long)h_vox_total[i] > s.vox_cap) {
-        used -= std::min(used, s.mem.bytes);
+        used -= std::min(used.load(), s.mem.bytes);
         s.mem.release();
         s.vox_cap = h_vox_total[i];
         std::string e2;
@@ -429,6 +608,7 @@ class Server {
           s.mem.release();
           s.request = -1;
           std::memset(&h_chains[i], 0, sizeof(ChainDev));
+          fresh.erase(std::remove(fresh.begin(), fresh.end(), i), fresh.end());
           reject(r, rc ? rc : -12, rc ? e2 : "voxel lists changed size between builds");
           continue;
         }
@@ -440,84 +620,148 @@ class Server {
     return 0;
   }
 
-  int step(int moves, int* n_active, int* n_queued, float* ms, std::string& err) {
-    cudaSetDevice(device);
-    int running = 0;
-    for (int i = 0; i < nslots; i++) {
-      launched[i] = slots[i].request >= 0;
-      running += launched[i];
-    }
-    if (!running) {  // nothing on the device: admit first, then launch what was admitted
-      admit_queued(0);
-      int rc = settle_admissions(err);
-      if (rc) return rc;
-      for (int i = 0; i < nslots; i++) {
-        launched[i] = slots[i].request >= 0;
-        running += launched[i];
-      }
-    }
+  // Completes launch buffer b: the control blocks it left, retirements, the deferred frees.
+  int complete(int b, int* n_active, float* ms, std::string& err) {
+    cudaError_t e = cudaEventSynchronize(ev_done[b]);
     float t = 0.f;
-    last_moves = 0;
-    cudaError_t e = cudaSuccess;
-    if (running) {
-      e = cudaMemcpyAsync(d_sys, h_sys, sizeof(SysConst) * nslots, cudaMemcpyHostToDevice, st);
-      if (e == cudaSuccess)
-        e = cudaMemcpyAsync(d_chains, h_chains, sizeof(ChainDev) * nslots, cudaMemcpyHostToDevice, st);
-      if (e == cudaSuccess) e = cudaEventRecord(ev_h2d, st);
-      BatchLaunch L;
-      std::memset(&L, 0, sizeof(L));
-      L.chains = d_chains;
-      L.systems = d_sys;
-      L.nchains = nslots;
-      L.moves = moves;
-      L.kmax_smem = kcap;
-      L.mixed = mixed;
-      L.recompute_every = recompute_every;
-      if (e == cudaSuccess) e = cudaEventRecord(ev0, st);
-      if (e == cudaSuccess) e = launch_batch(L, smem, tab_stride, st);
-      if (e == cudaSuccess) e = cudaEventRecord(ev1, st);
-      if (e == cudaSuccess)
-        e = cudaMemcpyAsync(h_out, d_chains, sizeof(ChainDev) * nslots, cudaMemcpyDeviceToHost, st);
-      // requests admitted now set up on the admission stream while the launch runs; their host
-      // control blocks change only after the launch's copy of them has been read
-      if (e == cudaSuccess) e = cudaEventSynchronize(ev_h2d);
-      if (e == cudaSuccess) admit_queued(running);
-      if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-      if (e == cudaSuccess) cudaEventElapsedTime(&t, ev0, ev1);
-      if (e != cudaSuccess) {
-        err = std::string("serving launch failed: ") + cudaGetErrorString(e);
-        return -100 - (int)e;
-      }
-      int rc = settle_admissions(err);
-      if (rc) return rc;
-      launches++;
-      launch_ms += t;
-      for (int i = 0; i < nslots; i++)
-        if (launched[i]) {
-          last_moves += h_out[i].moves_done - h_chains[i].moves_done;
-          h_chains[i] = h_out[i];
-        }
-      moves_run += last_moves;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&t, ev_start[b], ev_end[b]);
+    if (e != cudaSuccess) {
+      err = std::string("serving launch failed: ") + cudaGetErrorString(e);
+      return -100 - (int)e;
     }
-    // retirement of the chains that ran
+    launches++;
+    launch_ms += t;
+    last_moves = 0;
+    int ran = 0;
     for (int i = 0; i < nslots; i++) {
-      int id = slots[i].request;
-      if (id < 0 || !launched[i]) continue;
+      if (launched[b][i] < 0) continue;
+      ran++;
+      const int id = slots[i].request;
+      // cancelled while this launch ran, or retired by the launch before and taken by a new request
+      if (id != launched[b][i]) continue;
+      last_moves += h_out[b][i].moves_done - h_chains[i].moves_done;
+      h_chains[i] = h_out[b][i];
       const ChainDev& C = h_chains[i];
       if ((C.budget > 0 && C.moves_done >= C.budget) || !C.lgchk || C.status) {
+        // the chain switched itself off on the device: the launch queued behind this one skips it
         Request& r = req(id);
         snapshot(i, r);
         r.state = C.status ? kRejected : kDone;
         if (C.status) r.err = C.status == 75 ? "too many atoms in specified system" : "chain stopped with an unknown status";
+        done_log.push_back(id);
         release(i);
         retired++;
       }
     }
-    if (n_active) *n_active = running;
-    if (n_queued) *n_queued = (int)queue.size();
+    moves_run += last_moves;
+    for (size_t k = 0; k < deferred.size();) {
+      if (deferred[k].second == b) {
+        release(deferred[k].first);
+        deferred.erase(deferred.begin() + k);
+      } else {
+        k++;
+      }
+    }
+    if (n_active) *n_active = ran;
     if (ms) *ms = t;
     return 0;
   }
+
+  // Queues one launch of every running slot into buffer b, after the uploads of the slots admitted
+  // or cancelled since the last launch; the control blocks come back to h_out[b].
+  int enqueue_launch(int moves, int b, std::string& err) {
+    cudaError_t e = cudaSuccess;
+    // cancelled slots first: a slot cancelled and then taken by a new request gets the new block
+    for (int i : deactivate)
+      if (e == cudaSuccess) e = cudaMemcpyAsync(&d_chains[i].active, h_zero, sizeof(int), cudaMemcpyHostToDevice, st);
+    if (!fresh.empty() && e == cudaSuccess) e = cudaStreamWaitEvent(st, ev_admit, 0);  // their set-up
+    for (int i : fresh) {
+      if (e == cudaSuccess) e = cudaMemcpyAsync(d_sys + i, h_sys + i, sizeof(SysConst), cudaMemcpyHostToDevice, st);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_chains + i, h_chains + i, sizeof(ChainDev), cudaMemcpyHostToDevice, st);
+      slots[i].fresh = false;
+    }
+    fresh.clear();
+    deactivate.clear();
+    for (int i = 0; i < nslots; i++) launched[b][i] = slots[i].request >= 0 ? slots[i].request : -1;
+    BatchLaunch L;
+    std::memset(&L, 0, sizeof(L));
+    L.chains = d_chains;
+    L.systems = d_sys;
+    L.nchains = nslots;
+    L.moves = moves;
+    L.kmax_smem = kcap;
+    L.mixed = mixed;
+    L.recompute_every = recompute_every;
+    L.retire_finished = 1;
+    if (e == cudaSuccess) e = cudaEventRecord(ev_start[b], st);
+    if (e == cudaSuccess) e = launch_batch(L, smem, tab_stride, st);
+    if (e == cudaSuccess) e = cudaEventRecord(ev_end[b], st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h_out[b], d_chains, sizeof(ChainDev) * nslots, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaEventRecord(ev_done[b], st);
+    if (e != cudaSuccess) {
+      err = std::string("serving launch failed: ") + cudaGetErrorString(e);
+      return -100 - (int)e;
+    }
+    return 0;
+  }
+
+  int running_slots() const {
+    int n = 0;
+    for (const Slot& sl : slots) n += sl.request >= 0;
+    return n;
+  }
+
+  // One step: queue the next launch, then complete the one before it (see the file comment).
+  int step(int moves, int* n_active, int* n_queued, float* ms, std::string& err) {
+    cudaSetDevice(device);
+    if (n_active) *n_active = 0;
+    if (ms) *ms = 0.f;
+    int rc = 0;
+    if (!fresh.empty()) {  // last step's admissions: set up and checked before their first launch
+      rc = settle_admissions(err);
+      if (rc) return rc;
+    }
+    if (inflight < 0 && running_slots() == 0 && !queue.empty()) {  // idle device: admit first
+      admit_queued(0);
+      rc = settle_admissions(err);
+      if (rc) return rc;
+    }
+    const int prev = inflight;
+    inflight = -1;
+    if (running_slots() > 0) {
+      const int b = next_buf;
+      next_buf ^= 1;
+      rc = enqueue_launch(moves, b, err);
+      if (rc) return rc;
+      inflight = b;
+    }
+    if (prev >= 0) {
+      rc = complete(prev, n_active, ms, err);
+      if (rc) return rc;
+    }
+    if (inflight >= 0 || running_slots() == 0) {
+      admit_queued(inflight >= 0);  // built beside the launch in flight, launched by the next step
+      if (!fresh.empty()) cudaEventRecord(ev_admit, st2);
+    }
+    if (n_queued) *n_queued = (int)queue.size();
+    return 0;
+  }
+
+  // Requests that reached a final state since the last call (at most cap of them).
+  int poll_done(int* ids, int* states, double* results, int cap) {
+    const int n = std::min<int>(cap, (int)done_log.size());
+    for (int k = 0; k < n; k++) {
+      const Request& r = req(done_log[k]);
+      if (ids) ids[k] = done_log[k];
+      if (states) states[k] = r.state;
+      if (results) std::memcpy(results + 32 * k, r.result, sizeof(r.result));
+    }
+    done_log.erase(done_log.begin(), done_log.begin() + n);
+    return n;
+  }
+
+  bool busy() const { return inflight >= 0 || running_slots() > 0 || !queue.empty(); }
 };
 
 }  // namespace fmc
@@ -600,12 +844,30 @@ int fmc_server_poll(fmc_server* s, int request_id, int* state, double* out) {
   return 0;
 }
 
+int fmc_server_poll_done(fmc_server* s, int* ids, int* states, double* results, int cap, int* n) {
+  if (!s || cap < 0 || !n) {
+    fmc::set_last_error("bad server handle or capacity");
+    return -1;
+  }
+  *n = s->impl.poll_done(ids, states, results, cap);
+  return 0;
+}
+
+int fmc_server_busy(fmc_server* s, int* busy) {
+  if (!s || !busy) {
+    fmc::set_last_error("bad server handle");
+    return -1;
+  }
+  *busy = s->impl.busy() ? 1 : 0;
+  return 0;
+}
+
 int fmc_server_memory(fmc_server* s, long long* used, long long* budget) {
   if (!s) {
     fmc::set_last_error("bad server handle");
     return -1;
   }
-  if (used) *used = (long long)s->impl.used;
+  if (used) *used = (long long)s->impl.used.load();
   if (budget) *budget = (long long)s->impl.budget;
   return 0;
 }

@@ -543,8 +543,24 @@ class Server:
     def cancel(self, rid):
         check(lib().fmc_server_cancel(self.h, int(rid)))
 
+    def busy(self):
+        """True while a launch is in flight, a request runs or one is queued."""
+        b = ctypes.c_int(0)
+        check(lib().fmc_server_busy(self.h, ctypes.byref(b)))
+        return bool(b.value)
+
+    def poll_done(self, cap=4096):
+        """Requests that reached a final state since the last call: list of (id, state, result)."""
+        ids = np.zeros(cap, dtype=np.int32)
+        states = np.zeros(cap, dtype=np.int32)
+        res = np.zeros((cap, 32))
+        n = ctypes.c_int(0)
+        check(lib().fmc_server_poll_done(self.h, ip(ids), ip(states), dp(res), int(cap), ctypes.byref(n)))
+        return [(int(ids[k]), int(states[k]), dict(zip(self._OUT, res[k].tolist()))) for k in range(n.value)]
+
     def step(self, moves):
-        """One continuous-batching step; returns (active, queued, device ms)."""
+        """One pipelined continuous-batching step (queues the next launch, completes the previous
+        one); returns (active in the completed launch, queued, its device ms)."""
         a, q, ms = ctypes.c_int(0), ctypes.c_int(0), ctypes.c_float(0)
         check(lib().fmc_server_step(self.h, int(moves), ctypes.byref(a), ctypes.byref(q), ctypes.byref(ms)))
         return a.value, q.value, float(ms.value)

@@ -128,6 +128,8 @@ SIGNATURES = {
     "fmc_server_cancel": (_ci, [_vp, _ci]),
     "fmc_server_step": (_ci, [_vp, _ci, _ip, _ip, ctypes.POINTER(ctypes.c_float)]),
     "fmc_server_poll": (_ci, [_vp, _ci, _ip, _dp]),
+    "fmc_server_busy": (_ci, [_vp, _ip]),
+    "fmc_server_poll_done": (_ci, [_vp, _ip, _ip, _dp, _ci, _ip]),
     "fmc_server_stats": (_ci, [_vp, _dp]),
     "fmc_server_memory": (_ci, [_vp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
     "fmc_deck_vdw": (_ci, [ctypes.c_char_p, _ci, _dp, _ip]),

@@ -341,9 +341,22 @@ void fmc_server_close(fmc_server* s);
 int fmc_server_set_precision(fmc_server* s, int mixed, long long recompute_every);
 int fmc_server_submit(fmc_server* s, const char* dir, const int* seed, long long moves, int* request_id);
 int fmc_server_cancel(fmc_server* s, int request_id);
-/* *active: requests advanced by this step's launch; *queued: requests still waiting. */
+/* One step of the pipelined server: queues the next launch of every running request (after the
+ * uploads of the requests admitted by the previous step), then completes the launch queued by
+ * the previous step -- its finished requests are retired -- and admits queued requests into free
+ * slots, set up beside the launch in flight for the launch after it.  So the device runs launch
+ * after launch while the host retires and admits.  *active: requests in the completed launch
+ * (0 on a step that completed none); *device_ms: its device time; *queued: requests still
+ * waiting.  Requests keep stepping while fmc_server_busy reports work. */
 int fmc_server_step(fmc_server* s, int moves, int* active, int* queued, float* device_ms);
+/* *busy = 1 while a launch is in flight, a request runs or one is queued. */
+int fmc_server_busy(fmc_server* s, int* busy);
+/* Requests that reached a final state (done, rejected, cancelled) since the last call, oldest
+ * first, at most cap: ids[cap], states[cap] and results[cap*32] (the layout of fmc_server_poll)
+ * -- one call per step instead of a poll per live request. */
+int fmc_server_poll_done(fmc_server* s, int* ids, int* states, double* results, int cap, int* n);
 /* *state: 0 queued, 1 running, 2 done, -1 rejected (message in fmc_last_error), -2 cancelled.
+ * A running request's results are those of the last completed launch.
  * out[0..31]: moves done, status, nmol[4], energy[4] (kcal/mol), production moves,
  * species-0 <N>,<E>,<EN>,<N^2>,<E^2>, accepted insertions, accepted deletions, FP64 re-checks,
  * K, framework atoms, T, P(species 0), move budget, 1 if the deck's cycles finished,

@@ -2,7 +2,9 @@
 
 A served request must end in exactly the state the same deck and seed reach in a batch of
 their own (FP64: nmol, energies and production statistics bitwise), whatever the other
-requests in the launches were and however the move budget was cut into steps."""
+requests in the launches were and however the move budget was cut into steps.  Steps are
+pipelined: a step queues the next launch and then completes the previous one, so results, polls
+and cancellations refer to the last completed launch."""
 import numpy as np
 import pytest
 
@@ -31,17 +33,18 @@ def _same(res, st):
 def test_continuous_batching_matches_isolated_runs(fmc, decks):
     srv = fmc.Server(slots=3, k_capacity=2400)
     ids = [srv.submit(decks[n], s, m) for n, s, m in REQS]
-    seen_active, steps = [], 0
-    while True:
+    seen_active, steps, finished = [], 0, []
+    while srv.busy():
         active, queued, ms = srv.step(250)
+        finished += srv.poll_done()
         steps += 1
         seen_active.append(active)
         assert active <= 3
-        if active == 0 and queued == 0:
-            break
         assert steps < 100
     # more requests than slots: later requests waited for retirements
     assert max(seen_active) == 3
+    assert sorted(f[0] for f in finished) == sorted(ids)
+    assert all(f[1] == srv.DONE and f[2]["moves"] == REQS[ids.index(f[0])][2] for f in finished)
     for rid, (n, s, m) in zip(ids, REQS):
         res = srv.poll(rid)
         assert res["state"] == srv.DONE, res
@@ -62,16 +65,19 @@ def test_serve_cancel_and_reject(fmc, decks, tmp_path):
     b = srv.submit(decks["ortho0"], (31, 41, 59, 26), 5000)
     c = srv.submit(decks["ortho0"], (5, 5, 5, 5), 300)
     srv.cancel(c)  # cancelled while queued: never runs
-    srv.step(200)
+    srv.step(200)  # admits a and b and queues their first launch
     assert srv.poll(missing)["state"] == srv.REJECTED
     r = srv.poll(big)
     assert r["state"] == srv.REJECTED and "k-vector" in r["error"]
     assert srv.poll(a)["state"] == srv.RUNNING and srv.poll(b)["state"] == srv.RUNNING
-    srv.cancel(b)  # cancelled while running: slot freed, partial result kept
+    srv.step(200)  # queues the second launch, completes the first
+    srv.cancel(b)  # cancelled while its second launch runs: switched off, last completed state kept
     rb = srv.poll(b)
     assert rb["state"] == srv.CANCELLED and rb["moves"] == 200
-    while srv.step(200)[0]:
-        pass
+    done = [f[0] for f in srv.poll_done()]
+    assert set(done) == {c, big, missing, b}
+    while srv.busy():
+        srv.step(200)
     assert srv.poll(c)["state"] == srv.CANCELLED and srv.poll(c)["moves"] == 0
     ra = srv.poll(a)
     assert ra["state"] == srv.DONE
@@ -90,13 +96,13 @@ def test_serve_memory_budget_limits_admission(fmc, decks):
     srv = fmc.Server(slots=4, mem_budget=int(1.5 * slot_bytes))
     ids = [srv.submit(decks["small"], (i + 1, 2, 3, 4), 300) for i in range(3)]
     active_seen = []
-    for _ in range(20):
+    for _ in range(40):
+        if not srv.busy():
+            break
         active, queued, _ = srv.step(300)
         active_seen.append(active)
         used, budget = srv.memory()
         assert used <= budget
-        if not active and not queued:
-            break
     assert all(srv.poll(i)["state"] == srv.DONE for i in ids)
     assert max(active_seen) == 1
     tiny = fmc.Server(slots=2, mem_budget=1 << 20)
@@ -120,8 +126,9 @@ def test_serve_deck_cycle_budget_matches_oracle(fmc, oracle_mod, tmp_path):
     rid = srv.submit(d, seed)
     other = srv.submit(d, (1, 2, 3, 4), 700)
     for _ in range(200):
-        if not srv.step(900)[0]:
+        if not srv.busy():
             break
+        srv.step(900)
     res = srv.poll(rid)
     assert res["state"] == srv.DONE and res["finished"] == 1.0
     assert res["moves"] == n_ref
