@@ -18,7 +18,7 @@ namespace {
 
 struct MoveSmem {
   int mtype, g, mol, nold, nnew, accepted, ex_lo, ex_hi;
-  int commit_lo, seg_end, ns, randchoice, need_lrc, rande_drawn, recheck;
+  int commit_lo, seg_end, ns, randchoice, need_lrc, rande_drawn;
   double delrc, rande;
   double r[7], dis_delr, dis_rot;  // the trial's random numbers and step sizes (select_move)
   double ewld1, ewld2, vdw, ewld3, estep;
@@ -130,52 +130,34 @@ __device__ __forceinline__ void assemble(const SysConst& Y, MoveSmem& M, const d
 }
 
 // Thread 0: acceptance (energy_eval, utility_pack.f:3049-3095, with the displacement
-// shortcut of gcmc.f:1330-1338).  `band` (kcal/mol) bounds the error of M.estep; when the
-// decision could differ inside that band the move is marked for an FP64 re-evaluation
-// instead (returns 1).  Random numbers are drawn exactly where the reference draws them.
-__device__ __forceinline__ int decide(ChainDev& C, const SysConst& Y, MoveSmem& M, double band) {
+// shortcut of gcmc.f:1330-1338).  Random numbers are drawn exactly where the reference draws them.
+__device__ __forceinline__ void decide(ChainDev& C, const SysConst& Y, MoveSmem& M) {
   const int g = M.g, mtype = M.mtype, nmols = C.nmol[g];
   double e = M.estep;
   if (mtype == kNoop) {  // nothing to accept or reject; no draw
     M.accepted = 0;
-    return 0;
+    return;
   }
   if (mtype == kMultiJump) {
-    if (M.mj_stage == 1) {  // the first jump is kept for now; its dE must be the FP64 one
+    if (M.mj_stage == 1) {  // the first jump is kept for now
       M.accepted = 1;
-      return band > 0.0 ? 1 : 0;
+      return;
     }
     e = M.mj_estep + e;  // one test on the summed change (gcmc.f:1730-1739)
   }
   if (mtype == kInsert || mtype == kDelete) {
-    if (!M.rande_drawn) {
-      M.rande = duni_next(C.rng);
-      M.rande_drawn = 1;
-    }
-    if (band > 0.0) {
-      bool lo = accept_move(e + band, M.rande, Y.statvolm, C.press[g], nmols, C.temp, C.beta, mtype);
-      bool hi = accept_move(e - band, M.rande, Y.statvolm, C.press[g], nmols, C.temp, C.beta, mtype);
-      if (lo != hi) return 1;
-    }
-    M.accepted = accept_move(e, M.rande, Y.statvolm, C.press[g], nmols, C.temp, C.beta, mtype);
-    return 0;
-  }
-  if (band > 0.0 && fabs(e) <= band) return 1;  // the sign decides whether rande is drawn
-  if (e < 0.0) {
-    M.accepted = 1;
-    return 0;
-  }
-  if (!M.rande_drawn) {
     M.rande = duni_next(C.rng);
     M.rande_drawn = 1;
+    M.accepted = accept_move(e, M.rande, Y.statvolm, C.press[g], nmols, C.temp, C.beta, mtype);
+    return;
   }
-  if (band > 0.0) {
-    bool lo = accept_move(e + band, M.rande, Y.statvolm, C.press[g], nmols, C.temp, C.beta, kDisplace);
-    bool hi = accept_move(e - band, M.rande, Y.statvolm, C.press[g], nmols, C.temp, C.beta, kDisplace);
-    if (lo != hi) return 1;
+  if (e < 0.0) {
+    M.accepted = 1;
+    return;
   }
+  M.rande = duni_next(C.rng);
+  M.rande_drawn = 1;
   M.accepted = accept_move(e, M.rande, Y.statvolm, C.press[g], nmols, C.temp, C.beta, kDisplace);
-  return 0;
 }
 
 // Thread 0: counters, running energy, statistics and the trace record (gcmc.f:954-1380,
@@ -284,7 +266,6 @@ __device__ __noinline__ void bookkeep(ChainDev& C, const SysConst& Y, MoveSmem& 
   }
   C.last_dE = accepted ? estep : 0.0;
   C.moves_done++;
-  C.since_recompute++;
   if (rec) {
     rec->step = C.gcmccount;
     rec->iguest = g;
@@ -292,7 +273,7 @@ __device__ __noinline__ void bookkeep(ChainDev& C, const SysConst& Y, MoveSmem& 
     rec->randchoice = M.randchoice;
     rec->accepted = counted;  // as the reference's `accepted` reads after the move
     rec->nmols_after = C.nmol[g];
-    rec->pad0 = M.recheck;
+    rec->pad0 = 0;
     rec->pad1 = 0;
     rec->ewld1 = M.ewld1;
     rec->ewld2 = M.ewld2;
@@ -357,7 +338,7 @@ __device__ __forceinline__ Cand fetch_candidate(const DevSystem& S, const ChainD
   } else {
     int jg = j - M.vl[s], g = 0;
     while (g + 1 < nseg && jg >= M.gpre[g + 1]) g++;
-    int site_idx = C.seg_off[g] + (jg - M.gpre[g]);
+    const int site_idx = C.seg_off[g] + (jg - M.gpre[g]);
     if (site_idx < M.ex_lo || site_idx >= M.ex_hi) {
       c.a = C.gsite[site_idx];
       c.type = C.gtype[site_idx];
@@ -367,33 +348,7 @@ __device__ __forceinline__ Cand fetch_candidate(const DevSystem& S, const ChainD
   return c;
 }
 
-// ------------------------------------------------------------------ precision-templated stages
-// e^{i 2 pi j s} for j = 0..kmax in FP32: the fractional coordinate is reduced to [0,1) in FP64,
-// the base phase comes from sincospif, higher harmonics from the FP32 recurrence.
-__device__ __forceinline__ void axis_phases_f32(double s, int kmax, float2* tab) {
-  float f = (float)(s - floor(s));
-  float sn, cs;
-  sincospif(2.0f * f, &sn, &cs);
-  tab[0] = make_float2(1.0f, 0.0f);
-  if (kmax >= 1) tab[1] = make_float2(cs, sn);
-  for (int j = 2; j <= kmax; j++) {
-    float2 p = tab[j - 1];
-    tab[j] = make_float2(p.x * cs - p.y * sn, p.y * cs + p.x * sn);
-  }
-}
-
-__device__ __forceinline__ float interp3f(const float* tab, float rrr, float rdr) {
-  float x = rrr * rdr;
-  int l = (int)x;
-  float ppp = x - (float)l;
-  float v0 = tab[l], v1 = tab[l + 1], v2 = tab[l + 2];
-  float t1 = v0 + (v1 - v0) * ppp;
-  float t2 = v1 + (v2 - v1) * (ppp - 1.0f);
-  return t1 + (t2 - t1) * ppp * 0.5f;
-}
-
-// Warp 0: phase tables of the trial sites (ewald.f:95-137) in the working precision.
-template <bool kMixed>
+// Warp 0: phase tables of the trial sites (ewald.f:95-137).
 __device__ __forceinline__ void build_phases(const DevSystem& S, const MoveSmem& M, void* tabv, int stride, int lane) {
   const int nsite = M.nold + M.nnew, k1 = S.kmax[0], k2 = S.kmax[1];
   for (int w = lane; w < nsite * 3; w += 32) {
@@ -401,10 +356,7 @@ __device__ __forceinline__ void build_phases(const DevSystem& S, const MoveSmem&
     double f[3];
     frac_coords(S.cell, M.x[st], M.y[st], M.z[st], f);
     int off = st * stride + (ax == 0 ? 0 : (ax == 1 ? k1 + 1 : k1 + k2 + 2));
-    if (kMixed)
-      axis_phases_f32(f[ax], S.kmax[ax], reinterpret_cast<float2*>(tabv) + off);
-    else
-      axis_phases(f[ax], S.kmax[ax], reinterpret_cast<double2*>(tabv) + off);
+    axis_phases(f[ax], S.kmax[ax], reinterpret_cast<double2*>(tabv) + off);
   }
 }
 
@@ -482,7 +434,6 @@ __device__ __noinline__ void select_move(ChainDev& C, const SysConst& Y, MoveSme
   M.rande = -1.0;
   M.need_lrc = 0;
   M.rande_drawn = 0;
-  M.recheck = 0;
   double* r = M.r;
   if (mtype == kInsert) {
     C.ins_count++;
@@ -596,17 +547,22 @@ __device__ __forceinline__ void rotate_site(const double q[4], double& x, double
 // and the real-space work list, then their phase tables (ewald.f:95-137).
 template <bool kProf>
 __device__ __noinline__ void build_trial(ChainDev& C, const SysConst& Y, const DevSystem& S, MoveSmem& M, void* tab,
-                                         int stride, bool fp32_phases, int lane) {
+                                         int stride, int lane) {
   if (kProf && lane == 0) C.prof[8] -= clock64();
   const int mtype = M.mtype, ns = M.ns, nold = M.nold, nnew = M.nnew, nseg = Y.nspecies;
   const SpeciesConst& P = Y.sp[M.g];
   const bool mine = lane < ns;
   double ox = 0.0, oy = 0.0, oz = 0.0, nx = 0.0, ny = 0.0, nz = 0.0;
+  int vb_old = 0, vl_old = 0;
   if (nold && mine) {
     const double4 a = C.gsite[M.ex_lo + lane];
     ox = a.x;
     oy = a.y;
     oz = a.z;
+    // the old site's voxel list, looked up while the trial geometry is computed
+    const int v = voxel_of(S, ox, oy, oz);
+    vb_old = S.vox_off[v];
+    vl_old = S.vox_off[v + 1] - vb_old;
   }
   const double* r = M.r;
   const double* h = S.cell.h;
@@ -686,9 +642,8 @@ __device__ __noinline__ void build_trial(ChainDev& C, const SysConst& Y, const D
     M.z[lane] = oz;
     M.q[lane] = P.q[lane];
     M.type[lane] = P.type[lane];
-    const int v = voxel_of(S, ox, oy, oz);
-    M.vb[lane] = S.vox_off[v];
-    M.vl[lane] = S.vox_off[v + 1] - S.vox_off[v];
+    M.vb[lane] = vb_old;
+    M.vl[lane] = vl_old;
   }
   if (mine && nnew) {
     const int st = nold + lane;
@@ -702,166 +657,107 @@ __device__ __noinline__ void build_trial(ChainDev& C, const SysConst& Y, const D
     M.vl[st] = S.vox_off[v + 1] - S.vox_off[v];
   }
   __syncwarp();
-  if (fp32_phases)
-    build_phases<true>(S, M, tab, stride, lane);
-  else
-    build_phases<false>(S, M, tab, stride, lane);
+  build_phases(S, M, tab, stride, lane);
+  // work-list prefix over the sites: each site's voxel list plus every guest site (warp scan)
+  int gt = 0;
+  for (int g = 0; g < nseg; g++) gt += C.nmol[g] * Y.sp[g].nsite;
+  int w = lane < nold + nnew ? M.vl[lane] + gt : 0;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int u = __shfl_up_sync(0xffffffffu, w, o);
+    if (lane >= o) w += u;
+  }
+  if (lane < nold + nnew) M.pre[lane + 1] = w;
   if (lane == 0) {
-    int gt = 0;
+    M.pre[0] = 0;
+    int acc = 0;
     M.gpre[0] = 0;
     for (int g = 0; g < nseg; g++) {
-      gt += C.nmol[g] * Y.sp[g].nsite;
-      M.gpre[g + 1] = gt;
+      acc += C.nmol[g] * Y.sp[g].nsite;
+      M.gpre[g + 1] = acc;
     }
-    M.pre[0] = 0;
-    for (int st = 0; st < nold + nnew; st++) M.pre[st + 1] = M.pre[st] + M.vl[st] + gt;
     if (kProf) C.prof[8] += clock64();
   }
 }
 
-// All threads: this thread's share of the reciprocal sum and of the real-space pairs.
-// v[0] sum akk*d|S|^2, v[1] ewld2, v[2] vdw, v[3] and v[4] the absolute sums that bound the
-// rounding error of v[0] and v[1]+v[2] (mixed precision).  S_new goes to Sn when write_sn.
 // Real-space sums of one pass: every (site, candidate) pair, compiled per boundary condition so
 // the hot loop holds one minimum-image form.  Deeper unrolling (2-8 candidates per trip) was
 // measured slower: the larger loop costs more in instruction fetch than it hides in latency.
-template <bool kMixed, int kImcon>
+template <int kImcon>
 __device__ __noinline__ void real_space(const DevSystem& S, const ChainDev& C, const MoveSmem& M, int nseg,
-                                        const int* prow_s, int nt1, int fp32_mask, double* vout) {
+                                        const int* prow_s, int nt1, double* vout) {
   const int tid = threadIdx.x, nsite = M.nold + M.nnew, nold = M.nold, mtype = M.mtype;
-  double v[5] = {0.0, vout[1], vout[2], 0.0, vout[4]};
+  double v1 = vout[1], v2 = vout[2];
   const bool sub_old = (mtype != kInsert && mtype != kDelete);
   const int T = M.pre[nsite];
-  const float rdrf_e = (float)S.rdr_e, rdrf_v = (float)S.rdr_v;
   // a thread takes candidates tid, tid + 256, tid + 512, ... in that order
   // one candidate per loop trip, the next one's loads issued before this one is evaluated
   int s_next = 0;
   Cand pre = fetch_candidate(S, C, M, nseg, tid, s_next);
   for (int base = tid; base < T; base += kBatchThreads) {
-    Cand c[1];
-    c[0] = pre;
+    const Cand c = pre;
     pre = fetch_candidate(S, C, M, nseg, base + kBatchThreads, s_next);
-#pragma unroll
-    for (int u = 0; u < 1; u++) {
-      if (!c[u].live) continue;
-      const int st = c[u].site;
-      const int row = prow_s[M.type[st] * nt1 + c[u].type];
-      double ec = 0.0, ev = 0.0;
-      if (kMixed && (fp32_mask & 6)) {
-        // FP32 for the components selected by fp32_mask (bit 1 Coulomb, bit 2 vdW); the
-        // separation and minimum image stay FP64
-        double dx = M.x[st] - c[u].a.x, dy = M.y[st] - c[u].a.y, dz = M.z[st] - c[u].a.z;
-        if (kImcon < 0) min_image(S.cell, dx, dy, dz);
-        else min_image_t<kImcon>(S.cell, dx, dy, dz);
-        double rsq = dx * dx + dy * dy + dz * dz;
-        if (rsq < S.rcut2) {
-          const bool need64 = (fp32_mask & 6) != 6;
-          double r = need64 ? sqrt(rsq) : 0.0;
-          float rf = need64 ? (float)r : sqrtf((float)rsq);
-          double chgprd = M.q[st] * kR4pie0 * c[u].a.w;
-          if (fabs(chgprd) > 1e-10) {
-            if (fp32_mask & 2)
-              ec = (double)(interp3f(S.erc_f, rf, rdrf_e) * (float)chgprd);
-            else
-              ec = interp3(S.erc, r, S.rdr_e) * chgprd;
-          }
-          if (row >= 0) {
-            if (fp32_mask & 4)
-              ev = (double)interp3f(S.vvv_f + (size_t)row * S.tab_stride, rf, rdrf_v);
-            else
-              ev = interp3(S.vvv + (size_t)row * S.tab_stride, r, S.rdr_v);
-          }
-        }
-        v[4] += ((fp32_mask & 2) ? fabs(ec) : 0.0) + ((fp32_mask & 4) ? fabs(ev) : 0.0);
-      } else {
-        pair_energy<kImcon>(S, M.x[st] - c[u].a.x, M.y[st] - c[u].a.y, M.z[st] - c[u].a.z, M.q[st] * kR4pie0, c[u].a.w,
-                    row, ec, ev);
-      }
-      if (sub_old && st < nold) {
-        v[1] -= ec;
-        v[2] -= ev;
-      } else {
-        v[1] += ec;
-        v[2] += ev;
-      }
+    if (!c.live) continue;
+    const int st = c.site;
+    const int row = prow_s[M.type[st] * nt1 + c.type];
+    double ec = 0.0, ev = 0.0;
+    pair_energy<kImcon>(S, M.x[st] - c.a.x, M.y[st] - c.a.y, M.z[st] - c.a.z, M.q[st] * kR4pie0, c.a.w, row, ec,
+                        ev);
+    if (sub_old && st < nold) {
+      v1 -= ec;
+      v2 -= ev;
+    } else {
+      v1 += ec;
+      v2 += ev;
     }
   }
-  vout[1] = v[1];
-  vout[2] = v[2];
-  vout[4] = v[4];
+  vout[1] = v1;
+  vout[2] = v2;
 }
 
-template <bool kMixed>
-__device__ __noinline__ void sums(const DevSystem& S, const ChainDev& C, const MoveSmem& M, int nseg,
-                                     const int* prow_s, int nt1, const int* kp, const double* ak,
-                                     const double2* Sk, double2* Sn, const void* tabv, int stride, bool write_sn,
-                                     int fp32_mask, double* v) {
+// All threads: this thread's share of the reciprocal sum (v[0] = sum akk*d|S|^2) and of the
+// real-space pairs (v[1] ewld2, v[2] vdw); S_new goes to Sn.
+__device__ __noinline__ void sums(const DevSystem& S, const ChainDev& C, const MoveSmem& M, int nseg, const int* prow_s,
+                                  int nt1, const int* kp, const double* ak, const double2* Sk, double2* Sn,
+                                  const void* tabv, int stride, double* v) {
   const int tid = threadIdx.x, K = S.K, k1 = S.kmax[0], k2 = S.kmax[1];
   const int nsite = M.nold + M.nnew, nold = M.nold, mtype = M.mtype;
+  const double2* tb = reinterpret_cast<const double2*>(tabv);
   for (int k = tid; k < K; k += blockDim.x) {
     int l, m, n;
     kunpack(kp[k], l, m, n);
     int am = m < 0 ? -m : m, an = n < 0 ? -n : n;
     double2 so = Sk[k], sn;
-    if (kMixed && (fp32_mask & 1)) {
-      const float2* tb = reinterpret_cast<const float2*>(tabv);
-      float2 d = make_float2(0.0f, 0.0f);
-      for (int st = 0; st < nsite; st++) {
-        const float2* t = tb + st * stride;
-        float2 e1 = t[l], e2 = t[k1 + 1 + am], e3 = t[k1 + k2 + 2 + an];
-        float2 c = m >= 0 ? make_float2(e1.x * e2.x - e1.y * e2.y, e1.y * e2.x + e2.y * e1.x)
-                          : make_float2(e1.x * e2.x + e1.y * e2.y, e1.y * e2.x - e2.y * e1.x);
-        c = n >= 0 ? make_float2(c.x * e3.x - c.y * e3.y, c.y * e3.x + e3.y * c.x)
-                   : make_float2(c.x * e3.x + c.y * e3.y, c.y * e3.x - e3.y * c.x);
-        float q = (float)M.q[st];
-        if (st < nold) {
-          d.x -= q * c.x;
-          d.y -= q * c.y;
-        } else {
-          d.x += q * c.x;
-          d.y += q * c.y;
-        }
+    double2 aold = make_double2(0.0, 0.0), anew = make_double2(0.0, 0.0);
+    for (int st = 0; st < nsite; st++) {
+      const double2* t = tb + st * stride;
+      double2 c = m >= 0 ? cmul(t[l], t[k1 + 1 + am]) : cmulc(t[l], t[k1 + 1 + am]);
+      c = n >= 0 ? cmul(c, t[k1 + k2 + 2 + an]) : cmulc(c, t[k1 + k2 + 2 + an]);
+      double q = M.q[st];
+      if (st < nold) {
+        aold.x += q * c.x;
+        aold.y += q * c.y;
+      } else {
+        anew.x += q * c.x;
+        anew.y += q * c.y;
       }
-      // dE_k = akk (2 Re(S* dS) + |dS|^2): nothing cancels
-      double dx = (double)d.x, dy = (double)d.y;
-      sn = make_double2(so.x + dx, so.y + dy);
-      double t = 2.0 * (so.x * dx + so.y * dy) + (dx * dx + dy * dy);
-      v[0] += ak[k] * t;
-      v[3] += ak[k] * (2.0 * (fabs(so.x * dx) + fabs(so.y * dy)) + (dx * dx + dy * dy) + fabs(so.x) + fabs(so.y));
-    } else {
-      const double2* tb = reinterpret_cast<const double2*>(tabv);
-      double2 aold = make_double2(0.0, 0.0), anew = make_double2(0.0, 0.0);
-      for (int st = 0; st < nsite; st++) {
-        const double2* t = tb + st * stride;
-        double2 c = m >= 0 ? cmul(t[l], t[k1 + 1 + am]) : cmulc(t[l], t[k1 + 1 + am]);
-        c = n >= 0 ? cmul(c, t[k1 + k2 + 2 + an]) : cmulc(c, t[k1 + k2 + 2 + an]);
-        double q = M.q[st];
-        if (st < nold) {
-          aold.x += q * c.x;
-          aold.y += q * c.y;
-        } else {
-          anew.x += q * c.x;
-          anew.y += q * c.y;
-        }
-      }
-      if (mtype == kInsert)
-        sn = make_double2(anew.x + so.x, anew.y + so.y);
-      else if (mtype == kDelete)
-        sn = make_double2(so.x - aold.x, so.y - aold.y);
-      else
-        sn = make_double2((so.x - aold.x) + anew.x, (so.y - aold.y) + anew.y);
-      v[0] += ak[k] * (sn.x * sn.x + sn.y * sn.y - so.x * so.x - so.y * so.y);
     }
-    if (write_sn) Sn[k] = sn;
+    if (mtype == kInsert)
+      sn = make_double2(anew.x + so.x, anew.y + so.y);
+    else if (mtype == kDelete)
+      sn = make_double2(so.x - aold.x, so.y - aold.y);
+    else
+      sn = make_double2((so.x - aold.x) + anew.x, (so.y - aold.y) + anew.y);
+    v[0] += ak[k] * (sn.x * sn.x + sn.y * sn.y - so.x * so.x - so.y * so.y);
+    Sn[k] = sn;
   }
   // real space, per boundary condition
-  if (S.cell.imcon == 1) real_space<kMixed, 1>(S, C, M, nseg, prow_s, nt1, fp32_mask, v);
-  else if (S.cell.imcon == 2) real_space<kMixed, 2>(S, C, M, nseg, prow_s, nt1, fp32_mask, v);
-  else if (S.cell.imcon == 3) real_space<kMixed, 3>(S, C, M, nseg, prow_s, nt1, fp32_mask, v);
+  if (S.cell.imcon == 1) real_space<1>(S, C, M, nseg, prow_s, nt1, v);
+  else if (S.cell.imcon == 2) real_space<2>(S, C, M, nseg, prow_s, nt1, v);
+  else if (S.cell.imcon == 3) real_space<3>(S, C, M, nseg, prow_s, nt1, v);
   // the half-shift cells and the slab share one instantiation that reads the boundary condition
   // from the cell: each compiled copy of this loop costs instruction cache (one per cell kind
   // cost 8%)
-  else real_space<kMixed, -1>(S, C, M, nseg, prow_s, nt1, fp32_mask, v);
+  else real_space<-1>(S, C, M, nseg, prow_s, nt1, v);
 }
 
 // All threads, in production: storeprob (utility_pack.f:496-561) for the chain's state after the
@@ -905,45 +801,18 @@ __device__ __noinline__ void prob_store(const SysConst& Y, const ChainDev& C) {
   }
 }
 
-// All threads: FP64 recompute of S(k) = S_framework(k) + sum over guest sites (bounds the drift
-// of the mixed-precision running sums).  Each thread owns its k-vectors.
-__device__ __forceinline__ void recompute_sk(const DevSystem& S, const SysConst& Y, const ChainDev& C, int nseg,
-                                             const int* kp, double2* Sk) {
-  for (int k = threadIdx.x; k < S.K; k += blockDim.x) {
-    int l, m, n;
-    kunpack(kp[k], l, m, n);
-    double2 acc = Y.sk_fw[k];
-    for (int g = 0; g < nseg; g++) {
-      int lo = C.seg_off[g], hi = lo + C.nmol[g] * Y.sp[g].nsite;
-      for (int j = lo; j < hi; j++) {
-        double4 a = C.gsite[j];
-        double f[3];
-        frac_coords(S.cell, a.x, a.y, a.z, f);
-        double th = (double)l * f[0] + (double)m * f[1] + (double)n * f[2];
-        th = th - floor(th);
-        double sn, cs;
-        sincospi(2.0 * th, &sn, &cs);
-        acc.x += a.w * cs;
-        acc.y += a.w * sn;
-      }
-    }
-    Sk[k] = acc;
-  }
-}
-
-// kMixed: the mixed-precision build (FP32 components per L.mixed, FP64 re-checks); the FP64
-// build carries none of that code.
-template <bool kMixed, bool kProf>
+template <bool kProf>
 __global__ void __launch_bounds__(kBatchThreads, 2) fmc_batch_kernel(BatchLaunch L, int tab_stride) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ ChainDev C;
   __shared__ MoveSmem M;
   __shared__ SysConst Ysm;
-  __shared__ double red[32 * 5];
+  __shared__ double red[32 * 3];
   __shared__ int prow_s[(kBatchMaxTypes + 1) * (kBatchMaxTypes + 1)];
   DevSystem& S = Ysm.S;
-  const int tid = threadIdx.x, cidx = blockIdx.x, warp = tid >> 5, lane = tid & 31;
-  if (cidx >= L.nchains) return;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  if ((int)blockIdx.x >= L.nchains) return;
+  const int cidx = L.order ? L.order[blockIdx.x] : (int)blockIdx.x;  // the chain this CTA runs
   if (!L.chains[cidx].active) return;
   const long long t_start = L.timing && tid == 0 ? global_ns() : 0;
   {
@@ -961,7 +830,6 @@ __global__ void __launch_bounds__(kBatchThreads, 2) fmc_batch_kernel(BatchLaunch
   const SysConst& Y = Ysm;
   const int K = S.K, Kmax = L.kmax_smem, nseg = Y.nspecies;
   const int nt1 = S.ntypes + 1;
-  constexpr bool mixed = kMixed;
   for (int i = tid; i < nt1 * nt1; i += blockDim.x) prow_s[i] = S.pair_row[i];
   double2* Sk = reinterpret_cast<double2*>(smem_raw);
   double2* Sn = Sk + Kmax;
@@ -985,21 +853,13 @@ __global__ void __launch_bounds__(kBatchThreads, 2) fmc_batch_kernel(BatchLaunch
   if (tid == 0) M.mj_stage = 0;
   bool pending = false;  // the first half of a multi-jump ended the last trip; the move goes on
   for (int mv = 0; mv < nmoves;) {
-    if (mixed && L.recompute_every > 0 && C.since_recompute >= L.recompute_every && !pending) {
-      recompute_sk(S, Y, C, nseg, kp, Sk);
-      __syncthreads();
-      if (tid == 0) {
-        C.since_recompute = 0;
-        C.recomputes++;
-      }
-    }
     if (prof && tid == 0) t0 = clock64();
     if (warp == 0) {
       if (lane == 0) select_move<kProf>(C, Y, M);
       __syncwarp();
       // warp 1 may read select_move's results now (named barrier 1: warps 0 and 1)
       asm volatile("bar.arrive 1, 64;" ::: "memory");
-      if (!C.status) build_trial<kProf>(C, Y, S, M, tab, stride, mixed && (L.mixed & 1), lane);
+      if (!C.status) build_trial<kProf>(C, Y, S, M, tab, stride, lane);
     } else if (warp == 1) {
       asm volatile("bar.sync 1, 64;" ::: "memory");
       if (M.need_lrc && !C.status) lrc_warp(C, Y, M, lane);
@@ -1012,13 +872,10 @@ __global__ void __launch_bounds__(kBatchThreads, 2) fmc_batch_kernel(BatchLaunch
     }
     if (C.status) break;
     const bool last = !C.lgchk;  // lane 0 of warp 0 writes lgchk only in select_move
-    double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    if (mixed)
-      sums<true>(S, C, M, nseg, prow_s, nt1, kp, ak, Sk, Sn, tab, stride, true, L.mixed, v);
-    else
-      sums<false>(S, C, M, nseg, prow_s, nt1, kp, ak, Sk, Sn, tab, stride, true, 0, v);
+    double v[3] = {0.0, 0.0, 0.0};
+    sums(S, C, M, nseg, prow_s, nt1, kp, ak, Sk, Sn, tab, stride, v);
     if (prof && tid == 0) C.prof[6] += clock64() - t0;
-    block_sum<5>(v, red);
+    block_sum<3>(v, red);
     if (prof && tid == 0) {
       t1 = clock64();
       C.prof[2] += t1 - t0;
@@ -1026,47 +883,9 @@ __global__ void __launch_bounds__(kBatchThreads, 2) fmc_batch_kernel(BatchLaunch
     }
     if (tid == 0) {
       assemble(Y, M, v);
-      double band = 0.0;
-      if (mixed) {
-        // error band: relative FP32 bound on every term (a few ulp of float)
-        const double eps = 4.0e-6;
-        band = eps * (Y.S.recip_pref * v[3] + v[4]) / Y.engunit + 1e-9;
-      }
-      M.recheck = decide(C, Y, M, band);
+      decide(C, Y, M);
     }
     __syncthreads();
-    if (mixed && (M.recheck || L.shadow)) {
-      // FP64 evaluation of the same move: decisive when the margin fell inside the band,
-      // recorded (shadow) otherwise
-      const bool decisive = M.recheck != 0;
-      if (warp == 0) build_phases<false>(S, M, tab, stride, lane);
-      __syncthreads();
-      double w[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-      sums<false>(S, C, M, nseg, prow_s, nt1, kp, ak, Sk, Sn, tab, stride, decisive, 0, w);
-      block_sum<5>(w, red);
-      if (tid == 0) {
-        double e32 = M.estep;
-        double r1 = M.ewld1, r2 = M.ewld2, r3 = M.vdw;
-        assemble(Y, M, w);
-        if (L.shadow) {
-          double* sh = L.shadow + 4 * ((size_t)cidx * L.moves + mv);
-          sh[0] = M.ewld1;
-          sh[1] = M.ewld2;
-          sh[2] = M.vdw;
-          sh[3] = M.estep;
-        }
-        if (decisive) {
-          C.rechecks++;
-          decide(C, Y, M, 0.0);
-        } else {
-          M.estep = e32;
-          M.ewld1 = r1;
-          M.ewld2 = r2;
-          M.vdw = r3;
-        }
-      }
-      __syncthreads();
-    }
     if (tid == 0) bookkeep(C, Y, M, L.trace ? L.trace + (size_t)cidx * L.moves + mv : nullptr);
     __syncthreads();
     if (prof && tid == 0) {
@@ -1145,26 +964,18 @@ int batch_smem_bytes(int kmax_K, int tab_sites, int tab_stride) {
 }
 
 cudaError_t configure_batch_kernel(int smem_bytes) {
-  cudaError_t e = cudaFuncSetAttribute(fmc_batch_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaError_t e = cudaFuncSetAttribute(fmc_batch_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        smem_bytes);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(fmc_batch_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(fmc_batch_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(fmc_batch_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
+    e = cudaFuncSetAttribute(fmc_batch_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
   return e;
 }
 
 cudaError_t launch_batch(const BatchLaunch& L, int smem_bytes, int tab_stride, cudaStream_t st) {
-  if (L.mixed && L.profile)
-    fmc_batch_kernel<true, true><<<L.nchains, kBatchThreads, smem_bytes, st>>>(L, tab_stride);
-  else if (L.mixed)
-    fmc_batch_kernel<true, false><<<L.nchains, kBatchThreads, smem_bytes, st>>>(L, tab_stride);
-  else if (L.profile)
-    fmc_batch_kernel<false, true><<<L.nchains, kBatchThreads, smem_bytes, st>>>(L, tab_stride);
+  if (L.profile)
+    fmc_batch_kernel<true><<<L.nchains, kBatchThreads, smem_bytes, st>>>(L, tab_stride);
   else
-    fmc_batch_kernel<false, false><<<L.nchains, kBatchThreads, smem_bytes, st>>>(L, tab_stride);
+    fmc_batch_kernel<false><<<L.nchains, kBatchThreads, smem_bytes, st>>>(L, tab_stride);
   return cudaGetLastError();
 }
 

@@ -36,7 +36,6 @@ struct SysConst {
   double steadd[kBatchMaxTab + 1];
   int numfrz[kBatchMaxTypes + 1];
   double engunit, volm, statvolm;
-  const double2* sk_fw;  // S(k) of the framework alone (periodic FP64 recompute)
   // probability plots (storeprob): grid cells per axis, and per plot its species and sites
   int nplots, ngrid[3];
   int plot_guest[kMaxPlots], plot_nsite[kMaxPlots], plot_site[kMaxPlots][kMaxPlotSites];
@@ -77,9 +76,6 @@ struct ChainDev {
   // SM clock cycles spent per phase when the launch is profiled: begin (thread 0), phase
   // tables, k-space + real space + reduction, end (thread 0), commit
   long long prof[12];
-  // mixed precision: FP64 re-evaluations of the acceptance, moves since the last FP64 S(k)
-  // recompute, recomputes done
-  long long rechecks, since_recompute, recomputes;
   // buffers
   double2* sk;
   double4* gsite;
@@ -97,12 +93,9 @@ struct BatchLaunch {
   MoveRecord* trace;  // [nchains][moves] or null
   int kmax_smem;      // largest K in the batch rounded up to a multiple of 4 (smem sizing)
   int profile;        // accumulate per-phase clock counters into ChainDev::prof
-  int mixed;          // FP32 component mask (0 = all FP64): 1 reciprocal phases, 2 real-space
-                      // Coulomb, 4 vdW; S(k), totals and dE assembly stay FP64
-  long long recompute_every;  // mixed: moves between FP64 recomputes of S(k) (0: never)
-  double* shadow;     // mixed, optional [nchains][moves][4]: FP64 {ewld1, ewld2, vdw, dE} of every
-                      // move on the same state
-  long long* timing;  // optional [nchains][3]: the CTA's start and end (%globaltimer, ns) and its SM
+  const int* order;   // optional [nchains]: the chain each CTA runs (placement only: a chain's result
+                      // does not depend on its CTA)
+  long long* timing;  // optional [nchains][3] per chain: its CTA's start and end (%globaltimer, ns), its SM
   int retire_finished;  // a chain that ends its budget, its deck's cycles or on an error marks itself
                         // inactive, so that a launch queued behind this one skips it (serving)
 };
@@ -169,12 +162,14 @@ class Batch {
   MoveRecord* d_trace = nullptr;
   size_t trace_cap = 0;
   int kmax_all = 0, tab_sites = 0, tab_stride = 0, smem = 0;
-  int mixed = 0;
-  long long recompute_every = 0;
-  double* d_shadow = nullptr;
-  size_t shadow_cap = 0;
   long long* d_timing = nullptr;  // per chain {start ns, end ns, SM} of the last launch
   long long* h_timing = nullptr;  // pinned host copy
+  // placement of chains on CTAs: order[b] is the chain CTA b runs; after each launch it is
+  // chosen again from that launch's SM map and per-chain times (rebalance)
+  std::vector<int> order;
+  int* d_order = nullptr;
+  int* h_order = nullptr;         // pinned staging of order for the upload
+  void rebalance();
   int nchains = 0;
   ~Batch();
   int open(const std::vector<std::string>& dirs, const std::vector<int>& seeds, int device, std::string& err,
@@ -185,7 +180,7 @@ class Batch {
   int restart(int c, const std::string& revive_path, std::string& err);
   // One step: control blocks host->device, `moves` moves of every chain, control blocks (and
   // the optional per-move trace) device->host.  *ms: CUDA-event time of the kernel alone.
-  int run(int moves, MoveRecord* trace_host, float* ms, std::string& err, double* shadow_host = nullptr);
+  int run(int moves, MoveRecord* trace_host, float* ms, std::string& err);
   // numguests.out lines (gcmc.f:1937-1951) of chain c's last run, rebuilt from its move trace
   // and the per-species counts and energies the run started from
   int write_numguests(int c, const MoveRecord* trace, int nmoves, const std::string& outdir, bool append,

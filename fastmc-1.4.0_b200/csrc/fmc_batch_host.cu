@@ -31,7 +31,7 @@ std::string system_key(const std::string& dir, const InputDeck& d) {
 
 }  // namespace
 
-// Per-system constants from the host tables and the device arrays (Y.sk_fw left unset).
+// Per-system constants from the host tables and the device arrays.
 int fill_sysconst(const HostSystem& H, const DevSystem& S, SysConst& Y, int* tab_sites, std::string& err) {
   std::memset(&Y, 0, sizeof(Y));
   Y.S = S;
@@ -87,24 +87,10 @@ int fill_sysconst(const HostSystem& H, const DevSystem& S, SysConst& Y, int* tab
   return 0;
 }
 
-// Per-system constants of an opened system chain (its HostSystem, device arrays and the
-// framework S(k), which the chain holds while it has no guests).
+// Per-system constants of an opened system chain (its HostSystem and device arrays).
 int make_sysconst(const Chain& ch, SysConst& Y, std::vector<void*>& allocations, int* tab_sites, std::string& err) {
-  const HostSystem& H = ch.sys;
-  int rc = fill_sysconst(H, ch.dsys.view, Y, tab_sites, err);
-  if (rc) return rc;
-  {
-    double2* fw = nullptr;
-    cudaError_t e = cudaMalloc(&fw, sizeof(double2) * std::max(H.K, 1));
-    if (e == cudaSuccess) allocations.push_back(fw);
-    if (e == cudaSuccess) e = cudaMemcpy(fw, ch.sk, sizeof(double2) * H.K, cudaMemcpyDeviceToDevice);
-    if (e != cudaSuccess) {
-      err = std::string("framework S(k) copy failed: ") + cudaGetErrorString(e);
-      return -100 - (int)e;
-    }
-    Y.sk_fw = fw;
-  }
-  return 0;
+  (void)allocations;
+  return fill_sysconst(ch.sys, ch.dsys.view, Y, tab_sites, err);
 }
 
 // Parameters (from the chain's own deck) and initial state of one chain of system `sys`;
@@ -232,9 +218,9 @@ Batch::~Batch() {
     cudaStreamSynchronize(st);
     for (void* p : allocations) cudaFree(p);
     if (d_trace) cudaFree(d_trace);
-    if (d_shadow) cudaFree(d_shadow);
     if (h_chains) cudaFreeHost(h_chains);
     if (h_timing) cudaFreeHost(h_timing);
+    if (h_order) cudaFreeHost(h_order);
     cudaStreamDestroy(st);
   }
 }
@@ -314,6 +300,11 @@ int Batch::open(const std::vector<std::string>& dirs, const std::vector<int>& se
   if (e == cudaSuccess) e = cudaMemset(d_timing, 0, sizeof(long long) * 3 * nchains);
   if (e == cudaSuccess) e = cudaMallocHost(&h_timing, sizeof(long long) * 3 * nchains);
   if (e == cudaSuccess) std::memset(h_timing, 0, sizeof(long long) * 3 * nchains);
+  if (e == cudaSuccess) e = cudaMalloc(&d_order, sizeof(int) * nchains);
+  if (e == cudaSuccess) allocations.push_back(d_order);
+  if (e == cudaSuccess) e = cudaMallocHost(&h_order, sizeof(int) * nchains);
+  order.resize(nchains);
+  for (int c = 0; c < nchains; c++) order[c] = c;
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) {
     err = std::string("batch upload failed: ") + cudaGetErrorString(e);
@@ -469,7 +460,54 @@ int Batch::write_numguests(int c, const MoveRecord* trace, int nmoves, const std
   return 0;
 }
 
-int Batch::run(int moves, MoveRecord* trace_host, float* ms, std::string& err, double* shadow_host) {
+// Placement for the next launch from the one that just ran.  The GPU places CTAs on SMs in block
+// order, the same way launch after launch: with more chains than SMs, some SMs run two CTAs, each
+// of them then slower (about 12%), and the launch lasts as long as its slowest CTA.  So the
+// heaviest chains (per-chain device time of the last launch, with the sharing factor taken out)
+// go to the blocks that had an SM of their own, and the remaining blocks, two per SM, pair the
+// heaviest remaining chain with the lightest.  With a different placement the assignment is only
+// less balanced; every chain computes the same moves wherever it runs.
+void Batch::rebalance() {
+  const int n = nchains;
+  std::map<long long, std::vector<int>> by_sm;  // SM -> blocks
+  for (int b = 0; b < n; b++) {
+    const long long* t = h_timing + 3 * order[b];
+    if (t[1] <= t[0]) return;  // a CTA without a record: keep the placement
+    by_sm[t[2]].push_back(b);
+  }
+  std::vector<double> cost(n);
+  for (auto& kv : by_sm) {
+    if (kv.second.size() > 2) return;  // more CTAs on an SM than fit at once: placement not learned
+    for (int b : kv.second) {
+      const long long* t = h_timing + 3 * order[b];
+      cost[order[b]] = (double)(t[1] - t[0]) / (kv.second.size() == 2 ? 1.12 : 1.0);
+    }
+  }
+  std::vector<int> chains(n);
+  for (int c = 0; c < n; c++) chains[c] = c;
+  std::stable_sort(chains.begin(), chains.end(), [&cost](int x, int y) { return cost[x] > cost[y]; });
+  std::vector<int> single, paired_a, paired_b;
+  for (auto& kv : by_sm) {
+    if (kv.second.size() == 1) {
+      single.push_back(kv.second[0]);
+    } else {
+      paired_a.push_back(kv.second[0]);
+      paired_b.push_back(kv.second[1]);
+    }
+  }
+  std::sort(single.begin(), single.end());
+  std::vector<int> next(n);
+  size_t k = 0;
+  for (int b : single) next[b] = chains[k++];
+  const size_t np = paired_a.size();
+  for (size_t i = 0; i < np; i++) {
+    next[paired_a[i]] = chains[k + i];
+    next[paired_b[i]] = chains[n - 1 - i];
+  }
+  order = next;
+}
+
+int Batch::run(int moves, MoveRecord* trace_host, float* ms, std::string& err) {
   cudaSetDevice(device);
   run_nmol.resize((size_t)kMaxGuestTypes * nchains);
   run_energy.resize((size_t)kMaxGuestTypes * nchains);
@@ -479,29 +517,17 @@ int Batch::run(int moves, MoveRecord* trace_host, float* ms, std::string& err, d
       run_energy[(size_t)c * kMaxGuestTypes + i] = h_chains[c].energy[i];
     }
   BatchLaunch L;
+  std::memset(&L, 0, sizeof(L));
   L.chains = d_chains;
   L.systems = d_sys;
   L.nchains = nchains;
   L.moves = moves;
   L.kmax_smem = kmax_all;
   L.profile = profile;
-  L.mixed = mixed;
-  L.recompute_every = recompute_every;
   L.trace = nullptr;
-  L.shadow = nullptr;
   L.timing = d_timing;
-  L.retire_finished = 0;
+  L.order = d_order;
   cudaError_t e = cudaSuccess;
-  if (shadow_host && mixed) {
-    size_t need = (size_t)nchains * moves;
-    if (need > shadow_cap) {
-      if (d_shadow) cudaFree(d_shadow);
-      d_shadow = nullptr;
-      e = cudaMalloc(&d_shadow, sizeof(double) * 4 * need);
-      shadow_cap = e == cudaSuccess ? need : 0;
-    }
-    L.shadow = d_shadow;
-  }
   if (trace_host) {
     size_t need = (size_t)nchains * moves;
     if (need > trace_cap) {
@@ -516,15 +542,14 @@ int Batch::run(int moves, MoveRecord* trace_host, float* ms, std::string& err, d
   cudaEventCreate(&a);
   cudaEventCreate(&b);
   const size_t cb = sizeof(ChainDev) * nchains;
+  std::copy(order.begin(), order.end(), h_order);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_order, h_order, sizeof(int) * nchains, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(d_chains, h_chains, cb, cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaEventRecord(a, st);
   if (e == cudaSuccess) e = launch_batch(L, smem, tab_stride, st);
   if (e == cudaSuccess) e = cudaEventRecord(b, st);
   if (e == cudaSuccess && trace_host)
     e = cudaMemcpyAsync(trace_host, d_trace, sizeof(MoveRecord) * (size_t)nchains * moves, cudaMemcpyDeviceToHost,
-                        st);
-  if (e == cudaSuccess && L.shadow)
-    e = cudaMemcpyAsync(shadow_host, d_shadow, sizeof(double) * 4 * (size_t)nchains * moves, cudaMemcpyDeviceToHost,
                         st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(h_chains, d_chains, cb, cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess)
@@ -538,6 +563,7 @@ int Batch::run(int moves, MoveRecord* trace_host, float* ms, std::string& err, d
     err = std::string("batched launch failed: ") + cudaGetErrorString(e);
     return -100 - (int)e;
   }
+  rebalance();
   if (ms) *ms = t;
   return 0;
 }
@@ -639,37 +665,6 @@ int fmc_batch_profile(fmc_batch* b, int enable) {
   return 0;
 }
 
-int fmc_batch_set_precision(fmc_batch* b, int mixed, long long recompute_every) {
-  if (!b || recompute_every < 0) {
-    fmc::set_last_error("bad batch handle or recompute interval");
-    return -1;
-  }
-  b->impl.mixed = mixed & 7;
-  b->impl.recompute_every = recompute_every;
-  return 0;
-}
-
-int fmc_batch_run_shadow(fmc_batch* b, int moves, fmc_move_record* trace, double* shadow, float* device_ms) {
-  if (!b || moves < 0) {
-    fmc::set_last_error("bad batch handle or move count");
-    return -1;
-  }
-  std::string err;
-  int rc = b->impl.run(moves, reinterpret_cast<fmc::MoveRecord*>(trace), device_ms, err, shadow);
-  if (rc) {
-    fmc::set_last_error(err);
-    return rc;
-  }
-  for (int i = 0; i < b->impl.nchains; i++) {
-    const fmc::ChainDev& c = b->impl.h_chains[i];
-    if (c.status) {
-      fmc::set_last_error(c.status == 75 ? "too many atoms in specified system" : "chain stopped with an unknown status");
-      return c.status;
-    }
-  }
-  return 0;
-}
-
 int fmc_batch_run(fmc_batch* b, int moves, fmc_move_record* trace, float* device_ms) {
   if (!b || moves < 0) {
     fmc::set_last_error("bad batch handle or move count");
@@ -719,9 +714,7 @@ int fmc_batch_chain_state(fmc_batch* b, int chain, double* out) {
   v[26] = C.press[0];
   for (int k = 0; k < 5; k++) v[27 + k] = (double)C.prof[k];
   for (int k = 5; k < 9; k++) v[k + 27] = (double)C.prof[k];
-  v[36] = (double)C.rechecks;
-  v[37] = (double)C.recomputes;
-  v[38] = C.lgchk ? 0.0 : 1.0;
+  v[36] = C.lgchk ? 0.0 : 1.0;
   std::memcpy(out, v, sizeof(v));
   return 0;
 }

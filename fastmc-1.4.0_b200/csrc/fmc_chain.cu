@@ -90,11 +90,6 @@ int upload_system(const HostSystem& h, DeviceSystem& d, std::string& err) {
   v.rdr_v = 1.0 / h.dlrpot;
   if ((e = upload(d.allocations, &v.erc, h.erc)) != cudaSuccess) goto fail;
   if ((e = upload(d.allocations, &v.vvv, h.vvv)) != cudaSuccess) goto fail;
-  {
-    std::vector<float> ef(h.erc.begin(), h.erc.end()), vf(h.vvv.begin(), h.vvv.end());
-    if ((e = upload(d.allocations, &v.erc_f, ef)) != cudaSuccess) goto fail;
-    if ((e = upload(d.allocations, &v.vvv_f, vf)) != cudaSuccess) goto fail;
-  }
   v.tab_stride = h.mxgrid + 1;
   v.ntypes = h.ntypes;
   if ((e = upload(d.allocations, &v.pair_row, h.pair_row)) != cudaSuccess) goto fail;

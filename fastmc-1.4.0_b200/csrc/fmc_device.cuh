@@ -28,8 +28,6 @@ struct DevSystem {
   double rcut2, rdr_e, rdr_v;
   const double* erc;
   const double* vvv;
-  const float* erc_f;  // FP32 copies of the tables (mixed-precision path)
-  const float* vvv_f;
   int tab_stride;
   int ntypes;
   const int* pair_row;

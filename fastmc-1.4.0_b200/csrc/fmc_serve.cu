@@ -83,11 +83,10 @@ class Server {
   std::atomic<size_t> used{0};      // device bytes of admitted slots
   size_t prebuilt_bytes = 0;        // device bytes of slots built ahead (guarded by mu)
   int prebuilt_count = 0;
+  int building = 0;                 // slots being built ahead right now (guarded by mu)
   static constexpr int kMaxPrebuilt = 64;  // slots built ahead at most
   std::vector<WorkerRes> wres;
   cudaMemPool_t pool = nullptr;
-  int mixed = 0;
-  long long recompute_every = 0;
   std::vector<Slot> slots;
   std::vector<std::unique_ptr<Request>> reqs;  // the vector is guarded by mu; entries are stable
   std::deque<int> queue;                       // admission order (caller's thread only)
@@ -295,6 +294,7 @@ class Server {
       if (prebuilt_count >= kMaxPrebuilt || used.load() + prebuilt_bytes + r.bytes_estimate > budget) return;
       prebuilt_bytes += r.bytes_estimate;
       prebuilt_count++;
+      building++;
     }
     auto P = std::make_unique<Prebuilt>();
     P->mem.st = w.st;
@@ -323,6 +323,7 @@ class Server {
     }
     std::lock_guard<std::mutex> lk(mu);
     prebuilt_bytes -= r.bytes_estimate;
+    building--;
     if (ok) {
       P->C.budget = r.moves;
       prebuilt_bytes += P->mem.bytes;
@@ -418,8 +419,8 @@ class Server {
 
   // Frees a request's slot built ahead (its preparation has finished).
   void drop_prebuilt(Request& r) {
-    if (!r.pre) return;
     std::lock_guard<std::mutex> lk(mu);
+    if (!r.pre) return;
     prebuilt_bytes -= std::min(prebuilt_bytes, r.pre->mem.bytes);
     prebuilt_count--;
     r.pre->mem.release();
@@ -460,7 +461,7 @@ class Server {
     for (int k = 0; k < 5; k++) v[11 + k] = C.stats[0][k];
     v[16] = C.accept_ins;
     v[17] = C.accept_del;
-    v[18] = (double)C.rechecks;
+    v[18] = 0.0;
     v[19] = h_sys[i].S.K;
     v[20] = h_sys[i].S.nf;
     v[21] = C.temp;
@@ -549,6 +550,7 @@ class Server {
   // holds.  With nothing running, waits for the front request's preparation.
   void admit_queued(int running) {
     const double t0 = now_ms();
+    bool dropped = false;
     for (int i = 0; i < nslots && !queue.empty(); i++) {
       if (slots[i].request != -1) continue;  // running, or cancelled with its memory still held
       const int id = queue.front();
@@ -570,6 +572,27 @@ class Server {
         if (r.bytes_estimate > budget) {
           queue.pop_front();
           reject(r, -10, "the request's device footprint exceeds the server's memory budget");
+          i--;
+          continue;
+        }
+        if (ahead > 0 && !dropped) {
+          // the budget is held by slots built ahead for requests behind this one: free them
+          // (they are built again when their turn comes) rather than wait on them; with nothing
+          // running, first let the builds in progress finish so that they can be freed too
+          if (!running) {
+            const double w0 = now_ms();
+            for (;;) {
+              {
+                std::lock_guard<std::mutex> lk(mu);
+                if (building == 0) break;
+              }
+              std::this_thread::sleep_for(std::chrono::microseconds(200));
+            }
+            wait_ms += now_ms() - w0;
+          }
+          for (int q : queue)
+            if (q != id) drop_prebuilt(req(q));
+          dropped = true;
           i--;
           continue;
         }
@@ -691,8 +714,6 @@ class Server {
     L.nchains = nslots;
     L.moves = moves;
     L.kmax_smem = kcap;
-    L.mixed = mixed;
-    L.recompute_every = recompute_every;
     L.retire_finished = 1;
     if (e == cudaSuccess) e = cudaEventRecord(ev_start[b], st);
     if (e == cudaSuccess) e = launch_batch(L, smem, tab_stride, st);
@@ -793,16 +814,6 @@ int fmc_server_open(int slots, int device, long long mem_budget, int k_capacity,
 }
 
 void fmc_server_close(fmc_server* s) { delete s; }
-
-int fmc_server_set_precision(fmc_server* s, int mixed, long long recompute_every) {
-  if (!s || recompute_every < 0) {
-    fmc::set_last_error("bad server handle or recompute interval");
-    return -1;
-  }
-  s->impl.mixed = mixed & 7;
-  s->impl.recompute_every = recompute_every;
-  return 0;
-}
 
 int fmc_server_submit(fmc_server* s, const char* dir, const int* seed, long long moves, int* request_id) {
   if (!s || !dir || !seed || moves < 0 || !request_id) {

@@ -1,7 +1,7 @@
 // Serving slots: the device side of admitting one request, enqueued on the admission stream with
 // allocations from the server's memory pool and every host array staged into pinned memory, so
 // admitting needs no wait.  The slot holds only what the batched kernel reads: framework atoms,
-// inlined voxel lists, erfc / vdW tables (FP64 and FP32), the k-vector tables, the framework S(k)
+// inlined voxel lists, erfc / vdW tables, the k-vector tables, the framework S(k)
 // (ewald1 over the framework, ewald.f:368-630) and the chain's S(k) and guest segments.
 #include <algorithm>
 #include <cmath>
@@ -40,19 +40,17 @@ size_t al(size_t n) { return (n + 255) & ~size_t(255); }
 
 // Host arrays of a system in the order they are staged, with their byte sizes.
 struct Parts {
-  size_t fw, ftype, erc, vvv, erc_f, vvv_f, prow, kp, akk;
+  size_t fw, ftype, erc, vvv, prow, kp, akk;
   explicit Parts(const HostSystem& h)
       : fw(sizeof(double4) * h.nf),
         ftype(sizeof(int) * h.nf),
         erc(sizeof(double) * h.erc.size()),
         vvv(sizeof(double) * h.vvv.size()),
-        erc_f(sizeof(float) * h.erc.size()),
-        vvv_f(sizeof(float) * h.vvv.size()),
         prow(sizeof(int) * h.pair_row.size()),
         kp(sizeof(int) * h.K),
         akk(sizeof(double) * h.K) {}
   size_t total() const {
-    return al(fw) + al(ftype) + al(erc) + al(vvv) + al(erc_f) + al(vvv_f) + al(prow) + al(kp) + al(akk);
+    return al(fw) + al(ftype) + al(erc) + al(vvv) + al(prow) + al(kp) + al(akk);
   }
 };
 
@@ -91,7 +89,7 @@ int build_slot(const HostSystem& h, int slot, const int seed[4], SlotMemory& mem
     return at;
   };
   const size_t o_fw = place(P.fw), o_ft = place(P.ftype), o_erc = place(P.erc), o_vvv = place(P.vvv),
-               o_ercf = place(P.erc_f), o_vvvf = place(P.vvv_f), o_prow = place(P.prow), o_kp = place(P.kp),
+               o_prow = place(P.prow), o_kp = place(P.kp),
                o_akk = place(P.akk);
   {
     double4* fw = (double4*)(hs + o_fw);
@@ -99,10 +97,6 @@ int build_slot(const HostSystem& h, int slot, const int seed[4], SlotMemory& mem
     std::memcpy(hs + o_ft, h.ftype.data(), P.ftype);
     std::memcpy(hs + o_erc, h.erc.data(), P.erc);
     std::memcpy(hs + o_vvv, h.vvv.data(), P.vvv);
-    float* ef = (float*)(hs + o_ercf);
-    for (size_t i = 0; i < h.erc.size(); i++) ef[i] = (float)h.erc[i];
-    float* vf = (float*)(hs + o_vvvf);
-    for (size_t i = 0; i < h.vvv.size(); i++) vf[i] = (float)h.vvv[i];
     std::memcpy(hs + o_prow, h.pair_row.data(), P.prow);
     int* kp = (int*)(hs + o_kp);
     for (int k = 0; k < h.K; k++) kp[k] = kpack(h.kl[k], h.km[k], h.kn[k]);
@@ -124,8 +118,6 @@ int build_slot(const HostSystem& h, int slot, const int seed[4], SlotMemory& mem
   v.fw_type = (const int*)(d + o_ft);
   v.erc = (const double*)(d + o_erc);
   v.vvv = (const double*)(d + o_vvv);
-  v.erc_f = (const float*)(d + o_ercf);
-  v.vvv_f = (const float*)(d + o_vvvf);
   v.pair_row = (const int*)(d + o_prow);
   v.kpack = (const int*)(d + o_kp);
   v.akk = (const double*)(d + o_akk);
@@ -168,7 +160,6 @@ int build_slot(const HostSystem& h, int slot, const int seed[4], SlotMemory& mem
     int ts = 0;
     int rc = fill_sysconst(h, v, Y, &ts, err);
     if (rc) return rc;
-    Y.sk_fw = skfw;
     DevAllocFn alloc = [&mem](void** p, size_t n) { return mem.alloc(p, n); };
     // an empty framework: guest energy 0 (single_point, gcmc.f:2518-2710)
     return init_chain_state(h.deck, h, skfw, 0.0, slot, seed, C, alloc, st, err, true);

@@ -420,24 +420,7 @@ class Batch:
     _STATE = ["status", "moves", "gcmccount", "nmol0", "nmol1", "nmol2", "nmol3", "energy0", "energy1", "energy2",
               "energy3", "elrc", "accept_ins", "accept_del", "ins_count", "del_count", "prodcount", "N", "E", "EN",
               "N2", "E2", "system", "K", "nframework", "temp", "press0", "cyc_begin", "cyc_phase", "cyc_sums",
-              "cyc_end", "cyc_commit", "cyc_t0_kspace", "cyc_t0_real", "cyc_select", "cyc_trial", "rechecks",
-              "recomputes", "finished"]
-
-    # FP32 component masks of set_precision
-    FP32_RECIP, FP32_COULOMB, FP32_VDW = 1, 2, 4
-
-    def set_precision(self, mixed, recompute_every=0):
-        """mixed: mask of FP32 components (True = all three); 0/False = FP64."""
-        m = 7 if mixed is True else int(mixed)
-        check(lib().fmc_batch_set_precision(self.h, m, int(recompute_every)))
-
-    def run_shadow(self, moves):
-        """Mixed precision run that also returns the FP64 dE of every move on the same state."""
-        rec = np.zeros((self.n, moves), dtype=MOVE_DTYPE)
-        sh = np.zeros((self.n, moves, 4))
-        ms = ctypes.c_float(0)
-        check(lib().fmc_batch_run_shadow(self.h, int(moves), rec.ctypes.data, sh.ctypes.data, ctypes.byref(ms)))
-        return rec, sh, float(ms.value)
+              "cyc_end", "cyc_commit", "cyc_t0_kspace", "cyc_t0_real", "cyc_select", "cyc_trial", "finished"]
 
     def profile(self, enable=True):
         check(lib().fmc_batch_profile(self.h, int(bool(enable))))
@@ -511,7 +494,7 @@ class Server:
 
     QUEUED, RUNNING, DONE, REJECTED, CANCELLED = 0, 1, 2, -1, -2
     _OUT = ["moves", "status", "nmol0", "nmol1", "nmol2", "nmol3", "energy0", "energy1", "energy2", "energy3",
-            "prodcount", "N", "E", "EN", "N2", "E2", "accept_ins", "accept_del", "rechecks", "K", "nframework",
+            "prodcount", "N", "E", "EN", "N2", "E2", "accept_ins", "accept_del", "_r18", "K", "nframework",
             "temp", "press0", "budget", "finished", "N_1", "E_1", "EN_1", "N2_1", "E2_1", "gcmccount", "_"]
 
     def __init__(self, slots=296, device=0, mem_budget=0, k_capacity=2400):
@@ -528,10 +511,6 @@ class Server:
             self.close()
         except Exception:
             pass
-
-    def set_precision(self, mixed, recompute_every=0):
-        m = 7 if mixed is True else int(mixed)
-        check(lib().fmc_server_set_precision(self.h, m, int(recompute_every)))
 
     def submit(self, directory, seed, moves=0):
         """Queue one request; moves=0 runs the deck's own equilibration + production cycles."""

@@ -91,8 +91,6 @@ SIGNATURES = {
     "fmc_batch_close": (None, [_vp]),
     "fmc_batch_run": (_ci, [_vp, _ci, _vp, ctypes.POINTER(ctypes.c_float)]),
     "fmc_batch_profile": (_ci, [_vp, _ci]),
-    "fmc_batch_set_precision": (_ci, [_vp, _ci, ctypes.c_longlong]),
-    "fmc_batch_run_shadow": (_ci, [_vp, _ci, _vp, _vp, ctypes.POINTER(ctypes.c_float)]),
     "fmc_batch_chain_state": (_ci, [_vp, _ci, _dp]),
     "fmc_batch_chain_timing": (_ci, [_vp, _ci, ctypes.POINTER(ctypes.c_longlong)]),
     "fmc_batch_guest_coords": (_ci, [_vp, _ci, _ci, _dp, _ip, _ip]),
@@ -123,7 +121,6 @@ SIGNATURES = {
     "fmc_batch_write_prob": (_ci, [_vp, _ci, ctypes.c_char_p]),
     "fmc_server_open": (_ci, [_ci, _ci, ctypes.c_longlong, _ci, ctypes.POINTER(_vp)]),
     "fmc_server_close": (None, [_vp]),
-    "fmc_server_set_precision": (_ci, [_vp, _ci, ctypes.c_longlong]),
     "fmc_server_submit": (_ci, [_vp, ctypes.c_char_p, _ip, ctypes.c_longlong, _ip]),
     "fmc_server_cancel": (_ci, [_vp, _ci]),
     "fmc_server_step": (_ci, [_vp, _ci, _ip, _ip, ctypes.POINTER(ctypes.c_float)]),

@@ -277,17 +277,6 @@ void fmc_batch_close(fmc_batch* b);
  * stops after the move on which its deck's equilibration + production cycles end (the
  * reference's loop test, gcmc.f:594-736); its later records stay as the caller left them. */
 int fmc_batch_run(fmc_batch* b, int moves, fmc_move_record* trace, float* device_ms);
-/* Precision of later runs.  `mixed` is a mask of the components evaluated in FP32: 1 the
- * reciprocal-space phases and dS, 2 the real-space Coulomb pair terms, 4 the vdW pair terms
- * (0 = all FP64).  S(k), the energy totals and the dE assembly (2Re(S* dS) + |dS|^2) stay
- * FP64; a move whose acceptance margin lies inside the FP32 error band is re-evaluated in
- * FP64; S(k) is recomputed in FP64 from the framework's S(k) and the guest sites every
- * `recompute_every` moves (0: never). */
-int fmc_batch_set_precision(fmc_batch* b, int mixed, long long recompute_every);
-/* fmc_batch_run that also stores, for mixed precision, the FP64 {ewld1, ewld2, vdw, dE} of every
- * move evaluated on the same state (shadow[nchains*moves*4], chain-major) to measure the
- * mixed-precision error. */
-int fmc_batch_run_shadow(fmc_batch* b, int moves, fmc_move_record* trace, double* shadow, float* device_ms);
 /* enable != 0: later runs accumulate SM clock cycles per phase of the move (see
  * fmc_batch_chain_state out[27..31]). */
 int fmc_batch_profile(fmc_batch* b, int enable);
@@ -295,8 +284,8 @@ int fmc_batch_profile(fmc_batch* b, int enable);
  * insertions, accepted deletions, insert attempts, delete attempts, production moves,
  * species-0 <N>,<E>,<EN>,<N^2>,<E^2>, system index, K, framework atoms, T, P(species 0),
  * profiled cycles of: trial set-up, phase tables, energy sums, acceptance, commit, then
- * (thread 0's share) k-space, + real space, move selection, trial generation, then FP64
- * re-evaluations and S(k) recomputes (mixed precision), then 1 once the chain has finished. */
+ * (thread 0's share) k-space, + real space, move selection, trial generation, then 1 once the
+ * chain has finished (out[37..39] 0). */
 int fmc_batch_chain_state(fmc_batch* b, int chain, double* out);
 /* Load balance of the last run (no counterpart in the reference): out[0..2] = the chain's CTA
  * start and end on the device clock (%globaltimer, ns) and the SM it ran on.  Recorded on every
@@ -338,7 +327,6 @@ int fmc_batch_write_prob(fmc_batch* b, int chain, const char* outdir);
 typedef struct fmc_server fmc_server;
 int fmc_server_open(int slots, int device, long long mem_budget, int k_capacity, fmc_server** out);
 void fmc_server_close(fmc_server* s);
-int fmc_server_set_precision(fmc_server* s, int mixed, long long recompute_every);
 int fmc_server_submit(fmc_server* s, const char* dir, const int* seed, long long moves, int* request_id);
 int fmc_server_cancel(fmc_server* s, int request_id);
 /* One step of the pipelined server: queues the next launch of every running request (after the
@@ -358,7 +346,7 @@ int fmc_server_poll_done(fmc_server* s, int* ids, int* states, double* results, 
 /* *state: 0 queued, 1 running, 2 done, -1 rejected (message in fmc_last_error), -2 cancelled.
  * A running request's results are those of the last completed launch.
  * out[0..31]: moves done, status, nmol[4], energy[4] (kcal/mol), production moves,
- * species-0 <N>,<E>,<EN>,<N^2>,<E^2>, accepted insertions, accepted deletions, FP64 re-checks,
+ * species-0 <N>,<E>,<EN>,<N^2>,<E^2>, accepted insertions, accepted deletions, 0,
  * K, framework atoms, T, P(species 0), move budget, 1 if the deck's cycles finished,
  * species-1 <N>,<E>,<EN>,<N^2>,<E^2>, gcmccount, 0. */
 int fmc_server_poll(fmc_server* s, int request_id, int* state, double* out);
