@@ -575,11 +575,14 @@ def serve_record(args, dist, n_req, cycle_scale, tag):
     # pilot (warm-up): more requests than slots at once; the launches that ran with every slot busy
     # give the server's capacity in moves/s
     ids = [srv.submit(d, (12, 34, 56, 1 + r["id"] % 168)) for d, r in zip(dirs[:n_pilot], reqs[:n_pilot])]
-    full_ms = []
+    full_ms, full_wall, full_moves = [], 0.0, 0
     while srv.busy():
+        t_step = time.perf_counter()
         a, q, ms = srv.step(args.serve_moves)
         if a == args.serve_slots:
             full_ms.append(ms)
+            full_wall += time.perf_counter() - t_step
+            full_moves += int(srv.stats()["last_moves"])
     srv.poll_done()
     pil = [srv.poll(i) for i in ids]
     moves_per_req = float(np.mean([r["moves"] for r in pil]))
@@ -612,8 +615,13 @@ def serve_record(args, dist, n_req, cycle_scale, tag):
                     done_t[k] = (end - arrivals[k], state)
         wall = time.perf_counter() - wall0
     dist.barrier()
+    saturated = {"what": "the pilot's launches with every slot busy", "steps": len(full_ms),
+                 "moves": full_moves, "device_s": sum(full_ms) / 1000.0, "wall_s": full_wall,
+                 "moves_per_device_s": full_moves / max(sum(full_ms) / 1000.0, 1e-9),
+                 "moves_per_wall_s": full_moves / max(full_wall, 1e-9), "slot_occupancy": 1.0}
     return srv, log, done_t, arrivals, wall, clk, {"capacity": capacity, "rate": rate, "n_pilot": n_pilot,
-                                                   "moves_per_req": moves_per_req, "gen_s": gen_s, "kcap": kcap}
+                                                   "moves_per_req": moves_per_req, "gen_s": gen_s, "kcap": kcap,
+                                                   "saturated": saturated}
 
 
 def summarize_serve(args, dist, srv, log, done_t, arrivals, wall, meta, cycle_scale, n_req):
@@ -647,6 +655,7 @@ def summarize_serve(args, dist, srv, log, done_t, arrivals, wall, meta, cycle_sc
         "pilot_requests": meta["n_pilot"], "arrival_rate_hz": meta["rate"],
         "capacity_moves_per_s": meta["capacity"], "offered_load": 0.9, "moves_per_request_mean": meta["moves_per_req"],
         "moves_per_step": args.serve_moves, "k_capacity": meta["kcap"], "deck_generation_s": meta["gen_s"],
+        "saturated": meta["saturated"],
         "window": {"what": "device and end-to-end figures cover the steps started before the last arrival",
                    "steps": len(win), "moves": w_moves, "device_s": w_dev, "wall_s": w_wall,
                    "slot_occupancy": w_occ},
@@ -678,7 +687,8 @@ def run_serve(args, dist):
                    "moves_per_step": args.serve_moves, "k_capacity": rec["k_capacity"],
                    "l2": "per-chain S(k) shared-memory resident; frameworks + voxel lists exceed L2 (no flush)",
                    "parallelism": f"replicas{dist.world}"},
-        "latency_s": rec["latency_s"], "rejected": rec["rejected"], "window": rec["window"],
+        "latency_s": rec["latency_s"], "rejected": rec["rejected"], "saturated": rec["saturated"],
+        "window": rec["window"],
         "whole_run": rec["whole_run"], "gpu_launches": w["steps"],
         "e2e": {"value": rec["e2e_value"], "unit": "moves/s", "h2d_bytes_per_step": rec["h2d_bytes_per_step"],
                 "d2h_bytes_per_step": rec["d2h_bytes_per_step"]},
