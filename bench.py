@@ -22,6 +22,9 @@ import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "fastmc-1.4.0_b200"))
+# before any CUDA context: separate hardware queues for the serving worker streams (the package
+# sets the same default on import)
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 PASS_SITES_MEAN_KEY = "pass_sites"
 

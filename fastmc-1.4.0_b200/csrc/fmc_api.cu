@@ -618,6 +618,26 @@ int fmc_deck_inspect(const char* dir, int* ints, double* dbls, int* lmn, double*
   return inspect_deck(deck, ints, dbls, lmn, akk, erc, charges, K, nerc, nullptr, nullptr);
 }
 
+int fmc_deck_voxels(const char* dir, double voxel_edge, int* nvox, int* off, int* atoms, long long cap,
+                    long long* n_entries) {
+  if (!dir || !nvox || !n_entries) return fail(-1, "null argument");
+  fmc::InputDeck deck;
+  fmc::HostSystem S;
+  std::string err;
+  int rc = fmc::read_input_deck(dir, deck, err);
+  if (!rc) rc = fmc::build_host_system(deck, S, err, voxel_edge > 0.0 ? voxel_edge : 2.0);
+  if (rc) return fail(rc, err);
+  fmc::build_host_voxels(S);
+  for (int a = 0; a < 3; a++) nvox[a] = S.nvox[a];
+  *n_entries = S.vox_entries;
+  if (off) std::memcpy(off, S.vox_off.data(), sizeof(int) * S.vox_off.size());
+  if (atoms) {
+    if (cap < S.vox_entries) return fail(-2, "atoms buffer smaller than the voxel entries");
+    std::memcpy(atoms, S.vox_atoms.data(), sizeof(int) * S.vox_atoms.size());
+  }
+  return 0;
+}
+
 int fmc_desc_inspect(const fmc_system_desc* desc, int* ints, double* dbls, int* lmn, double* akk, double* erc,
                      double* charges, int* K, int* nerc, double* vvv, int* ntables) {
   if (!desc) return fail(-1, "null argument");

@@ -109,6 +109,8 @@ int fill_sysconst(const HostSystem& H, const DevSystem& S, SysConst& Y, int* tab
 int make_sysconst(const Chain& ch, SysConst& Y, std::vector<void*>& allocations, int* tab_sites, std::string& err);
 // record_samples: allocate the first production samples of N and E (gasmol / gaseng, 16 MB a
 // species) that the final report's blocked errors need up to 500,000 production moves.
+// Device bytes init_chain_state allocates for a chain (before alignment).
+size_t chain_state_bytes(const InputDeck& d, const HostSystem& H, bool record_samples);
 int init_chain_state(const InputDeck& d, const HostSystem& H, const double2* sk_src, double energy0, int sys,
                      const int* seed, ChainDev& C, const DevAllocFn& alloc, cudaStream_t st, std::string& err,
                      bool record_samples);
@@ -122,6 +124,11 @@ struct SlotMemory {
   cudaMemPool_t pool = nullptr;
   std::vector<void*> ptrs;
   size_t bytes = 0;
+  // one pool allocation that later alloc() calls carve (256-byte aligned) until it is used up;
+  // a slot's buffers then cost one allocation call instead of one each
+  unsigned char* arena = nullptr;
+  size_t arena_cap = 0, arena_used = 0;
+  cudaError_t reserve(size_t n);
   cudaError_t alloc(void** p, size_t n);
   void release();  // stream-ordered frees of every allocation
 };

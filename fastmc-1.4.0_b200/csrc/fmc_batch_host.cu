@@ -95,6 +95,16 @@ int make_sysconst(const Chain& ch, SysConst& Y, std::vector<void*>& allocations,
 
 // Parameters (from the chain's own deck) and initial state of one chain of system `sys`;
 // allocates its S(k) (a copy of sk_src, the framework's) and guest-site segments.
+size_t chain_state_bytes(const InputDeck& d, const HostSystem& H, bool record_samples) {
+  const size_t ng = d.guests.size(), sites = std::max<size_t>(ng * (size_t)d.maxguest, 1);
+  size_t b = sizeof(double2) * std::max(H.K, 1) + (sizeof(double4) + sizeof(int)) * sites;
+  if (record_samples) b += 2 * sizeof(double) * (ng * (size_t)kSampleCap + 1);
+  if (!H.deck.plots.empty())
+    b += sizeof(unsigned long long) * H.deck.plots.size() * (size_t)H.deck.ngrid[0] * H.deck.ngrid[1] *
+         H.deck.ngrid[2];
+  return b;
+}
+
 int init_chain_state(const InputDeck& d, const HostSystem& H, const double2* sk_src, double energy0, int sys,
                      const int* seed, ChainDev& C, const DevAllocFn& alloc, cudaStream_t st, std::string& err,
                      bool record_samples) {
@@ -725,6 +735,34 @@ int fmc_batch_chain_timing(fmc_batch* b, int chain, long long* out) {
     return -1;
   }
   for (int k = 0; k < 3; k++) out[k] = b->impl.h_timing ? b->impl.h_timing[3 * chain + k] : 0;
+  return 0;
+}
+
+int fmc_batch_voxels(fmc_batch* b, int chain, int* nvox, int* off, int* atoms, long long cap, long long* n_entries) {
+  if (!b || chain < 0 || chain >= b->impl.nchains || !nvox || !n_entries) {
+    fmc::set_last_error("bad batch handle, chain index or argument");
+    return -1;
+  }
+  const fmc::Chain& sc = *b->impl.sys_chains[b->impl.chain_sys[chain]];
+  const fmc::DevSystem& v = sc.dsys.view;
+  for (int a = 0; a < 3; a++) nvox[a] = v.nvox[a];
+  *n_entries = sc.dsys.vox_entries;
+  const int nv = v.nvox[0] * v.nvox[1] * v.nvox[2];
+  cudaSetDevice(b->impl.device);
+  cudaError_t e = cudaSuccess;
+  if (off) e = cudaMemcpy(off, v.vox_off, sizeof(int) * (nv + 1), cudaMemcpyDeviceToHost);
+  if (atoms && e == cudaSuccess) {
+    if (cap < sc.dsys.vox_entries) {
+      fmc::set_last_error("atoms buffer smaller than the voxel entries");
+      return -2;
+    }
+    if (sc.dsys.vox_entries)
+      e = cudaMemcpy(atoms, v.vox_atoms, sizeof(int) * sc.dsys.vox_entries, cudaMemcpyDeviceToHost);
+  }
+  if (e != cudaSuccess) {
+    fmc::set_last_error(cudaGetErrorString(e));
+    return -100 - (int)e;
+  }
   return 0;
 }
 

@@ -58,12 +58,23 @@ int upload_system(const HostSystem& h, DeviceSystem& d, std::string& err) {
     // voxel lists built on the device: count per voxel, prefix sum, ordered fill
     const int nv = h.nvox[0] * h.nvox[1] * h.nvox[2];
     int* counts = nullptr;
+    unsigned* code = nullptr;  // per-atom voxel codes of an orthorhombic cell (list prefilter)
     if ((e = cudaMalloc(&counts, sizeof(int) * nv)) != cudaSuccess) goto fail;
-    e = launch_voxel_count(h.cell, h.nvox, v.fw, h.nf, h.vox_lim2, counts, 0);
+    if (voxel_prefilter_applies(h.cell, h.nvox) && h.nf > 0) {
+      if ((e = cudaMalloc(&code, sizeof(unsigned) * h.nf)) != cudaSuccess) {
+        cudaFree(counts);
+        goto fail;
+      }
+      e = launch_voxel_codes(h.cell, h.nvox, v.fw, h.nf, code, 0);
+    }
+    if (e == cudaSuccess) e = launch_voxel_count(h.cell, h.nvox, v.fw, h.nf, h.vox_lim2, code, counts, 0);
     std::vector<int> cnt(nv), offv(nv + 1, 0);
     if (e == cudaSuccess) e = cudaMemcpy(cnt.data(), counts, sizeof(int) * nv, cudaMemcpyDeviceToHost);
     cudaFree(counts);
-    if (e != cudaSuccess) goto fail;
+    if (e != cudaSuccess) {
+      cudaFree(code);
+      goto fail;
+    }
     for (int i = 0; i < nv; i++) offv[i + 1] = offv[i] + cnt[i];
     const size_t ne = (size_t)offv[nv];
     d.vox_entries = (long long)ne;
@@ -71,14 +82,16 @@ int upload_system(const HostSystem& h, DeviceSystem& d, std::string& err) {
     unsigned short* a16 = nullptr;
     double4* xyzq = nullptr;
     unsigned char* vt = nullptr;
-    if ((e = upload(d.allocations, &v.vox_off, offv)) != cudaSuccess) goto fail;
-    if ((e = dalloc(d.allocations, &atoms, ne)) != cudaSuccess) goto fail;
-    if (h.nf <= 65535 && (e = dalloc(d.allocations, &a16, ne)) != cudaSuccess) goto fail;
-    if ((e = dalloc(d.allocations, &xyzq, ne)) != cudaSuccess) goto fail;
-    if ((e = dalloc(d.allocations, &vt, ne)) != cudaSuccess) goto fail;
-    e = launch_voxel_fill(h.cell, h.nvox, v.fw, v.fw_type, h.nf, h.vox_lim2, v.vox_off, atoms, a16, xyzq, vt,
-                          (long long)ne, 0);
+    e = upload(d.allocations, &v.vox_off, offv);
+    if (e == cudaSuccess) e = dalloc(d.allocations, &atoms, ne);
+    if (e == cudaSuccess && h.nf <= 65535) e = dalloc(d.allocations, &a16, ne);
+    if (e == cudaSuccess) e = dalloc(d.allocations, &xyzq, ne);
+    if (e == cudaSuccess) e = dalloc(d.allocations, &vt, ne);
+    if (e == cudaSuccess)
+      e = launch_voxel_fill(h.cell, h.nvox, v.fw, v.fw_type, h.nf, h.vox_lim2, code, v.vox_off, atoms, a16, xyzq, vt,
+                            (long long)ne, 0);
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    cudaFree(code);
     if (e != cudaSuccess) goto fail;
     v.vox_atoms = atoms;
     v.vox_atoms16 = a16;

@@ -6,10 +6,12 @@
 #include "fmc_inputs.h"
 
 #include <algorithm>
+#include <charconv>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <string_view>
 
 namespace fmc {
 namespace {
@@ -25,11 +27,13 @@ struct InputError {
 class Record {
  public:
   char c[kRecLen];
-  void set(const std::string& s) {
-    for (int i = 0; i < kRecLen; i++) {
-      char ch = i < (int)s.size() ? s[i] : ' ';
+  void set(const char* s, size_t n) {
+    const int m = n < (size_t)kRecLen ? (int)n : kRecLen;
+    for (int i = 0; i < m; i++) {
+      const char ch = s[i];
       c[i] = (ch == '\t' || ch == '\r') ? ' ' : ch;
     }
+    std::memset(c + m, ' ', kRecLen - m);
   }
   // lowcase (parse_module.f:331): only the first n characters
   void lower(int n = kRecLen) {
@@ -100,23 +104,26 @@ class Record {
   }
   // getword (parse_module.f:547): next blank-delimited word, at most len1 characters,
   // returned blank-padded to 8 characters.
+  // The reference shifts the record one character per character examined; the shift is done
+  // once here, by the number examined.
   std::string take_word(int len1) {
-    std::string w;
-    int i = 0;
+    char w[kRecLen];
+    int nw = 0, i = 0;
     bool fin = false;
     while (!fin && i < kRecLen) {
-      i++;
-      if (c[0] == ' ') {
-        if (!w.empty()) fin = true;
+      const char ch = c[i++];
+      if (ch == ' ') {
+        if (nw) fin = true;
       } else {
-        w.push_back(c[0]);
-        if ((int)w.size() == len1) fin = true;
+        w[nw++] = ch;
+        if (nw == len1) fin = true;
       }
-      std::memmove(c, c + 1, kRecLen - 1);
-      c[kRecLen - 1] = ' ';
     }
-    w.resize(8, ' ');
-    return w;
+    std::memmove(c, c + i, kRecLen - i);
+    std::memset(c + kRecLen - i, ' ', i);
+    std::string out(w, nw);
+    out.resize(8, ' ');
+    return out;
   }
 
  private:
@@ -150,27 +157,45 @@ class Record {
   }
 };
 
+// A file read whole, served a line at a time (lines as std::getline splits them: at '\n', the
+// last one counted only when it holds characters).
 class Deck {
  public:
   Deck(const std::string& path, int eof_code, const char* eof_msg) : code_(eof_code), msg_(eof_msg) {
-    std::ifstream f(path);
+    std::ifstream f(path, std::ios::binary);
     if (!f) raise(code_, std::string("cannot open ") + path);
-    std::string s;
-    while (std::getline(f, s)) lines_.push_back(s);
+    f.seekg(0, std::ios::end);
+    const std::streamoff n = f.tellg();
+    f.seekg(0, std::ios::beg);
+    buf_.resize(n > 0 ? (size_t)n : 0);
+    if (n > 0 && !f.read(&buf_[0], n)) raise(code_, std::string("cannot read ") + path);
+    size_t at = 0;
+    while (at < buf_.size()) {
+      const void* nl = std::memchr(buf_.data() + at, '\n', buf_.size() - at);
+      const size_t end = nl ? (size_t)((const char*)nl - buf_.data()) : buf_.size();
+      lines_.push_back({at, end - at});
+      at = end + 1;
+    }
   }
   Record next() {
     if (pos_ >= lines_.size()) raise(code_, msg_);
     Record r;
-    r.set(lines_[pos_++]);
+    const Line& l = lines_[pos_++];
+    r.set(buf_.data() + l.at, l.len);
     return r;
   }
-  const std::string& raw() {
+  std::string_view raw() {
     if (pos_ >= lines_.size()) raise(55, "end of CONFIG file encountered");
-    return lines_[pos_++];
+    const Line& l = lines_[pos_++];
+    return std::string_view(buf_.data() + l.at, l.len);
   }
 
  private:
-  std::vector<std::string> lines_;
+  struct Line {
+    size_t at, len;
+  };
+  std::string buf_;
+  std::vector<Line> lines_;
   size_t pos_ = 0;
   int code_;
   std::string msg_;
@@ -529,14 +554,24 @@ void read_field(const std::string& dir, InputDeck& d, const Scan& s, std::vector
 }
 
 // Fortran '(3f20.0)' read: three 20-character numeric fields
-double f20(const std::string& s, int k) {
-  std::string t;
+double f20(std::string_view s, int k) {
+  char t[24];
+  int n = 0;
   for (int i = 20 * k; i < 20 * k + 20 && i < (int)s.size(); i++) {
     char ch = s[i];
     if (ch == ' ' || ch == '\r' || ch == '\t') continue;
-    t.push_back(ch == 'd' || ch == 'D' ? 'e' : ch);
+    t[n++] = ch == 'd' || ch == 'D' ? 'e' : ch;
   }
-  return t.empty() ? 0.0 : std::strtod(t.c_str(), nullptr);
+  t[n] = 0;
+  if (!n) return 0.0;
+  // std::from_chars rounds correctly, as strtod does, and is several times faster; strtod keeps
+  // what from_chars does not read the same way (a leading '+', hexadecimal, out of range)
+  if (t[0] != '+' && !std::memchr(t, 'x', n) && !std::memchr(t, 'X', n)) {
+    double v = 0.0;
+    const std::from_chars_result r = std::from_chars(t, t + n, v);
+    if (r.ec == std::errc()) return v;
+  }
+  return std::strtod(t, nullptr);
 }
 
 // ---------------------------------------------------------------- CONFIG (readinputs.f:309-513)
@@ -562,14 +597,17 @@ void read_config(const std::string& dir, InputDeck& d, const std::vector<MolBloc
     int at = 0;
     for (int l = 0; l < b.nummols; l++)
       for (int m = 0; m < b.numatoms; m++, at++) {
-        std::string name_line = f.raw();
-        std::string coord_line = f.raw();
+        const std::string_view name_line = f.raw();
+        const std::string_view coord_line = f.raw();
         for (int e = 0; e < levcfg; e++) f.raw();
-        std::string an = name_line.substr(0, std::min<size_t>(8, name_line.size()));
-        size_t k = an.find_first_not_of(' ');
-        an = k == std::string::npos ? std::string() : an.substr(k);
-        an.resize(8, ' ');
-        if (an != b.names[m]) raise(25, "wrong atom type found in CONFIG file");
+        // the first 8 characters, leading blanks dropped, blank-padded to 8
+        std::string_view an = name_line.substr(0, std::min<size_t>(8, name_line.size()));
+        const size_t k = an.find_first_not_of(' ');
+        an = k == std::string_view::npos ? std::string_view() : an.substr(k);
+        const std::string& want = b.names[m];
+        if (want.size() != 8 || want.compare(0, an.size(), an) != 0 ||
+            want.find_first_not_of(' ', an.size()) != std::string::npos)
+          raise(25, "wrong atom type found in CONFIG file");
         double x = f20(coord_line, 0), y = f20(coord_line, 1), z = f20(coord_line, 2);
         if (gxyz) {
           (*gxyz)[3 * at] = x;

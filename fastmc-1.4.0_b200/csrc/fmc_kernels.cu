@@ -11,6 +11,8 @@
 // fmc_commit_kernel : S(k) <- S_new and the guest-site array update of an accepted move.
 // fmc_recip_*       : full S(k) of a set of atoms (ewald1, ewald.f:368-630).
 // fmc_sp_kernel     : per-guest-site real-space energies for the single-point energy.
+#include <cmath>
+
 #include "fmc_device.cuh"
 #include "fmc_kernels.h"
 
@@ -345,14 +347,52 @@ __device__ __forceinline__ void voxel_centre(const CellGeom& c, int v, int n0, i
 
 constexpr int kVoxThreads = 128;
 
+// Voxel prefilter of orthorhombic cells (imcon 1, 2).  code[j] packs atom j's voxel along
+// a, b, c (10 bits each); an atom whose voxel lies more than reach voxels away (cyclically)
+// along any axis from the list's voxel cannot be within the list radius, so the list kernels
+// skip its FP64 distance test.  reach = floor((lim + 0.01 A) / edge + 1.5): half a voxel for
+// the atom's place inside its voxel, one for an atom binned into a neighbouring voxel by
+// rounding, 0.01 A for rounding of the distance test itself and of the periods.  The lists
+// keep exactly the atoms, and the order, of the unfiltered test.
+__device__ __forceinline__ int cyclic_gap(int d, int n) {
+  d = d < 0 ? -d : d;
+  return min(d, n - d);
+}
+
+__device__ __forceinline__ bool voxel_near(unsigned cd, int va, int vb, int vc, int n0, int n1, int n2, int3 r) {
+  return cyclic_gap(va - (int)(cd & 1023u), n0) <= r.x && cyclic_gap(vb - (int)((cd >> 10) & 1023u), n1) <= r.y &&
+         cyclic_gap(vc - (int)(cd >> 20), n2) <= r.z;
+}
+
+__global__ void __launch_bounds__(kVoxThreads) fmc_voxel_code_kernel(CellGeom cell, int n0, int n1, int n2,
+                                                                     const double4* __restrict__ fw, int nf,
+                                                                     unsigned* __restrict__ code) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= nf) return;
+  const double4 a = fw[j];
+  const double x[3] = {a.x, a.y, a.z};
+  const int n[3] = {n0, n1, n2};
+  unsigned out = 0;
+  for (int k = 0; k < 3; k++) {
+    double f = x[k] / cell.h[4 * k];
+    f -= floor(f);
+    const int i = min(max((int)(f * n[k]), 0), n[k] - 1);
+    out |= (unsigned)i << (10 * k);
+  }
+  code[j] = out;
+}
+
 __global__ void __launch_bounds__(kVoxThreads) fmc_voxel_count_kernel(CellGeom cell, int n0, int n1, int n2,
                                                                       const double4* __restrict__ fw, int nf,
-                                                                      double lim2, int* counts) {
+                                                                      double lim2, const unsigned* __restrict__ code,
+                                                                      int3 reach, int* counts) {
   __shared__ int ws[kVoxThreads / 32];
   double p[3];
   voxel_centre(cell, blockIdx.x, n0, n1, n2, p);
+  const int va = blockIdx.x / (n1 * n2), vb = (blockIdx.x / n2) % n1, vc = blockIdx.x % n2;
   int cnt = 0;
   for (int j = threadIdx.x; j < nf; j += blockDim.x) {
+    if (code && !voxel_near(code[j], va, vb, vc, n0, n1, n2, reach)) continue;
     double4 a = fw[j];
     if (true_dist2_dev(cell, p[0] - a.x, p[1] - a.y, p[2] - a.z) < lim2) cnt++;
   }
@@ -369,6 +409,7 @@ __global__ void __launch_bounds__(kVoxThreads) fmc_voxel_count_kernel(CellGeom c
 __global__ void __launch_bounds__(kVoxThreads) fmc_voxel_fill_kernel(CellGeom cell, int n0, int n1, int n2,
                                                                      const double4* __restrict__ fw,
                                                                      const int* __restrict__ ftype, int nf, double lim2,
+                                                                     const unsigned* __restrict__ code, int3 reach,
                                                                      const int* __restrict__ off, int* atoms,
                                                                      unsigned short* atoms16, double4* xyzq,
                                                                      unsigned char* vtype, long long cap) {
@@ -377,6 +418,7 @@ __global__ void __launch_bounds__(kVoxThreads) fmc_voxel_fill_kernel(CellGeom ce
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   double p[3];
   voxel_centre(cell, blockIdx.x, n0, n1, n2, p);
+  const int va = blockIdx.x / (n1 * n2), vb = (blockIdx.x / n2) % n1, vc = blockIdx.x % n2;
   if (threadIdx.x == 0) running = 0;
   const int base = off[blockIdx.x];
   __syncthreads();
@@ -384,7 +426,7 @@ __global__ void __launch_bounds__(kVoxThreads) fmc_voxel_fill_kernel(CellGeom ce
     int j = chunk + threadIdx.x;
     bool flag = false;
     double4 a = make_double4(0, 0, 0, 0);
-    if (j < nf) {
+    if (j < nf && (!code || voxel_near(code[j], va, vb, vc, n0, n1, n2, reach))) {
       a = fw[j];
       flag = true_dist2_dev(cell, p[0] - a.x, p[1] - a.y, p[2] - a.z) < lim2;
     }
@@ -411,19 +453,47 @@ __global__ void __launch_bounds__(kVoxThreads) fmc_voxel_fill_kernel(CellGeom ce
   }
 }
 
+namespace {
+int3 voxel_reach(const CellGeom& cell, const int* nvox, double lim2) {
+  const double lim = std::sqrt(lim2) + 0.01;
+  int r[3];
+  for (int a = 0; a < 3; a++) r[a] = (int)std::floor(lim / (cell.h[4 * a] / nvox[a]) + 1.5);
+  return make_int3(r[0], r[1], r[2]);
+}
+}  // namespace
+
+bool voxel_prefilter_applies(const CellGeom& cell, const int* nvox) {
+  if (cell.imcon != 1 && cell.imcon != 2) return false;
+  for (int a = 0; a < 3; a++)
+    if (nvox[a] < 1 || nvox[a] > 1023 || !(cell.h[4 * a] > 0.0)) return false;
+  return true;
+}
+
+cudaError_t launch_voxel_codes(const CellGeom& cell, const int* nvox, const double4* fw, int nf, unsigned* code,
+                               cudaStream_t st) {
+  if (nf > 0)
+    fmc_voxel_code_kernel<<<(nf + kVoxThreads - 1) / kVoxThreads, kVoxThreads, 0, st>>>(cell, nvox[0], nvox[1],
+                                                                                       nvox[2], fw, nf, code);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_voxel_count(const CellGeom& cell, const int* nvox, const double4* fw, int nf, double lim2,
-                               int* counts, cudaStream_t st) {
+                               const unsigned* code, int* counts, cudaStream_t st) {
   int nv = nvox[0] * nvox[1] * nvox[2];
-  fmc_voxel_count_kernel<<<nv, kVoxThreads, 0, st>>>(cell, nvox[0], nvox[1], nvox[2], fw, nf, lim2, counts);
+  if (code && !voxel_prefilter_applies(cell, nvox)) code = nullptr;
+  const int3 r = code ? voxel_reach(cell, nvox, lim2) : make_int3(0, 0, 0);
+  fmc_voxel_count_kernel<<<nv, kVoxThreads, 0, st>>>(cell, nvox[0], nvox[1], nvox[2], fw, nf, lim2, code, r, counts);
   return cudaGetLastError();
 }
 
 cudaError_t launch_voxel_fill(const CellGeom& cell, const int* nvox, const double4* fw, const int* ftype, int nf,
-                              double lim2, const int* off, int* atoms, unsigned short* atoms16, double4* xyzq,
-                              unsigned char* vtype, long long cap, cudaStream_t st) {
+                              double lim2, const unsigned* code, const int* off, int* atoms, unsigned short* atoms16,
+                              double4* xyzq, unsigned char* vtype, long long cap, cudaStream_t st) {
   int nv = nvox[0] * nvox[1] * nvox[2];
-  fmc_voxel_fill_kernel<<<nv, kVoxThreads, 0, st>>>(cell, nvox[0], nvox[1], nvox[2], fw, ftype, nf, lim2, off, atoms,
-                                                    atoms16, xyzq, vtype, cap);
+  if (code && !voxel_prefilter_applies(cell, nvox)) code = nullptr;
+  const int3 r = code ? voxel_reach(cell, nvox, lim2) : make_int3(0, 0, 0);
+  fmc_voxel_fill_kernel<<<nv, kVoxThreads, 0, st>>>(cell, nvox[0], nvox[1], nvox[2], fw, ftype, nf, lim2, code, r,
+                                                    off, atoms, atoms16, xyzq, vtype, cap);
   return cudaGetLastError();
 }
 

@@ -55,11 +55,19 @@ double recip_energy_from_parts(const DevSystem& S, const double* host_parts);
 cudaError_t launch_single_point_rs(const DevSystem& S, const GuestView& G, int nsites, const int* sites, const int* lo,
                                    const int* hi, double* out, cudaStream_t st);
 
+// Voxel lists: per voxel, the framework atoms within sqrt(lim2) of its centre by true minimum
+// image, in ascending atom order.  Orthorhombic cells (voxel_prefilter_applies) can pass
+// per-atom voxel codes (launch_voxel_codes, nf words) so that the FP64 test runs only for atoms
+// within reach; code = nullptr tests every atom.  Both give the same lists.
+bool voxel_prefilter_applies(const CellGeom& cell, const int* nvox);
+cudaError_t launch_voxel_codes(const CellGeom& cell, const int* nvox, const double4* fw, int nf, unsigned* code,
+                               cudaStream_t st);
 cudaError_t launch_voxel_count(const CellGeom& cell, const int* nvox, const double4* fw, int nf, double lim2,
-                               int* counts, cudaStream_t st);
+                               const unsigned* code, int* counts, cudaStream_t st);
 cudaError_t launch_voxel_fill(const CellGeom& cell, const int* nvox, const double4* fw, const int* ftype, int nf,
-                              double lim2, const int* off, int* atoms, unsigned short* atoms16, double4* xyzq,
-                              unsigned char* vtype, long long cap, cudaStream_t st);  // entries >= cap not written
+                              double lim2, const unsigned* code, const int* off, int* atoms, unsigned short* atoms16,
+                              double4* xyzq, unsigned char* vtype, long long cap,
+                              cudaStream_t st);  // entries >= cap not written
 // off[0..n]: exclusive prefix sum of counts[0..n-1], off[n] the total (one CTA)
 cudaError_t launch_exclusive_scan(const int* counts, int n, int* off, cudaStream_t st);
 

@@ -6,9 +6,12 @@
 // that used their budget (a move count, or with 0 the deck's own equilibration + production
 // cycles; a finished chain marks itself inactive, so the launch already queued skips it) and
 // admits prepared requests from the front of the queue into free slots while the device-memory
-// budget allows, building them on a second stream beside the running launch for the launch after
-// it.  So launches follow one another without waiting for the host.  The reference runs one
-// such isotherm point per MPI rank (gcmc.f:334-417).
+// budget allows.  Worker threads enqueue each request's device slot on their own streams ahead
+// of admission without waiting for it (an event marks the build's end), so a worker goes on to
+// the next deck while the device builds; admission installs a slot whose build has completed,
+// or builds one on a second stream beside the running launch for the launch after it.  So
+// launches follow one another without waiting for the host.  The reference runs one such
+// isotherm point per MPI rank (gcmc.f:334-417).
 #include <algorithm>
 #include <atomic>
 #include <chrono>
@@ -34,11 +37,17 @@ double now_ms() {
 }
 }  // namespace
 
+// A slot built ahead by a worker: its build is enqueued on the worker's stream and `done` is
+// recorded after it; *vox_total (pinned) receives the exact voxel-list size, checked against
+// vox_cap once `done` has completed.
 struct Prebuilt {
   SlotMemory mem;
   SysConst Y;
   ChainDev C;
   long long vox_cap = 0;
+  cudaEvent_t done = nullptr;
+  int word = -1;  // index of vox_total in the server's pinned words
+  int* vox_total = nullptr;
 };
 
 class Server {
@@ -60,11 +69,15 @@ class Server {
     // the device slot a worker built ahead of admission (null: built at admission instead)
     std::unique_ptr<struct Prebuilt> pre;
   };
-  // A worker's own stream, pinned staging and voxel-count word for building slots ahead.
+  // A worker's own stream and a ring of pinned staging buffers for building slots ahead: a
+  // buffer is reused once the build that read it has completed (its event).
+  static constexpr int kRing = 4;
   struct WorkerRes {
     cudaStream_t st = nullptr;
-    Staging stage;
-    int* vox_total = nullptr;
+    Staging stage[kRing];
+    cudaEvent_t stage_done[kRing] = {};
+    bool stage_busy[kRing] = {};
+    int next = 0;
   };
   struct Slot {
     int request = -1;
@@ -86,6 +99,8 @@ class Server {
   int building = 0;                 // slots being built ahead right now (guarded by mu)
   static constexpr int kMaxPrebuilt = 64;  // slots built ahead at most
   std::vector<WorkerRes> wres;
+  int* h_words = nullptr;           // pinned voxel-list sizes of slots built ahead
+  std::vector<int> free_words;      // (guarded by mu)
   cudaMemPool_t pool = nullptr;
   std::vector<Slot> slots;
   std::vector<std::unique_ptr<Request>> reqs;  // the vector is guarded by mu; entries are stable
@@ -117,7 +132,8 @@ class Server {
   // accounting
   long long admitted = 0, retired = 0, launches = 0, moves_run = 0, last_moves = 0;
   double admit_ms = 0, launch_ms = 0, wait_ms = 0;
-  std::atomic<long long> prep_us{0};
+  std::atomic<long long> prep_us{0}, prep_host_us{0}, prep_dev_us{0};
+  long long admit_prebuilt = 0, admit_built = 0;
 
   ~Server() {
     {
@@ -131,6 +147,7 @@ class Server {
     for (auto& r : reqs)
       if (r->pre) {
         r->pre->mem.release();
+        if (r->pre->done) cudaEventDestroy(r->pre->done);
         r->pre.reset();
       }
     cudaStreamSynchronize(st);
@@ -139,10 +156,13 @@ class Server {
     if (st2) cudaStreamSynchronize(st2);
     for (WorkerRes& w : wres) {
       if (w.st) cudaStreamSynchronize(w.st);
-      if (w.stage.base) cudaFreeHost(w.stage.base);
-      if (w.vox_total) cudaFreeHost(w.vox_total);
+      for (int k = 0; k < kRing; k++) {
+        if (w.stage[k].base) cudaFreeHost(w.stage[k].base);
+        if (w.stage_done[k]) cudaEventDestroy(w.stage_done[k]);
+      }
       if (w.st) cudaStreamDestroy(w.st);
     }
+    if (h_words) cudaFreeHost(h_words);
     if (pool) cudaMemPoolDestroy(pool);
     for (int b = 0; b < 2; b++) {
       if (ev_start[b]) cudaEventDestroy(ev_start[b]);
@@ -233,17 +253,24 @@ class Server {
     std::memset(h_chains, 0, sizeof(ChainDev) * n);
     wres.resize(nworkers);
     for (WorkerRes& w : wres) {
-      if (cudaStreamCreateWithFlags(&w.st, cudaStreamNonBlocking) != cudaSuccess ||
-          cudaMallocHost(&w.vox_total, sizeof(int)) != cudaSuccess) {
+      if (cudaStreamCreateWithFlags(&w.st, cudaStreamNonBlocking) != cudaSuccess) {
         err = "cannot create a worker's stream";
         return -100;
       }
-      w.stage.cap = 8u << 20;
-      if (cudaMallocHost(&w.stage.base, w.stage.cap) != cudaSuccess) {
-        err = "cannot allocate a worker's staging buffer";
-        return -100;
+      for (int k = 0; k < kRing; k++) {
+        w.stage[k].cap = 4u << 20;
+        if (cudaMallocHost(&w.stage[k].base, w.stage[k].cap) != cudaSuccess ||
+            cudaEventCreateWithFlags(&w.stage_done[k], cudaEventDisableTiming) != cudaSuccess) {
+          err = "cannot allocate a worker's staging buffers";
+          return -100;
+        }
       }
     }
+    if (cudaMallocHost(&h_words, sizeof(int) * kMaxPrebuilt) != cudaSuccess) {
+      err = "cannot allocate the pinned voxel-size words";
+      return -100;
+    }
+    for (int k = kMaxPrebuilt - 1; k >= 0; k--) free_words.push_back(k);
     for (int w = 0; w < nworkers; w++) workers.emplace_back([this, w] { worker(w); });
     return 0;
   }
@@ -276,50 +303,69 @@ class Server {
         }
     r.prep_rc = rc;
     r.prep_err = err;
+    const double t1 = now_ms();
+    prep_host_us += (long long)((t1 - t0) * 1000.0);
     if (!rc) {
       r.bytes_estimate = slot_bytes_estimate(*h);
       r.host = std::move(h);
-      if (w) prebuild(r, *w);
+      if (w) {
+        prebuild(r, *w);
+        prep_dev_us += (long long)((now_ms() - t1) * 1000.0);
+      }
     }
     prep_us += (long long)((now_ms() - t0) * 1000.0);
     r.prepared.store(1, std::memory_order_release);
   }
 
-  // A worker builds the request's device slot on its own stream, while the memory budget allows,
-  // and checks its voxel lists, so that admission only installs it.  On any failure the slot is
-  // left to be built at admission.
+  // A worker enqueues the request's device slot on its own stream, while the memory budget
+  // allows, and records an event after it without waiting: admission installs the slot once
+  // the event has completed and the voxel lists have been checked against their estimate.  On
+  // any failure the slot is left to be built at admission.
   void prebuild(Request& r, WorkerRes& w) {
+    int word = -1;
     {
       std::lock_guard<std::mutex> lk(mu);
-      if (prebuilt_count >= kMaxPrebuilt || used.load() + prebuilt_bytes + r.bytes_estimate > budget) return;
+      if (prebuilt_count >= kMaxPrebuilt || free_words.empty() ||
+          used.load() + prebuilt_bytes + r.bytes_estimate > budget)
+        return;
       prebuilt_bytes += r.bytes_estimate;
       prebuilt_count++;
       building++;
+      word = free_words.back();
+      free_words.pop_back();
     }
     auto P = std::make_unique<Prebuilt>();
     P->mem.st = w.st;
     P->mem.pool = pool;
+    P->word = word;
+    P->vox_total = h_words + word;
+    *P->vox_total = 0;
+    const int k = w.next;
+    w.next = (w.next + 1) % kRing;
+    Staging& sg = w.stage[k];
+    bool ok = !w.stage_busy[k] || cudaEventSynchronize(w.stage_done[k]) == cudaSuccess;  // read by now
     const size_t need = slot_staging_bytes(*r.host);
-    bool ok = true;
-    if (need > w.stage.cap) {
-      cudaFreeHost(w.stage.base);
-      w.stage.cap = need;
-      if (cudaMallocHost(&w.stage.base, w.stage.cap) != cudaSuccess) {
-        w.stage.base = nullptr;
-        w.stage.cap = 0;
+    if (ok && need > sg.cap) {
+      cudaFreeHost(sg.base);
+      sg.cap = need;
+      if (cudaMallocHost(&sg.base, sg.cap) != cudaSuccess) {
+        sg.base = nullptr;
+        sg.cap = 0;
         ok = false;
       }
     }
     std::string err;
-    for (int attempt = 0; ok && attempt < 2; attempt++) {
-      w.stage.used = 0;
-      if (attempt == 0) P->vox_cap = slot_voxel_capacity(*r.host);
-      ok = build_slot(*r.host, 0, r.seed, P->mem, w.stage, P->vox_cap, w.vox_total, P->Y, P->C, err) == 0 &&
-           cudaStreamSynchronize(w.st) == cudaSuccess;
-      if (ok && (long long)*w.vox_total <= P->vox_cap) break;
-      P->mem.release();  // the lists outgrew the estimate: once more at their exact size
-      P->vox_cap = *w.vox_total;
-      ok = ok && attempt == 0;
+    sg.used = 0;
+    P->vox_cap = slot_voxel_capacity(*r.host);
+    ok = ok && build_slot(*r.host, 0, r.seed, P->mem, sg, P->vox_cap, P->vox_total, P->Y, P->C, err) == 0;
+    ok = ok && cudaEventCreateWithFlags(&P->done, cudaEventDisableTiming) == cudaSuccess &&
+         cudaEventRecord(P->done, w.st) == cudaSuccess;
+    w.stage_busy[k] = cudaEventRecord(w.stage_done[k], w.st) == cudaSuccess;
+    if (!ok) {
+      // nothing enqueued may write the word or read the memory once the stream has drained
+      P->mem.release();
+      cudaStreamSynchronize(w.st);
+      if (P->done) cudaEventDestroy(P->done);
     }
     std::lock_guard<std::mutex> lk(mu);
     prebuilt_bytes -= r.bytes_estimate;
@@ -330,10 +376,7 @@ class Server {
       r.pre = std::move(P);
     } else {
       prebuilt_count--;
-      if (P->mem.bytes) {
-        P->mem.release();
-        cudaStreamSynchronize(w.st);
-      }
+      free_words.push_back(word);
     }
   }
 
@@ -417,20 +460,33 @@ class Server {
     return 0;
   }
 
-  // Frees a request's slot built ahead (its preparation has finished).
+  // Frees a request's slot built ahead (its preparation has finished; its build may still run:
+  // the frees are ordered after it on its stream).
   void drop_prebuilt(Request& r) {
+    std::unique_ptr<Prebuilt> P;
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      if (!r.pre) return;
+      P = std::move(r.pre);
+      prebuilt_bytes -= std::min(prebuilt_bytes, P->mem.bytes);
+      prebuilt_count--;
+    }
+    P->mem.release();
+    cudaEventSynchronize(P->done);  // the build no longer writes its word
+    cudaEventDestroy(P->done);
     std::lock_guard<std::mutex> lk(mu);
-    if (!r.pre) return;
-    prebuilt_bytes -= std::min(prebuilt_bytes, r.pre->mem.bytes);
-    prebuilt_count--;
-    r.pre->mem.release();
-    r.pre.reset();
+    free_words.push_back(P->word);
   }
 
+  // Frees slot i's memory on the stream that built it (ordered after that build) and gives the
+  // slot back the admission stream, on which any later build of the slot at admission runs:
+  // settle_admissions and the next launch wait for that stream only.
   void release(int i) {
     Slot& s = slots[i];
     used -= std::min(used.load(), s.mem.bytes);
     s.mem.release();
+    s.mem.st = st2;
+    s.mem.pool = pool;
     s.request = -1;
     h_chains[i].active = 0;
   }
@@ -493,26 +549,36 @@ class Server {
       reject(r, r.prep_rc, r.prep_err);
       return 0;
     }
-    if (r.pre) {  // built ahead by a worker: install it
+    long long vox_cap = slot_voxel_capacity(*r.host);
+    if (r.pre) {  // built ahead by a worker (its build has completed): install it
+      std::unique_ptr<Prebuilt> P = std::move(r.pre);
+      const long long total = *P->vox_total;
+      cudaEventDestroy(P->done);
       {
         std::lock_guard<std::mutex> lk(mu);
-        prebuilt_bytes -= std::min(prebuilt_bytes, r.pre->mem.bytes);
+        prebuilt_bytes -= std::min(prebuilt_bytes, P->mem.bytes);
         prebuilt_count--;
+        free_words.push_back(P->word);
       }
-      s.mem = std::move(r.pre->mem);
-      s.vox_cap = r.pre->vox_cap;
-      h_sys[i] = r.pre->Y;
-      h_chains[i] = r.pre->C;
-      h_chains[i].sys = i;
-      r.pre.reset();
-      r.host.reset();
-      s.request = id;
-      s.fresh = false;  // checked by its worker
-      fresh.push_back(i);
-      r.state = kRunning;
-      r.slot = i;
-      admitted++;
-      return s.mem.bytes;
+      if (total <= P->vox_cap) {
+        s.mem = std::move(P->mem);
+        s.vox_cap = P->vox_cap;
+        h_sys[i] = P->Y;
+        h_chains[i] = P->C;
+        h_chains[i].sys = i;
+        r.host.reset();
+        s.request = id;
+        s.fresh = false;  // its lists were checked above
+        fresh.push_back(i);
+        r.state = kRunning;
+        r.slot = i;
+        admitted++;
+        admit_prebuilt++;
+        return s.mem.bytes;
+      }
+      // the lists outgrew their estimate: built again below at their exact size
+      P->mem.release();
+      vox_cap = total;
     }
     const size_t need = slot_staging_bytes(*r.host);
     if (stage.used + need > stage.cap) {  // the staged bytes of earlier admissions are read by now
@@ -528,7 +594,9 @@ class Server {
       }
     }
     std::string err;
-    s.vox_cap = slot_voxel_capacity(*r.host);
+    s.vox_cap = vox_cap;
+    s.mem.st = st2;  // the admission stream, which settle_admissions and the next launch wait for
+    s.mem.pool = pool;
     int rc = build_slot(*r.host, i, r.seed, s.mem, stage, s.vox_cap, &h_vox_total[i], h_sys[i], h_chains[i], err);
     if (rc) {
       s.mem.release();
@@ -543,6 +611,7 @@ class Server {
     r.state = kRunning;
     r.slot = i;
     admitted++;
+    admit_built++;
     return s.mem.bytes;
   }
 
@@ -562,6 +631,16 @@ class Server {
         const double w0 = now_ms();
         while (!r.prepared.load(std::memory_order_acquire)) std::this_thread::sleep_for(std::chrono::microseconds(200));
         wait_ms += now_ms() - w0;
+      }
+      if (r.pre) {  // its slot was built ahead: installed once that build has completed
+        cudaError_t q = cudaEventQuery(r.pre->done);
+        if (q == cudaErrorNotReady) {
+          if (running) break;
+          const double w0 = now_ms();
+          q = cudaEventSynchronize(r.pre->done);
+          wait_ms += now_ms() - w0;
+        }
+        if (q != cudaSuccess) drop_prebuilt(r);  // built again at admission, which reports the error
       }
       size_t ahead;
       {
@@ -899,6 +978,10 @@ int fmc_server_stats(fmc_server* s, double* out) {
   out[7] = (double)v.workers.size();
   out[8] = (double)v.moves_run;
   out[9] = (double)v.last_moves;
+  out[10] = (double)v.prep_host_us.load() / 1000.0;
+  out[11] = (double)v.prep_dev_us.load() / 1000.0;
+  out[12] = (double)v.admit_prebuilt;
+  out[13] = (double)v.admit_built;
   return 0;
 }
 

@@ -11,8 +11,28 @@
 
 namespace fmc {
 
+cudaError_t SlotMemory::reserve(size_t n) {
+  void* p = nullptr;
+  n = (n + 255) & ~size_t(255);
+  cudaError_t e = pool ? cudaMallocFromPoolAsync(&p, n, pool, st) : cudaMallocAsync(&p, n, st);
+  if (e == cudaSuccess) {
+    ptrs.push_back(p);
+    bytes += n;
+    arena = (unsigned char*)p;
+    arena_cap = n;
+    arena_used = 0;
+  }
+  return e;
+}
+
 cudaError_t SlotMemory::alloc(void** p, size_t n) {
   n = std::max<size_t>(n, 16);
+  const size_t need = (n + 255) & ~size_t(255);
+  if (arena && arena_used + need <= arena_cap) {
+    *p = arena + arena_used;
+    arena_used += need;
+    return cudaSuccess;
+  }
   cudaError_t e = pool ? cudaMallocFromPoolAsync(p, n, pool, st) : cudaMallocAsync(p, n, st);
   if (e == cudaSuccess) {
     ptrs.push_back(*p);
@@ -25,6 +45,8 @@ void SlotMemory::release() {
   for (void* p : ptrs) cudaFreeAsync(p, st);
   ptrs.clear();
   bytes = 0;
+  arena = nullptr;
+  arena_cap = arena_used = 0;
 }
 
 void* Staging::take(size_t n) {
@@ -105,13 +127,26 @@ int build_slot(const HostSystem& h, int slot, const int seed[4], SlotMemory& mem
   unsigned char* d = nullptr;
   const int nv = h.nvox[0] * h.nvox[1] * h.nvox[2];
   if (vox_cap <= 0) vox_cap = slot_voxel_capacity(h);
+  const bool prefilter = voxel_prefilter_applies(h.cell, h.nvox) && h.nf > 0;
+  v.K = h.K;
+  for (int a = 0; a < 3; a++) v.kmax[a] = h.deck.kmax[a];
   int* counts = nullptr;
+  unsigned* code = nullptr;
   int* off = nullptr;
   double4* xyzq = nullptr;
   unsigned char* vt = nullptr;
   double2* skfw = nullptr;
   double* scratch = nullptr;
   double* parts = nullptr;
+  {
+    // every buffer of the slot, set-up scratch included, from one pool allocation
+    const size_t arena = total + al(sizeof(int) * nv) + (prefilter ? al(sizeof(unsigned) * h.nf) : 0) +
+                         al(sizeof(int) * (nv + 1)) + al(sizeof(double4) * vox_cap) + al(vox_cap) +
+                         al(sizeof(double2) * std::max(h.K, 1)) +
+                         al(sizeof(double) * std::max<size_t>(recip_scratch_doubles(v, h.nf), 1)) +
+                         al(sizeof(double) * (recip_nparts(v) + 1)) + chain_state_bytes(h.deck, h, true) + 16 * 256;
+    if ((e = mem.reserve(arena)) != cudaSuccess) goto fail;
+  }
   if ((e = mem.alloc((void**)&d, total)) != cudaSuccess) goto fail;
   if ((e = cudaMemcpyAsync(d, hs, total, cudaMemcpyHostToDevice, st)) != cudaSuccess) goto fail;
   v.fw = (const double4*)(d + o_fw);
@@ -123,16 +158,19 @@ int build_slot(const HostSystem& h, int slot, const int seed[4], SlotMemory& mem
   v.akk = (const double*)(d + o_akk);
   for (int a = 0; a < 3; a++) v.nvox[a] = h.nvox[a];
   // voxel lists: count, device prefix sum, fill up to the capacity
-  if ((e = cudaMallocFromPoolAsync((void**)&counts, sizeof(int) * nv, mem.pool, st)) != cudaSuccess) goto fail;
+  if ((e = mem.alloc((void**)&counts, sizeof(int) * nv)) != cudaSuccess) goto fail;
   if ((e = mem.alloc((void**)&off, sizeof(int) * (nv + 1))) != cudaSuccess) goto fail;
   if ((e = mem.alloc((void**)&xyzq, sizeof(double4) * vox_cap)) != cudaSuccess) goto fail;
   if ((e = mem.alloc((void**)&vt, vox_cap)) != cudaSuccess) goto fail;
-  e = launch_voxel_count(h.cell, h.nvox, v.fw, h.nf, h.vox_lim2, counts, st);
+  if (prefilter) {
+    if ((e = mem.alloc((void**)&code, sizeof(unsigned) * h.nf)) != cudaSuccess) goto fail;
+    e = launch_voxel_codes(h.cell, h.nvox, v.fw, h.nf, code, st);
+  }
+  if (e == cudaSuccess) e = launch_voxel_count(h.cell, h.nvox, v.fw, h.nf, h.vox_lim2, code, counts, st);
   if (e == cudaSuccess) e = launch_exclusive_scan(counts, nv, off, st);
-  if (e == cudaSuccess) cudaFreeAsync(counts, st);
   if (e == cudaSuccess)
-    e = launch_voxel_fill(h.cell, h.nvox, v.fw, v.fw_type, h.nf, h.vox_lim2, off, nullptr, nullptr, xyzq, vt, vox_cap,
-                          st);
+    e = launch_voxel_fill(h.cell, h.nvox, v.fw, v.fw_type, h.nf, h.vox_lim2, code, off, nullptr, nullptr, xyzq, vt,
+                          vox_cap, st);
   if (e == cudaSuccess) e = cudaMemcpyAsync(vox_total, off + nv, sizeof(int), cudaMemcpyDeviceToHost, st);
   if (e != cudaSuccess) goto fail;
   v.vox_off = off;
@@ -143,18 +181,12 @@ int build_slot(const HostSystem& h, int slot, const int seed[4], SlotMemory& mem
   v.rdr_v = 1.0 / h.dlrpot;
   v.tab_stride = h.mxgrid + 1;
   v.ntypes = h.ntypes;
-  v.K = h.K;
-  for (int a = 0; a < 3; a++) v.kmax[a] = h.deck.kmax[a];
   v.recip_pref = h.recip_pref;
-  // framework S(k); the scratch goes back to the pool once the kernels have run
+  // framework S(k)
   if ((e = mem.alloc((void**)&skfw, sizeof(double2) * std::max(h.K, 1))) != cudaSuccess) goto fail;
-  e = cudaMallocFromPoolAsync((void**)&scratch, sizeof(double) * std::max<size_t>(recip_scratch_doubles(v, h.nf), 1),
-                              mem.pool, st);
-  if (e == cudaSuccess)
-    e = cudaMallocFromPoolAsync((void**)&parts, sizeof(double) * (recip_nparts(v) + 1), mem.pool, st);
+  e = mem.alloc((void**)&scratch, sizeof(double) * std::max<size_t>(recip_scratch_doubles(v, h.nf), 1));
+  if (e == cudaSuccess) e = mem.alloc((void**)&parts, sizeof(double) * (recip_nparts(v) + 1));
   if (e == cudaSuccess) e = launch_recip_full(v, v.fw, h.nf, skfw, scratch, parts, st);
-  if (scratch) cudaFreeAsync(scratch, st);
-  if (parts) cudaFreeAsync(parts, st);
   if (e != cudaSuccess) goto fail;
   {
     int ts = 0;

@@ -387,6 +387,11 @@ void build_host_voxels(HostSystem& s) {
         double cx = fa * h[0] + fb * h[3] + fc * h[6];
         double cy = fa * h[1] + fb * h[4] + fc * h[7];
         double cz = fa * h[2] + fb * h[5] + fc * h[8];
+        if (s.cell.imcon == 6) {  // slab: in-plane cell, z layers from zlo
+          cx = fa * h[0] + fb * h[3];
+          cy = fa * h[1] + fb * h[4];
+          cz = s.cell.zlo + (c + 0.5) * s.cell.dz;
+        }
         int v = (a * s.nvox[1] + b) * s.nvox[2] + c;
         for (int j = 0; j < s.nf; j++)
           if (true_dist2(s.cell, cx - s.fx[j], cy - s.fy[j], cz - s.fz[j]) < s.vox_lim2) s.vox_atoms.push_back(j);

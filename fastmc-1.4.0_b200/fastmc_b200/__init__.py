@@ -8,19 +8,45 @@ loop, all evaluated on the GPU through libfastmc_b200.so.
 import ctypes
 import os
 
+# The server builds request slots on up to 8 worker streams beside its launch and admission
+# streams.  With CUDA's default of 8 hardware work queues, streams share queues and a slot
+# build can wait behind a whole batched launch queued on the same one.  32 queues (the maximum)
+# keep the streams apart; the setting takes effect only if no CUDA context exists yet.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 import numpy as np
 
 from . import _lib
 from ._lib import (DELETE, DISPLACE, INSERT, JUMP, MOVE_DTYPE, MULTIJUMP, NOOP, ROTATE, TRANSLATE, FastMCError, check,
                    dp, ip, lib)
 
-__all__ = ["Chain", "SystemDesc", "Batch", "Server", "deck_inspect", "FastMCError", "INSERT", "DELETE", "DISPLACE", "TRANSLATE", "ROTATE",
+__all__ = ["Chain", "SystemDesc", "Batch", "Server", "deck_inspect", "deck_voxels", "FastMCError", "INSERT", "DELETE", "DISPLACE", "TRANSLATE", "ROTATE",
            "MOVE_DTYPE"]
 
 _INFO_INTS = ["imcon", "kmax1", "kmax2", "kmax3", "K", "natoms", "nspecies", "ntypes", "mxgrid", "nframework",
               "moves", "nvoxels", "guest_capacity", "voxel_entries", "r14", "r15"]
 _INFO_DBLS = ["alpha", "rcut", "delr", "volm", "engunit", "temp", "beta", "drewd", "dlrpot", "spenergy", "dlpeng",
               "ewald1sum", "elrc", "energy", "statvolm", "r15"]
+
+
+def _voxel_lists(call):
+    """(nvox, off, atoms) from a two-call voxel-list entry (sizes first, then the arrays)."""
+    nvox = np.zeros(3, dtype=np.int32)
+    n = ctypes.c_longlong(0)
+    check(call(nvox, None, None, 0, n))
+    off = np.zeros(int(np.prod(nvox)) + 1, dtype=np.int32)
+    atoms = np.zeros(max(n.value, 1), dtype=np.int32)
+    check(call(nvox, off, atoms, atoms.size, n))
+    return tuple(int(v) for v in nvox), off, atoms[:n.value]
+
+
+def deck_voxels(directory, voxel_edge=2.0):
+    """The neighbour lists of a deck's framework built on the host by testing every atom against
+    every voxel centre: (nvox, CSR offsets, atom indices)."""
+    d = str(directory).encode()
+    return _voxel_lists(lambda nv, off, at, cap, n: lib().fmc_deck_voxels(
+        d, float(voxel_edge), ip(nv), None if off is None else ip(off), None if at is None else ip(at), int(cap),
+        ctypes.byref(n)))
 
 
 def deck_inspect(directory):
@@ -438,6 +464,12 @@ class Batch:
             check(lib().fmc_batch_chain_timing(self.h, c, out[c].ctypes.data_as(ctypes.POINTER(ctypes.c_longlong))))
         return out
 
+    def voxels(self, chain):
+        """The device-built neighbour lists of a chain's system: (nvox, CSR offsets, atom indices)."""
+        return _voxel_lists(lambda nv, off, at, cap, n: lib().fmc_batch_voxels(
+            self.h, int(chain), ip(nv), None if off is None else ip(off), None if at is None else ip(at), int(cap),
+            ctypes.byref(n)))
+
     def pressures(self, chain):
         ng = self._ng(chain)
         out = np.zeros(ng + 1)
@@ -555,10 +587,11 @@ class Server:
         return res
 
     def stats(self):
-        out = np.zeros(10)
+        out = np.zeros(14)
         check(lib().fmc_server_stats(self.h, dp(out)))
         return dict(zip(["admitted", "retired", "launches", "admit_ms", "launch_ms", "prep_wait_ms", "prep_ms",
-                         "workers", "moves", "last_moves"], out.tolist()))
+                         "workers", "moves", "last_moves", "prep_host_ms", "prep_device_ms", "admit_prebuilt",
+                         "admit_built"], out.tolist()))
 
     def memory(self):
         u, b = ctypes.c_longlong(0), ctypes.c_longlong(0)

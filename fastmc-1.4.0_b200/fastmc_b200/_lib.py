@@ -93,6 +93,7 @@ SIGNATURES = {
     "fmc_batch_profile": (_ci, [_vp, _ci]),
     "fmc_batch_chain_state": (_ci, [_vp, _ci, _dp]),
     "fmc_batch_chain_timing": (_ci, [_vp, _ci, ctypes.POINTER(ctypes.c_longlong)]),
+    "fmc_batch_voxels": (_ci, [_vp, _ci, _ip, _ip, _ip, ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)]),
     "fmc_batch_guest_coords": (_ci, [_vp, _ci, _ci, _dp, _ip, _ip]),
     "fmc_revive_write_state": (_ci, [ctypes.c_char_p, ctypes.c_char_p, _ci, _ip, _dp, _dp, _dp, ctypes.c_double]),
     "fmc_revive_read": (_ci, [ctypes.c_char_p, ctypes.c_char_p, _ip, _ip, _dp, _dp, _dp, _ip]),
@@ -131,6 +132,8 @@ SIGNATURES = {
     "fmc_server_memory": (_ci, [_vp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
     "fmc_deck_vdw": (_ci, [ctypes.c_char_p, _ci, _dp, _ip]),
     "fmc_deck_inspect": (_ci, [ctypes.c_char_p, _ip, _dp, _ip, _dp, _dp, _dp, _ip, _ip]),
+    "fmc_deck_voxels": (_ci, [ctypes.c_char_p, ctypes.c_double, _ip, _ip, _ip, ctypes.c_longlong,
+                              ctypes.POINTER(ctypes.c_longlong)]),
 }
 
 _lib = None

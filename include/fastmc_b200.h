@@ -292,6 +292,11 @@ int fmc_batch_chain_state(fmc_batch* b, int chain, double* out);
  * run (two clock reads per CTA); 0 for a chain that has not run. */
 int fmc_batch_chain_timing(fmc_batch* b, int chain, long long* out);
 int fmc_batch_guest_coords(fmc_batch* b, int chain, int iguest, double* xyz, int* nmol, int* nsite);
+/* The neighbour lists of a chain's system as the device built them (guestlistgen's candidate
+ * sets, utility_pack.f:3113-3177, precomputed per voxel): nvox[0..2], off[nvox+1] (CSR
+ * offsets; NULL to skip), atoms[cap] (0-based framework atom indices, ascending in each voxel;
+ * NULL to skip), *n_entries. */
+int fmc_batch_voxels(fmc_batch* b, int chain, int* nvox, int* off, int* atoms, long long cap, long long* n_entries);
 /* Checkpoint / restart of one chain of a batch (formats as fmc_chain_write_revive).  A restart
  * before the chain's first run matches the reference's restart, which re-seeds duni. */
 int fmc_batch_write_revive(fmc_batch* b, int chain, const char* outdir);
@@ -351,11 +356,14 @@ int fmc_server_poll_done(fmc_server* s, int* ids, int* states, double* results, 
  * species-1 <N>,<E>,<EN>,<N^2>,<E^2>, gcmccount, 0. */
 int fmc_server_poll(fmc_server* s, int request_id, int* state, double* out);
 int fmc_server_memory(fmc_server* s, long long* used, long long* budget);
-/* out[0..9]: requests admitted, retired, launches, host ms spent admitting (device set-up of
+/* out[0..13]: requests admitted, retired, launches, host ms spent admitting (device set-up of
  * new slots, incl. waits), device ms of the launches, ms waited for host preparation with
- * nothing running, worker ms preparing decks (summed over threads), worker threads, trial
- * moves run in all launches, trial moves run in the last step's launch.  Deck parsing and
- * host tables run on worker threads ahead of admission. */
+ * nothing running, worker ms preparing requests (summed over threads), worker threads, trial
+ * moves run in all launches, trial moves run in the last step's launch, worker ms parsing
+ * decks and building host tables, worker ms enqueueing device slots ahead (the builds run on
+ * the workers' streams without the workers waiting), admissions that installed a slot built
+ * ahead, admissions built at admission.  Deck parsing and host tables run on worker threads
+ * ahead of admission. */
 int fmc_server_stats(fmc_server* s, double* out);
 
 /* Launch accounting and timing of the plain path.  enable != 0 turns on CUDA-event timing of
@@ -396,6 +404,10 @@ int fmc_ewald1_guest_noalloc(int K, const int* kmax, const double* cell, const i
 int fmc_deck_vdw(const char* dir, int k, double* out, int* ntables);
 int fmc_deck_inspect(const char* dir, int* ints, double* dbls, int* lmn, double* akk, double* erc, double* charges,
                      int* K, int* nerc);
+/* Host only: the same lists as fmc_batch_voxels, built on the host by testing every framework
+ * atom against every voxel centre (voxel_edge <= 0: 2 A). */
+int fmc_deck_voxels(const char* dir, double voxel_edge, int* nvox, int* off, int* atoms, long long cap,
+                    long long* n_entries);
 
 #ifdef __cplusplus
 }

@@ -119,3 +119,16 @@ def test_dblstr_semantics_through_ewald_line(fmc, oracle_mod, decks, tmp_path):
     assert (info["kmax1"], info["kmax2"], info["kmax3"]) == (i["kmax1"], i["kmax2"], i["kmax3"])
     assert info["alpha"] == orc.scalars()["alpha"]
     assert info["K"] == i["newld"]
+
+
+def test_host_voxel_lists_are_ascending_and_complete(fmc, decks):
+    """fmc_deck_voxels (the host's every-atom test): CSR offsets, ascending atom indices per voxel,
+    and every atom in the list of the voxel that holds it."""
+    nvox, off, atoms = fmc.deck_voxels(decks["ortho0"], 2.0)
+    info = fmc.deck_inspect(decks["ortho0"])
+    assert off[0] == 0 and off[-1] == atoms.size and np.all(np.diff(off) >= 0)
+    assert atoms.min() >= 0 and atoms.max() < info["nframework"]
+    for v in range(0, int(np.prod(nvox)), 37):
+        seg = atoms[off[v]:off[v + 1]]
+        assert np.all(np.diff(seg) > 0)
+    assert len(np.unique(atoms)) == info["nframework"]
