@@ -155,6 +155,7 @@ int fmc_ewald1_guest(fmc_chain* c, int iguest, int natms, const double* xyz, int
     A.q[w] = G.charge[i];
     A.type[w] = (unsigned char)G.type[i];
   }
+  C.take_pending(A);  // an update left by fmc_commit is read through and written by this pass
   cudaError_t e = fmc::launch_pass(C.dsys.view, C.guest_view(), A, C.sk, C.sk_new, C.W, C.st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(C.st);  // the kernel wrote the result to pinned memory
   if (e != cudaSuccess) return fail(-100 - (int)e, cudaGetErrorString(e));
@@ -190,6 +191,7 @@ int fmc_guest_realspace(fmc_chain* c, int iguest, int natms, const double* xyz, 
     A.q[i] = G.charge[i];
     A.type[i] = (unsigned char)G.type[i];
   }
+  C.take_pending(A);  // an update left by fmc_commit is read through and written by this pass
   cudaError_t e = fmc::launch_pass(C.dsys.view, C.guest_view(), A, C.sk, C.sk_new, C.W, C.st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(C.st);  // the kernel wrote the result to pinned memory
   if (e != cudaSuccess) return fail(-100 - (int)e, cudaGetErrorString(e));

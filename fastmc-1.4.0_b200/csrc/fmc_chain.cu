@@ -243,6 +243,8 @@ int Chain::open_prepared(HostSystem&& prepared, const int seed[4], int dev, std:
   FMC_CUDA(cudaMalloc(&sk_save, sizeof(double2) * std::max(K, 1)));
   FMC_CUDA(cudaMalloc(&gsite, sizeof(double4) * std::max(gcap, 1)));
   FMC_CUDA(cudaMalloc(&gtype, sizeof(int) * std::max(gcap, 1)));
+  W.gsite = gsite;
+  W.gtype = gtype;
   FMC_CUDA(cudaMalloc(&W.recip_part, sizeof(double) * (pass_recip_blocks(dsys.view) + 1)));
   FMC_CUDA(cudaMalloc(&W.site_e, sizeof(double) * 2 * kMaxPassSites));
   FMC_CUDA(cudaMalloc(&W.counter, sizeof(unsigned)));
@@ -300,6 +302,7 @@ int Chain::open_prepared(HostSystem&& prepared, const int seed[4], int dev, std:
 int Chain::set_guests(int g, int nmol, const double* xyz) {
   Species& s = sp[g];
   if (nmol * s.nsite > s.cap_sites) return -75;
+  if (int rc = flush_commit()) return rc;
   s.nmol = nmol;
   s.xyz.assign(xyz, xyz + 3 * nmol * s.nsite);
   const GuestSpecies& G = sys.deck.guests[g];
@@ -380,6 +383,7 @@ int Chain::restart(const Revive& r, std::string& err) {
 
 // S(k) over all current atoms: guests in species order, then the framework (condense order).
 int Chain::full_recip(double* e_out) {
+  if (int rc = flush_commit()) return rc;
   int n = 0;
   cudaError_t e = cudaSuccess;
   for (auto& s : sp) {
@@ -410,6 +414,7 @@ int Chain::full_recip(double* e_out) {
 // real-space energies (guest-framework once, guest-guest halved), the intramolecular
 // correction and the tail correction.
 int Chain::single_point() {
+  if (int rc = flush_commit()) return rc;
   // framework only
   cudaError_t e = launch_recip_full(dsys.view, dsys.view.fw, sys.nf, sk, recip_scratch, recip_parts, st);
   std::vector<double> parts(recip_nparts(dsys.view));
@@ -541,6 +546,7 @@ int Chain::pass(int move, int g, int mol, const double* old_xyz, const double* n
   if (profile) cudaEventRecord(ev0, st);
   pass_seq += 1.0;
   A.seq = pass_seq;
+  take_pending(A);
   cudaError_t e = launch_pass(dsys.view, guest_view(), A, sk, sk_new, W, st);
   if (profile) cudaEventRecord(ev1, st);
   if (e == cudaSuccess && !profile) {
@@ -571,31 +577,78 @@ int Chain::pass(int move, int g, int mol, const double* old_xyz, const double* n
   return 0;
 }
 
+void Chain::take_pending(PassArgs& A) {
+  if (pend_live) {
+    A.pc = pend;
+    pend_live = false;
+  } else {
+    A.pc.op = 0;
+    A.pc.seg = -1;
+  }
+}
+
+int Chain::flush_commit() {
+  if (!pend_live) return 0;
+  pend_live = false;
+  CommitArgs C;
+  std::memset(&C, 0, sizeof(C));
+  C.op = pend.op;
+  C.lo = pend.lo;
+  C.ns = pend.ns;
+  C.seg_end = pend.seg_end;
+  for (int i = 0; i < pend.ns && pend.op != kDelete; i++) {
+    C.x[i] = pend.site[i].x;
+    C.y[i] = pend.site[i].y;
+    C.z[i] = pend.site[i].z;
+    C.q[i] = pend.site[i].w;
+    C.type[i] = pend.type[i];
+  }
+  cudaError_t e = launch_commit(0, sk, sk_new, C, gsite, gtype, st);  // guest sites only
+  if (e != cudaSuccess) return sync_error(e);
+  commits++;
+  return 0;
+}
+
 int Chain::commit(int move, int g, int mol, const double* new_xyz) {
   Species& s = sp[g];
   const GuestSpecies& G = sys.deck.guests[g];
-  CommitArgs C;
-  std::memset(&C, 0, sizeof(C));
-  C.op = move;
-  C.ns = s.nsite;
-  if (move == kInsert) {
-    if ((s.nmol + 1) * s.nsite > s.cap_sites) return -75;
-    C.lo = s.seg_off + s.nmol * s.nsite;
-  } else {
-    C.lo = s.seg_off + mol * s.nsite;
-  }
-  C.seg_end = s.seg_off + s.nmol * s.nsite;
+  if (move == kInsert && (s.nmol + 1) * s.nsite > s.cap_sites) return -75;
+  int rc = flush_commit();  // an update still pending is written first
+  if (rc) return rc;
+  std::swap(sk, sk_new);  // S_new of the pass becomes S(k); the old buffer takes the next S_new
+  PendingCommit& P = pend;
+  P.op = move;
+  P.seg = g;
+  P.ns = s.nsite;
+  P.lo = s.seg_off + (move == kInsert ? s.nmol : mol) * s.nsite;
+  P.seg_end = s.seg_off + s.nmol * s.nsite;
   if (move != kDelete)
-    for (int i = 0; i < s.nsite; i++) {
-      C.x[i] = new_xyz[3 * i];
-      C.y[i] = new_xyz[3 * i + 1];
-      C.z[i] = new_xyz[3 * i + 2];
-      C.q[i] = G.charge[i];
-      C.type[i] = G.type[i];
+    for (int i = 0; i < s.nsite && i < kMaxPendSites; i++) {
+      P.site[i] = make_double4(new_xyz[3 * i], new_xyz[3 * i + 1], new_xyz[3 * i + 2], G.charge[i]);
+      P.type[i] = G.type[i];
     }
-  cudaError_t e = launch_commit(sys.K, sk, sk_new, C, gsite, gtype, st);
-  if (e != cudaSuccess) return sync_error(e);
-  commits++;
+  pend_live = true;
+  if (s.nsite > kMaxPendSites) {
+    // too many sites to carry in the next pass's arguments: written now
+    CommitArgs C;
+    std::memset(&C, 0, sizeof(C));
+    C.op = move;
+    C.ns = s.nsite;
+    C.lo = P.lo;
+    C.seg_end = P.seg_end;
+    if (move != kDelete)
+      for (int i = 0; i < s.nsite; i++) {
+        C.x[i] = new_xyz[3 * i];
+        C.y[i] = new_xyz[3 * i + 1];
+        C.z[i] = new_xyz[3 * i + 2];
+        C.q[i] = G.charge[i];
+        C.type[i] = G.type[i];
+      }
+    pend_live = false;
+    cudaError_t e = launch_commit(0, sk, sk_new, C, gsite, gtype, st);
+    if (e != cudaSuccess) return sync_error(e);
+    commits++;
+  }
   // host mirror (framwkxxx updates of gcmc.f:966-970, 1134-1138, 1352-1357)
   int n3 = 3 * s.nsite;
   if (move == kInsert) {

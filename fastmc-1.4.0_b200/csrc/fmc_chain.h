@@ -102,7 +102,16 @@ class Chain {
   GuestView guest_view() const;
   // Energies of one trial pass.  old_xyz/new_xyz are interleaved xyz of the molecule's sites.
   int pass(int move, int g, int mol, const double* old_xyz, const double* new_xyz, double out[3]);
+  // An accepted move: S(k) <- S_new by exchanging the two buffers, and the guest-site update
+  // left pending for the next pass to read through and write (no launch of its own); a second
+  // update before the next pass, or one of more than kMaxPendSites sites, is written at once.
   int commit(int move, int g, int mol, const double* new_xyz);
+  // Hands the pending guest-site update to a pass about to launch (or marks none).
+  void take_pending(PassArgs& A);
+  // Writes the pending guest-site update now (before anything else reads the device sites).
+  int flush_commit();
+  PendingCommit pend{};
+  bool pend_live = false;
   int full_recip(double* e_recip_plus_self);  // S(k) over all current atoms (ewald1)
   int single_point();
   int step(MoveRecord* rec);

@@ -127,19 +127,49 @@ __device__ __forceinline__ int voxel_of(const DevSystem& S, double x, double y, 
   return (v[0] * S.nvox[1] + v[1]) * S.nvox[2] + v[2];
 }
 
+// A guest-site update accepted on the host and not yet written to the device arrays (an
+// insert appends a molecule to its species' segment, a delete removes one and shifts the rest
+// down, a displacement overwrites one).  The next trial pass reads the guest sites as if the
+// update were written (GuestView indices are those after it) and writes it once every block of
+// that pass has read them.
+constexpr int kMaxPendSites = 8;
+struct PendingCommit {
+  int op;       // 0: none; kInsert, kDelete, kDisplace
+  int seg;      // species segment index (-1: none)
+  int lo;       // first site of the molecule (insert: the segment's end before the insert)
+  int ns;       // sites per molecule
+  int seg_end;  // end of the segment before the update
+  double4 site[kMaxPendSites];
+  int type[kMaxPendSites];
+};
+
 // Thread-partial real-space energy of one site against the framework (voxel list) and the
 // guest sites outside [ex_lo, ex_hi).  Threads stride by `nthr` starting at `tid`.
-__device__ __forceinline__ void site_partial(const DevSystem& S, const GuestView& G, double px, double py, double pz,
-                                             double q, int ty, int ex_lo, int ex_hi, int tid, int nthr, double& ec_fw,
-                                             double& ev_fw, double& ec_g, double& ev_g) {
+__device__ __forceinline__ void site_partial(const DevSystem& S, const GuestView& G, const PendingCommit& P, double px,
+                                             double py, double pz, double q, int ty, int ex_lo, int ex_hi, int tid,
+                                             int nthr, double& ec_fw, double& ev_fw, double& ec_g, double& ev_g) {
   const double chgea = q * kR4pie0;
   const int* prow = S.pair_row + ty * (S.ntypes + 1);
   for (int sg = 0; sg < G.nseg; sg++) {
     int lo = G.seg_off[sg], hi = lo + G.seg_len[sg];
     for (int j = lo + tid; j < hi; j += nthr) {
       if (j >= ex_lo && j < ex_hi) continue;
-      double4 a = G.site[j];
-      pair_energy(S, px - a.x, py - a.y, pz - a.z, chgea, a.w, prow[G.type[j]], ec_g, ev_g);
+      double4 a;
+      int t;
+      if (sg != P.seg || j < P.lo) {
+        a = G.site[j];
+        t = G.type[j];
+      } else if (P.op == kDelete) {  // the sites after the removed molecule, one molecule on
+        a = G.site[j + P.ns];
+        t = G.type[j + P.ns];
+      } else if (j < P.lo + P.ns) {  // the inserted or displaced molecule
+        a = P.site[j - P.lo];
+        t = P.type[j - P.lo];
+      } else {
+        a = G.site[j];
+        t = G.type[j];
+      }
+      pair_energy(S, px - a.x, py - a.y, pz - a.z, chgea, a.w, prow[t], ec_g, ev_g);
     }
   }
   int v = voxel_of(S, px, py, pz);

@@ -12,6 +12,8 @@
 // fmc_recip_*       : full S(k) of a set of atoms (ewald1, ewald.f:368-630).
 // fmc_sp_kernel     : per-guest-site real-space energies for the single-point energy.
 #include <cmath>
+#include <cstddef>
+#include <cstring>
 
 #include "fmc_device.cuh"
 #include "fmc_kernels.h"
@@ -19,9 +21,40 @@
 namespace fmc {
 
 constexpr int kPassThreads = 256;
+static_assert(2 * kMaxPassSites <= kPassThreads, "the combine stages every site energy in one pass");
+
+// A guest-site update by one block (all its threads): a delete removes [lo, lo+ns) and shifts
+// the rest of the segment down in order; an insert writes at the segment end, a displacement
+// over the molecule.
+__device__ __forceinline__ void apply_commit(const PendingCommit& P, double4* site, int* type) {
+  const int tid = threadIdx.x;
+  if (P.op == kDelete) {
+    const int ns = P.ns;
+    for (int base = P.lo; base < P.seg_end - ns; base += blockDim.x) {
+      const int i = base + tid;
+      const bool act = i < P.seg_end - ns;
+      double4 a = make_double4(0.0, 0.0, 0.0, 0.0);
+      int t = 0;
+      if (act) {
+        a = site[i + ns];
+        t = type[i + ns];
+      }
+      __syncthreads();
+      if (act) {
+        site[i] = a;
+        type[i] = t;
+      }
+      __syncthreads();
+    }
+  } else if (tid < P.ns) {
+    site[P.lo + tid] = P.site[tid];
+    type[P.lo + tid] = P.type[tid];
+  }
+}
 
 // ------------------------------------------------------------------------------ pass
-__global__ void __launch_bounds__(kPassThreads) fmc_pass_kernel(DevSystem S, GuestView G, PassArgs A,
+template <int N>
+__global__ void __launch_bounds__(kPassThreads) fmc_pass_kernel(DevSystem S, GuestView G, PassArgsT<N> A,
                                                                 const double2* __restrict__ sk, double2* sk_new,
                                                                 PassScratch W) {
   extern __shared__ double2 sm_tab[];
@@ -80,8 +113,8 @@ __global__ void __launch_bounds__(kPassThreads) fmc_pass_kernel(DevSystem S, Gue
     const int s = blockIdx.x - nbk;
     double v[2] = {0.0, 0.0};
     double ec_fw = 0.0, ev_fw = 0.0, ec_g = 0.0, ev_g = 0.0;
-    site_partial(S, G, A.x[s], A.y[s], A.z[s], A.q[s], A.type[s], A.ex_lo, A.ex_hi, tid, blockDim.x, ec_fw, ev_fw,
-                 ec_g, ev_g);
+    site_partial(S, G, A.pc, A.x[s], A.y[s], A.z[s], A.q[s], A.type[s], A.ex_lo, A.ex_hi, tid, blockDim.x, ec_fw,
+                 ev_fw, ec_g, ev_g);
     v[0] = ec_g + ec_fw;
     v[1] = ev_g + ev_fw;
     block_sum<2>(v, red);
@@ -90,22 +123,34 @@ __global__ void __launch_bounds__(kPassThreads) fmc_pass_kernel(DevSystem S, Gue
       W.site_e[2 * s + 1] = v[1];
     }
   }
-  // ---- last block combines in a fixed order
+  // ---- last block combines in a fixed order: the partials are loaded by all its threads at
+  // once and summed by thread 0 in block / site order
   if (tid == 0) {
     __threadfence();
     unsigned done = atomicAdd(W.counter, 1u);
     am_last = (done == gridDim.x - 1);
   }
   __syncthreads();
-  if (am_last && tid == 0) {
-    __threadfence();
-    double r = 0.0;
-    for (int b = 0; b < nbk; b++) r += ((volatile double*)W.recip_part)[b];
+  if (!am_last) return;
+  __shared__ double comb[kPassThreads];
+  __threadfence();
+  double r = 0.0;
+  for (int base = 0; base < nbk; base += kPassThreads) {
+    if (base + tid < nbk) comb[tid] = ((volatile double*)W.recip_part)[base + tid];
+    __syncthreads();
+    if (tid == 0)
+      for (int i = 0; i < kPassThreads && base + i < nbk; i++) r += comb[i];
+    __syncthreads();
+  }
+  const int nse = A.do_real ? 2 * nsite : 0;  // <= 2 * N <= kPassThreads
+  if (tid < nse) comb[tid] = ((volatile double*)W.site_e)[tid];
+  __syncthreads();
+  if (tid == 0) {
     double ewld1 = S.recip_pref * r;
     if (A.move == kInsert) ewld1 = ewld1 + A.engsic;
     if (A.move == kDelete) ewld1 = ewld1 - A.engsic;
     double e2 = 0.0, ev = 0.0;
-    const volatile double* se = W.site_e;
+    const double* se = comb;
     for (int s = 0; s < (A.do_real ? nsite : 0); s++) {
       if (s < A.nold && A.move == kDisplace) {
         e2 = e2 - se[2 * s];
@@ -122,6 +167,8 @@ __global__ void __launch_bounds__(kPassThreads) fmc_pass_kernel(DevSystem S, Gue
     ((volatile double*)W.result)[3] = A.seq;
     *W.counter = 0u;
   }
+  // every block has read the guest sites: the last one writes the pending update
+  if (A.pc.op) apply_commit(A.pc, W.gsite, W.gtype);
 }
 
 int pass_smem_bytes(const DevSystem& S, int nsite) {
@@ -135,13 +182,32 @@ cudaError_t launch_pass(const DevSystem& S, const GuestView& G, const PassArgs& 
   int nsite = A.nold + A.nnew;
   int smem = A.nbk > 0 ? pass_smem_bytes(S, nsite) : 0;
   int grid = A.nbk + (A.do_real ? nsite : 0);
-  if (grid == 0) return cudaSuccess;
-  fmc_pass_kernel<<<grid, kPassThreads, smem, st>>>(S, G, A, sk, sk_new, W);
+  if (grid == 0) return A.pc.op ? cudaErrorInvalidValue : cudaSuccess;  // a pending update needs a block
+  if (nsite <= kSmallPassSites) {
+    // the common case (molecules of up to 8 sites): a parameter block of ~1.3 KB instead of ~4 KB
+    PassArgsT<kSmallPassSites> B;
+    std::memcpy(&B, &A, offsetof(PassArgs, x));
+    for (int i = 0; i < nsite; i++) {
+      B.x[i] = A.x[i];
+      B.y[i] = A.y[i];
+      B.z[i] = A.z[i];
+      B.q[i] = A.q[i];
+      B.type[i] = A.type[i];
+    }
+    B.pc = A.pc;
+    fmc_pass_kernel<kSmallPassSites><<<grid, kPassThreads, smem, st>>>(S, G, B, sk, sk_new, W);
+  } else {
+    fmc_pass_kernel<kMaxPassSites><<<grid, kPassThreads, smem, st>>>(S, G, A, sk, sk_new, W);
+  }
   return cudaGetLastError();
 }
 
 cudaError_t configure_kernels() {
-  return cudaFuncSetAttribute(fmc_pass_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaError_t e = cudaFuncSetAttribute(fmc_pass_kernel<kSmallPassSites>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       200 * 1024);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(fmc_pass_kernel<kMaxPassSites>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  return e;
 }
 
 
@@ -298,7 +364,12 @@ __global__ void fmc_sp_kernel(DevSystem S, GuestView G, const int* __restrict__ 
   const int b = blockIdx.x, i = sites[b];
   double4 a = G.site[i];
   double v[4] = {0.0, 0.0, 0.0, 0.0};
-  site_partial(S, G, a.x, a.y, a.z, a.w, G.type[i], lo[b], hi[b], threadIdx.x, blockDim.x, v[0], v[1], v[2], v[3]);
+  PendingCommit none;
+  none.op = 0;
+  none.seg = -1;
+  none.lo = none.ns = none.seg_end = 0;
+  site_partial(S, G, none, a.x, a.y, a.z, a.w, G.type[i], lo[b], hi[b], threadIdx.x, blockDim.x, v[0], v[1], v[2],
+               v[3]);
   block_sum<4>(v, red);
   if (threadIdx.x == 0)
     for (int k = 0; k < 4; k++) out[4 * b + k] = v[k];

@@ -9,7 +9,11 @@ namespace fmc {
 // One trial pass: the sites whose reciprocal and real-space contributions change.
 // Sites [0, nold) are the molecule's current positions (removed), sites [nold, nold+nnew)
 // the trial positions (added).  insert: nold=0; delete: nnew=0; displace: both, fused.
-struct PassArgs {
+// Arguments of one trial pass for up to N old + new sites.  The kernel is built for N = 16
+// (molecules of up to 8 sites, launched with a small parameter block) and for the reference's
+// largest molecules (kMaxPassSites); launch_pass picks the smaller one that holds the trial.
+template <int N>
+struct PassArgsT {
   int move;           // kInsert / kDelete / kDisplace
   int nbk;            // reciprocal blocks (0: skip the reciprocal part)
   int do_real;        // 1: one real-space block per site
@@ -17,9 +21,12 @@ struct PassArgs {
   int ex_lo, ex_hi;   // guest-site range of the moving molecule (excluded from real space)
   double engsic;      // self-interaction term of the species (ewald.f:87-93)
   double seq;         // copied to result[3] after the energies, for a host that polls (0: none)
-  double x[kMaxPassSites], y[kMaxPassSites], z[kMaxPassSites], q[kMaxPassSites];
-  unsigned char type[kMaxPassSites];
+  double x[N], y[N], z[N], q[N];
+  unsigned char type[N];
+  PendingCommit pc;   // an accepted guest-site update this pass reads through and then writes
 };
+constexpr int kSmallPassSites = 16;
+using PassArgs = PassArgsT<kMaxPassSites>;
 
 // Scratch of one pass launch (global memory beyond inputs and outputs).
 struct PassScratch {
@@ -27,6 +34,8 @@ struct PassScratch {
   double* site_e;      // [2*kMaxPassSites]
   unsigned* counter;   // last-block ticket, left at zero by the kernel
   double* result;      // {ewld1, ewld2, vdw, seq} in pinned host memory, written by the kernel directly
+  double4* gsite;      // the chain's guest sites and types, written by the last block when the
+  int* gtype;          // pass carries a pending update (PassArgs::pc)
 };
 
 struct CommitArgs {
