@@ -51,6 +51,8 @@ def parse():
                     help="batched: the first N of the 256 chains (framework-major), for reduced profiling cases")
     ap.add_argument("--voxel-edge", type=float, default=0.0,
                     help="batched: neighbour-list voxel edge in A (0: picked by the autotuner)")
+    ap.add_argument("--tile", type=int, default=-1,
+                    help="batched: index into the kernel's tile shapes (-1: picked by the autotuner)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="bounded CPU baseline sample")
     ap.add_argument("--skip-baselines", action="store_true",
                     help="omit the plain-path and CPU samples (profiling runs of the batched kernel)")
@@ -359,7 +361,15 @@ def run_batched(args, dist):
     edge = args.voxel_edge
     if edge <= 0:
         edge, tune = fm.autotune_voxel_edge(dirs, seeds, device=dist.local)
+    # tile shape (threads per chain, k-vectors and candidates per loop trip): timed on one more
+    # throwaway batch at that edge, each tile twice in palindromic order
+    tiles = fm.batch_tiles()
+    tile, tile_tune = args.tile, None
+    if tile < 0:
+        tile, tile_tune = fm.autotune_tiles(dirs, seeds, device=dist.local, voxel_edge=edge, warm_moves=args.moves,
+                                            moves=args.moves // 2)
     b = fm.Batch(dirs, seeds, device=dist.local, voxel_edge=edge)
+    b.tile = tile
     setup_s = time.perf_counter() - t0
     infos = {}
     for d in dirs:
@@ -424,6 +434,10 @@ def run_batched(args, dist):
                    "K_range": [int(min(i["K"] for i in infos.values())), int(max(i["K"] for i in infos.values()))],
                    "setup_s": setup_s, "voxel_edge_A": edge, "load_balance": balance,
                    "voxel_autotune_ms": tune,
+                   "tile": {"index": tile, "threads_per_chain": tiles[tile][0], "kvec_per_trip": tiles[tile][1],
+                            "cand_per_trip": tiles[tile][2], "chains_per_cta": 1},
+                   "tile_autotune_ms": ({f"{tiles[k][0]}/{tiles[k][1]}/{tiles[k][2]}": v for k, v in tile_tune.items()}
+                                        if tile_tune else None),
                    "l2": "per-chain S(k) is shared-memory resident; frameworks + voxel lists exceed L2 (no flush)",
                    "parallelism": f"replicas{dist.world}"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,

@@ -682,32 +682,73 @@ __device__ __noinline__ void build_trial(ChainDev& C, const SysConst& Y, const D
 // Real-space sums of one pass: every (site, candidate) pair, compiled per boundary condition so
 // the hot loop holds one minimum-image form.  Deeper unrolling (2-8 candidates per trip) was
 // measured slower: the larger loop costs more in instruction fetch than it hides in latency.
-template <int kImcon>
+template <int kImcon, int NT, int CPT>
 __device__ __noinline__ void real_space(const DevSystem& S, const ChainDev& C, const MoveSmem& M, int nseg,
                                         const int* prow_s, int nt1, double* vout) {
   const int tid = threadIdx.x, nsite = M.nold + M.nnew, nold = M.nold, mtype = M.mtype;
   double v1 = vout[1], v2 = vout[2];
   const bool sub_old = (mtype != kInsert && mtype != kDelete);
   const int T = M.pre[nsite];
-  // a thread takes candidates tid, tid + 256, tid + 512, ... in that order
-  // one candidate per loop trip, the next one's loads issued before this one is evaluated
-  int s_next = 0;
-  Cand pre = fetch_candidate(S, C, M, nseg, tid, s_next);
-  for (int base = tid; base < T; base += kBatchThreads) {
-    const Cand c = pre;
-    pre = fetch_candidate(S, C, M, nseg, base + kBatchThreads, s_next);
-    if (!c.live) continue;
-    const int st = c.site;
-    const int row = prow_s[M.type[st] * nt1 + c.type];
-    double ec = 0.0, ev = 0.0;
-    pair_energy<kImcon>(S, M.x[st] - c.a.x, M.y[st] - c.a.y, M.z[st] - c.a.z, M.q[st] * kR4pie0, c.a.w, row, ec,
-                        ev);
-    if (sub_old && st < nold) {
-      v1 -= ec;
-      v2 -= ev;
-    } else {
-      v1 += ec;
-      v2 += ev;
+  // a thread takes candidates tid, tid + NT, tid + 2 NT, ... and adds them in that order;
+  // CPT candidates per loop trip, the next trip's loads issued before this one is evaluated
+  // (the pair's accumulation is written out in each loop: passing the candidate to a helper
+  // made ptxas spill in this loop)
+  if (CPT == 1) {
+    int s_next = 0;
+    Cand pre = fetch_candidate(S, C, M, nseg, tid, s_next);
+    for (int base = tid; base < T; base += NT) {
+      const Cand c = pre;
+      pre = fetch_candidate(S, C, M, nseg, base + NT, s_next);
+      if (!c.live) continue;
+      const int st = c.site;
+      const int row = prow_s[M.type[st] * nt1 + c.type];
+      double ec = 0.0, ev = 0.0;
+      pair_energy<kImcon>(S, M.x[st] - c.a.x, M.y[st] - c.a.y, M.z[st] - c.a.z, M.q[st] * kR4pie0, c.a.w, row, ec,
+                          ev);
+      if (sub_old && st < nold) {
+        v1 -= ec;
+        v2 -= ev;
+      } else {
+        v1 += ec;
+        v2 += ev;
+      }
+    }
+  } else {
+    int s0 = 0, s1 = 0;
+    Cand p0 = fetch_candidate(S, C, M, nseg, tid, s0);
+    Cand p1 = fetch_candidate(S, C, M, nseg, tid + NT, s1);
+    for (int base = tid; base < T; base += 2 * NT) {
+      const Cand c0 = p0, c1 = p1;
+      p0 = fetch_candidate(S, C, M, nseg, base + 2 * NT, s0);
+      p1 = fetch_candidate(S, C, M, nseg, base + 3 * NT, s1);
+      if (c0.live) {
+        const int st = c0.site;
+        const int row = prow_s[M.type[st] * nt1 + c0.type];
+        double ec = 0.0, ev = 0.0;
+        pair_energy<kImcon>(S, M.x[st] - c0.a.x, M.y[st] - c0.a.y, M.z[st] - c0.a.z, M.q[st] * kR4pie0, c0.a.w, row,
+                            ec, ev);
+        if (sub_old && st < nold) {
+          v1 -= ec;
+          v2 -= ev;
+        } else {
+          v1 += ec;
+          v2 += ev;
+        }
+      }
+      if (c1.live) {
+        const int st = c1.site;
+        const int row = prow_s[M.type[st] * nt1 + c1.type];
+        double ec = 0.0, ev = 0.0;
+        pair_energy<kImcon>(S, M.x[st] - c1.a.x, M.y[st] - c1.a.y, M.z[st] - c1.a.z, M.q[st] * kR4pie0, c1.a.w, row,
+                            ec, ev);
+        if (sub_old && st < nold) {
+          v1 -= ec;
+          v2 -= ev;
+        } else {
+          v1 += ec;
+          v2 += ev;
+        }
+      }
     }
   }
   vout[1] = v1;
@@ -716,48 +757,67 @@ __device__ __noinline__ void real_space(const DevSystem& S, const ChainDev& C, c
 
 // All threads: this thread's share of the reciprocal sum (v[0] = sum akk*d|S|^2) and of the
 // real-space pairs (v[1] ewld2, v[2] vdw); S_new goes to Sn.
+// One k-vector's change: S_new(k) from S(k) and the trial sites' phases; returns
+// akk (|S_new|^2 - |S_old|^2).
+__device__ __forceinline__ double recip_term(int k, const MoveSmem& M, const int* kp, const double* ak,
+                                             const double2* Sk, double2* Sn, const double2* tb, int stride, int k1,
+                                             int k2) {
+  const int nsite = M.nold + M.nnew, nold = M.nold, mtype = M.mtype;
+  int l, m, n;
+  kunpack(kp[k], l, m, n);
+  int am = m < 0 ? -m : m, an = n < 0 ? -n : n;
+  double2 so = Sk[k], sn;
+  double2 aold = make_double2(0.0, 0.0), anew = make_double2(0.0, 0.0);
+  for (int st = 0; st < nsite; st++) {
+    const double2* t = tb + st * stride;
+    double2 c = m >= 0 ? cmul(t[l], t[k1 + 1 + am]) : cmulc(t[l], t[k1 + 1 + am]);
+    c = n >= 0 ? cmul(c, t[k1 + k2 + 2 + an]) : cmulc(c, t[k1 + k2 + 2 + an]);
+    double q = M.q[st];
+    if (st < nold) {
+      aold.x += q * c.x;
+      aold.y += q * c.y;
+    } else {
+      anew.x += q * c.x;
+      anew.y += q * c.y;
+    }
+  }
+  if (mtype == kInsert)
+    sn = make_double2(anew.x + so.x, anew.y + so.y);
+  else if (mtype == kDelete)
+    sn = make_double2(so.x - aold.x, so.y - aold.y);
+  else
+    sn = make_double2((so.x - aold.x) + anew.x, (so.y - aold.y) + anew.y);
+  Sn[k] = sn;
+  return ak[k] * (sn.x * sn.x + sn.y * sn.y - so.x * so.x - so.y * so.y);
+}
+
+// All threads: this thread's share of the reciprocal sum (v[0] = sum akk*d|S|^2) and of the
+// real-space pairs (v[1] ewld2, v[2] vdw); S_new goes to Sn.  A thread takes k-vectors tid,
+// tid + NT, ... and adds their terms in that order, KPT of them per trip.
+template <int NT, int KPT, int CPT>
 __device__ __noinline__ void sums(const DevSystem& S, const ChainDev& C, const MoveSmem& M, int nseg, const int* prow_s,
                                   int nt1, const int* kp, const double* ak, const double2* Sk, double2* Sn,
                                   const void* tabv, int stride, double* v) {
   const int tid = threadIdx.x, K = S.K, k1 = S.kmax[0], k2 = S.kmax[1];
-  const int nsite = M.nold + M.nnew, nold = M.nold, mtype = M.mtype;
   const double2* tb = reinterpret_cast<const double2*>(tabv);
-  for (int k = tid; k < K; k += blockDim.x) {
-    int l, m, n;
-    kunpack(kp[k], l, m, n);
-    int am = m < 0 ? -m : m, an = n < 0 ? -n : n;
-    double2 so = Sk[k], sn;
-    double2 aold = make_double2(0.0, 0.0), anew = make_double2(0.0, 0.0);
-    for (int st = 0; st < nsite; st++) {
-      const double2* t = tb + st * stride;
-      double2 c = m >= 0 ? cmul(t[l], t[k1 + 1 + am]) : cmulc(t[l], t[k1 + 1 + am]);
-      c = n >= 0 ? cmul(c, t[k1 + k2 + 2 + an]) : cmulc(c, t[k1 + k2 + 2 + an]);
-      double q = M.q[st];
-      if (st < nold) {
-        aold.x += q * c.x;
-        aold.y += q * c.y;
-      } else {
-        anew.x += q * c.x;
-        anew.y += q * c.y;
-      }
+  if (KPT == 1) {
+    for (int k = tid; k < K; k += NT) v[0] += recip_term(k, M, kp, ak, Sk, Sn, tb, stride, k1, k2);
+  } else {
+    int k = tid;
+    for (; k + NT < K; k += 2 * NT) {  // two independent k-vectors in flight, added in order
+      v[0] += recip_term(k, M, kp, ak, Sk, Sn, tb, stride, k1, k2);
+      v[0] += recip_term(k + NT, M, kp, ak, Sk, Sn, tb, stride, k1, k2);
     }
-    if (mtype == kInsert)
-      sn = make_double2(anew.x + so.x, anew.y + so.y);
-    else if (mtype == kDelete)
-      sn = make_double2(so.x - aold.x, so.y - aold.y);
-    else
-      sn = make_double2((so.x - aold.x) + anew.x, (so.y - aold.y) + anew.y);
-    v[0] += ak[k] * (sn.x * sn.x + sn.y * sn.y - so.x * so.x - so.y * so.y);
-    Sn[k] = sn;
+    if (k < K) v[0] += recip_term(k, M, kp, ak, Sk, Sn, tb, stride, k1, k2);
   }
   // real space, per boundary condition
-  if (S.cell.imcon == 1) real_space<1>(S, C, M, nseg, prow_s, nt1, v);
-  else if (S.cell.imcon == 2) real_space<2>(S, C, M, nseg, prow_s, nt1, v);
-  else if (S.cell.imcon == 3) real_space<3>(S, C, M, nseg, prow_s, nt1, v);
+  if (S.cell.imcon == 1) real_space<1, NT, CPT>(S, C, M, nseg, prow_s, nt1, v);
+  else if (S.cell.imcon == 2) real_space<2, NT, CPT>(S, C, M, nseg, prow_s, nt1, v);
+  else if (S.cell.imcon == 3) real_space<3, NT, CPT>(S, C, M, nseg, prow_s, nt1, v);
   // the half-shift cells and the slab share one instantiation that reads the boundary condition
   // from the cell: each compiled copy of this loop costs instruction cache (one per cell kind
   // cost 8%)
-  else real_space<-1>(S, C, M, nseg, prow_s, nt1, v);
+  else real_space<-1, NT, CPT>(S, C, M, nseg, prow_s, nt1, v);
 }
 
 // All threads, in production: storeprob (utility_pack.f:496-561) for the chain's state after the
@@ -801,8 +861,9 @@ __device__ __noinline__ void prob_store(const SysConst& Y, const ChainDev& C) {
   }
 }
 
-template <bool kProf>
-__global__ void __launch_bounds__(kBatchThreads, 2) fmc_batch_kernel(BatchLaunch L, int tab_stride) {
+template <bool kProf, int NT, int KPT, int CPT>
+__global__ void __launch_bounds__(NT, NT <= 128 ? 4 : (NT <= 256 ? 2 : 1)) fmc_batch_kernel(BatchLaunch L,
+                                                                                           int tab_stride) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ ChainDev C;
   __shared__ MoveSmem M;
@@ -873,7 +934,7 @@ __global__ void __launch_bounds__(kBatchThreads, 2) fmc_batch_kernel(BatchLaunch
     if (C.status) break;
     const bool last = !C.lgchk;  // lane 0 of warp 0 writes lgchk only in select_move
     double v[3] = {0.0, 0.0, 0.0};
-    sums(S, C, M, nseg, prow_s, nt1, kp, ak, Sk, Sn, tab, stride, v);
+    sums<NT, KPT, CPT>(S, C, M, nseg, prow_s, nt1, kp, ak, Sk, Sn, tab, stride, v);
     if (prof && tid == 0) C.prof[6] += clock64() - t0;
     block_sum<3>(v, red);
     if (prof && tid == 0) {
@@ -963,19 +1024,28 @@ int batch_smem_bytes(int kmax_K, int tab_sites, int tab_stride) {
          tab_sites * tab_stride * (int)sizeof(double2);
 }
 
+namespace {
+using BatchKernel = void (*)(BatchLaunch, int);
+// the kernel of each tile of kBatchTiles, in the same order
+constexpr BatchKernel kTileKernels[kNumBatchTiles] = {
+    fmc_batch_kernel<false, 256, 1, 1>, fmc_batch_kernel<false, 256, 2, 1>, fmc_batch_kernel<false, 256, 1, 2>,
+    fmc_batch_kernel<false, 256, 2, 2>, fmc_batch_kernel<false, 128, 1, 1>, fmc_batch_kernel<false, 128, 2, 1>,
+    fmc_batch_kernel<false, 128, 1, 2>, fmc_batch_kernel<false, 128, 2, 2>, fmc_batch_kernel<false, 384, 1, 1>,
+    fmc_batch_kernel<false, 384, 2, 1>, fmc_batch_kernel<false, 384, 1, 2>, fmc_batch_kernel<false, 384, 2, 2>};
+constexpr BatchKernel kProfKernel = fmc_batch_kernel<true, 256, 1, 1>;
+}  // namespace
+
 cudaError_t configure_batch_kernel(int smem_bytes) {
-  cudaError_t e = cudaFuncSetAttribute(fmc_batch_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       smem_bytes);
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(fmc_batch_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
+  cudaError_t e = cudaFuncSetAttribute(kProfKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
+  for (int t = 0; t < kNumBatchTiles && e == cudaSuccess; t++)
+    e = cudaFuncSetAttribute(kTileKernels[t], cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
   return e;
 }
 
 cudaError_t launch_batch(const BatchLaunch& L, int smem_bytes, int tab_stride, cudaStream_t st) {
-  if (L.profile)
-    fmc_batch_kernel<true><<<L.nchains, kBatchThreads, smem_bytes, st>>>(L, tab_stride);
-  else
-    fmc_batch_kernel<false><<<L.nchains, kBatchThreads, smem_bytes, st>>>(L, tab_stride);
+  if (L.tile < 0 || L.tile >= kNumBatchTiles || (L.profile && L.tile != 0)) return cudaErrorInvalidValue;
+  const BatchKernel k = L.profile ? kProfKernel : kTileKernels[L.tile];
+  k<<<L.nchains, kBatchTiles[L.tile].threads, smem_bytes, st>>>(L, tab_stride);
   return cudaGetLastError();
 }
 

@@ -17,6 +17,20 @@ constexpr int kBatchMaxSites = 16;  // sites per guest species on the batched pa
 constexpr int kBatchMaxTypes = 16;  // unique atom types
 constexpr int kBatchMaxTab = kBatchMaxTypes * (kBatchMaxTypes + 1) / 2;
 constexpr int kBatchThreads = 256;
+
+// Tile shapes of the batched kernel the autotuner chooses among: threads per chain (CTA size),
+// k-vectors each thread takes per trip of the reciprocal loop (ewald.f:145-331) and neighbour
+// candidates per trip of the real-space loop (ewald.f:656-690, vdw_terms.f:455-495).  Tile 0
+// is the default.  Within one thread-count the tiles give bit-identical results (each thread
+// sums its k-vectors and candidates in the same order); another thread count sums in another
+// order.  One chain per CTA throughout: two chains share an SM as two CTAs.
+struct BatchTile {
+  int threads, kvec_per_trip, cand_per_trip;
+};
+constexpr int kNumBatchTiles = 12;
+constexpr BatchTile kBatchTiles[kNumBatchTiles] = {
+    {256, 1, 1}, {256, 2, 1}, {256, 1, 2}, {256, 2, 2}, {128, 1, 1}, {128, 2, 1},
+    {128, 1, 2}, {128, 2, 2}, {384, 1, 1}, {384, 2, 1}, {384, 1, 2}, {384, 2, 2}};
 constexpr int kMaxPlots = 8;      // probability plots per system
 constexpr int kMaxPlotSites = 8;  // sites per plot (0 = centre of mass)
 
@@ -98,6 +112,7 @@ struct BatchLaunch {
   long long* timing;  // optional [nchains][3] per chain: its CTA's start and end (%globaltimer, ns), its SM
   int retire_finished;  // a chain that ends its budget, its deck's cycles or on an error marks itself
                         // inactive, so that a launch queued behind this one skips it (serving)
+  int tile;             // index into kBatchTiles (profiling runs tile 0 only)
 };
 
 cudaError_t launch_batch(const BatchLaunch& L, int smem_bytes, int tab_stride, cudaStream_t st);
@@ -158,6 +173,7 @@ int build_slot(const HostSystem& h, int slot, const int seed[4], SlotMemory& mem
 class Batch {
  public:
   int device = 0;
+  int tile = 0;  // kBatchTiles index of the launches
   cudaStream_t st = nullptr;
   std::vector<std::unique_ptr<Chain>> sys_chains;  // one opened chain per unique system
   std::vector<int> chain_sys;

@@ -537,6 +537,7 @@ int Batch::run(int moves, MoveRecord* trace_host, float* ms, std::string& err) {
   L.trace = nullptr;
   L.timing = d_timing;
   L.order = d_order;
+  L.tile = tile;
   cudaError_t e = cudaSuccess;
   if (trace_host) {
     size_t need = (size_t)nchains * moves;
@@ -671,7 +672,72 @@ int fmc_batch_profile(fmc_batch* b, int enable) {
     fmc::set_last_error("bad batch handle");
     return -1;
   }
+  if (enable && b->impl.tile != 0) {
+    fmc::set_last_error("phase profiling is built for the default tile (0) only");
+    return -1;
+  }
   b->impl.profile = enable;
+  return 0;
+}
+
+int fmc_batch_tiles(int* threads, int* kvec_per_trip, int* cand_per_trip, int cap) {
+  for (int t = 0; t < fmc::kNumBatchTiles && t < cap; t++) {
+    if (threads) threads[t] = fmc::kBatchTiles[t].threads;
+    if (kvec_per_trip) kvec_per_trip[t] = fmc::kBatchTiles[t].kvec_per_trip;
+    if (cand_per_trip) cand_per_trip[t] = fmc::kBatchTiles[t].cand_per_trip;
+  }
+  return fmc::kNumBatchTiles;
+}
+
+int fmc_batch_set_tile(fmc_batch* b, int tile) {
+  if (!b || tile < 0 || tile >= fmc::kNumBatchTiles) {
+    fmc::set_last_error("bad batch handle or tile index");
+    return -1;
+  }
+  if (tile != 0 && b->impl.profile) {
+    fmc::set_last_error("phase profiling is built for the default tile (0) only");
+    return -1;
+  }
+  b->impl.tile = tile;
+  return 0;
+}
+
+int fmc_batch_get_tile(fmc_batch* b) { return b ? b->impl.tile : -1; }
+
+int fmc_batch_autotune_tiles(int nchains, const char* const* dirs, const int* seeds, int device, double voxel_edge,
+                             const int* tiles, int ntiles, int warm_moves, int moves, int* best_tile, float* ms) {
+  if (!dirs || !seeds || !tiles || ntiles < 1 || moves < 1 || warm_moves < 0 || !best_tile) {
+    fmc::set_last_error("bad autotune arguments");
+    return -1;
+  }
+  for (int i = 0; i < ntiles; i++)
+    if (tiles[i] < 0 || tiles[i] >= fmc::kNumBatchTiles) {
+      fmc::set_last_error("tile index out of range");
+      return -1;
+    }
+  // one throwaway batch of the same chains: warmed up, then every tile launched twice in
+  // palindromic order (t0 .. tn-1, tn-1 .. t0) so that the chains' drift over the runs (they
+  // fill with guests) weighs on every tile alike; a tile's time is the mean of its two launches
+  fmc_batch* b = nullptr;
+  int rc = fmc_batch_open_edge(nchains, dirs, seeds, device, voxel_edge, &b);
+  float t = 0.0f;
+  if (!rc && warm_moves > 0) rc = fmc_batch_run(b, warm_moves, nullptr, &t);
+  std::vector<float> sum(ntiles, 0.0f);
+  for (int pass = 0; pass < 2 && !rc; pass++)
+    for (int j = 0; j < ntiles && !rc; j++) {
+      const int i = pass == 0 ? j : ntiles - 1 - j;
+      rc = fmc_batch_set_tile(b, tiles[i]);
+      if (!rc) rc = fmc_batch_run(b, moves, nullptr, &t);
+      sum[i] += t;
+    }
+  if (b) fmc_batch_close(b);
+  if (rc) return rc;
+  int best = 0;
+  for (int i = 0; i < ntiles; i++) {
+    if (ms) ms[i] = 0.5f * sum[i];
+    if (sum[i] < sum[best]) best = i;
+  }
+  *best_tile = tiles[best];
   return 0;
 }
 

@@ -20,7 +20,7 @@ from . import _lib
 from ._lib import (DELETE, DISPLACE, INSERT, JUMP, MOVE_DTYPE, MULTIJUMP, NOOP, ROTATE, TRANSLATE, FastMCError, check,
                    dp, ip, lib)
 
-__all__ = ["Chain", "SystemDesc", "Batch", "Server", "deck_inspect", "deck_voxels", "FastMCError", "INSERT", "DELETE", "DISPLACE", "TRANSLATE", "ROTATE",
+__all__ = ["Chain", "SystemDesc", "Batch", "Server", "deck_inspect", "deck_voxels", "batch_tiles", "autotune_tiles", "FastMCError", "INSERT", "DELETE", "DISPLACE", "TRANSLATE", "ROTATE",
            "MOVE_DTYPE"]
 
 _INFO_INTS = ["imcon", "kmax1", "kmax2", "kmax3", "K", "natoms", "nspecies", "ntypes", "mxgrid", "nframework",
@@ -407,6 +407,27 @@ def autotune_voxel_edge(directories, seeds=None, device=0, edges=(2.0, 1.5, 1.2,
     return best.value, {float(k): float(v) for k, v in zip(e, ms)}
 
 
+def batch_tiles():
+    """The batched kernel's tile shapes: a list of (threads per chain, k-vectors per thread per
+    trip, candidates per trip); index 0 is the default."""
+    n = lib().fmc_batch_tiles(None, None, None, 0)
+    t, k, c = (np.zeros(n, dtype=np.int32) for _ in range(3))
+    lib().fmc_batch_tiles(ip(t), ip(k), ip(c), n)
+    return [(int(a), int(b), int(d)) for a, b, d in zip(t, k, c)]
+
+
+def autotune_tiles(directories, seeds=None, device=0, voxel_edge=2.0, tiles=None, warm_moves=1000, moves=500):
+    """The tile under which these chains run fastest, timed on one throwaway batch (each tile
+    launched twice in palindromic order); returns (best tile index, {tile index: mean ms})."""
+    arr, s, n = _chain_args(directories, seeds)
+    t = np.ascontiguousarray(np.asarray(tiles if tiles is not None else range(len(batch_tiles())), dtype=np.int32))
+    ms = (ctypes.c_float * len(t))()
+    best = ctypes.c_int(0)
+    check(lib().fmc_batch_autotune_tiles(n, arr, ip(s), int(device), float(voxel_edge), ip(t), len(t),
+                                         int(warm_moves), int(moves), ctypes.byref(best), ms))
+    return best.value, {int(k): float(v) for k, v in zip(t, ms)}
+
+
 class Batch:
     """Many independent chains advanced by one persistent kernel (the batched path)."""
 
@@ -463,6 +484,15 @@ class Batch:
         for c in range(self.n):
             check(lib().fmc_batch_chain_timing(self.h, c, out[c].ctypes.data_as(ctypes.POINTER(ctypes.c_longlong))))
         return out
+
+    @property
+    def tile(self):
+        """Index into batch_tiles() of the kernel this batch launches."""
+        return int(lib().fmc_batch_get_tile(self.h))
+
+    @tile.setter
+    def tile(self, index):
+        check(lib().fmc_batch_set_tile(self.h, int(index)))
 
     def voxels(self, chain):
         """The device-built neighbour lists of a chain's system: (nvox, CSR offsets, atom indices)."""

@@ -88,6 +88,11 @@ SIGNATURES = {
                                   ctypes.POINTER(_vp)]),
     "fmc_batch_autotune": (_ci, [_ci, ctypes.POINTER(ctypes.c_char_p), _ip, _ci, _dp, _ci, _ci, _dp,
                                  ctypes.POINTER(ctypes.c_float)]),
+    "fmc_batch_autotune_tiles": (_ci, [_ci, ctypes.POINTER(ctypes.c_char_p), _ip, _ci, ctypes.c_double, _ip, _ci, _ci,
+                                       _ci, _ip, ctypes.POINTER(ctypes.c_float)]),
+    "fmc_batch_tiles": (_ci, [_ip, _ip, _ip, _ci]),
+    "fmc_batch_set_tile": (_ci, [_vp, _ci]),
+    "fmc_batch_get_tile": (_ci, [_vp]),
     "fmc_batch_close": (None, [_vp]),
     "fmc_batch_run": (_ci, [_vp, _ci, _vp, ctypes.POINTER(ctypes.c_float)]),
     "fmc_batch_profile": (_ci, [_vp, _ci]),

@@ -291,6 +291,20 @@ int fmc_batch_chain_state(fmc_batch* b, int chain, double* out);
  * start and end on the device clock (%globaltimer, ns) and the SM it ran on.  Recorded on every
  * run (two clock reads per CTA); 0 for a chain that has not run. */
 int fmc_batch_chain_timing(fmc_batch* b, int chain, long long* out);
+/* Tile shapes of the batched kernel (no counterpart in the reference, which evaluates one trial
+ * per call): threads per chain, k-vectors per thread per trip of the reciprocal loop
+ * (ewald.f:145-331), neighbour candidates per trip of the real-space loop (ewald.f:656-690,
+ * vdw_terms.f:455-495).  fmc_batch_tiles fills up to cap entries and returns the count; tile 0
+ * is the default.  Tiles of one thread count give bit-identical results.  Phase profiling
+ * (fmc_batch_profile) runs tile 0 only. */
+int fmc_batch_tiles(int* threads, int* kvec_per_trip, int* cand_per_trip, int cap);
+int fmc_batch_set_tile(fmc_batch* b, int tile);
+int fmc_batch_get_tile(fmc_batch* b);
+/* Times the given tiles on a throwaway batch of the same chains at voxel_edge: warm_moves
+ * moves first, then `moves` per launch, each tile launched twice in palindromic order; ms[i]
+ * the mean launch time of tiles[i], *best_tile the fastest. */
+int fmc_batch_autotune_tiles(int nchains, const char* const* dirs, const int* seeds, int device, double voxel_edge,
+                             const int* tiles, int ntiles, int warm_moves, int moves, int* best_tile, float* ms);
 int fmc_batch_guest_coords(fmc_batch* b, int chain, int iguest, double* xyz, int* nmol, int* nsite);
 /* The neighbour lists of a chain's system as the device built them (guestlistgen's candidate
  * sets, utility_pack.f:3113-3177, precomputed per voxel): nvox[0..2], off[nvox+1] (CSR
