@@ -51,6 +51,8 @@ def parse():
                     help="batched: the first N of the 256 chains (framework-major), for reduced profiling cases")
     ap.add_argument("--voxel-edge", type=float, default=0.0,
                     help="batched: neighbour-list voxel edge in A (0: picked by the autotuner)")
+    ap.add_argument("--resident", action="store_true",
+                    help="plain: passes through the resident pass kernel instead of a launch each")
     ap.add_argument("--tile", type=int, default=-1,
                     help="batched: index into the kernel's tile shapes (-1: picked by the autotuner)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="bounded CPU baseline sample")
@@ -252,12 +254,14 @@ def run_plain(args, dist):
     deck = make_plain_deck(tmp)
     seed = (12, 34, 56, (78 + dist.rank) % 169)
     chain = fm.Chain(deck, seed=seed, device=dist.local)
+    chain.resident(args.resident)
     info = chain.info()
     for _ in range(args.warmup):
         chain.run(args.moves, trace=False)
     chain.profile(-1)  # clear the launch counters ...
     chain.profile(0)  # ... and time no pass on its own inside the timed loop
     guests_at_start = chain.guest_coords(0)
+    _, rl0, rp0 = chain.resident()
     dist.barrier()
     ms_total = 0.0
     traces = []
@@ -271,6 +275,7 @@ def run_plain(args, dist):
         wall = time.perf_counter() - wall0
     dist.barrier()
     counts = chain.profile(0)  # passes and commits of the timed loop
+    _, rl1, rp1 = chain.resident()
     # the pass kernel's own time for the roofline, from CUDA events around every pass of a further
     # run after the timed loop (per-pass events would slow the loop they time)
     chain.profile(-1)
@@ -289,7 +294,9 @@ def run_plain(args, dist):
     avg_kernel_s = prof["pass_ms"] / max(prof["timed_passes"], 1) / 1000.0
     achieved = bytes_per_launch / avg_kernel_s / 1e9
     peak, peak_kind = peaks()
-    launches = int(counts["passes"] + counts["commits"])
+    # launches in the timed loop: one per pass, or with the resident kernel its own launches plus
+    # any pass it did not serve; commit kernels only where an update could not wait for the next pass
+    launches = int(counts["passes"] - (rp1 - rp0) + (rl1 - rl0) + counts["commits"])
     # bytes crossing PCIe per step: trial sites (xyz, q, type) of every pass and of every commit
     # go host->device as kernel arguments; each pass returns {ewld1, ewld2, vdw} device->host
     acc = tr["accepted"] == 1
@@ -310,6 +317,8 @@ def run_plain(args, dist):
         "dtype": "f64",
         "data": "synthetic (seeded framework generator, FastMC input formats)",
         "config": {"workload": PLAIN_WORKLOAD, "moves_per_step": args.moves,
+                   "resident_kernel": {"on": bool(args.resident), "launches": int(rl1 - rl0),
+                                       "passes_served": int(rp1 - rp0)},
                    "chains_per_gpu": 1, "guests_mean": float(np.mean(tr["nmols_after"])),
                    "l2": "working set (S(k) 67 KB + framework 130 KB) is L2-resident; no flush between moves",
                    "parallelism": f"replicas{dist.world}"},

@@ -155,6 +155,7 @@ int fmc_ewald1_guest(fmc_chain* c, int iguest, int natms, const double* xyz, int
     A.q[w] = G.charge[i];
     A.type[w] = (unsigned char)G.type[i];
   }
+  if (int rc0 = C.stop_server()) return fail(rc0, "the resident pass kernel did not end");
   C.take_pending(A);  // an update left by fmc_commit is read through and written by this pass
   cudaError_t e = fmc::launch_pass(C.dsys.view, C.guest_view(), A, C.sk, C.sk_new, C.W, C.st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(C.st);  // the kernel wrote the result to pinned memory
@@ -191,6 +192,7 @@ int fmc_guest_realspace(fmc_chain* c, int iguest, int natms, const double* xyz, 
     A.q[i] = G.charge[i];
     A.type[i] = (unsigned char)G.type[i];
   }
+  if (int rc0 = C.stop_server()) return fail(rc0, "the resident pass kernel did not end");
   C.take_pending(A);  // an update left by fmc_commit is read through and written by this pass
   cudaError_t e = fmc::launch_pass(C.dsys.view, C.guest_view(), A, C.sk, C.sk_new, C.W, C.st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(C.st);  // the kernel wrote the result to pinned memory
@@ -277,9 +279,22 @@ int fmc_single_point(fmc_chain* c, double* spenergy, double* dlpeng) {
   return 0;
 }
 
+int fmc_chain_resident(fmc_chain* c, int enable, long long* launches, long long* passes) {
+  CHECK_CHAIN(c);
+  fmc::Chain& C = c->impl;
+  if (enable >= 0) {
+    if (int rc = C.stop_server()) return fail(rc, "the resident pass kernel did not end");
+    C.use_server = enable != 0;
+  }
+  if (launches) *launches = C.srv_launches;
+  if (passes) *passes = C.srv_passes;
+  return C.use_server ? 1 : 0;
+}
+
 int fmc_get_sk(fmc_chain* c, int pending, double* re, double* im) {
   CHECK_CHAIN(c);
   fmc::Chain& C = c->impl;
+  if (int rc0 = C.stop_server()) return fail(rc0, "the resident pass kernel did not end");
   std::vector<double2> h(C.sys.K);
   cudaError_t e = cudaMemcpyAsync(h.data(), pending ? C.sk_new : C.sk, sizeof(double2) * C.sys.K,
                                   cudaMemcpyDeviceToHost, C.st);

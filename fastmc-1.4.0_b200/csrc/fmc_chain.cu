@@ -5,6 +5,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstring>
 
 namespace fmc {
@@ -163,6 +164,12 @@ Chain::~Chain() {
   if (ev1) cudaEventDestroy(ev1);
   if (st) {
     cudaSetDevice(device);
+    stop_server();
+    if (srv_st) cudaStreamDestroy(srv_st);
+    if (mb) cudaFreeHost(mb);
+    if (h_fl) cudaFreeHost(h_fl);
+    if (srv_words) cudaFreeHost(srv_words);
+    if (d_fl) cudaFree(d_fl);
     cudaStreamSynchronize(st);
     for (void* p : {(void*)sk, (void*)sk_new, (void*)sk_save, (void*)gsite, (void*)gtype, (void*)W.recip_part, (void*)W.site_e,
                     (void*)W.counter, (void*)recip_scratch, (void*)recip_parts, (void*)all_atoms})
@@ -252,6 +259,13 @@ int Chain::open_prepared(HostSystem&& prepared, const int seed[4], int dev, std:
   // the pass result goes straight to pinned host memory, which the kernel addresses through unified
   // addressing: a copy back per pass cost as much as a third of the plain path's time
   FMC_CUDA(cudaMallocHost(&W.result, sizeof(double) * 4));
+  FMC_CUDA(cudaStreamCreateWithFlags(&srv_st, cudaStreamNonBlocking));
+  FMC_CUDA(cudaMallocHost(&mb, sizeof(PassMailbox)));
+  FMC_CUDA(cudaMallocHost(&h_fl, sizeof(PassServerFlags)));
+  FMC_CUDA(cudaMallocHost(&srv_words, sizeof(int) * 2));
+  FMC_CUDA(cudaMalloc(&d_fl, sizeof(PassServerFlags)));
+  std::memset(mb, 0, sizeof(PassMailbox));
+  srv_words[0] = srv_words[1] = 0;
   all_cap = sys.nf + gcap;
   FMC_CUDA(cudaMalloc(&all_atoms, sizeof(double4) * std::max(all_cap, 1)));
   recip_scratch_n = recip_scratch_doubles(dsys.view, all_cap);
@@ -302,6 +316,7 @@ int Chain::open_prepared(HostSystem&& prepared, const int seed[4], int dev, std:
 int Chain::set_guests(int g, int nmol, const double* xyz) {
   Species& s = sp[g];
   if (nmol * s.nsite > s.cap_sites) return -75;
+  if (int rc = stop_server()) return rc;
   if (int rc = flush_commit()) return rc;
   s.nmol = nmol;
   s.xyz.assign(xyz, xyz + 3 * nmol * s.nsite);
@@ -383,6 +398,7 @@ int Chain::restart(const Revive& r, std::string& err) {
 
 // S(k) over all current atoms: guests in species order, then the framework (condense order).
 int Chain::full_recip(double* e_out) {
+  if (int rc0 = stop_server()) return rc0;  // nothing else runs beside the resident kernel
   if (int rc = flush_commit()) return rc;
   int n = 0;
   cudaError_t e = cudaSuccess;
@@ -414,6 +430,7 @@ int Chain::full_recip(double* e_out) {
 // real-space energies (guest-framework once, guest-guest halved), the intramolecular
 // correction and the tail correction.
 int Chain::single_point() {
+  if (int rc0 = stop_server()) return rc0;  // nothing else runs beside the resident kernel
   if (int rc = flush_commit()) return rc;
   // framework only
   cudaError_t e = launch_recip_full(dsys.view, dsys.view.fw, sys.nf, sk, recip_scratch, recip_parts, st);
@@ -508,6 +525,101 @@ int Chain::single_point() {
   return 0;
 }
 
+int Chain::start_server() {
+  cudaError_t e = cudaStreamSynchronize(st);  // work on the chain's stream (and its updates) is done
+  if (e != cudaSuccess) return sync_error(e);
+  st_dirty = false;
+  srv_words[0] = srv_words[1] = 0;
+  *(volatile int*)&mb->quit = 0;
+  h_fl->done = (unsigned long long)pass_seq_done;
+  h_fl->go = (unsigned long long)pass_seq_done;
+  h_fl->stop = 0;
+  h_fl->exit_count = 0;
+  e = cudaMemcpyAsync(d_fl, h_fl, sizeof(PassServerFlags), cudaMemcpyHostToDevice, srv_st);
+  if (e == cudaSuccess) e = cudaMemsetAsync(W.counter, 0, sizeof(unsigned), srv_st);
+  if (e != cudaSuccess) return sync_error(e);
+  // 20 ms without a pass end the kernel
+  e = launch_pass_server(dsys.view, mb, d_fl, srv_words, W, (long long)pass_seq_done, 20000000LL, srv_st);
+  if (e != cudaSuccess) {
+    // the blocks cannot all be resident at once (the GPU is busy): passes launch one by one
+    cudaGetLastError();
+    e = cudaStreamSynchronize(srv_st);
+    if (e != cudaSuccess) return sync_error(e);
+    use_server = false;
+    return 0;
+  }
+  srv_live = true;
+  srv_launches++;
+  return 0;
+}
+
+int Chain::stop_server() {
+  if (!srv_live) return 0;
+  *(volatile int*)&mb->quit = 1;
+  cudaError_t e = cudaStreamSynchronize(srv_st);  // block 0 sees the flag at its next poll
+  srv_live = false;
+  *(volatile int*)&mb->quit = 0;
+  if (e != cudaSuccess) return sync_error(e);
+  return 0;
+}
+
+// One pass through the resident kernel: the pass goes into the mailbox, then its number; the
+// kernel publishes the energies and then the number, as the one-launch kernel does.  A kernel
+// that ended meanwhile (idle limit reached as the pass was posted) is started again and picks
+// the posted pass up.
+int Chain::pass_resident(const PassArgs& A, double out[3]) {
+  if (st_dirty) {
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return sync_error(e);
+    st_dirty = false;
+  }
+  if (!srv_live) {
+    int rc = start_server();
+    if (rc) return rc;
+    if (!srv_live) return 1;  // not available: the caller launches the pass
+  }
+  PassArgsT<kSmallPassSites>& B = mb->A;
+  std::memcpy(&B, &A, offsetof(PassArgs, x));
+  const int nsite = A.nold + A.nnew;
+  for (int i = 0; i < nsite; i++) {
+    B.x[i] = A.x[i];
+    B.y[i] = A.y[i];
+    B.z[i] = A.z[i];
+    B.q[i] = A.q[i];
+    B.type[i] = A.type[i];
+  }
+  B.pc = A.pc;
+  mb->G = guest_view();
+  mb->sk = sk;
+  mb->sk_new = sk_new;
+  std::atomic_thread_fence(std::memory_order_release);
+  *(volatile long long*)&mb->cmd = (long long)A.seq;
+  volatile double* flag = W.result + 3;
+  for (int restarts = 0;;) {
+    long long spins = 0;
+    while (*flag != A.seq && !*(volatile int*)&srv_words[0] && ++spins < 400000000LL) {
+    }
+    std::atomic_thread_fence(std::memory_order_acquire);
+    if (*flag == A.seq) break;
+    // the kernel ended without the pass, or nothing came back in time: end it, start it again
+    *(volatile int*)&mb->quit = 1;
+    cudaError_t e = cudaStreamSynchronize(srv_st);
+    srv_live = false;
+    *(volatile int*)&mb->quit = 0;
+    if (e != cudaSuccess) return sync_error(e);
+    if (*flag == A.seq) break;
+    if (srv_words[1] || ++restarts > 3) return -13;  // a wait inside the kernel ran out
+    int rc = start_server();
+    if (rc) return rc;
+    if (!srv_live) return -13;
+  }
+  out[0] = W.result[0];
+  out[1] = W.result[1];
+  out[2] = W.result[2];
+  srv_passes++;
+  return 0;
+}
+
 int Chain::pass(int move, int g, int mol, const double* old_xyz, const double* new_xyz, double out[3]) {
   PassArgs A;
   std::memset(&A, 0, sizeof(A));
@@ -547,6 +659,19 @@ int Chain::pass(int move, int g, int mol, const double* old_xyz, const double* n
   pass_seq += 1.0;
   A.seq = pass_seq;
   take_pending(A);
+  if (use_server && !profile && A.nold + A.nnew <= kSmallPassSites) {
+    int rc = pass_resident(A, out);
+    if (rc <= 0) {
+      if (rc == 0) {
+        passes++;
+        pass_seq_done = pass_seq;
+      }
+      return rc;
+    }
+  } else {
+    int rc = stop_server();
+    if (rc) return rc;
+  }
   cudaError_t e = launch_pass(dsys.view, guest_view(), A, sk, sk_new, W, st);
   if (profile) cudaEventRecord(ev1, st);
   if (e == cudaSuccess && !profile) {
@@ -574,6 +699,7 @@ int Chain::pass(int move, int g, int mol, const double* old_xyz, const double* n
   out[1] = W.result[1];
   out[2] = W.result[2];
   passes++;
+  pass_seq_done = pass_seq;
   return 0;
 }
 
@@ -589,6 +715,7 @@ void Chain::take_pending(PassArgs& A) {
 
 int Chain::flush_commit() {
   if (!pend_live) return 0;
+  if (int rc0 = stop_server()) return rc0;  // nothing else runs beside the resident kernel
   pend_live = false;
   CommitArgs C;
   std::memset(&C, 0, sizeof(C));
@@ -645,6 +772,7 @@ int Chain::commit(int move, int g, int mol, const double* new_xyz) {
         C.type[i] = G.type[i];
       }
     pend_live = false;
+    if (int rc0 = stop_server()) return rc0;
     cudaError_t e = launch_commit(0, sk, sk_new, C, gsite, gtype, st);
     if (e != cudaSuccess) return sync_error(e);
     commits++;
@@ -857,6 +985,7 @@ int Chain::step(MoveRecord* rec) {
     const double origenergy = energy[g];
     cudaError_t ce = cudaMemcpyAsync(sk_save, sk, sizeof(double2) * std::max(sys.K, 1), cudaMemcpyDeviceToDevice, st);
     if (ce != cudaSuccess) return sync_error(ce);
+    st_dirty = true;
     int first = 0, mol = -1;
     double first_old[3 * kMaxGuestSites];
     for (int mv = 1; mv <= 2; mv++) {
@@ -907,6 +1036,7 @@ int Chain::step(MoveRecord* rec) {
       // S(k) back to its state before the move; the first molecule back to its old sites
       ce = cudaMemcpyAsync(sk_new, sk_save, sizeof(double2) * std::max(sys.K, 1), cudaMemcpyDeviceToDevice, st);
       if (ce != cudaSuccess) return sync_error(ce);
+      st_dirty = true;
       if ((rc = commit(kDisplace, g, first - 1, first_old))) return rc;
       energy[g] = origenergy;
     }

@@ -112,6 +112,22 @@ class Chain {
   int flush_commit();
   PendingCommit pend{};
   bool pend_live = false;
+  // Resident pass kernel (fmc_pass_server_kernel on its own stream): passes of up to
+  // kSmallPassSites sites go through its mailbox instead of a launch each.  Any other device
+  // work on the chain stops it first (stop_server); the next pass starts it again.
+  bool use_server = false;  // off by default: opt in with fmc_chain_resident
+  bool srv_live = false;
+  bool st_dirty = false;           // work queued on `st` since the last synchronisation
+  cudaStream_t srv_st = nullptr;
+  PassMailbox* mb = nullptr;       // pinned
+  PassServerFlags* d_fl = nullptr;
+  PassServerFlags* h_fl = nullptr; // pinned staging of the flags a launch starts from
+  int* srv_words = nullptr;        // pinned: [0] ended, [1] reason a wait ran out
+  double pass_seq_done = 0.0;      // last pass whose result the host has read
+  long long srv_launches = 0, srv_passes = 0;
+  int start_server();
+  int stop_server();
+  int pass_resident(const PassArgs& A, double out[3]);
   int full_recip(double* e_recip_plus_self);  // S(k) over all current atoms (ewald1)
   int single_point();
   int step(MoveRecord* rec);

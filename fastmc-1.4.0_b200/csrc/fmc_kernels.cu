@@ -53,17 +53,19 @@ __device__ __forceinline__ void apply_commit(const PendingCommit& P, double4* si
 }
 
 // ------------------------------------------------------------------------------ pass
-template <int N>
-__global__ void __launch_bounds__(kPassThreads) fmc_pass_kernel(DevSystem S, GuestView G, PassArgsT<N> A,
-                                                                const double2* __restrict__ sk, double2* sk_new,
-                                                                PassScratch W) {
-  extern __shared__ double2 sm_tab[];
-  __shared__ double red[32 * 2];
-  __shared__ bool am_last;
+// One block's share of a trial pass (block `blk` of `nblocks`): blocks [0, nbk) the reciprocal
+// change of 256 k-vectors each, the next nsite blocks the real-space energy of one trial site
+// each (further blocks idle), then the last block to finish combines the partials in a fixed
+// order into {ewld1, ewld2, vdw}, publishes them with the sequence number and writes the pending
+// guest-site update.  Returns (to every thread) whether this block was the last.
+template <class Args>
+__device__ __forceinline__ bool pass_block(const DevSystem& S, const GuestView& G, const Args& A, const double2* sk,
+                                           double2* sk_new, const PassScratch& W, int blk, int nblocks,
+                                           double2* sm_tab, double* red, double* comb, bool& am_last) {
   const int nsite = A.nold + A.nnew;
   const int nbk = A.nbk;
   const int tid = threadIdx.x;
-  if ((int)blockIdx.x < nbk) {
+  if (blk < nbk) {
     // ---- reciprocal space
     const int k1 = S.kmax[0], k2 = S.kmax[1], k3 = S.kmax[2];
     const int stride = (k1 + 1) + (k2 + 1) + (k3 + 1);
@@ -76,7 +78,7 @@ __global__ void __launch_bounds__(kPassThreads) fmc_pass_kernel(DevSystem S, Gue
     }
     __syncthreads();
     double v[1] = {0.0};
-    int k = blockIdx.x * blockDim.x + tid;
+    int k = blk * blockDim.x + tid;
     if (k < S.K) {
       int l, m, n;
       kunpack(S.kpack[k], l, m, n);
@@ -107,10 +109,10 @@ __global__ void __launch_bounds__(kPassThreads) fmc_pass_kernel(DevSystem S, Gue
       v[0] = S.akk[k] * (sn.x * sn.x + sn.y * sn.y - so.x * so.x - so.y * so.y);
     }
     block_sum<1>(v, red);
-    if (tid == 0) W.recip_part[blockIdx.x] = v[0];
-  } else {
+    if (tid == 0) W.recip_part[blk] = v[0];
+  } else if (A.do_real && blk - nbk < nsite) {
     // ---- real space of one trial site
-    const int s = blockIdx.x - nbk;
+    const int s = blk - nbk;
     double v[2] = {0.0, 0.0};
     double ec_fw = 0.0, ev_fw = 0.0, ec_g = 0.0, ev_g = 0.0;
     site_partial(S, G, A.pc, A.x[s], A.y[s], A.z[s], A.q[s], A.type[s], A.ex_lo, A.ex_hi, tid, blockDim.x, ec_fw,
@@ -128,11 +130,10 @@ __global__ void __launch_bounds__(kPassThreads) fmc_pass_kernel(DevSystem S, Gue
   if (tid == 0) {
     __threadfence();
     unsigned done = atomicAdd(W.counter, 1u);
-    am_last = (done == gridDim.x - 1);
+    am_last = (done == (unsigned)nblocks - 1);
   }
   __syncthreads();
-  if (!am_last) return;
-  __shared__ double comb[kPassThreads];
+  if (!am_last) return false;
   __threadfence();
   double r = 0.0;
   for (int base = 0; base < nbk; base += kPassThreads) {
@@ -142,7 +143,7 @@ __global__ void __launch_bounds__(kPassThreads) fmc_pass_kernel(DevSystem S, Gue
       for (int i = 0; i < kPassThreads && base + i < nbk; i++) r += comb[i];
     __syncthreads();
   }
-  const int nse = A.do_real ? 2 * nsite : 0;  // <= 2 * N <= kPassThreads
+  const int nse = A.do_real ? 2 * nsite : 0;  // <= 2 * kMaxPassSites <= kPassThreads
   if (tid < nse) comb[tid] = ((volatile double*)W.site_e)[tid];
   __syncthreads();
   if (tid == 0) {
@@ -169,6 +170,160 @@ __global__ void __launch_bounds__(kPassThreads) fmc_pass_kernel(DevSystem S, Gue
   }
   // every block has read the guest sites: the last one writes the pending update
   if (A.pc.op) apply_commit(A.pc, W.gsite, W.gtype);
+  return true;
+}
+
+template <int N>
+__global__ void __launch_bounds__(kPassThreads) fmc_pass_kernel(DevSystem S, GuestView G, PassArgsT<N> A,
+                                                                const double2* __restrict__ sk, double2* sk_new,
+                                                                PassScratch W) {
+  extern __shared__ double2 sm_tab[];
+  __shared__ double red[32 * 2];
+  __shared__ double comb[kPassThreads];
+  __shared__ bool am_last;
+  pass_block(S, G, A, sk, sk_new, W, (int)blockIdx.x, (int)gridDim.x, sm_tab, red, comb, am_last);
+}
+
+// ------------------------------------------------------------------------------ resident pass
+// Every wait of the resident kernel is bounded on the device clock (%globaltimer, ns): block 0
+// ends the kernel after `idle_ns` without a pass (the host passes the limit); the other blocks
+// wait for block 0 up to 64 times as long, and for the previous pass's update up to kDoneNs:
+// past either limit a block records why in host_words[1] and ends.
+constexpr unsigned long long kDoneNs = 1000000000ULL;
+
+__device__ __forceinline__ unsigned long long now_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__global__ void __launch_bounds__(kPassThreads) fmc_pass_server_kernel(DevSystem S, const PassMailbox* mb,
+                                                                       PassServerFlags* fl, int* host_words,
+                                                                       PassScratch W, long long seq0,
+                                                                       long long idle_ns) {
+  extern __shared__ double2 sm_tab[];
+  __shared__ double red[32 * 2];
+  __shared__ double comb[kPassThreads];
+  __shared__ bool am_last;
+  __shared__ long long s_cmd;
+  __shared__ PassArgsT<kSmallPassSites> A;
+  __shared__ GuestView G;
+  __shared__ const double2* s_sk;
+  __shared__ double2* s_sk_new;
+  const int tid = threadIdx.x;
+  const bool leader = blockIdx.x == 0;
+  long long seq = seq0;
+  for (;;) {
+    if (tid == 0) {
+      // block 0 polls the mailbox in host memory, the other blocks block 0's flag in device memory
+      const volatile long long* cmd = &mb->cmd;
+      const volatile unsigned long long* go = &fl->go;
+      const unsigned long long limit = (unsigned long long)(leader ? idle_ns : 64 * idle_ns);
+      const unsigned long long t0 = now_ns();
+      long long c = -1;
+      for (;;) {
+        c = leader ? *cmd : (long long)*go;
+        if (c > seq) break;
+        if (leader ? *(const volatile int*)&mb->quit != 0 : *(volatile int*)&fl->stop != 0) {
+          c = -1;
+          break;
+        }
+        if (now_ns() - t0 >= limit) {
+          if (!leader) atomicExch(host_words + 1, 1);
+          c = -1;
+          break;
+        }
+        __nanosleep(leader ? 64 : 32);
+      }
+      if (c > seq) {
+        // the previous pass's guest-site update is written before this pass reads the sites
+        const unsigned long long t1 = now_ns();
+        bool late = false;
+        while (*(volatile unsigned long long*)&fl->done < (unsigned long long)(c - 1)) {
+          if (now_ns() - t1 >= kDoneNs) {
+            late = true;
+            break;
+          }
+          __nanosleep(32);
+        }
+        if (late) {
+          atomicExch(host_words + 1, 2);
+          c = -1;
+        }
+      }
+      if (c < 0 && leader) {
+        *(volatile int*)&fl->stop = 1;
+        __threadfence();
+      }
+      s_cmd = c;
+    }
+    __syncthreads();
+    const long long c = s_cmd;
+    if (c < 0) break;
+    // the pass into shared memory: block 0 from the mailbox (host memory), which it then copies
+    // to device memory for the others; the others from there
+    {
+      const volatile unsigned long long* src =
+          reinterpret_cast<const volatile unsigned long long*>(leader ? (const void*)&mb->A : (const void*)&fl->A);
+      unsigned long long* dst = reinterpret_cast<unsigned long long*>(&A);
+      for (int i = tid; i < (int)(sizeof(A) / 8); i += blockDim.x) dst[i] = src[i];
+      const volatile unsigned long long* gs =
+          reinterpret_cast<const volatile unsigned long long*>(leader ? (const void*)&mb->G : (const void*)&fl->G);
+      unsigned long long* gd = reinterpret_cast<unsigned long long*>(&G);
+      for (int i = tid; i < (int)(sizeof(G) / 8); i += blockDim.x) gd[i] = gs[i];
+      if (tid == 0) {
+        s_sk = leader ? *(const double2* const volatile*)&mb->sk : *(const double2* const volatile*)&fl->sk;
+        s_sk_new = leader ? *(double2* const volatile*)&mb->sk_new : *(double2* const volatile*)&fl->sk_new;
+      }
+    }
+    __syncthreads();
+    if (leader) {
+      unsigned long long* dA = reinterpret_cast<unsigned long long*>(&fl->A);
+      const unsigned long long* sA = reinterpret_cast<const unsigned long long*>(&A);
+      for (int i = tid; i < (int)(sizeof(A) / 8); i += blockDim.x) dA[i] = sA[i];
+      unsigned long long* dG = reinterpret_cast<unsigned long long*>(&fl->G);
+      const unsigned long long* sG = reinterpret_cast<const unsigned long long*>(&G);
+      for (int i = tid; i < (int)(sizeof(G) / 8); i += blockDim.x) dG[i] = sG[i];
+      if (tid == 0) {
+        fl->sk = s_sk;
+        fl->sk_new = s_sk_new;
+      }
+      __threadfence();
+      __syncthreads();
+      if (tid == 0) *(volatile unsigned long long*)&fl->go = (unsigned long long)c;
+    }
+    const bool last = pass_block(S, G, A, s_sk, s_sk_new, W, (int)blockIdx.x, (int)gridDim.x, sm_tab, red, comb,
+                                 am_last);
+    if (last) {
+      __syncthreads();  // the update is written by every thread of this block
+      if (tid == 0) {
+        __threadfence();
+        *(volatile unsigned long long*)&fl->done = (unsigned long long)c;
+      }
+    }
+    seq = c;
+    __syncthreads();
+  }
+  // the last block to end tells the host
+  if (tid == 0) {
+    __threadfence();
+    const unsigned n = atomicAdd(&fl->exit_count, 1u);
+    if (n == gridDim.x - 1) {
+      __threadfence_system();
+      *(volatile int*)host_words = 1;
+    }
+  }
+}
+
+int pass_server_blocks(const DevSystem& S) { return pass_recip_blocks(S) + kServerBlocksExtra; }
+
+cudaError_t launch_pass_server(const DevSystem& S, PassMailbox* mb, PassServerFlags* fl, int* host_words,
+                               const PassScratch& W, long long seq0, long long idle_ns, cudaStream_t st) {
+  static_assert(sizeof(PassArgsT<kSmallPassSites>) % 8 == 0 && sizeof(GuestView) % 8 == 0, "word copies");
+  const int grid = pass_server_blocks(S);
+  const int smem = pass_smem_bytes(S, kSmallPassSites);
+  void* args[] = {(void*)&S, (void*)&mb, (void*)&fl, (void*)&host_words, (void*)&W, (void*)&seq0, (void*)&idle_ns};
+  return cudaLaunchCooperativeKernel((const void*)fmc_pass_server_kernel, grid, kPassThreads, args, smem, st);
 }
 
 int pass_smem_bytes(const DevSystem& S, int nsite) {
@@ -205,6 +360,8 @@ cudaError_t launch_pass(const DevSystem& S, const GuestView& G, const PassArgs& 
 cudaError_t configure_kernels() {
   cudaError_t e = cudaFuncSetAttribute(fmc_pass_kernel<kSmallPassSites>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        200 * 1024);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(fmc_pass_server_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(fmc_pass_kernel<kMaxPassSites>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
   return e;

@@ -47,6 +47,41 @@ struct CommitArgs {
   int type[kMaxGuestSites];
 };
 
+// The resident pass kernel (`fmc_pass_server_kernel`): one launch serves the passes of a chain
+// while the host keeps posting them.  The host writes a pass into the mailbox (pinned host
+// memory) and then its sequence number; every block polls the number, copies the pass into
+// shared memory and does its share as the one-launch kernel does; results go to the same pinned
+// words.  Block 0 ends the kernel after an idle time (no pass posted) or on `quit`; every wait
+// is bounded on the device clock.
+struct PassMailbox {
+  long long cmd;     // sequence number of the posted pass, written after everything else
+  int quit;          // 1: the kernel ends at its next poll
+  int pad;
+  GuestView G;
+  const double2* sk;
+  double2* sk_new;
+  PassArgsT<kSmallPassSites> A;
+};
+// Device-side state of the resident kernel (device memory, set by the host before a launch).
+// Only block 0 polls the mailbox over PCIe: it copies each pass into `pass` and then raises
+// `go`, which the other blocks poll in device memory.
+struct PassServerFlags {
+  unsigned long long done;  // last pass whose pending guest-site update has been written
+  unsigned long long go;    // last pass block 0 has copied into `pass`
+  int stop;                 // block 0 ended the kernel: the other blocks end too
+  unsigned exit_count;      // blocks that have ended
+  GuestView G;
+  const double2* sk;
+  double2* sk_new;
+  PassArgsT<kSmallPassSites> A;
+};
+// Pinned host words the resident kernel writes: [0] 1 once every block has ended, [1] 0 or the
+// reason a wait ran out (1 a block waited too long for block 0, 2 for the previous pass).
+constexpr int kServerBlocksExtra = kSmallPassSites;  // site blocks beyond the reciprocal blocks
+cudaError_t launch_pass_server(const DevSystem& S, PassMailbox* mb, PassServerFlags* fl, int* host_words,
+                               const PassScratch& W, long long seq0, long long idle_ns, cudaStream_t st);
+int pass_server_blocks(const DevSystem& S);
+
 int pass_smem_bytes(const DevSystem& S, int nsite);
 int pass_recip_blocks(const DevSystem& S);
 cudaError_t configure_kernels();  // once per device, before the first launch

@@ -300,6 +300,16 @@ class Chain:
         check(lib().fmc_single_point(self.h, ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
 
+    def resident(self, enable=None):
+        """Passes through the resident kernel: enable True / False switches it, None only reports.
+        Returns (on, launches of the kernel, passes it served)."""
+        a, b = ctypes.c_longlong(0), ctypes.c_longlong(0)
+        rc = lib().fmc_chain_resident(self.h, -1 if enable is None else int(bool(enable)), ctypes.byref(a),
+                                      ctypes.byref(b))
+        if rc < 0:
+            check(rc)
+        return bool(rc), a.value, b.value
+
     def sk(self, pending=False):
         K = self.info()["K"]
         re, im = np.zeros(K), np.zeros(K)

@@ -47,6 +47,13 @@ const char* fmc_last_error(void);
  * computes the single-point energy (gcmc.f:2518-2710) and S(k) of all atoms (gcmc.f:522), and
  * seeds duni (gcmc.f:2712) with seed[0..3] = the (i,j,k,l) the reference prints. */
 int fmc_chain_open(const char* dir, const int* seed, int device, fmc_chain** out);
+/* Passes of up to 8-site molecules run through a resident kernel (no counterpart in the
+ * reference): it stays on the GPU while passes keep coming, takes each from pinned host memory
+ * and ends after ~20 ms without one; the next pass starts it again.  enable 1 / 0 turns it on /
+ * off (off by default), -1 only reports; *launches and *passes count its launches and the passes
+ * it served.  Returns 1 if on, 0 if off (it also switches itself off when the GPU cannot hold all
+ * its blocks at once). */
+int fmc_chain_resident(fmc_chain* c, int enable, long long* launches, long long* passes);
 void fmc_chain_close(fmc_chain* c);
 
 /* ---------------------------------------------------------------- system from caller arrays
