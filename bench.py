@@ -39,6 +39,7 @@ def parse():
     ap.add_argument("--serve-requests", type=int, default=1500)
     ap.add_argument("--serve-slots", type=int, default=296)
     ap.add_argument("--serve-moves", type=int, default=1000, help="moves per slot per serving step")
+    ap.add_argument("--serve-voxel-edge", type=float, default=2.0, help="neighbour-list voxel edge of serving slots (A)")
     ap.add_argument("--serve-kcap", type=int, default=0, help="0: the largest request's K")
     ap.add_argument("--serve-cycle-scale", type=float, default=0.1,
                     help="scale of the U(2k,20k) cycle budgets so that requests finish within the run")
@@ -597,7 +598,7 @@ def serve_record(args, dist, n_req, cycle_scale, tag):
 
     # k capacity: the largest request's K (cubic cells: K grows with the edge)
     kcap = args.serve_kcap or int(fm.deck_inspect(dirs[int(np.argmax([r["edge"] for r in reqs]))])["K"])
-    srv = fm.Server(slots=args.serve_slots, device=dist.local, k_capacity=kcap)
+    srv = fm.Server(slots=args.serve_slots, device=dist.local, k_capacity=kcap, voxel_edge=args.serve_voxel_edge)
     # pilot (warm-up): more requests than slots at once; the launches that ran with every slot busy
     # give the server's capacity in moves/s
     ids = [srv.submit(d, (12, 34, 56, 1 + r["id"] % 168)) for d, r in zip(dirs[:n_pilot], reqs[:n_pilot])]
@@ -681,6 +682,7 @@ def summarize_serve(args, dist, srv, log, done_t, arrivals, wall, meta, cycle_sc
         "pilot_requests": meta["n_pilot"], "arrival_rate_hz": meta["rate"],
         "capacity_moves_per_s": meta["capacity"], "offered_load": 0.9, "moves_per_request_mean": meta["moves_per_req"],
         "moves_per_step": args.serve_moves, "k_capacity": meta["kcap"], "deck_generation_s": meta["gen_s"],
+        "voxel_edge_A": args.serve_voxel_edge,
         "saturated": meta["saturated"],
         "window": {"what": "device and end-to-end figures cover the steps started before the last arrival",
                    "steps": len(win), "moves": w_moves, "device_s": w_dev, "wall_s": w_wall,
@@ -711,6 +713,7 @@ def run_serve(args, dist):
                    "arrival_rate_hz": rec["arrival_rate_hz"], "capacity_moves_per_s": rec["capacity_moves_per_s"],
                    "offered_load": 0.9, "moves_per_request_mean": rec["moves_per_request_mean"],
                    "moves_per_step": args.serve_moves, "k_capacity": rec["k_capacity"],
+                   "voxel_edge_A": args.serve_voxel_edge,
                    "l2": "per-chain S(k) shared-memory resident; frameworks + voxel lists exceed L2 (no flush)",
                    "parallelism": f"replicas{dist.world}"},
         "latency_s": rec["latency_s"], "rejected": rec["rejected"], "saturated": rec["saturated"],

@@ -133,6 +133,7 @@ class Server {
   long long admitted = 0, retired = 0, launches = 0, moves_run = 0, last_moves = 0;
   double admit_ms = 0, launch_ms = 0, wait_ms = 0;
   std::atomic<long long> prep_us{0}, prep_host_us{0}, prep_dev_us{0};
+  std::atomic<double> voxel_edge{2.0};  // neighbour-list voxel edge (A) of requests prepared from now on
   long long admit_prebuilt = 0, admit_built = 0;
 
   ~Server() {
@@ -280,7 +281,7 @@ class Server {
     const double t0 = now_ms();
     auto h = std::make_unique<HostSystem>();
     std::string err;
-    int rc = prepare_system(r.dir, *h, err);
+    int rc = prepare_system(r.dir, *h, err, voxel_edge.load());
     if (!rc)
       for (auto& g : h->deck.guests)
         if (g.nmols) {
@@ -871,6 +872,15 @@ struct fmc_server {
 };
 
 extern "C" {
+
+int fmc_server_set_voxel_edge(fmc_server* s, double edge) {
+  if (!s || !(edge >= 1.0 && edge <= 4.0)) {
+    fmc::set_last_error("bad server handle or voxel edge (1-4 A)");
+    return -1;
+  }
+  s->impl.voxel_edge.store(edge);
+  return 0;
+}
 
 int fmc_server_open(int slots, int device, long long mem_budget, int k_capacity, fmc_server** out) {
   if (!out || slots < 1 || k_capacity < 1 || mem_budget < 0) {

@@ -569,9 +569,11 @@ class Server:
             "prodcount", "N", "E", "EN", "N2", "E2", "accept_ins", "accept_del", "_r18", "K", "nframework",
             "temp", "press0", "budget", "finished", "N_1", "E_1", "EN_1", "N2_1", "E2_1", "gcmccount", "_"]
 
-    def __init__(self, slots=296, device=0, mem_budget=0, k_capacity=2400):
+    def __init__(self, slots=296, device=0, mem_budget=0, k_capacity=2400, voxel_edge=2.0):
+        """voxel_edge: neighbour-list voxel edge (A) of the request slots."""
         self.h = ctypes.c_void_p()
         check(lib().fmc_server_open(int(slots), int(device), int(mem_budget), int(k_capacity), ctypes.byref(self.h)))
+        check(lib().fmc_server_set_voxel_edge(self.h, float(voxel_edge)))
 
     def close(self):
         if self.h:

@@ -354,6 +354,10 @@ typedef struct fmc_server fmc_server;
 int fmc_server_open(int slots, int device, long long mem_budget, int k_capacity, fmc_server** out);
 void fmc_server_close(fmc_server* s);
 int fmc_server_submit(fmc_server* s, const char* dir, const int* seed, long long moves, int* request_id);
+/* Neighbour-list voxel edge (A, 1-4; 2 by default) of the slots of requests prepared after the
+ * call: coarser voxels mean fewer lists to build at admission and less slot memory, and more
+ * candidates per trial site. */
+int fmc_server_set_voxel_edge(fmc_server* s, double edge);
 int fmc_server_cancel(fmc_server* s, int request_id);
 /* One step of the pipelined server: queues the next launch of every running request (after the
  * uploads of the requests admitted by the previous step), then completes the launch queued by
