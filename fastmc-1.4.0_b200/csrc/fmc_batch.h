@@ -16,8 +16,6 @@ namespace fmc {
 constexpr int kBatchMaxSites = 16;  // sites per guest species on the batched path
 constexpr int kBatchMaxTypes = 16;  // unique atom types
 constexpr int kBatchMaxTab = kBatchMaxTypes * (kBatchMaxTypes + 1) / 2;
-constexpr int kBatchThreads = 256;
-
 // Tile shapes of the batched kernel the autotuner chooses among: threads per chain (CTA size),
 // k-vectors each thread takes per trip of the reciprocal loop (ewald.f:145-331) and neighbour
 // candidates per trip of the real-space loop (ewald.f:656-690, vdw_terms.f:455-495).  Tile 0

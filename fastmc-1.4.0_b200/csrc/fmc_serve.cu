@@ -873,6 +873,28 @@ struct fmc_server {
 
 extern "C" {
 
+int fmc_deck_footprint(const char* dir, double voxel_edge, long long* bytes, double* move_cost) {
+  if (!dir || !(voxel_edge >= 1.0 && voxel_edge <= 4.0)) {
+    fmc::set_last_error("bad deck directory or voxel edge (1-4 A)");
+    return -1;
+  }
+  fmc::HostSystem h;
+  std::string err;
+  int rc = fmc::prepare_system(dir, h, err, voxel_edge);
+  if (rc) {
+    fmc::set_last_error(err);
+    return rc;
+  }
+  if (bytes) *bytes = (long long)fmc::Server::slot_bytes_estimate(h);
+  if (move_cost) {
+    // algorithmic bytes of one move of an empty framework: S(k), akk and S_new (40 B a k-vector)
+    // and 4.5 sites' neighbours within rcut (36 B each)
+    const double nrc = (double)h.nf / h.cell.volm * (4.0 / 3.0 * fmc::kPi * h.rcut * h.rcut * h.rcut);
+    *move_cost = 40.0 * h.K + 4.5 * nrc * 36.0;
+  }
+  return 0;
+}
+
 int fmc_server_set_voxel_edge(fmc_server* s, double edge) {
   if (!s || !(edge >= 1.0 && edge <= 4.0)) {
     fmc::set_last_error("bad server handle or voxel edge (1-4 A)");

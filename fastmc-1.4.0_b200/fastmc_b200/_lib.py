@@ -136,6 +136,8 @@ SIGNATURES = {
     "fmc_server_poll_done": (_ci, [_vp, _ip, _ip, _dp, _ci, _ip]),
     "fmc_server_stats": (_ci, [_vp, _dp]),
     "fmc_server_set_voxel_edge": (_ci, [_vp, ctypes.c_double]),
+    "fmc_deck_footprint": (_ci, [ctypes.c_char_p, ctypes.c_double, ctypes.POINTER(ctypes.c_longlong),
+                                 ctypes.POINTER(ctypes.c_double)]),
     "fmc_server_memory": (_ci, [_vp, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
     "fmc_deck_vdw": (_ci, [ctypes.c_char_p, _ci, _dp, _ip]),
     "fmc_deck_inspect": (_ci, [ctypes.c_char_p, _ip, _dp, _ip, _dp, _dp, _dp, _ip, _ip]),

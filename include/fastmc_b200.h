@@ -358,6 +358,10 @@ int fmc_server_submit(fmc_server* s, const char* dir, const int* seed, long long
  * call: coarser voxels mean fewer lists to build at admission and less slot memory, and more
  * candidates per trial site. */
 int fmc_server_set_voxel_edge(fmc_server* s, double edge);
+/* Host only: a deck's device footprint as a serving slot or batched chain (*bytes, the estimate
+ * admission uses) and the algorithmic bytes of one of its moves (*move_cost), for placing
+ * chains and requests on GPUs by HBM footprint and load (fastmc_b200.placement). */
+int fmc_deck_footprint(const char* dir, double voxel_edge, long long* bytes, double* move_cost);
 int fmc_server_cancel(fmc_server* s, int request_id);
 /* One step of the pipelined server: queues the next launch of every running request (after the
  * uploads of the requests admitted by the previous step), then completes the launch queued by
