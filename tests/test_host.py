@@ -132,3 +132,27 @@ def test_host_voxel_lists_are_ascending_and_complete(fmc, decks):
         seg = atoms[off[v]:off[v + 1]]
         assert np.all(np.diff(seg) > 0)
     assert len(np.unique(atoms)) == info["nframework"]
+
+
+def test_deck_reader_line_endings(fmc, decks, tmp_path):
+    """The reader takes each file whole and splits it the way line-by-line reading does: CRLF
+    line endings and a last line without a newline give the same deck, table for table."""
+    src = decks["small"]
+    dst = tmp_path / "crlf"
+    dst.mkdir()
+    for name in ("CONTROL", "FIELD", "CONFIG"):
+        text = open(os.path.join(src, name)).read()
+        crlf = text.replace("\n", "\r\n")
+        if name == "CONFIG":
+            crlf = crlf.rstrip("\r\n")  # no newline after the last record
+        (dst / name).write_bytes(crlf.encode())
+    a, b = fmc.deck_inspect(src), fmc.deck_inspect(str(dst))
+    for k in ("K", "natoms", "nframework", "ntypes", "mxgrid", "nvoxels"):
+        assert a[k] == b[k], k
+    for k in ("alpha", "rcut", "volm", "temp", "beta"):
+        assert a[k] == b[k], k
+    for k in ("lmn", "akk", "erc", "charges"):
+        assert np.array_equal(a[k], b[k]), k
+    nv_a, off_a, at_a = fmc.deck_voxels(src, 2.0)
+    nv_b, off_b, at_b = fmc.deck_voxels(str(dst), 2.0)
+    assert nv_a == nv_b and np.array_equal(off_a, off_b) and np.array_equal(at_a, at_b)
