@@ -20,13 +20,6 @@ def _tile_index(fmc, shape):
     return fmc.batch_tiles().index(shape)
 
 
-def test_tile_table(fmc):
-    tiles = fmc.batch_tiles()
-    assert tiles[0] == (256, 1, 1)
-    assert len(set(tiles)) == len(tiles)
-    assert {t[0] for t in tiles} == {128, 256, 384}
-
-
 @pytest.mark.parametrize("shape", [(128, 1, 1), (384, 2, 2), (256, 2, 2), (128, 2, 2)])
 def test_non_default_tile_replays_oracle(fmc, oracle_mod, decks, shape):
     dirs = [decks[n] for n in NAMES]

@@ -156,3 +156,13 @@ def test_deck_reader_line_endings(fmc, decks, tmp_path):
     nv_a, off_a, at_a = fmc.deck_voxels(src, 2.0)
     nv_b, off_b, at_b = fmc.deck_voxels(str(dst), 2.0)
     assert nv_a == nv_b and np.array_equal(off_a, off_b) and np.array_equal(at_a, at_b)
+
+
+def test_batch_tile_table(fmc):
+    """The batched kernel's tile shapes (host only): tile 0 the default, every shape once, the
+    thread counts the autotuner chooses among."""
+    tiles = fmc.batch_tiles()
+    assert tiles[0] == (256, 1, 1)
+    assert len(set(tiles)) == len(tiles) == 12
+    assert {t[0] for t in tiles} == {128, 256, 384}
+    assert {t[1] for t in tiles} == {1, 2} and {t[2] for t in tiles} == {1, 2}
