@@ -166,3 +166,30 @@ def test_batch_tile_table(fmc):
     assert len(set(tiles)) == len(tiles) == 12
     assert {t[0] for t in tiles} == {128, 256, 384}
     assert {t[1] for t in tiles} == {1, 2} and {t[2] for t in tiles} == {1, 2}
+
+
+def test_deck_reader_matches_oracle_parser_on_random_decks(fmc, oracle_mod, tmp_path):
+    """The library's deck reader (whole-file reads, correctly rounded coordinate parsing) against
+    the oracle's own restatement of readinputs.f on request decks of random size, gas and
+    conditions: framework coordinates, charges, k-vectors and erfc table bit for bit."""
+    from fastmc_b200 import synth
+
+    for r in synth.serving_requests(12, seed=23):
+        r["natoms"] = min(r["natoms"], 1500)  # keep the oracle's set-up quick
+        r["edge"] = max((r["natoms"] / 0.025) ** (1.0 / 3.0), 25.2)
+        d = synth.write_request(str(tmp_path / f"r{r['id']}"), r)
+        desc = fmc.SystemDesc.from_deck(d)
+        nf = desc.s.nframework
+        xyz = np.ctypeslib.as_array(desc.s.fw_xyz, shape=(3 * nf,)).reshape(nf, 3)
+        q = np.ctypeslib.as_array(desc.s.fw_charge, shape=(nf,))
+        orc = oracle_mod.Chain(d)
+        oxyz, oq, _, _ = orc.atoms()
+        assert np.array_equal(xyz, oxyz[len(oq) - nf:]), r["id"]
+        assert np.array_equal(q, oq[len(oq) - nf:]), r["id"]
+        info = fmc.deck_inspect(d)
+        lmn, akk = orc.kvectors()
+        assert np.array_equal(info["lmn"], lmn) and np.array_equal(info["akk"], akk)
+        assert np.array_equal(info["erc"], orc.erc())
+        s = orc.scalars()
+        for k in ("temp", "alpha", "rcut", "volm", "beta", "statvolm"):
+            assert info[k] == s[k], (r["id"], k)
