@@ -35,18 +35,46 @@ int fmc_version(void) { return 10400; }
 
 const char* fmc_last_error(void) { return g_err.c_str(); }
 
-int fmc_chain_open(const char* dir, const int* seed, int device, fmc_chain** out) {
+int fmc_chain_open_node(const char* dir, const int* seed, int device, int idnode, fmc_chain** out) {
   if (!dir || !seed || !out) return fail(-1, "null argument");
+  *out = nullptr;
   fmc_chain* c = new fmc_chain();
   std::string err;
   int rc = c->impl.open(dir, seed, device, err);
+  // CONTROL `restart`: this node's branch REVIVE, read after duni is seeded as gcmc.f:334-394
+  // does (a single point never continues a run)
+  const fmc::InputDeck& d = c->impl.sys.deck;
+  if (!rc && d.lrestart && !d.lspe) {
+    fmc::BranchChoice b;
+    rc = fmc::choose_branch(dir, idnode, b, err);
+    fmc::Revive r;
+    if (!rc && !b.revive.empty()) rc = fmc::read_revive(b.revive, d, r, err);
+    if (!rc && !b.revive.empty()) rc = c->impl.restart(r, err);
+  }
   if (rc) {
     delete c;
-    *out = nullptr;
     return fail(rc, err);
   }
   *out = c;
   return 0;
+}
+
+int fmc_chain_open(const char* dir, const int* seed, int device, fmc_chain** out) {
+  return fmc_chain_open_node(dir, seed, device, 0, out);
+}
+
+int fmc_restart_branch(const char* workdir, int idnode, char* revive_path, int revive_cap, char* outdir,
+                       int outdir_cap, int* prevnodes) {
+  if (!workdir || (!revive_path && revive_cap) || (!outdir && outdir_cap)) return fail(-1, "bad arguments");
+  fmc::BranchChoice b;
+  std::string err;
+  if (int rc = fmc::choose_branch(workdir, idnode, b, err)) return fail(rc, err);
+  if ((revive_path && (int)b.revive.size() >= revive_cap) || (outdir && (int)b.outdir.size() >= outdir_cap))
+    return fail(-1, "path buffer too small");
+  if (revive_path) std::memcpy(revive_path, b.revive.c_str(), b.revive.size() + 1);
+  if (outdir) std::memcpy(outdir, b.outdir.c_str(), b.outdir.size() + 1);
+  if (prevnodes) *prevnodes = b.prevnodes;
+  return b.revive.empty() ? 0 : 1;
 }
 
 void fmc_chain_close(fmc_chain* c) { delete c; }

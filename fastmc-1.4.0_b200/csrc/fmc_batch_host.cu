@@ -592,6 +592,30 @@ struct fmc_batch {
   fmc::Batch impl;
 };
 
+namespace {
+
+// CONTROL `restart` on a batch: the chains opened from one deck directory are that job's
+// nodes, numbered in the order they appear; each reads its branch REVIVE (gcmc.f:353-394)
+// before its first run, as fmc_batch_restart does.
+int restart_from_branches(fmc::Batch& B, const std::vector<std::string>& dirs, std::string& err) {
+  std::map<std::string, int> seen;
+  for (int c = 0; c < B.nchains; c++) {
+    const int node = seen[dirs[c]]++;
+    const fmc::InputDeck& d = B.sys_chains[B.chain_sys[c]]->sys.deck;
+    if (!d.lrestart || d.lspe) continue;
+    fmc::BranchChoice ch;
+    int rc = fmc::choose_branch(dirs[c], node, ch, err);
+    if (!rc && !ch.revive.empty()) rc = B.restart(c, ch.revive, err);
+    if (rc) {
+      err = dirs[c] + ": " + err;
+      return rc;
+    }
+  }
+  return 0;
+}
+
+}  // namespace
+
 extern "C" {
 
 int fmc_batch_control_block_bytes(void) { return (int)sizeof(fmc::ChainDev); }
@@ -607,6 +631,7 @@ int fmc_batch_open(int nchains, const char* const* dirs, const int* seeds, int d
   std::vector<int> s(seeds, seeds + 4 * nchains);
   std::string err;
   int rc = b->impl.open(d, s, device, err);
+  if (!rc) rc = restart_from_branches(b->impl, d, err);
   if (rc) {
     delete b;
     *out = nullptr;
@@ -628,6 +653,7 @@ int fmc_batch_open_edge(int nchains, const char* const* dirs, const int* seeds, 
   std::vector<int> s(seeds, seeds + 4 * nchains);
   std::string err;
   int rc = b->impl.open(d, s, device, err, voxel_edge);
+  if (!rc) rc = restart_from_branches(b->impl, d, err);
   if (rc) {
     delete b;
     *out = nullptr;

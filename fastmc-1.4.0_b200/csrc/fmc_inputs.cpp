@@ -663,7 +663,7 @@ void read_control(const std::string& dir, InputDeck& d) {
     r.strip();
     if (r.blank_or_comment()) continue;
     if (r.has("restart")) {
-      raise(-2, "restart from branch directories is handled by the chain snapshot API, not CONTROL");
+      d.lrestart = true;
     } else if (r.has("temp")) {
       d.temp = r.take_double();
       ltemp = true;

@@ -70,6 +70,9 @@ struct InputDeck {
   double despre = 0, packf = 0;
   std::vector<double> adspres, adsguen;
   bool laccsample = false, lspe = false;
+  // CONTROL `restart` (readinputs.f:604-608): continue from the REVIVE of this chain's branch
+  // directory beside the deck (gcmc.f:353-418; choose_branch in fmc_restart.h)
+  bool lrestart = false;
   std::vector<double> press;  // Pa, per guest
   std::vector<std::array<double, 9>> movefreq;  // ins,del,dis,jmp,flx,swp,tra,rot,mjp (raw)
   std::vector<double> disp_ratio, tran_ratio;
@@ -77,8 +80,7 @@ struct InputDeck {
 };
 
 // Reads dir/{CONTROL,FIELD,CONFIG}.  Returns 0, or the reference's error code (>0); `err`
-// receives a message.  Directives outside this path (the restart scan) are rejected with a
-// negative code.
+// receives a message.  Directives outside this path are rejected with a negative code.
 int read_input_deck(const std::string& dir, InputDeck& deck, std::string& err);
 
 // A deck whose arrays a caller filled in memory (the state the reference's module arrays hold

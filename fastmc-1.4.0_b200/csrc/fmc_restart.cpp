@@ -1,6 +1,9 @@
 // REVIVE / REVCON in the reference's formats (revive, revread: utility_pack.f:1772-1878).
 #include "fmc_restart.h"
 
+#include <dirent.h>
+#include <sys/stat.h>
+
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -421,6 +424,31 @@ std::vector<std::vector<double>> revive_guest_xyz(const InputDeck& d, const Revi
     }
   }
   return out;
+}
+
+int choose_branch(const std::string& workdir, int idnode, BranchChoice& out, std::string& err) {
+  out = BranchChoice();
+  if (idnode < 0 || idnode > 98) {
+    err = "node index outside 0-98 (branch directories are named branch01-branch99)";
+    return -1;
+  }
+  // `ls | grep -c branch`: every listed name (not the hidden ones) that contains "branch"
+  if (DIR* dp = opendir(workdir.c_str())) {
+    while (dirent* e = readdir(dp))
+      if (e->d_name[0] != '.' && std::strstr(e->d_name, "branch")) out.prevnodes++;
+    closedir(dp);
+  }
+  auto branch = [&](int n) {
+    char b[16];
+    std::snprintf(b, sizeof(b), "branch%02d", n);
+    return workdir + "/" + b;
+  };
+  out.outdir = branch(idnode + 1);
+  if (out.prevnodes == 0) return 0;
+  const std::string local = idnode + 1 > out.prevnodes ? branch((idnode + 1) % out.prevnodes + 1) : out.outdir;
+  struct stat sb;
+  if (stat((local + "/REVIVE").c_str(), &sb) == 0 && S_ISREG(sb.st_mode)) out.revive = local + "/REVIVE";
+  return 0;
 }
 
 }  // namespace fmc

@@ -65,6 +65,21 @@ void window_stats_out(const WindowStats& W, int ng, double* out);
 int write_report(const std::string& path, const InputDeck& d, const double* final_cs, const WindowStats& W,
                  double temp, std::string& err);
 
+// Where node `idnode` (0-based) of a job whose CONTROL says `restart` takes its state from
+// (gcmc.f:353-394): prevnodes counts the entries of `workdir` whose names contain "branch" (revscan,
+// utility_pack.f:1819-1839, lists the working directory); with none the node starts from the
+// CONFIG; node idnode < prevnodes reads branch{idnode+1}/REVIVE, a node beyond them
+// branch{mod(idnode+1, prevnodes)+1}/REVIVE; a missing REVIVE also means the CONFIG (revread's
+// status-old test, utility_pack.f:1855-1860).  The node's own output directory is
+// branch{idnode+1} either way.
+struct BranchChoice {
+  int prevnodes = 0;
+  std::string outdir;  // workdir/branchNN of this node
+  std::string revive;  // the REVIVE to read, or empty: start from the CONFIG
+};
+// 0, or -1 with a message for a node index beyond the reference's two-digit branch names.
+int choose_branch(const std::string& workdir, int idnode, BranchChoice& out, std::string& err);
+
 // Per-species interleaved guest coordinates of a REVIVE.
 std::vector<std::vector<double>> revive_guest_xyz(const InputDeck& d, const Revive& r);
 

@@ -27,6 +27,7 @@
 
 #include "../../include/fastmc_b200.h"
 #include "fmc_batch.h"
+#include "fmc_restart.h"
 
 namespace fmc {
 void set_last_error(const std::string& msg);
@@ -288,6 +289,15 @@ class Server {
           rc = -8;
           err = "serving starts chains from an empty framework (NUMMOLS 0 for guests)";
         }
+    if (!rc && h->deck.lrestart && !h->deck.lspe) {
+      // CONTROL `restart` with a branch REVIVE beside the deck would continue from its guests
+      BranchChoice b;
+      rc = choose_branch(r.dir, 0, b, err);
+      if (!rc && !b.revive.empty()) {
+        rc = -8;
+        err = "serving starts chains from an empty framework (CONTROL restart finds " + b.revive + ")";
+      }
+    }
     if (!rc && h->K > kcap) {
       rc = -9;
       err = "the request's k-vector count exceeds the server's capacity";

@@ -214,13 +214,16 @@ class Chain:
     """One GCMC chain on one GPU (the plain FP64 path), opened from a deck directory or created
     from a SystemDesc."""
 
-    def __init__(self, directory, seed=(12, 34, 56, 78), device=0):
+    def __init__(self, directory, seed=(12, 34, 56, 78), device=0, node=0):
+        """node: this chain's node index (0-based) in a job run from one deck directory; only a
+        CONTROL `restart` reads it, to pick the branch REVIVE to continue from (restart_branch)."""
         self.h = ctypes.c_void_p()
         s = np.asarray(seed, dtype=np.int32)
         if isinstance(directory, SystemDesc):
             check(lib().fmc_chain_create(ctypes.byref(directory.s), ip(s), int(device), ctypes.byref(self.h)))
         else:
-            check(lib().fmc_chain_open(str(directory).encode(), ip(s), int(device), ctypes.byref(self.h)))
+            check(lib().fmc_chain_open_node(str(directory).encode(), ip(s), int(device), int(node),
+                                            ctypes.byref(self.h)))
 
     def close(self):
         if self.h:
@@ -657,6 +660,17 @@ def write_revive_state(deck_dir, outdir, guests, production=False, chainstats=No
     en = np.ascontiguousarray(energy if energy is not None else np.zeros(ng), dtype=np.float64)
     check(lib().fmc_revive_write_state(str(deck_dir).encode(), str(outdir).encode(), int(bool(production)), ip(nmol),
                                        dp(xyz), dp(cs), dp(en), float(eng)))
+
+
+def restart_branch(workdir, node=0):
+    """The branch choice of CONTROL `restart` for node `node` (gcmc.f:353-394): a dict with the
+    REVIVE to continue from (None: start from the CONFIG), the node's output directory and the
+    number of branch entries found."""
+    rev, out, prev = ctypes.create_string_buffer(4096), ctypes.create_string_buffer(4096), ctypes.c_int()
+    rc = lib().fmc_restart_branch(str(workdir).encode(), int(node), rev, 4096, out, 4096, ctypes.byref(prev))
+    check(rc if rc < 0 else 0)
+    return {"revive": rev.value.decode() if rc == 1 else None, "outdir": out.value.decode(),
+            "prevnodes": prev.value}
 
 
 def _species_sites(deck_dir, g):

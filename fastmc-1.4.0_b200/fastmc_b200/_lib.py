@@ -58,6 +58,8 @@ SIGNATURES = {
     "fmc_version": (_ci, []),
     "fmc_last_error": (ctypes.c_char_p, []),
     "fmc_chain_open": (_ci, [ctypes.c_char_p, _ip, _ci, ctypes.POINTER(_vp)]),
+    "fmc_chain_open_node": (_ci, [ctypes.c_char_p, _ip, _ci, _ci, ctypes.POINTER(_vp)]),
+    "fmc_restart_branch": (_ci, [ctypes.c_char_p, _ci, ctypes.c_char_p, _ci, ctypes.c_char_p, _ci, _ip]),
     "fmc_chain_resident": (_ci, [_vp, _ci, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]),
     "fmc_chain_close": (None, [_vp]),
     "fmc_chain_create": (_ci, [ctypes.POINTER(SystemDescStruct), _ip, _ci, ctypes.POINTER(_vp)]),

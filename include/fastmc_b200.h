@@ -45,8 +45,24 @@ const char* fmc_last_error(void);
 /* Reads dir/CONTROL, dir/FIELD and dir/CONFIG (readinputs.f:11-914, utility_pack.f:176-457),
  * builds the tables (erfcgen ewald.f:1; forgen vdw_terms.f:189), uploads the rigid framework,
  * computes the single-point energy (gcmc.f:2518-2710) and S(k) of all atoms (gcmc.f:522), and
- * seeds duni (gcmc.f:2712) with seed[0..3] = the (i,j,k,l) the reference prints. */
+ * seeds duni (gcmc.f:2712) with seed[0..3] = the (i,j,k,l) the reference prints.  When CONTROL
+ * says `restart` (readinputs.f:604-608) the chain is node 0 of its job and continues from the
+ * REVIVE fmc_restart_branch picks beside the deck, as fmc_chain_restart would. */
 int fmc_chain_open(const char* dir, const int* seed, int device, fmc_chain** out);
+/* fmc_chain_open as node `idnode` (0-based; the reference's MPI rank) of a job run from one deck
+ * directory: only a CONTROL `restart` reads it, to pick the node's branch (gcmc.f:353-394). */
+int fmc_chain_open_node(const char* dir, const int* seed, int device, int idnode, fmc_chain** out);
+/* The branch choice of CONTROL `restart` (gcmc.f:353-394 with revscan, utility_pack.f:1819-1839):
+ * prevnodes = the entries of `workdir` whose names contain "branch"; node idnode reads
+ * branch{idnode+1}/REVIVE when idnode < prevnodes, else branch{mod(idnode+1, prevnodes)+1}/REVIVE,
+ * and starts from the CONFIG when there are no branches or that REVIVE does not exist (revread,
+ * utility_pack.f:1855-1860).  Writes the REVIVE's path ("" for the CONFIG) and the node's output
+ * directory workdir/branch{idnode+1} (NUL-terminated; either buffer may be NULL with cap 0) and
+ * *prevnodes (may be NULL).  Returns 1 when a REVIVE is read, 0 when the node starts from the
+ * CONFIG, < 0 for bad arguments, idnode outside 0-98 or a buffer too small.  A batch
+ * (fmc_batch_open) numbers the chains of one deck directory 0, 1, ... in order as its nodes. */
+int fmc_restart_branch(const char* workdir, int idnode, char* revive_path, int revive_cap, char* outdir,
+                       int outdir_cap, int* prevnodes);
 /* Passes of up to 8-site molecules run through a resident kernel (no counterpart in the
  * reference): it stays on the GPU while passes keep coming, takes each from pinned host memory
  * and ends after ~20 ms without one; the next pass starts it again.  enable 1 / 0 turns it on /

@@ -423,7 +423,7 @@ struct Chain {
   std::vector<double> erc;  // [0..mxegrd]
   // ---- readcontrol
   double temp = 0;
-  bool ltemp = false, lspe = false, laccsample = false;
+  bool ltemp = false, lspe = false, laccsample = false, lrestart = false;
   int mcsteps = 1, eqsteps = 0, nwind = 100000;
   // numguests.out / his.xyz (readinputs.f:708-717, 860-866; gcmc.f:418-450, 785-792, 1937-1951)
   int nnumg = 1, nhis = 0;
@@ -1028,7 +1028,9 @@ static void readcontrol(Chain& C, const std::string& dir) {
     char* d = r.c;  // "directive" is a copy of the record
     if (d[0] == '#' || d[0] == ' ') {
     } else if (findstring("restart", d)) {
-      fail(-2, "restart from branch directories is not part of this restatement");
+      // readinputs.f:604-608; the branch REVIVE itself is loaded by the caller (load_guests +
+      // orc_restart_flags), as gcmc.f:353-418 does after the deck is read
+      C.lrestart = true;
     } else if (findstring("temp", d)) {
       C.temp = dblstr(d, LENREC);
       C.ltemp = true;

@@ -6,6 +6,7 @@ from the golden fixture).  After a restart the move sequence must be the oracle'
 restart (guests loaded, fresh single point, production flag and chain statistics restored)."""
 import json
 import os
+import shutil
 
 import numpy as np
 import pytest
@@ -82,3 +83,26 @@ def test_batch_checkpoint_restarts_on_the_plain_path(fmc, oracle_mod, revive, tm
     sp = c.info()["spenergy"]
     assert abs(sp - orc.scalars()["spenergy"]) <= REL * abs(sp)
     assert os.path.getsize(tmp_path / "REVCON") > 0
+
+
+def test_control_restart_reads_the_branch_revive(fmc, oracle_mod, revive, tmp_path):
+    """A deck whose CONTROL says `restart` continues from branch01/REVIVE beside it on both paths
+    (gcmc.f:353-418): the plain chain (node 0) and both chains of a batch opened from that deck
+    (node 1 of a run that left one branch reads branch01 too) follow the oracle's restarted chain."""
+    from test_restart_branch import restart_deck
+
+    path, guests, exp = revive
+    work = restart_deck(tmp_path / "job")
+    os.makedirs(os.path.join(work, "branch01"))
+    shutil.copy(path, os.path.join(work, "branch01", "REVIVE"))
+    c = fmc.Chain(work, seed=SEED)
+    assert c.guest_coords(0).shape[0] == len(guests)
+    _compare_traces(c.run(400), _oracle_restart(oracle_mod, guests, exp).run(400))
+    b = fmc.Batch([work, work], [SEED, (1, 2, 3, 4)])
+    assert b.state(0)["nmol0"] == len(guests) and b.state(1)["nmol0"] == len(guests)
+    tr, _ = b.run(400, trace=True)
+    _compare_traces(tr[0], _oracle_restart(oracle_mod, guests, exp).run(400))
+    _compare_traces(tr[1], _oracle_restart(oracle_mod, guests, exp, seed=(1, 2, 3, 4)).run(400))
+    # without a branch REVIVE the deck starts from its CONFIG, like the deck without the directive
+    empty = restart_deck(tmp_path / "fresh")
+    assert fmc.Chain(empty, seed=SEED).guest_coords(0).shape[0] == 0
