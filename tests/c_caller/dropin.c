@@ -29,11 +29,18 @@ int main(int argc, char** argv) {
     rc = fmc_deck_footprint(deck, 2.0, &bytes, &cost);
     if (rc) return fail("fmc_deck_footprint", rc);
     int nt = fmc_batch_tiles(NULL, NULL, NULL, 0);
+    /* where node 0 would continue from if CONTROL said `restart` */
+    char revive[1024], outdir[1024];
+    int prev = -1;
+    int restart_rc = fmc_restart_branch(deck, 0, revive, (int)sizeof(revive), outdir, (int)sizeof(outdir), &prev);
+    if (restart_rc < 0) return fail("fmc_restart_branch", restart_rc);
     /* a directory that holds no deck: an error code and a message, no crash */
     rc = fmc_deck_inspect("/nonexistent-deck-directory", ints, dbls, NULL, NULL, NULL, NULL, &K, &nerc);
     printf("{\"K\": %d, \"nerc\": %d, \"imcon\": %d, \"bytes\": %lld, \"move_cost\": %.6f, \"tiles\": %d, "
+           "\"restart_rc\": %d, \"prevnodes\": %d, \"revive\": \"%s\", \"outdir\": \"%s\", "
            "\"missing_rc\": %d, \"missing_msg\": %d}\n",
-           K, nerc, ints[0], bytes, cost, nt, rc, (int)(strlen(fmc_last_error()) > 0));
+           K, nerc, ints[0], bytes, cost, nt, restart_rc, prev, revive, outdir, rc,
+           (int)(strlen(fmc_last_error()) > 0));
     return 0;
   }
   if (strcmp(argv[1], "chain") == 0) {

@@ -1,7 +1,7 @@
 """The drop-in ABI from a C program (tests/c_caller/dropin.c): compiled against
 include/fastmc_b200.h alone and linked to the library, as a C host or a Fortran code through
-bind(C) would use it.  On the host: the deck tables, the footprint, the tile list and the error
-path; on the GPU: one insertion pass and its commit, equal to the same calls through Python."""
+bind(C) would use it.  On the host: the deck tables, the footprint, the tile list, the restart
+branch choice and the error path; on the GPU: one insertion pass and its commit, equal to the same calls through Python."""
 import json
 import os
 import shutil
@@ -42,6 +42,9 @@ def test_c_caller_host_entry_points(fmc, decks, dropin, name):
     b, c = placement.footprint(decks[name])
     assert got["bytes"] == b and abs(got["move_cost"] - c) <= 1e-6 * c
     assert got["tiles"] == len(fmc.batch_tiles())
+    br = fmc.restart_branch(decks[name], 0)
+    assert got["restart_rc"] == (br["revive"] is not None) and got["prevnodes"] == br["prevnodes"]
+    assert got["revive"] == (br["revive"] or "") and got["outdir"] == br["outdir"]
     assert got["missing_rc"] != 0 and got["missing_msg"] == 1
 
 
