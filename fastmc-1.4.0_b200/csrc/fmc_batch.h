@@ -159,14 +159,30 @@ size_t slot_staging_bytes(const HostSystem& h);
 // Voxel-list entries of a system estimated from its framework density (+15% and 4096).
 long long slot_voxel_capacity(const HostSystem& h);
 
+// A slot that starts with guests instead of the empty framework: the guests the deck preloads
+// (FIELD NUMMOLS > 0), or a REVIVE's (CONTROL `restart`), with the S(k) of every atom and the
+// single-point energy (gcmc.f:500-556) that a chain opened on the same deck computed, all in
+// host memory.  From a REVIVE also its production flag and chain statistics (gcmc.f:396-409).
+struct SlotStart {
+  std::vector<double2> sk;                  // K entries
+  double spenergy = 0.0;                    // kcal/mol, every species' starting energy
+  std::vector<int> nmol;                    // per species
+  std::vector<std::vector<double4>> sites;  // per species, nmol * nsite sites (x, y, z, q)
+  std::vector<std::vector<int>> types;      // per species, their atom types
+  bool from_revive = false;
+  bool production = false;
+  std::vector<double> chainstats;           // 1 + 14 * species
+};
+
 // A serving slot built from a prepared host system: the device system (framework, voxel lists,
-// tables), the framework S(k), the per-system constants and an empty chain, all enqueued on
+// tables), the framework S(k), the per-system constants and an empty chain (or one starting
+// from `start`, whose host arrays the call copies before it returns), all enqueued on
 // mem.st without waiting (one staged host-to-device copy; voxel lists sized by vox_cap entries,
 // the exact count copied to *vox_total, pinned, for the caller to check once mem.st has
 // drained: a total above vox_cap means the lists are cut and the slot must be rebuilt with
 // vox_cap = total).
 int build_slot(const HostSystem& h, int slot, const int seed[4], SlotMemory& mem, Staging& stg, long long vox_cap,
-               int* vox_total, SysConst& Y, ChainDev& C, std::string& err);
+               int* vox_total, SysConst& Y, ChainDev& C, std::string& err, const SlotStart* start = nullptr);
 
 class Batch {
  public:

@@ -66,6 +66,7 @@ class Server {
     int prep_rc = 0;
     std::string prep_err;
     std::unique_ptr<HostSystem> host;
+    std::unique_ptr<SlotStart> start;  // null: the empty framework
     size_t bytes_estimate = 0;
     // the device slot a worker built ahead of admission (null: built at admission instead)
     std::unique_ptr<struct Prebuilt> pre;
@@ -283,20 +284,11 @@ class Server {
     auto h = std::make_unique<HostSystem>();
     std::string err;
     int rc = prepare_system(r.dir, *h, err, voxel_edge.load());
-    if (!rc)
-      for (auto& g : h->deck.guests)
-        if (g.nmols) {
-          rc = -8;
-          err = "serving starts chains from an empty framework (NUMMOLS 0 for guests)";
-        }
+    std::string revive;  // CONTROL `restart`: the REVIVE of branch01 beside the deck, if any
     if (!rc && h->deck.lrestart && !h->deck.lspe) {
-      // CONTROL `restart` with a branch REVIVE beside the deck would continue from its guests
       BranchChoice b;
       rc = choose_branch(r.dir, 0, b, err);
-      if (!rc && !b.revive.empty()) {
-        rc = -8;
-        err = "serving starts chains from an empty framework (CONTROL restart finds " + b.revive + ")";
-      }
+      revive = b.revive;
     }
     if (!rc && h->K > kcap) {
       rc = -9;
@@ -312,6 +304,9 @@ class Server {
           rc = -9;
           err = "a guest of the request has more sites than the server's capacity";
         }
+    bool preloaded = false;
+    for (auto& g : h->deck.guests) preloaded = preloaded || g.nmols > 0;
+    if (!rc && (preloaded || !revive.empty())) rc = start_state(r, revive, err);
     r.prep_rc = rc;
     r.prep_err = err;
     const double t1 = now_ms();
@@ -326,6 +321,50 @@ class Server {
     }
     prep_us += (long long)((now_ms() - t0) * 1000.0);
     r.prepared.store(1, std::memory_order_release);
+  }
+
+  // The state a request with guests starts from (the deck's preloaded guests, or the REVIVE of
+  // its CONTROL `restart`): a plain chain opened on the deck at the server's voxel edge computes
+  // the single point and S(k) of every atom on the device, as the batched path's own chain
+  // does; its results and guest sites are kept in host memory and the chain is closed.
+  int start_state(Request& r, const std::string& revive, std::string& err) {
+    Chain ch;
+    int rc = ch.open(r.dir, r.seed, device, err, voxel_edge.load());
+    Revive rv;
+    if (!rc && !revive.empty()) rc = read_revive(revive, ch.sys.deck, rv, err);
+    if (!rc && !revive.empty()) rc = ch.restart(rv, err);
+    if (rc) return rc;
+    auto S = std::make_unique<SlotStart>();
+    const InputDeck& d = ch.sys.deck;
+    S->sk.resize(ch.sys.K);
+    cudaError_t e = cudaStreamSynchronize(ch.st);
+    if (e == cudaSuccess && ch.sys.K)
+      e = cudaMemcpy(S->sk.data(), ch.sk, sizeof(double2) * ch.sys.K, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) {
+      err = std::string("start state read-back failed: ") + cudaGetErrorString(e);
+      return -100 - (int)e;
+    }
+    S->spenergy = ch.spenergy;
+    for (size_t g = 0; g < ch.sp.size(); g++) {
+      const GuestSpecies& G = d.guests[g];
+      const int n = ch.sp[g].nmol * G.nsite;
+      S->nmol.push_back(ch.sp[g].nmol);
+      S->sites.emplace_back(n);
+      S->types.emplace_back(n);
+      for (int i = 0; i < n; i++) {
+        const double* x = &ch.sp[g].xyz[3 * i];
+        S->sites[g][i] = make_double4(x[0], x[1], x[2], G.charge[i % G.nsite]);
+        S->types[g][i] = G.type[i % G.nsite];
+      }
+    }
+    if (!revive.empty()) {
+      S->from_revive = true;
+      S->production = rv.production;
+      S->chainstats = rv.chainstats;
+      if ((int)S->chainstats.size() != 1 + 14 * (int)d.guests.size()) S->chainstats.assign(1 + 14 * d.guests.size(), 0.0);
+    }
+    r.start = std::move(S);
+    return 0;
   }
 
   // A worker enqueues the request's device slot on its own stream, while the memory budget
@@ -368,7 +407,7 @@ class Server {
     std::string err;
     sg.used = 0;
     P->vox_cap = slot_voxel_capacity(*r.host);
-    ok = ok && build_slot(*r.host, 0, r.seed, P->mem, sg, P->vox_cap, P->vox_total, P->Y, P->C, err) == 0;
+    ok = ok && build_slot(*r.host, 0, r.seed, P->mem, sg, P->vox_cap, P->vox_total, P->Y, P->C, err, r.start.get()) == 0;
     ok = ok && cudaEventCreateWithFlags(&P->done, cudaEventDisableTiming) == cudaSuccess &&
          cudaEventRecord(P->done, w.st) == cudaSuccess;
     w.stage_busy[k] = cudaEventRecord(w.stage_done[k], w.st) == cudaSuccess;
@@ -544,6 +583,7 @@ class Server {
     r.err = err;
     r.result[1] = rc;
     r.host.reset();
+    r.start.reset();
     for (int id = (int)reqs.size() - 1; id >= 0; id--)
       if (reqs[id].get() == &r) {
         done_log.push_back(id);
@@ -578,6 +618,7 @@ class Server {
         h_chains[i] = P->C;
         h_chains[i].sys = i;
         r.host.reset();
+        r.start.reset();
         s.request = id;
         s.fresh = false;  // its lists were checked above
         fresh.push_back(i);
@@ -608,7 +649,8 @@ class Server {
     s.vox_cap = vox_cap;
     s.mem.st = st2;  // the admission stream, which settle_admissions and the next launch wait for
     s.mem.pool = pool;
-    int rc = build_slot(*r.host, i, r.seed, s.mem, stage, s.vox_cap, &h_vox_total[i], h_sys[i], h_chains[i], err);
+    int rc = build_slot(*r.host, i, r.seed, s.mem, stage, s.vox_cap, &h_vox_total[i], h_sys[i], h_chains[i], err,
+                        r.start.get());
     if (rc) {
       s.mem.release();
       std::memset(&h_chains[i], 0, sizeof(ChainDev));
@@ -714,7 +756,8 @@ class Server {
         s.mem.release();
         s.vox_cap = h_vox_total[i];
         std::string e2;
-        int rc = build_slot(*r.host, i, r.seed, s.mem, stage, s.vox_cap, &h_vox_total[i], h_sys[i], h_chains[i], e2);
+        int rc = build_slot(*r.host, i, r.seed, s.mem, stage, s.vox_cap, &h_vox_total[i], h_sys[i], h_chains[i], e2,
+                            r.start.get());
         if (rc == 0 && cudaStreamSynchronize(st2) != cudaSuccess) rc = -100;
         stage.used = 0;
         if (rc || (long long)h_vox_total[i] > s.vox_cap) {
@@ -729,6 +772,7 @@ class Server {
         used += s.mem.bytes;
       }
       r.host.reset();
+      r.start.reset();
     }
     return 0;
   }

@@ -76,6 +76,55 @@ struct Parts {
   }
 };
 
+// The guests a slot starts with, over the chain state init_chain_state enqueued (framework
+// S(k), no guests): S(k) of every atom and the sites, copied from pageable host memory in stream
+// order (each copy has read its source when it returns), and the control block's counts.  The
+// counts follow the batched path's preloaded guests (init_chain) and REVIVE restart
+// (Batch::restart, gcmc.f:396-409, 547-556).
+int load_slot_start(const HostSystem& h, const SlotStart& s, ChainDev& C, cudaStream_t st, std::string& err) {
+  const InputDeck& d = h.deck;
+  const int ng = (int)d.guests.size();
+  if ((int)s.sk.size() != h.K || (int)s.nmol.size() != ng || (int)s.sites.size() != ng || (int)s.types.size() != ng ||
+      (s.from_revive && (int)s.chainstats.size() != 1 + 14 * ng)) {
+    err = "slot start state does not match the deck";
+    return -12;
+  }
+  for (int g = 0; g < ng; g++)
+    if (s.nmol[g] * d.guests[g].nsite > C.seg_cap[g] || (int)s.sites[g].size() != s.nmol[g] * d.guests[g].nsite ||
+        s.types[g].size() != s.sites[g].size()) {
+      err = "guests of the start state exceed the chain's capacity (max guest atoms)";
+      return -75;
+    }
+  cudaError_t e = h.K ? cudaMemcpyAsync(C.sk, s.sk.data(), sizeof(double2) * h.K, cudaMemcpyHostToDevice, st)
+                      : cudaSuccess;
+  for (int g = 0; g < ng && e == cudaSuccess; g++) {
+    const size_t n = s.sites[g].size();
+    if (!n) continue;
+    e = cudaMemcpyAsync(C.gsite + C.seg_off[g], s.sites[g].data(), sizeof(double4) * n, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(C.gtype + C.seg_off[g], s.types[g].data(), sizeof(int) * n, cudaMemcpyHostToDevice, st);
+  }
+  if (e != cudaSuccess) {
+    err = std::string("slot start upload failed: ") + cudaGetErrorString(e);
+    return -100 - (int)e;
+  }
+  for (int g = 0; g < ng; g++) {
+    C.nmol[g] = s.nmol[g];
+    C.totatm += (int)s.sites[g].size();
+    for (int t : s.types[g]) C.numtyp[t]++;
+  }
+  if (s.from_revive) {
+    for (int g = 0; g < ng; g++)
+      for (int k = 0; k < 6; k++) C.stats[g][k] = s.chainstats[1 + 14 * g + k];
+    C.prodcount = 0;
+    C.last_dE = 0.0;
+    C.production = s.production;
+    if (C.production && C.eqsteps > 0) C.production = 0;  // gcmc.f:396-409
+    if (C.eqsteps == 0) C.production = 1;                 // gcmc.f:553-554
+  }
+  return 0;
+}
+
 }  // namespace
 
 size_t slot_staging_bytes(const HostSystem& h) { return Parts(h).total() + 256; }
@@ -89,7 +138,7 @@ long long slot_voxel_capacity(const HostSystem& h) {
 }
 
 int build_slot(const HostSystem& h, int slot, const int seed[4], SlotMemory& mem, Staging& stg, long long vox_cap,
-               int* vox_total, SysConst& Y, ChainDev& C, std::string& err) {
+               int* vox_total, SysConst& Y, ChainDev& C, std::string& err, const SlotStart* start) {
   DevSystem v;
   std::memset(&v, 0, sizeof(v));
   v.cell = h.cell;
@@ -194,7 +243,10 @@ int build_slot(const HostSystem& h, int slot, const int seed[4], SlotMemory& mem
     if (rc) return rc;
     DevAllocFn alloc = [&mem](void** p, size_t n) { return mem.alloc(p, n); };
     // an empty framework: guest energy 0 (single_point, gcmc.f:2518-2710)
-    return init_chain_state(h.deck, h, skfw, 0.0, slot, seed, C, alloc, st, err, true);
+    if (!start) return init_chain_state(h.deck, h, skfw, 0.0, slot, seed, C, alloc, st, err, true);
+    rc = init_chain_state(h.deck, h, skfw, start->spenergy, slot, seed, C, alloc, st, err, true);
+    if (rc) return rc;
+    return load_slot_start(h, *start, C, st, err);
   }
 fail:
   err = std::string("slot set-up failed on the device: ") + cudaGetErrorString(e);

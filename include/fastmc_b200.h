@@ -365,7 +365,11 @@ int fmc_batch_write_prob(fmc_batch* b, int chain, const char* outdir);
  * freeing their slots for the next step.  k_capacity bounds the k-vectors of any request
  * (with guests of up to 4 sites and kmax <= 32 per axis; larger requests are rejected).
  * A request's budget is `moves` trial moves, or with moves = 0 its deck's own equilibration +
- * production cycles (CONTROL `equilibration` / `steps`). */
+ * production cycles (CONTROL `equilibration` / `steps`).  A request starts from the empty
+ * framework, or from the guests its deck preloads (FIELD NUMMOLS > 0), or, when CONTROL says
+ * `restart`, from the REVIVE fmc_restart_branch picks for node 0 (written by the reference, a
+ * plain chain or a batched one); the single point of such a start state is computed on the
+ * device at preparation by a chain opened on the deck and closed again. */
 typedef struct fmc_server fmc_server;
 int fmc_server_open(int slots, int device, long long mem_budget, int k_capacity, fmc_server** out);
 void fmc_server_close(fmc_server* s);

@@ -137,3 +137,34 @@ def test_serve_deck_cycle_budget_matches_oracle(fmc, oracle_mod, tmp_path):
     for k in ("N", "E", "EN", "N2", "E2"):
         assert abs(res[k] - ref[k]) <= 1e-8 * max(abs(ref[k]), 1.0), k
     assert srv.poll(other)["moves"] == 700 and srv.poll(other)["finished"] == 0.0
+
+
+def test_serve_starts_from_preloaded_guests_and_a_revive(fmc, decks, tmp_path):
+    """Requests that start with guests -- the deck's own (FIELD NUMMOLS > 0: the reference's
+    binary CO2 + TIP4P-Ew deck on 90 CO2) or a REVIVE's (CONTROL `restart` with branch01/REVIVE
+    beside the CALF-20 deck, gcmc.f:353-418) -- end in the state the same deck and seed reach in
+    a batch of their own, beside a request from the empty framework and across steps."""
+    import json
+    import os
+
+    from test_restart_branch import CALF, restart_deck
+
+    exp = json.load(open(os.path.join(CALF, "expected.json")))
+    guests = np.load(os.path.join(CALF, "revive_guests.npy"))
+    work = restart_deck(tmp_path / "job")
+    os.makedirs(os.path.join(work, "branch01"))
+    fmc.write_revive_state(CALF, os.path.join(work, "branch01"), [guests], production=True,
+                           chainstats=exp["revive_chainstats"], energy=[exp["revive_energy_kcal"]])
+    reqs = [(work, (103, 112, 53, 153), 900), (decks["binary_preloaded"], (1, 2, 3, 4), 700),
+            (decks["ortho0"], (5, 6, 7, 8), 500)]
+    srv = fmc.Server(slots=2, k_capacity=2400)
+    ids = [srv.submit(d, s, m) for d, s, m in reqs]
+    for _ in range(100):
+        if not srv.busy():
+            break
+        srv.step(300)
+    for rid, (d, s, m) in zip(ids, reqs):
+        res = srv.poll(rid)
+        assert res["state"] == srv.DONE, res
+        _same(res, _alone(fmc, d, s, m))
+    assert srv.poll(ids[0])["nmol0"] > 0 and srv.poll(ids[1])["nmol0"] > 0
