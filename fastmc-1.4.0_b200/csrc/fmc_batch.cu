@@ -9,6 +9,8 @@
 // {sum akk*d|S|^2, ewld2, vdw}, thread 0 applies energy_eval, and on acceptance every thread
 // commits its own k-vectors while the block updates the guest-site segment.
 #include <cstring>
+#include <map>
+#include <mutex>
 
 #include "fmc_batch.h"
 
@@ -1035,10 +1037,22 @@ constexpr BatchKernel kTileKernels[kNumBatchTiles] = {
 constexpr BatchKernel kProfKernel = fmc_batch_kernel<true, 256, 1, 1>;
 }  // namespace
 
+// The dynamic shared-memory limit belongs to the kernel, shared by every batch and server of the
+// process on the current device: it only ever rises, so that opening a batch with smaller tables
+// cannot make the launches of one opened before it (with larger tables) exceed the limit.
 cudaError_t configure_batch_kernel(int smem_bytes) {
-  cudaError_t e = cudaFuncSetAttribute(kProfKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
+  static std::mutex mu;
+  static std::map<int, int> limit;  // device -> the limit set on it
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(mu);
+  int& have = limit[dev];
+  if (smem_bytes <= have) return cudaSuccess;
+  e = cudaFuncSetAttribute(kProfKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
   for (int t = 0; t < kNumBatchTiles && e == cudaSuccess; t++)
     e = cudaFuncSetAttribute(kTileKernels[t], cudaFuncAttributeMaxDynamicSharedMemorySize, smem_bytes);
+  if (e == cudaSuccess) have = smem_bytes;
   return e;
 }
 

@@ -67,6 +67,16 @@ class Server {
     std::string prep_err;
     std::unique_ptr<HostSystem> host;
     std::unique_ptr<SlotStart> start;  // null: the empty framework
+    // the chain's state when it finished (kept while keep_final is on): guest sites per species
+    // (x, y, z molecule-major), the production flag, chainstats, energies and the last energy
+    // change, what a REVIVE / REVCON holds
+    struct Final {
+      std::vector<std::vector<double>> xyz;
+      bool production = false;
+      std::vector<double> chainstats, energy;
+      double last_dE = 0.0;
+    };
+    std::unique_ptr<Final> fin;
     size_t bytes_estimate = 0;
     // the device slot a worker built ahead of admission (null: built at admission instead)
     std::unique_ptr<struct Prebuilt> pre;
@@ -121,6 +131,7 @@ class Server {
   std::vector<int> deactivate;    // cancelled slots to switch off on the device before the next launch
   std::vector<std::pair<int, int>> deferred;  // (slot, buffer): memory freed once that launch completed
   std::vector<int> done_log;      // requests that reached a final state, for poll_done
+  std::vector<int> cancelled_unprepared;  // cancelled while a worker prepared them (caller's thread only)
   cudaStream_t st2 = nullptr;     // admission stream (slot set-up beside the running launch)
   Staging stage;                  // pinned staging of slot uploads
   cudaEvent_t ev_start[2] = {nullptr, nullptr}, ev_end[2] = {nullptr, nullptr}, ev_done[2] = {nullptr, nullptr};
@@ -137,6 +148,8 @@ class Server {
   std::atomic<long long> prep_us{0}, prep_host_us{0}, prep_dev_us{0};
   std::atomic<double> voxel_edge{2.0};  // neighbour-list voxel edge (A) of requests prepared from now on
   long long admit_prebuilt = 0, admit_built = 0;
+  bool keep_final = false;         // copy a finished chain's guests to the host before its slot is freed
+  cudaStream_t st3 = nullptr;      // those copies (created when keep_final is first turned on)
 
   ~Server() {
     {
@@ -178,6 +191,7 @@ class Server {
     if (h_zero) cudaFreeHost(h_zero);
     if (stage.base) cudaFreeHost(stage.base);
     if (st2) cudaStreamDestroy(st2);
+    if (st3) cudaStreamDestroy(st3);
     if (d_sys) cudaFree(d_sys);
     if (d_chains) cudaFree(d_chains);
     if (h_sys) cudaFreeHost(h_sys);
@@ -485,7 +499,10 @@ class Server {
         }
       r.state = kCancelled;
       done_log.push_back(id);
-      if (r.prepared.load(std::memory_order_acquire)) drop_prebuilt(r);
+      if (r.prepared.load(std::memory_order_acquire))
+        drop_prebuilt(r);
+      else
+        cancelled_unprepared.push_back(id);  // its worker may still build a slot ahead for it
     } else if (r.state == kRunning) {
       const int i = r.slot;
       snapshot(i, r);  // the state as of the last completed launch
@@ -552,6 +569,75 @@ class Server {
     b += 36.0 * h.deck.maxguest * h.deck.guests.size();
     b += 2.0 * 8.0 * ((double)kSampleCap * h.deck.guests.size() + 1);  // stored production samples
     return (size_t)b + (64u << 10);
+  }
+
+  // Slot i's chain has finished and switched itself off on the device, so the launch in flight
+  // does not touch its memory: its guest sites are copied to the host before the slot is freed,
+  // with the control block's REVIVE fields (as Batch::write_revive takes them).
+  int keep_final_state(int i, Request& r, std::string& err) {
+    const ChainDev& C = h_chains[i];
+    const SysConst& Y = h_sys[i];
+    auto F = std::make_unique<Request::Final>();
+    const int ng = Y.nspecies;
+    F->xyz.resize(ng);
+    std::vector<std::vector<double4>> a(ng);
+    cudaError_t e = cudaSuccess;
+    for (int g = 0; g < ng && e == cudaSuccess; g++) {
+      const int n = C.nmol[g] * Y.sp[g].nsite;
+      a[g].resize(n);
+      if (n) e = cudaMemcpyAsync(a[g].data(), C.gsite + C.seg_off[g], sizeof(double4) * n, cudaMemcpyDeviceToHost, st3);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st3);
+    if (e != cudaSuccess) {
+      err = std::string("final-state copy failed: ") + cudaGetErrorString(e);
+      return -100 - (int)e;
+    }
+    F->chainstats.assign(1 + 14 * ng, 0.0);
+    F->chainstats[0] = (double)C.prodcount;
+    for (int g = 0; g < ng; g++) {
+      for (const double4& p : a[g]) {
+        F->xyz[g].push_back(p.x);
+        F->xyz[g].push_back(p.y);
+        F->xyz[g].push_back(p.z);
+      }
+      for (int k = 0; k < 6; k++) F->chainstats[1 + 14 * g + k] = C.stats[g][k];
+      F->energy.push_back(C.energy[g]);
+    }
+    F->production = C.production != 0;
+    F->last_dE = C.last_dE;
+    r.fin = std::move(F);
+    return 0;
+  }
+
+  int set_keep_final(bool on) {
+    if (on && !st3 && cudaStreamCreateWithFlags(&st3, cudaStreamNonBlocking) != cudaSuccess) return -100;
+    keep_final = on;
+    return 0;
+  }
+
+  // REVIVE + REVCON of a finished request whose final state was kept (the deck is read again
+  // for the framework and the formats).
+  int write_revive(int id, const std::string& outdir, std::string& err) {
+    if (id < 0 || id >= nreqs()) {
+      err = "bad request id";
+      return -1;
+    }
+    Request& r = req(id);
+    if (r.state != kDone || !r.fin) {
+      err = "the request has not finished, or finished while its final state was not kept";
+      return -1;
+    }
+    InputDeck d;
+    int rc = read_input_deck(r.dir, d, err);
+    if (rc) return rc;
+    if ((int)r.fin->xyz.size() != (int)d.guests.size()) {
+      err = "the request's deck changed since it ran";
+      return -2;
+    }
+    Revive rv = revive_state(d, r.fin->production, r.fin->xyz, r.fin->chainstats, r.fin->energy);
+    rc = fmc::write_revive(outdir + "/REVIVE", rv, err);
+    if (!rc) rc = fmc::write_revcon(outdir + "/REVCON", d, rv, r.fin->last_dE, err);
+    return rc;
   }
 
   void snapshot(int i, Request& r) {
@@ -803,6 +889,10 @@ class Server {
         // the chain switched itself off on the device: the launch queued behind this one skips it
         Request& r = req(id);
         snapshot(i, r);
+        if (keep_final && !C.status) {
+          int rc = keep_final_state(i, r, err);
+          if (rc) return rc;
+        }
         r.state = C.status ? kRejected : kDone;
         if (C.status) r.err = C.status == 75 ? "too many atoms in specified system" : "chain stopped with an unknown status";
         done_log.push_back(id);
@@ -873,6 +963,18 @@ class Server {
     if (n_active) *n_active = 0;
     if (ms) *ms = 0.f;
     int rc = 0;
+    // requests cancelled during their preparation: the slots their workers built ahead are freed
+    for (size_t k = 0; k < cancelled_unprepared.size();) {
+      Request& r = req(cancelled_unprepared[k]);
+      if (!r.prepared.load(std::memory_order_acquire)) {
+        k++;
+        continue;
+      }
+      drop_prebuilt(r);
+      r.host.reset();
+      r.start.reset();
+      cancelled_unprepared.erase(cancelled_unprepared.begin() + k);
+    }
     if (!fresh.empty()) {  // last step's admissions: set up and checked before their first launch
       rc = settle_admissions(err);
       if (rc) return rc;
@@ -995,6 +1097,29 @@ int fmc_server_cancel(fmc_server* s, int request_id) {
     return -1;
   }
   return 0;
+}
+
+int fmc_server_keep_final_state(fmc_server* s, int enable) {
+  if (!s) {
+    fmc::set_last_error("bad server handle");
+    return -1;
+  }
+  if (s->impl.set_keep_final(enable != 0)) {
+    fmc::set_last_error("cannot create the final-state copy stream");
+    return -100;
+  }
+  return 0;
+}
+
+int fmc_server_write_revive(fmc_server* s, int request_id, const char* outdir) {
+  if (!s || !outdir) {
+    fmc::set_last_error("bad server handle or directory");
+    return -1;
+  }
+  std::string err;
+  int rc = s->impl.write_revive(request_id, outdir, err);
+  if (rc) fmc::set_last_error(err);
+  return rc;
 }
 
 int fmc_server_step(fmc_server* s, int moves, int* active, int* queued, float* device_ms) {

@@ -599,6 +599,14 @@ class Server:
     def cancel(self, rid):
         check(lib().fmc_server_cancel(self.h, int(rid)))
 
+    def keep_final_state(self, enable=True):
+        """Keep the guests of requests that finish from now on, for write_revive."""
+        check(lib().fmc_server_keep_final_state(self.h, int(bool(enable))))
+
+    def write_revive(self, rid, directory):
+        """REVIVE + REVCON of finished request `rid` (its final state kept) into `directory`."""
+        check(lib().fmc_server_write_revive(self.h, int(rid), str(directory).encode()))
+
     def busy(self):
         """True while a launch is in flight, a request runs or one is queued."""
         b = ctypes.c_int(0)

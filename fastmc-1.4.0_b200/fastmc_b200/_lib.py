@@ -132,6 +132,8 @@ SIGNATURES = {
     "fmc_server_close": (None, [_vp]),
     "fmc_server_submit": (_ci, [_vp, ctypes.c_char_p, _ip, ctypes.c_longlong, _ip]),
     "fmc_server_cancel": (_ci, [_vp, _ci]),
+    "fmc_server_keep_final_state": (_ci, [_vp, _ci]),
+    "fmc_server_write_revive": (_ci, [_vp, _ci, ctypes.c_char_p]),
     "fmc_server_step": (_ci, [_vp, _ci, _ip, _ip, ctypes.POINTER(ctypes.c_float)]),
     "fmc_server_poll": (_ci, [_vp, _ci, _ip, _dp]),
     "fmc_server_busy": (_ci, [_vp, _ip]),

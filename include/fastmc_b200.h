@@ -383,6 +383,15 @@ int fmc_server_set_voxel_edge(fmc_server* s, double edge);
  * chains and requests on GPUs by HBM footprint and load (fastmc_b200.placement). */
 int fmc_deck_footprint(const char* dir, double voxel_edge, long long* bytes, double* move_cost);
 int fmc_server_cancel(fmc_server* s, int request_id);
+/* Checkpoints of served requests (revive, utility_pack.f:1772-1817, for requests instead of MPI
+ * ranks): with enable = 1, every request that finishes from then on has its guests copied to the
+ * host as its slot is freed (off by default: one small device-to-host copy per retirement);
+ * fmc_server_write_revive then writes that final state as REVIVE + REVCON into outdir, in the
+ * formats fmc_chain_write_revive writes.  A later request on the same deck with CONTROL `restart`
+ * and that REVIVE as branch01/REVIVE resumes from it.  Only finished requests are kept (not
+ * cancelled or rejected ones); writing any other request fails. */
+int fmc_server_keep_final_state(fmc_server* s, int enable);
+int fmc_server_write_revive(fmc_server* s, int request_id, const char* outdir);
 /* One step of the pipelined server: queues the next launch of every running request (after the
  * uploads of the requests admitted by the previous step), then completes the launch queued by
  * the previous step -- its finished requests are retired -- and admits queued requests into free

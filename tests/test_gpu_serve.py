@@ -168,3 +168,50 @@ def test_serve_starts_from_preloaded_guests_and_a_revive(fmc, decks, tmp_path):
         assert res["state"] == srv.DONE, res
         _same(res, _alone(fmc, d, s, m))
     assert srv.poll(ids[0])["nmol0"] > 0 and srv.poll(ids[1])["nmol0"] > 0
+
+
+def test_serve_checkpoint_of_a_finished_request_resumes(fmc, decks, tmp_path):
+    """A finished request's REVIVE / REVCON (final state kept at retirement) are byte for byte the
+    files the same deck and seed write after the same moves in a batch of their own, and a
+    request on the deck with CONTROL `restart` and that REVIVE resumes as the batch does."""
+    import os
+    import shutil
+
+    d, seed, m = decks["ortho0"], (12, 34, 56, 78), 900
+    srv = fmc.Server(slots=2)
+    srv.keep_final_state(True)
+    rid = srv.submit(d, seed, m)
+    other = srv.submit(d, (1, 2, 3, 4), 1300)
+    cancelled = srv.submit(d, (4, 3, 2, 1), 5000)
+    srv.cancel(cancelled)
+    for _ in range(100):
+        if not srv.busy():
+            break
+        srv.step(400)
+    got, ref = tmp_path / "served", tmp_path / "batch"
+    os.makedirs(got)
+    os.makedirs(ref)
+    srv.write_revive(rid, got)
+    b = fmc.Batch([d], [seed])
+    b.run(m)
+    b.write_revive(0, str(ref))
+    for f in ("REVIVE", "REVCON"):
+        assert (got / f).read_bytes() == (ref / f).read_bytes(), f
+    with pytest.raises(fmc.FastMCError):
+        srv.write_revive(cancelled, tmp_path)
+    # resume: the deck with `restart` and the served REVIVE as branch01/REVIVE
+    job = tmp_path / "resume"
+    shutil.copytree(d, job)
+    ctl = (job / "CONTROL").read_text().split("\n")
+    (job / "CONTROL").write_text("\n".join([ctl[0], "restart"] + ctl[1:]))
+    os.makedirs(job / "branch01")
+    shutil.copy(got / "REVIVE", job / "branch01" / "REVIVE")
+    again = srv.submit(str(job), (7, 7, 7, 7), 600)
+    for _ in range(100):
+        if not srv.busy():
+            break
+        srv.step(400)
+    res = srv.poll(again)
+    assert res["state"] == srv.DONE and res["nmol0"] > 0
+    _same(res, _alone(fmc, str(job), (7, 7, 7, 7), 600))
+    assert srv.poll(other)["state"] == srv.DONE
