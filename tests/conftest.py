@@ -75,6 +75,10 @@ def decks(tmp_path_factory):
     (binary / "FIELD").write_text("\n".join(fld))
     out["binary_preloaded"] = str(binary)
     out["calf20_co2_n2"] = os.path.join(GOLDEN, "calf20_co2_n2")
+    # the reference's single-gas examples: CO2 in CALF-20's primitive cell, N2 in MOMJIJ, CH4 in
+    # MASMIC (all triclinic, 4 A cutoff)
+    for name in ("simple_calf20_co2", "simple_momjij_n2", "simple_masmic_ch4"):
+        out[name] = os.path.join(GOLDEN, name)
     out["guest_moves"] = os.path.join(GOLDEN, "guest_moves")
     # CO2 + N2 with the reference's pressure equilibration: the partial pressures move every 400
     # moves until the forced stop at 50 x 100 cycles, then equilibration and production follow

@@ -18,7 +18,8 @@ expected.json come from that example's OUTPUT and REVIVE:
               so that a writer restating revive (utility_pack.f:1772-1817) can be checked
               byte for byte without the files themselves
 * OUTPUT      the per-node report block (report_node0.txt), to check the report writer's layout
-* examples/advance/2 and 3, examples/restart/2 inputs as further parity decks
+* examples/advance/2 and 3, examples/restart/2 and examples/simple/1-3 inputs as further parity
+  decks
 """
 import hashlib
 import json
@@ -98,10 +99,14 @@ def main(ref):
         json.dump(wins, f)
     print("wrote", len(wins), "atmnumber windows")
     # the other shipped examples as parity decks: a CO2/N2 mixture with probability plots, guest-
-    # specific move and acceptance directives, and a binary CO2 + TIP4P-Ew deck whose CONFIG is the
-    # unary run's REVCON (its README's recipe; the test sets the CO2 NUMMOLS)
+    # specific move and acceptance directives, the three single-gas examples (CO2 in CALF-20's
+    # primitive cell, N2 in MOMJIJ, CH4 in MASMIC) and a binary CO2 + TIP4P-Ew deck whose CONFIG
+    # is the unary run's REVCON (its README's recipe; the test sets the CO2 NUMMOLS)
     for name, sub in (("calf20_co2_n2", "examples/advance/2_absorbtion_of_co2_n2_in_calf-20"),
-                      ("guest_moves", "examples/advance/3_guest_specific_move")):
+                      ("guest_moves", "examples/advance/3_guest_specific_move"),
+                      ("simple_calf20_co2", "examples/simple/1_absorbtion_of_co2_in_calf-20"),
+                      ("simple_momjij_n2", "examples/simple/2_absorbtion_of_n2_in_MOMJIJ"),
+                      ("simple_masmic_ch4", "examples/simple/3_absorbtion_of_ch4_in_MASMIC")):
         dst = os.path.join(HERE, name)
         os.makedirs(dst, exist_ok=True)
         for f in ("CONTROL", "FIELD", "CONFIG"):

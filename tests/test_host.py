@@ -31,7 +31,8 @@ def test_library_exports_every_declared_symbol(fmc):
 
 
 @pytest.mark.parametrize("name", ["calf20", "small", "large", "ortho0", "ortho1", "mixture", "imcon4", "imcon5",
-                                  "imcon6", "imcon7"])
+                                  "imcon6", "imcon7", "simple_calf20_co2", "simple_momjij_n2",
+                                  "simple_masmic_ch4"])
 def test_deck_tables_match_oracle_bit_exact(fmc, oracle_mod, decks, name):
     info = fmc.deck_inspect(decks[name])
     orc = oracle_mod.Chain(decks[name])
@@ -56,6 +57,19 @@ def test_every_vdw_form_tabulates_like_the_oracle(fmc, oracle_mod, decks):
     orc = oracle_mod.Chain(decks["forms"])
     ntpvdw = int(next(l for l in field.splitlines() if l.startswith("vdw")).split()[1])
     assert ntpvdw >= 9 and len(tabs) >= ntpvdw
+    for k in range(1, ntpvdw + 1):
+        assert np.array_equal(tabs[k - 1], orc.vvv(k)), k
+
+
+@pytest.mark.parametrize("name", ["calf20", "simple_momjij_n2", "simple_masmic_ch4", "calf20_co2_n2"])
+def test_shipped_example_vdw_tables_match_the_oracle(fmc, oracle_mod, decks, name):
+    """The vdW pair tables of the reference's own example decks (lj pairs of MOF atoms with the
+    guests' sites, zero-table pairs where FIELD gives none)."""
+    tabs = fmc.deck_vdw(decks[name])
+    orc = oracle_mod.Chain(decks[name])
+    field = open(decks[name] + "/FIELD").read().lower().splitlines()
+    ntpvdw = int(next(l for l in field if l.startswith("vdw")).split()[1])
+    assert ntpvdw > 0 and len(tabs) >= ntpvdw
     for k in range(1, ntpvdw + 1):
         assert np.array_equal(tabs[k - 1], orc.vvv(k)), k
 
