@@ -176,9 +176,6 @@ int build_host_system(const InputDeck& d, HostSystem& s, std::string& err, doubl
     err = "cells without periodic boundaries (imcon 0) are not supported on the device";
     return -4;
   }
-  if (d.lspe) {
-    err = "CONTROL requests a single point only (no GCMC steps)";
-  }
   // ---- cell
   for (int i = 0; i < 9; i++) s.cell.h[i] = d.cell[i];
   invert3(d.cell, s.cell.rh);
