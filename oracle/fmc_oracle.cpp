@@ -2166,6 +2166,7 @@ static void setup(Chain& C, const std::string& dir, int si, int sj, int sk, int 
     C.grid.assign(C.plots.size(), std::vector<double>((size_t)C.ngrid[0] * C.ngrid[1] * C.ngrid[2], 0.0));
   }
   C.production = (C.eqsteps == 0);
+  C.lgchk = !C.lspe;  // gcmc.f:565-567: a single-point deck stops before the move loop
   int maxs = 64;
   C.ind.assign(maxs, -1);
   C.newx.assign(maxs, 0.0);

@@ -106,3 +106,20 @@ def test_binary_deck_on_unary_revcon_single_point_pin(oracle_mod, decks):
     ref = expected()["revive_energy_kcal"]
     assert c.ints()["ntpguest"] == 2
     assert abs(c.scalars()["spenergy"] - ref) <= 1e-8 * abs(ref)
+
+
+def test_single_point_deck_runs_no_moves(oracle_mod, tmp_path):
+    """CONTROL without `steps` means a single point (readinputs.f: mcsteps 1, lspe): the
+    reference computes the energy and stops before the move loop (gcmc.f:565-567); with `steps`
+    the same deck runs until its cycles end."""
+    import shutil
+
+    calf = os.path.join(GOLDEN, "calf20")
+    sp = tmp_path / "sp"
+    shutil.copytree(calf, sp)
+    ctl = [ln for ln in (sp / "CONTROL").read_text().split("\n") if not ln.startswith("steps")]
+    (sp / "CONTROL").write_text("\n".join(ctl))
+    a, b = oracle_mod.Chain(str(sp)), oracle_mod.Chain(calf)
+    assert a.scalars()["spenergy"] == b.scalars()["spenergy"]
+    assert a.run_to_completion(500) == 0
+    assert b.run_to_completion(500) == 500
