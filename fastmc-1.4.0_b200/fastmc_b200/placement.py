@@ -7,8 +7,14 @@ chain goes, whole, to one GPU, chosen so that the GPUs carry similar work and no
 device memory.  Every rank computes the same partition from the same list (the assignment is a
 deterministic function of its inputs), so placing needs no communication; the one collective is
 the gather of per-chain results at the end of a run.
+
+A rank that fails or leaves between steps is found on the host, through the process group's
+key-value store, before the others enter their next step or the gather (`Liveness`): the
+reference has no recovery beyond a manual restart (error.f stops a rank), and here the others
+stop with an error that names the lost rank instead of waiting in a collective.
 """
 import ctypes
+import time
 
 from ._lib import check, lib
 
@@ -55,13 +61,78 @@ def share(items, placement, rank):
     return [(i, it) for i, (it, g) in enumerate(zip(items, placement)) if g == rank]
 
 
-def gather(results, dist_module=None):
+class RankLost(RuntimeError):
+    """A rank did not check in for a step in time, or left the run; `.rank` and `.step` say
+    which and when, `.left` whether it left on purpose."""
+
+    def __init__(self, rank, step, left=False, detail=""):
+        what = "left the run" if left else "did not check in"
+        super().__init__(f"rank {rank} {what} at step {step!r}" + (f" ({detail})" if detail else ""))
+        self.rank, self.step, self.left = rank, step, left
+
+
+class Liveness:
+    """Per-step check-ins of the ranks of one run through a key-value store (the process group's
+    TCPStore, or any object with set / get / check).  Each rank calls `check_in(step)` once it has
+    finished a step, and `wait_all(step)` before it starts the next one (or the gather): that
+    returns once every rank has checked in for the step and raises RankLost as soon as one has
+    left (`leave`) or after `timeout_s` without its check-in (a rank that raised, was killed or
+    never got there).  Keys are namespaced by `prefix`, so one store serves several runs."""
+
+    def __init__(self, store, rank, world, timeout_s=30.0, prefix="fmc", poll_s=0.02):
+        self.store, self.rank, self.world = store, int(rank), int(world)
+        self.timeout_s, self.prefix, self.poll_s = float(timeout_s), str(prefix), float(poll_s)
+
+    def _key(self, step, rank):
+        return f"{self.prefix}/step/{step}/{rank}"
+
+    def _left(self, rank):
+        return f"{self.prefix}/left/{rank}"
+
+    def check_in(self, step):
+        self.store.set(self._key(step, self.rank), "1")
+
+    def leave(self, step):
+        """This rank stops after `step` (between steps, with nothing in flight)."""
+        self.store.set(self._left(self.rank), str(step))
+
+    def wait_all(self, step):
+        pending = [r for r in range(self.world) if r != self.rank]
+        deadline = time.monotonic() + self.timeout_s
+        while pending:
+            still = []
+            for r in pending:
+                try:
+                    if self.store.check([self._key(step, r)]):
+                        continue
+                    if self.store.check([self._left(r)]):
+                        after = self.store.get(self._left(r))
+                        after = after.decode() if isinstance(after, bytes) else str(after)
+                        raise RankLost(r, step, left=True, detail=f"after step {after}")
+                except RankLost:
+                    raise
+                except Exception as e:  # the store itself is gone (rank 0 hosts it)
+                    raise RankLost(r, step, detail=f"store unreachable: {e}") from e
+                still.append(r)
+            pending = still
+            if pending and time.monotonic() > deadline:
+                raise RankLost(pending[0], step, detail=f"no check-in within {self.timeout_s:g} s")
+            if pending:
+                time.sleep(self.poll_s)
+
+
+def gather(results, dist_module=None, liveness=None):
     """Every rank's list of (index, result) pairs, merged and in index order, on every rank
-    (torch.distributed.all_gather_object; a single process returns its own list)."""
+    (torch.distributed.all_gather_object; a single process returns its own list).  With a
+    Liveness, every rank checks in for the gather first, so a lost rank raises RankLost here
+    instead of leaving the others in the collective."""
     if dist_module is None:
         import torch.distributed as dist_module
     if not dist_module.is_available() or not dist_module.is_initialized():
         return sorted(results, key=lambda x: x[0])
+    if liveness is not None:
+        liveness.check_in("gather")
+        liveness.wait_all("gather")
     parts = [None] * dist_module.get_world_size()
     dist_module.all_gather_object(parts, list(results))
     merged = [r for p in parts for r in p]
