@@ -123,3 +123,30 @@ def test_single_point_deck_runs_no_moves(oracle_mod, tmp_path):
     assert a.scalars()["spenergy"] == b.scalars()["spenergy"]
     assert a.run_to_completion(500) == 0
     assert b.run_to_completion(500) == 500
+
+
+def test_tables_against_their_closed_forms(oracle_mod):
+    """The two interpolation tables against the formulas they tabulate, on the CALF-20 deck
+    (the product's tables equal the oracle's bit for bit, tests/test_host.py): erc(i) * r_i is
+    A&S 7.1.26's erfc(alpha r_i) (erfcgen, ewald.f:1-30), within that approximation's published
+    bound of 1.5e-7; every lj row of vvv is 4 eps [(sigma/r)^12 - (sigma/r)^6] in internal units
+    (forgen, vdw_terms.f:238-250) at r_i = i * dlrpot."""
+    import math
+
+    c = oracle_mod.Chain(CALF)
+    s = c.scalars()
+    erc, a, dr = c.erc(), s["alpha"], s["drewd"]
+    err = max(abs(erc[i] * i * dr - math.erfc(a * i * dr)) for i in range(1, len(erc)))
+    assert 1e-9 < err <= 1.5e-7
+    lines = open(os.path.join(CALF, "FIELD")).read().splitlines()
+    i0 = next(i for i, ln in enumerate(lines) if ln.lower().startswith("vdw"))
+    npair = int(lines[i0].split()[1])
+    assert npair == 28
+    for k in range(1, npair + 1):
+        f = lines[i0 + k].split()
+        assert f[2] == "lj"
+        eps, sig = float(f[3]), float(f[4])
+        v = c.vvv(k)
+        r = np.arange(1, len(v)) * s["dlrpot"]
+        ref = 4.0 * eps * ((sig / r) ** 12 - (sig / r) ** 6) * s["engunit"]
+        assert np.all(np.abs(v[1:] - ref) <= 1e-11 * np.abs(ref)), k
