@@ -77,11 +77,14 @@ class Liveness:
     finished a step, and `wait_all(step)` before it starts the next one (or the gather): that
     returns once every rank has checked in for the step and raises RankLost as soon as one has
     left (`leave`) or after `timeout_s` without its check-in (a rank that raised, was killed or
-    never got there).  Keys are namespaced by `prefix`, so one store serves several runs."""
+    never got there).  A store that stops answering is reported as the loss of `store_host`, the
+    rank whose process serves it (rank 0 for the process group's own store).  Keys are namespaced
+    by `prefix`, so one store serves several runs."""
 
-    def __init__(self, store, rank, world, timeout_s=30.0, prefix="fmc", poll_s=0.02):
+    def __init__(self, store, rank, world, timeout_s=30.0, prefix="fmc", poll_s=0.02, store_host=0):
         self.store, self.rank, self.world = store, int(rank), int(world)
         self.timeout_s, self.prefix, self.poll_s = float(timeout_s), str(prefix), float(poll_s)
+        self.store_host = int(store_host)
 
     def _key(self, step, rank):
         return f"{self.prefix}/step/{step}/{rank}"
@@ -111,8 +114,8 @@ class Liveness:
                         raise RankLost(r, step, left=True, detail=f"after step {after}")
                 except RankLost:
                     raise
-                except Exception as e:  # the store itself is gone (rank 0 hosts it)
-                    raise RankLost(r, step, detail=f"store unreachable: {e}") from e
+                except Exception as e:  # the store itself is gone with its host
+                    raise RankLost(self.store_host, step, detail=f"store unreachable: {e}") from e
                 still.append(r)
             pending = still
             if pending and time.monotonic() > deadline:
